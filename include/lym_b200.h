@@ -1,0 +1,191 @@
+/*
+ * lym_b200.h -- C ABI of the B200 (sm_100a) Wilson / Wilson-clover operator and
+ * Krylov-solver library.  Drop-in boundary for LeonardYM's fermion hot path.
+ *
+ * Plain C: opaque context, plain pointers and sizes, no CUDA or torch types.
+ * Every entry point returns an int status: 0 success, 1 solver not converged,
+ * < 0 error (see lym_status); lym_last_error() gives the message.  No entry point
+ * calls exit().  One CUDA stream per context; calls on one context are
+ * serialised by a mutex (thread safe per context).
+ *
+ * Host vectors use the reference's raw memory layout (Lattice<T,LocalLayout>::
+ * getRawData(), MPILattice/Lattice.h:228-234; LatticeDefinitions.h:86-161):
+ *   spinor  reduced_dirac_vector_t : double[V][4 spin][3 colour][re,im]
+ *   links   extended_fermion_lattice_t : per site 4 links, Eigen column-major,
+ *           complex double[3][3] (SU(3) fundamental) or double[3][3] (SU(2) adjoint)
+ *   site    t + Lt*(z + Lz*(y + Ly*x))            (MPILattice/LocalLayout.h:149-163)
+ * "_device" variants take device pointers with the same layout.
+ */
+#ifndef LYM_B200_H
+#define LYM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct lym_context lym_context;
+
+enum lym_status {
+    LYM_OK = 0,
+    LYM_NOT_CONVERGED = 1,
+    LYM_ERR_ARGUMENT = -1,
+    LYM_ERR_CUDA = -2,
+    LYM_ERR_MEMORY = -3,
+    LYM_ERR_UNSUPPORTED = -4,
+    LYM_ERR_BREAKDOWN = -5,
+    LYM_ERR_NOT_FOUND = -6,
+    LYM_ERR_TIMEOUT = -7,
+    LYM_ERR_NUMERIC = -8
+};
+
+/* Representations: the compile-time NUMCOLORS / ADJOINT choices of the reference
+ * (MatrixTypedef.h:73-90) become a run-time choice. */
+enum lym_rep {
+    LYM_REP_SU3_FUNDAMENTAL = 0,  /* NUMCOLORS=3: FermionicGroup = complex 3x3 */
+    LYM_REP_SU2_ADJOINT = 1       /* NUMCOLORS=2 -DADJOINT: FermionicGroup = real 3x3 */
+};
+
+/* Operator kinds: the names DiracOperator::getInstance registers
+ * (dirac_operators/DiracOperator.cpp:20-165) and the even-odd operator. */
+enum lym_operator_kind {
+    LYM_OP_DIRAC_WILSON = 0,            /* DiracWilsonOperator                      */
+    LYM_OP_IMPROVED = 1,                /* ImprovedDiracWilsonOperator              */
+    LYM_OP_EVEN_ODD_IMPROVED = 2,       /* EvenOddImprovedDiracWilsonOperator       */
+    LYM_OP_SQUARE_DIRAC_WILSON = 3,     /* SquareDiracWilsonOperator                */
+    LYM_OP_SQUARE_IMPROVED = 4,         /* SquareImprovedDiracWilsonOperator        */
+    LYM_OP_SQUARE_EVEN_ODD_IMPROVED = 5 /* SquareEvenOddImprovedDiracWilsonOperator */
+};
+
+enum lym_boundary {
+    LYM_BC_PERIODIC = 0,           /* "fermion_periodic"     */
+    LYM_BC_ANTIPERIODIC = 1        /* "fermion_antiperiodic" (LatticeBoundaryConditions.h:8-14) */
+};
+
+enum lym_solver {
+    LYM_SOLVER_CG = 0,               /* ConjugateGradient::solve (inverters/ConjugateGradient.cpp:10-74)   */
+    LYM_SOLVER_BICGSTAB = 1,         /* BiConjugateGradient::solve (inverters/BiConjugateGradient.cpp:321-507) */
+    LYM_SOLVER_EO_BICGSTAB = 2,      /* PreconditionedBiCGStab::solve (inverters/PreconditionedBiCGStab.cpp:33-100) */
+    LYM_SOLVER_EO_CG = 3,            /* even-odd Schur CG on (g5 S)^2, D x = b, FP64 throughout          */
+    LYM_SOLVER_EO_CG_MIXED_SINGLE = 4, /* same, FP32 stencil inner iterations, FP64 reliable updates     */
+    LYM_SOLVER_EO_CG_MIXED_HALF = 5    /* same, FP16 spinor storage (per-site norm) inner iterations     */
+};
+
+enum lym_multishift_solver {
+    LYM_MULTISHIFT_ME = 0,    /* "mass_estrapolation": MEMultishiftSolver (inverters/MEMultishiftSolver.cpp:10-143) */
+    LYM_MULTISHIFT_MMMR = 1,  /* "minimal_residual": MMMRMultishiftSolver (inverters/MMMRMultishiftSolver.cpp:42-198) */
+    LYM_MULTISHIFT_CG = 2     /* multishift CG (no reference counterpart; a new MultishiftSolver subclass) */
+};
+
+typedef struct {
+    int steps;             /* Solver::getLastSteps semantics (inverters/Solver.h:53-55)          */
+    int iterations;        /* operator applications of the Krylov recursion                        */
+    int reliable_updates;  /* FP64 residual recomputations (mixed precision)                       */
+    int converged;
+    double last_error;     /* Solver::getLastError semantics: last squared residual of the recursion */
+    double true_residual;  /* ||b - A x|| / ||b|| recomputed in FP64 after the solve                */
+    double seconds;        /* device time of the solve                                             */
+} lym_solve_stats;
+
+/* ---- context: one lattice geometry and representation on one GPU --------------
+ * Replaces the process-global LocalLayout::initialize (MPILattice/LocalLayout.h:34-110). */
+int lym_context_create(const int dims[4], int rep, int device, lym_context **ctx);
+void lym_context_destroy(lym_context *ctx);
+const char *lym_last_error(lym_context *ctx);
+int lym_context_volume(lym_context *ctx);
+/* bytes of device memory held by the context (gauge fields, clover terms, work vectors) */
+size_t lym_context_device_bytes(lym_context *ctx);
+int lym_synchronize(lym_context *ctx);
+
+/* ---- gauge fields, resident by id ----------------------------------------------
+ * lym_gauge_upload takes the fermion link field exactly as
+ * DiracOperator::setLattice(const extended_fermion_lattice_t&) receives it
+ * (dirac_operators/DiracOperator.h:125, DiracOperator.cpp:332-334).
+ * lym_gauge_upload_fundamental builds the fermion links from fundamental gauge links
+ * as Environment::synchronize does (Environment.cpp:21-79): adjoint map for SU(2)
+ * (utils/ConvertLattice.h:24-34) and the boundary condition folded into U_t. */
+int lym_gauge_upload(lym_context *ctx, int gauge_id, const double *fermion_links);
+int lym_gauge_upload_device(lym_context *ctx, int gauge_id, const double *fermion_links_device);
+int lym_gauge_upload_fundamental(lym_context *ctx, int gauge_id, const double *gauge_links, int boundary);
+int lym_gauge_evict(lym_context *ctx, int gauge_id);
+
+/* ---- operators ------------------------------------------------------------------
+ * DiracOperator::getInstance(name, power, ...) + setKappa/setCSW/setGamma5/setLattice
+ * (DiracOperator.cpp:20-165, DiracOperator.h:107-127, ImprovedDiracWilsonOperator.h:34-35).
+ * The clover term F (ImprovedDiracWilsonOperator.cpp:502-523) and the even-even
+ * inverse (EvenOddImprovedDiracWilsonOperator.cpp:285-317) are built on the GPU in
+ * FP64 when first needed. */
+int lym_operator_create(lym_context *ctx, int gauge_id, int kind, double kappa, double csw, int gamma5, int *op_id);
+int lym_operator_set_gamma5(lym_context *ctx, int op_id, int gamma5);
+int lym_operator_set_kappa(lym_context *ctx, int op_id, double kappa);
+int lym_operator_set_csw(lym_context *ctx, int op_id, double csw);
+int lym_operator_set_gauge(lym_context *ctx, int op_id, int gauge_id);
+int lym_operator_destroy(lym_context *ctx, int op_id);
+
+/* ---- operator application -------------------------------------------------------
+ * DiracOperator::multiply(output, input) (DiracOperator.h:90) and
+ * multiplyAdd(output, v1, v2, alpha) = Op v1 + alpha v2 (DiracOperator.h:99).
+ * EvenOddImprovedDiracWilsonOperator::multiplyAdd is not implemented in the
+ * reference (EvenOddImprovedDiracWilsonOperator.cpp:49-52): LYM_ERR_UNSUPPORTED. */
+int lym_multiply(lym_context *ctx, int op_id, double *out, const double *in);
+int lym_multiply_add(lym_context *ctx, int op_id, double *out, const double *v1, const double *v2, double alpha_re,
+                     double alpha_im);
+int lym_multiply_device(lym_context *ctx, int op_id, double *out, const double *in);
+int lym_multiply_add_device(lym_context *ctx, int op_id, double *out, const double *v1, const double *v2,
+                            double alpha_re, double alpha_im);
+/* storage precision of the single-precision / half-precision operator path, for
+ * parity tests of the sloppy stencils: prec 0 FP64, 1 FP32 (12-real links), 2 FP16 */
+int lym_multiply_precision(lym_context *ctx, int op_id, int prec, double *out, const double *in);
+
+/* field strength F_{mu nu} of an operator's gauge field, reference layout
+ * (reduced_field_strength_lattice_t: V x 6 x 3x3 complex column-major) */
+int lym_field_strength(lym_context *ctx, int op_id, double *F);
+
+/* ---- solvers ---------------------------------------------------------------------
+ * Solver::solve(DiracOperator*, source, solution, guess) -> bool (inverters/Solver.h:13).
+ * `precision` is the reference's absolute threshold on the squared residual norm
+ * (ConjugateGradient.cpp:50, BiConjugateGradient.cpp:489).  For the even-odd CG
+ * solvers, `precision` <= 0 selects the relative criterion ||b - D x|| <= `tol` ||b||
+ * with tol = -precision (0 -> 1e-10). guess may be NULL. */
+int lym_solve(lym_context *ctx, int op_id, int solver, double precision, int max_steps, const double *source,
+              double *solution, const double *guess, lym_solve_stats *stats);
+int lym_solve_device(lym_context *ctx, int op_id, int solver, double precision, int max_steps, const double *source,
+                     double *solution, const double *guess, lym_solve_stats *stats);
+/* BiConjugateGradient::solve(dirac, source, solution, shift, guess): (A + shift) x = b
+ * (BiConjugateGradient.cpp:510-690) */
+int lym_solve_shifted(lym_context *ctx, int op_id, double shift_re, double shift_im, double precision, int max_steps,
+                      const double *source, double *solution, const double *guess, lym_solve_stats *stats);
+
+/* ---- multishift -------------------------------------------------------------------
+ * MultishiftSolver::solve(dirac, source, solutions, shifts) -> bool
+ * (inverters/MultishiftSolver.h:28); the operator must be Hermitian positive
+ * definite (a Square* kind).  solutions[i] receives (A + shifts[i])^{-1} source. */
+int lym_multishift(lym_context *ctx, int op_id, int algorithm, int nshift, const double *shifts, double precision,
+                   int max_steps, const double *source, double **solutions, lym_solve_stats *stats);
+int lym_multishift_device(lym_context *ctx, int op_id, int algorithm, int nshift, const double *shifts,
+                          double precision, int max_steps, const double *source, double **solutions,
+                          lym_solve_stats *stats);
+
+/* ---- layout self-checks (no reference counterpart: test hooks for the layout) --------
+ * reference-order neighbour tables sup/sdn [V][4] (LocalLayout.h:34-110, Lattice.h:201-207)
+ * and the stencil's computed indices [2][V/2][9] (own site, 8 neighbour half-indices). */
+int lym_neighbour_tables(lym_context *ctx, int *sup, int *sdn);
+int lym_stencil_indices(lym_context *ctx, int *out);
+
+/* ---- measurement hooks (no reference counterpart) ----------------------------------
+ * kernels this context has enqueued (a CUDA-graph replay counts its kernel nodes), and
+ * the device time of one stencil launch on the context's stream (CUDA events, after 3
+ * warm-up launches): which 0 = odd-parity output with the clover term and xpay epilogue
+ * (second half of the Schur operator), 1 = even-parity output with T_ee^-1 (first half). */
+unsigned long long lym_context_kernel_launches(lym_context *ctx);
+int lym_time_stencil(lym_context *ctx, int op_id, int prec, int which, int iters, double *ms_per_launch);
+
+/* ---- pinned host memory for callers that want fast transfers ---------------------- */
+void *lym_host_alloc(size_t bytes);
+void lym_host_free(void *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1491 @@
+// C ABI of the library: contexts, resident gauge fields, operators, operator
+// application and the Krylov solvers.  See include/lym_b200.h for the contract.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/lym_b200.h"
+#include "lym_internal.h"
+#include "lym_solver_ops.cuh"
+
+using namespace lym;
+
+namespace {
+
+constexpr int kBlasGridMax = 148 * 8;
+
+struct GaugeEntry {
+    GaugeDev dev;
+    int recon_err = 0;
+};
+
+struct OpEntry {
+    int gauge_id = -1;
+    int kind = LYM_OP_DIRAC_WILSON;
+    double kappa = 0.0, csw = 0.0;
+    int gamma5 = 1;
+    CloverDev clover;
+    bool clover_ok = false;
+};
+
+struct LymError {
+    int code;
+};
+
+}  // namespace
+
+struct lym_context {
+    Geom g;
+    int rep = REP_SU3;
+    int device = 0;
+    cudaStream_t st = nullptr;
+    std::mutex mu;
+    std::string err;
+    std::map<int, GaugeEntry> gauges;
+    std::map<int, OpEntry> ops;
+    int next_op = 1;
+    // reductions
+    double *partials = nullptr;
+    unsigned int *counter = nullptr;
+    int *d_err = nullptr;
+    void *d_state = nullptr;      // solver state (device)
+    void *h_state = nullptr;      // pinned mirror
+    double *d_scal = nullptr;     // scratch scalars
+    double *h_scal = nullptr;
+    // host-layout staging buffers (V * 24 doubles)
+    double *aos[3] = {nullptr, nullptr, nullptr};
+    std::vector<Spinor> pool;
+    size_t bytes = 0;
+    unsigned long long launches = 0;  // kernels enqueued (graph replays count their nodes)
+    bool capturing = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+constexpr size_t kStateBytes = 4096;
+
+int fail(lym_context *c, int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    throw LymError{code};
+}
+
+void ck(lym_context *c, cudaError_t e, const char *what)
+{
+    if (e != cudaSuccess) fail(c, LYM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call) ck(c, (call), #call)
+
+template <class F> int guarded(lym_context *c, F f)
+{
+    if (!c) return LYM_ERR_ARGUMENT;
+    std::lock_guard<std::mutex> lock(c->mu);
+    try {
+        cudaSetDevice(c->device);
+        return f();
+    } catch (const LymError &e) {
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        c->err = "host allocation failed";
+        return LYM_ERR_MEMORY;
+    }
+}
+
+void *dev_alloc(lym_context *c, size_t bytes)
+{
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(c, LYM_ERR_MEMORY, "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    }
+    CK(cudaMemsetAsync(p, 0, bytes, c->st));
+    c->bytes += bytes;
+    return p;
+}
+
+void dev_free(lym_context *c, void *p, size_t bytes)
+{
+    if (p) {
+        cudaFree(p);
+        c->bytes -= bytes;
+    }
+}
+
+size_t spinor_bytes(const Geom &g, int prec, int nparity)
+{
+    const size_t s = g.stride;
+    switch (prec) {
+    case PREC_D: return nparity * 12 * s * sizeof(double2);
+    case PREC_F: return nparity * 6 * s * sizeof(float4);
+    default: return nparity * (3 * s * sizeof(int4) + s * sizeof(float));
+    }
+}
+
+// --------------------------------------------------------- spinor pool -----
+struct Vec {
+    lym_context *c = nullptr;
+    Spinor s;
+    Vec() = default;
+    Vec(lym_context *ctx, int prec, int nparity) : c(ctx)
+    {
+        for (size_t i = 0; i < c->pool.size(); ++i) {
+            if (c->pool[i].prec == prec && c->pool[i].nparity == nparity) {
+                s = c->pool[i];
+                c->pool.erase(c->pool.begin() + i);
+                return;
+            }
+        }
+        s.prec = prec;
+        s.nparity = nparity;
+        s.stride = c->g.stride;
+        const size_t b = spinor_bytes(c->g, prec, nparity);
+        char *base = (char *)dev_alloc(c, b);
+        s.v = base;
+        if (prec == PREC_H) s.norm = (float *)(base + (size_t)nparity * 3 * c->g.stride * sizeof(int4));
+        s.owned = true;
+    }
+    ~Vec()
+    {
+        if (c && s.v) c->pool.push_back(s);
+    }
+    Vec(const Vec &) = delete;
+    Vec &operator=(const Vec &) = delete;
+    const Spinor &operator*() const { return s; }
+    Spinor par(int p) const { return s.parity(p); }
+};
+
+// --------------------------------------------------------- site kernels ----
+void count(lym_context *c, int n)
+{
+    if (!c->capturing) c->launches += n;
+}
+
+template <class Op> void run_site(lym_context *c, const Op &op, int nparity, Gate gate = Gate{nullptr, nullptr})
+{
+    count(c, 1);
+    int grid = (c->g.Vh + kBlasThreads - 1) / kBlasThreads;
+    grid = std::min(grid, kBlasGridMax);
+    site_kernel<Op><<<grid, kBlasThreads, 0, c->st>>>(op, c->g.Vh, nparity, RedBuf{c->partials, c->counter}, gate);
+}
+
+double2 C2(double re, double im = 0.0) { return make_double2(re, im); }
+
+// y = a x + b y for any precisions of x and y
+void axpby(lym_context *c, const Spinor &x, const Spinor &y, double2 a, double2 b)
+{
+    const int np = y.nparity;
+    auto go = [&](auto X) {
+        if (y.prec == PREC_D) run_site(c, OpAxpby<decltype(X), SpinorD>{X, y.d(), a, b}, np);
+        else if (y.prec == PREC_F) run_site(c, OpAxpby<decltype(X), SpinorF>{X, y.f(), a, b}, np);
+        else run_site(c, OpAxpby<decltype(X), SpinorH>{X, y.h(), a, b}, np);
+    };
+    if (x.prec == PREC_D) go(x.d());
+    else if (x.prec == PREC_F) go(x.f());
+    else go(x.h());
+}
+
+void copy(lym_context *c, const Spinor &dst, const Spinor &src)
+{
+    if (dst.prec == src.prec && dst.nparity == src.nparity) {
+        CK(cudaMemcpyAsync(dst.v, src.v, spinor_bytes(c->g, src.prec, src.nparity), cudaMemcpyDeviceToDevice, c->st));
+        return;
+    }
+    launch_convert(c->g, dst, src, c->st);
+}
+
+void zero(lym_context *c, const Spinor &s) { CK(cudaMemsetAsync(s.v, 0, spinor_bytes(c->g, s.prec, s.nparity), c->st)); }
+
+double norm2_now(lym_context *c, const Spinor &x)
+{
+    run_site(c, OpNorm<SpinorD>{x.d(), c->d_scal}, x.nparity);
+    CK(cudaMemcpyAsync(c->h_scal, c->d_scal, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return c->h_scal[0];
+}
+
+void gamma5_inplace(lym_context *c, const Spinor &x) { run_site(c, OpGamma5<SpinorD>{x.d()}, x.nparity); }
+
+// ------------------------------------------------------------ operators ----
+GaugeEntry &gauge_of(lym_context *c, int id)
+{
+    auto it = c->gauges.find(id);
+    if (it == c->gauges.end()) fail(c, LYM_ERR_NOT_FOUND, "gauge field %d is not resident", id);
+    return it->second;
+}
+
+OpEntry &op_of(lym_context *c, int id)
+{
+    auto it = c->ops.find(id);
+    if (it == c->ops.end()) fail(c, LYM_ERR_NOT_FOUND, "operator %d does not exist", id);
+    return it->second;
+}
+
+bool kind_has_clover(int kind)
+{
+    return kind == LYM_OP_IMPROVED || kind == LYM_OP_EVEN_ODD_IMPROVED || kind == LYM_OP_SQUARE_IMPROVED ||
+           kind == LYM_OP_SQUARE_EVEN_ODD_IMPROVED;
+}
+
+size_t clover_bytes(const Geom &g, int prec)
+{
+    const size_t s = g.stride;
+    if (prec == PREC_D) return 4 * 18 * s * sizeof(double2);
+    if (prec == PREC_F) return 4 * 9 * s * sizeof(float4);
+    return 4 * 9 * s * sizeof(uint2);
+}
+
+void free_clover(lym_context *c, OpEntry &op)
+{
+    for (int p = 0; p < 3; ++p) {
+        dev_free(c, op.clover.T[p], clover_bytes(c->g, p));
+        dev_free(c, op.clover.Tinv[p], clover_bytes(c->g, p));
+        op.clover.T[p] = op.clover.Tinv[p] = nullptr;
+    }
+    op.clover_ok = false;
+}
+
+void ensure_clover(lym_context *c, OpEntry &op, double *F_out = nullptr)
+{
+    if (op.clover_ok && !F_out) return;
+    GaugeEntry &ge = gauge_of(c, op.gauge_id);
+    for (int p = 0; p < 3; ++p) {
+        if (!op.clover.T[p]) op.clover.T[p] = dev_alloc(c, clover_bytes(c->g, p));
+        if (!op.clover.Tinv[p]) op.clover.Tinv[p] = dev_alloc(c, clover_bytes(c->g, p));
+    }
+    CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st));
+    launch_clover_build(c->g, ge.dev, op.kappa * op.csw, op.clover, F_out, c->d_err, c->st);
+    launch_clover_compress(c->g, op.clover, c->st);
+    int herr = 0;
+    CK(cudaMemcpyAsync(c->h_scal, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    memcpy(&herr, c->h_scal, sizeof(int));
+    CK(cudaGetLastError());
+    if (herr) fail(c, LYM_ERR_NUMERIC, "clover block not invertible (error bits %d)", herr);
+    op.clover_ok = true;
+}
+
+void require_recon(lym_context *c, GaugeEntry &ge, int prec)
+{
+    if (prec == PREC_D) return;
+    if (!ge.dev.recon_ok)
+        fail(c, LYM_ERR_UNSUPPORTED,
+             "reduced-precision links need +-SU(3) / +-SO(3) links (unitarity check bits %d)", ge.recon_err);
+}
+
+// full operator: out = G5^g (T in_p - kappa H in_{1-p}) + alpha v2 on both parities
+void apply_full(lym_context *c, OpEntry &op, int prec, const Spinor &out, const Spinor &in, int gamma5,
+                const Spinor *v2, double2 alpha, const int *skip = nullptr)
+{
+    GaugeEntry &ge = gauge_of(c, op.gauge_id);
+    const bool clov = kind_has_clover(op.kind);
+    if (clov) ensure_clover(c, op);
+    require_recon(c, ge, prec);
+    for (int p = 0; p < 2; ++p) {
+        DslashParams P;
+        P.g = c->g;
+        P.prec = prec;
+        P.rep = c->rep;
+        P.epi = EPI_XPAY_;
+        P.parity = p;
+        P.in = in.parity(1 - p);
+        P.out = out.parity(p);
+        P.y = in.parity(p);
+        if (v2) {
+            P.v2 = v2->parity(p);
+            P.has_v2 = 1;
+            P.alpha_re = alpha.x;
+            P.alpha_im = alpha.y;
+        } else {
+            P.v2 = P.y;
+        }
+        P.U = &ge.dev;
+        P.clover = clov ? op.clover.T[prec] : nullptr;
+        P.gamma5 = gamma5;
+        P.b = -op.kappa;
+        P.skip_if = skip;
+        launch_dslash(P, c->st);
+        count(c, 1);
+    }
+}
+
+// Schur complement on the odd sites:
+//   out_o = G5^g (T_oo in_o - kappa^2 H_oe T_ee^{-1} H_eo in_o) + alpha v2_o
+void apply_schur(lym_context *c, OpEntry &op, int prec, const Spinor &out_o, const Spinor &in_o, const Spinor &tmp_e,
+                 int gamma5, const Spinor *v2 = nullptr, double2 alpha = make_double2(0, 0),
+                 const int *skip = nullptr)
+{
+    GaugeEntry &ge = gauge_of(c, op.gauge_id);
+    const bool clov = kind_has_clover(op.kind);
+    if (clov) ensure_clover(c, op);
+    require_recon(c, ge, prec);
+    DslashParams P;
+    P.g = c->g;
+    P.prec = prec;
+    P.rep = c->rep;
+    P.U = &ge.dev;
+    P.skip_if = skip;
+    // K1: tmp_e = Tinv_ee H_eo in_o
+    P.epi = clov ? EPI_CLOVINV_ : EPI_SCALE_;
+    P.parity = 0;
+    P.in = in_o;
+    P.out = tmp_e;
+    P.y = tmp_e;
+    P.v2 = tmp_e;
+    P.clover = clov ? op.clover.Tinv[prec] : nullptr;
+    P.a = 1.0;
+    launch_dslash(P, c->st);
+    // K2: out_o = G5^g (T_oo in_o - kappa^2 H_oe tmp_e) + alpha v2
+    P.epi = EPI_XPAY_;
+    P.parity = 1;
+    P.in = tmp_e;
+    P.out = out_o;
+    P.y = in_o;
+    P.clover = clov ? op.clover.T[prec] : nullptr;
+    P.b = -op.kappa * op.kappa;
+    P.gamma5 = gamma5;
+    if (v2) {
+        P.v2 = *v2;
+        P.has_v2 = 1;
+        P.alpha_re = alpha.x;
+        P.alpha_im = alpha.y;
+    } else {
+        P.v2 = in_o;
+    }
+    launch_dslash(P, c->st);
+    count(c, 2);
+}
+
+bool is_even_odd(int kind) { return kind == LYM_OP_EVEN_ODD_IMPROVED || kind == LYM_OP_SQUARE_EVEN_ODD_IMPROVED; }
+
+// DiracOperator::multiply / multiplyAdd on full device spinors (reference semantics).
+void op_apply(lym_context *c, OpEntry &op, int prec, const Spinor &out, const Spinor &in, const Spinor *v2,
+              double2 alpha, const int *skip = nullptr)
+{
+    const int g5 = op.gamma5;
+    switch (op.kind) {
+    case LYM_OP_DIRAC_WILSON:
+    case LYM_OP_IMPROVED: apply_full(c, op, prec, out, in, g5, v2, alpha, skip); return;
+    case LYM_OP_SQUARE_DIRAC_WILSON:
+    case LYM_OP_SQUARE_IMPROVED: {
+        Vec tmp(c, prec, 2);
+        apply_full(c, op, prec, *tmp, in, g5, nullptr, alpha, skip);
+        apply_full(c, op, prec, out, *tmp, g5, v2, alpha, skip);
+        return;
+    }
+    case LYM_OP_EVEN_ODD_IMPROVED: {
+        if (v2) fail(c, LYM_ERR_UNSUPPORTED, "EvenOddImprovedDiracWilsonOperator::multiplyAdd is not implemented");
+        Vec te(c, prec, 1);
+        copy(c, out.parity(0), in.parity(0));
+        apply_schur(c, op, prec, out.parity(1), in.parity(1), *te, g5, nullptr, alpha, skip);
+        return;
+    }
+    case LYM_OP_SQUARE_EVEN_ODD_IMPROVED: {
+        Vec te(c, prec, 1), to(c, prec, 1);
+        apply_schur(c, op, prec, *to, in.parity(1), *te, g5, nullptr, alpha, skip);
+        Spinor v2o;
+        if (v2) v2o = v2->parity(1);
+        apply_schur(c, op, prec, out.parity(1), *to, *te, g5, v2 ? &v2o : nullptr, alpha, skip);
+        copy(c, out.parity(0), in.parity(0));
+        if (v2) axpby(c, v2->parity(0), out.parity(0), alpha, C2(1.0));
+        return;
+    }
+    default: fail(c, LYM_ERR_ARGUMENT, "unknown operator kind %d", op.kind);
+    }
+}
+
+// ------------------------------------------------------ host <-> device -----
+double *staging(lym_context *c, int k)
+{
+    if (!c->aos[k]) c->aos[k] = (double *)dev_alloc(c, (size_t)c->g.V * 24 * sizeof(double));
+    return c->aos[k];
+}
+
+void upload_vec(lym_context *c, const Spinor &dst, const double *src, bool device_ptr, int slot)
+{
+    const size_t b = (size_t)c->g.V * 24 * sizeof(double);
+    const double *d = src;
+    if (!device_ptr) {
+        double *s = staging(c, slot);
+        CK(cudaMemcpyAsync(s, src, b, cudaMemcpyHostToDevice, c->st));
+        d = s;
+    }
+    launch_pack(c->g, d, dst, c->st);
+}
+
+void download_vec(lym_context *c, double *dst, const Spinor &src, bool device_ptr, int slot)
+{
+    const size_t b = (size_t)c->g.V * 24 * sizeof(double);
+    if (device_ptr) {
+        launch_unpack(c->g, src, dst, c->st);
+        return;
+    }
+    double *s = staging(c, slot);
+    launch_unpack(c->g, src, s, c->st);
+    CK(cudaMemcpyAsync(dst, s, b, cudaMemcpyDeviceToHost, c->st));
+}
+
+// ------------------------------------------------------------- solvers -----
+CGState *cg_state(lym_context *c) { return (CGState *)c->d_state; }
+CGState &cg_host(lym_context *c) { return *(CGState *)c->h_state; }
+BiCGState *bi_state(lym_context *c) { return (BiCGState *)c->d_state; }
+BiCGState &bi_host(lym_context *c) { return *(BiCGState *)c->h_state; }
+
+void pull_state(lym_context *c, size_t bytes)
+{
+    CK(cudaMemcpyAsync(c->h_state, c->d_state, bytes, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+}
+void push_state(lym_context *c, size_t bytes)
+{
+    CK(cudaMemcpyAsync(c->d_state, c->h_state, bytes, cudaMemcpyHostToDevice, c->st));
+}
+
+// Run `step` (one iteration; every kernel gated on the state's `pause` flag)
+// until the device state pauses.  Batches of iterations are captured once into a
+// CUDA graph and replayed; the host reads the state once per batch.
+template <class S, class Step> void run_gated_state(lym_context *c, S *d, Step step, int batch, long max_iterations)
+{
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeRelaxed));
+    c->capturing = true;
+    try {
+        for (int k = 0; k < batch; ++k) step();
+    } catch (...) {
+        c->capturing = false;
+        cudaStreamEndCapture(c->st, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+    }
+    c->capturing = false;
+    CK(cudaStreamEndCapture(c->st, &graph));
+    CK(cudaGraphInstantiate(&exec, graph, 0));
+    size_t nodes = 0;
+    cudaGraphGetNodes(graph, nullptr, &nodes);
+    // every iteration pauses the state by itself at its iteration limit; the host
+    // bound below only guards against a state that never pauses
+    const long max_launches = max_iterations / batch + 4;
+    bool paused = false;
+    for (long l = 0; l < max_launches; ++l) {
+        CK(cudaGraphLaunch(exec, c->st));
+        c->launches += nodes;
+        CK(cudaMemcpyAsync(c->h_state, d, sizeof(S), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        if (((S *)c->h_state)->pause) {
+            paused = true;
+            break;
+        }
+    }
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    CK(cudaGetLastError());
+    if (!paused) fail(c, LYM_ERR_TIMEOUT, "solver state did not stop within %ld iterations", max_iterations);
+}
+
+// --- CG (ConjugateGradient::solve, inverters/ConjugateGradient.cpp:10-74) ---
+template <class MatVec>
+int cg_solve(lym_context *c, MatVec matvec, int nparity, const Spinor &b, const Spinor &x, const Spinor *guess,
+             double eps, int max_steps, lym_solve_stats *st)
+{
+    Vec r(c, PREC_D, nparity), p(c, PREC_D, nparity), ap(c, PREC_D, nparity);
+    copy(c, x, guess ? *guess : b);
+    matvec(*ap, x, nullptr);
+    run_site(c, OpSubNorm<SpinorD, SpinorD, SpinorD>{b.d(), (*ap).d(), (*r).d(), c->d_scal}, nparity);
+    copy(c, *p, *r);
+    CK(cudaMemcpyAsync(c->h_scal, c->d_scal, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    CGState &H = cg_host(c);
+    memset(&H, 0, sizeof(H));
+    H.rr = c->h_scal[0];
+    H.rr_max = H.rr;
+    H.eps = eps;
+    H.max_iter = max_steps;
+    push_state(c, sizeof(CGState));
+    CGState *S = cg_state(c);
+    Gate gate{&S->pause, nullptr};
+    auto step = [&]() {
+        matvec(*ap, *p, &S->pause);
+        run_site(c, OpCGAlpha<SpinorD, SpinorD>{(*p).d(), (*ap).d(), S}, nparity, gate);
+        run_site(c, OpCGUpdate<SpinorD, SpinorD, SpinorD, SpinorD>{x.d(), (*p).d(), (*r).d(), (*ap).d(), S}, nparity,
+                 gate);
+        run_site(c, OpCGDirection<SpinorD, SpinorD>{(*p).d(), (*r).d(), S}, nparity, gate);
+    };
+    if (max_steps > 0) run_gated_state(c, S, step, 8, max_steps);
+    else pull_state(c, sizeof(CGState));
+    CGState &R = cg_host(c);
+    if (st) {
+        st->converged = R.converged;
+        st->iterations = R.iter;
+        st->steps = R.converged ? R.iter - 1 : max_steps;
+        st->last_error = R.rr;
+    }
+    if (R.failed) fail(c, LYM_ERR_NUMERIC, "CG produced a non-finite residual");
+    return R.converged ? LYM_OK : LYM_NOT_CONVERGED;
+}
+
+// --- BiCGStab (BiConjugateGradient::solve, BiConjugateGradient.cpp:321-507) ---
+template <class MatVec>
+int bicgstab_solve(lym_context *c, MatVec matvec, int nparity, const Spinor &b, const Spinor &x,
+                   const Spinor *guess, double precision, int max_steps, double norm_offset, lym_solve_stats *st)
+{
+    Vec r(c, PREC_D, nparity), rhat(c, PREC_D, nparity), p(c, PREC_D, nparity), nu(c, PREC_D, nparity),
+        s(c, PREC_D, nparity), t(c, PREC_D, nparity);
+    if (guess) {
+        copy(c, x, *guess);
+    } else {
+        const double ns = norm2_now(c, b) + norm_offset;
+        if (ns > precision) {
+            copy(c, x, b);
+        } else {
+            // the reference draws a time-seeded uniform random start here (AlgebraUtils.h:123-167);
+            // a fixed deterministic start is used instead
+            std::vector<double> host((size_t)c->g.V * 24);
+            unsigned long long z = 0x9E3779B97F4A7C15ull;
+            for (auto &v : host) {
+                z += 0x9E3779B97F4A7C15ull;
+                unsigned long long q = z;
+                q = (q ^ (q >> 30)) * 0xBF58476D1CE4E5B9ull;
+                q = (q ^ (q >> 27)) * 0x94D049BB133111EBull;
+                q ^= q >> 31;
+                v = (double)(q >> 11) * (1.0 / 9007199254740992.0);
+            }
+            Vec full(c, PREC_D, 2);
+            upload_vec(c, *full, host.data(), false, 2);
+            CK(cudaStreamSynchronize(c->st));
+            copy(c, x, nparity == 2 ? *full : full.par(1));
+        }
+    }
+    matvec(*p, x, nullptr);
+    // r = b - A x ; rhat = b + A x
+    copy(c, *r, b);
+    axpby(c, *p, *r, C2(-1.0), C2(1.0));
+    copy(c, *rhat, b);
+    axpby(c, *p, *rhat, C2(1.0), C2(1.0));
+    zero(c, *p);
+    zero(c, *nu);
+    BiCGState &H = bi_host(c);
+    memset(&H, 0, sizeof(H));
+    H.rho = C2(1.0);
+    H.alpha = C2(1.0);
+    H.omega = C2(1.0);
+    H.precision = precision;
+    H.max_steps = max_steps;
+    push_state(c, sizeof(BiCGState));
+    BiCGState *S = bi_state(c);
+    Gate gate{&S->pause, nullptr};
+    run_site(c, OpBiRho<SpinorD, SpinorD>{(*rhat).d(), (*r).d(), S}, nparity);
+    auto step = [&]() {
+        run_site(c, OpBiDirection<SpinorD, SpinorD, SpinorD>{(*p).d(), (*r).d(), (*nu).d(), S}, nparity, gate);
+        matvec(*nu, *p, &S->pause);
+        run_site(c, OpBiAlpha<SpinorD, SpinorD>{(*rhat).d(), (*nu).d(), S}, nparity, gate);
+        run_site(c, OpBiS<SpinorD, SpinorD, SpinorD>{(*s).d(), (*r).d(), (*nu).d(), S}, nparity, gate);
+        matvec(*t, *s, &S->pause);
+        run_site(c, OpBiOmega<SpinorD, SpinorD>{(*t).d(), (*s).d(), S}, nparity, gate);
+        run_site(c,
+                 OpBiUpdate<SpinorD, SpinorD, SpinorD, SpinorD, SpinorD, SpinorD>{x.d(), (*p).d(), (*s).d(), (*t).d(),
+                                                                                  (*r).d(), (*rhat).d(), S},
+                 nparity, gate);
+    };
+    pull_state(c, sizeof(BiCGState));
+    if (!bi_host(c).pause && max_steps > 0) run_gated_state(c, S, step, 4, max_steps);
+    BiCGState &R = bi_host(c);
+    if (R.degenerate) copy(c, x, b);  // BiConjugateGradient.cpp:455-464
+    if (st) {
+        st->converged = R.converged && !R.breakdown;
+        st->iterations = R.step + (R.converged ? 1 : 0);
+        st->steps = R.converged ? R.step : max_steps;
+        st->last_error = R.last_error;
+    }
+    if (R.breakdown) {
+        c->err = "BiConjugateGradient: breakdown (rho = 0 or non-finite residual)";
+        return LYM_ERR_BREAKDOWN;
+    }
+    return R.converged ? LYM_OK : LYM_NOT_CONVERGED;
+}
+
+// b'_o = b_o + kappa H_oe Tinv_ee b_e  (source of the Schur system)
+void schur_source(lym_context *c, OpEntry &op, const Spinor &b, const Spinor &bprime_o)
+{
+    GaugeEntry &ge = gauge_of(c, op.gauge_id);
+    const bool clov = kind_has_clover(op.kind);
+    if (clov) ensure_clover(c, op);
+    Vec te(c, PREC_D, 1);
+    if (clov) launch_clover(c->g, PREC_D, *te, b.parity(0), op.clover.Tinv[PREC_D], 0, 0, c->st);
+    else copy(c, *te, b.parity(0));
+    DslashParams P;
+    P.g = c->g;
+    P.prec = PREC_D;
+    P.rep = c->rep;
+    P.U = &ge.dev;
+    P.epi = EPI_XPAY_;
+    P.parity = 1;
+    P.in = *te;
+    P.out = bprime_o;
+    P.y = b.parity(1);
+    P.v2 = b.parity(1);
+    P.b = op.kappa;
+    launch_dslash(P, c->st);
+}
+
+// x_e = Tinv_ee (b_e + kappa H_eo x_o)
+void schur_reconstruct(lym_context *c, OpEntry &op, const Spinor &b, const Spinor &x)
+{
+    GaugeEntry &ge = gauge_of(c, op.gauge_id);
+    const bool clov = kind_has_clover(op.kind);
+    DslashParams P;
+    P.g = c->g;
+    P.prec = PREC_D;
+    P.rep = c->rep;
+    P.U = &ge.dev;
+    P.epi = clov ? EPI_XPAY_INV_ : EPI_XPAY_;
+    P.parity = 0;
+    P.in = x.parity(1);
+    P.out = x.parity(0);
+    P.y = b.parity(0);
+    P.v2 = b.parity(0);
+    P.clover = clov ? op.clover.Tinv[PREC_D] : nullptr;
+    P.b = op.kappa;
+    launch_dslash(P, c->st);
+}
+
+double true_residual(lym_context *c, OpEntry &op, const Spinor &b, const Spinor &x)
+{
+    // ||b - D x|| / ||b|| with the FP64 full operator D (gamma5 = false)
+    Vec ax(c, PREC_D, 2), r(c, PREC_D, 2);
+    apply_full(c, op, PREC_D, *ax, x, 0, nullptr, C2(0.0));
+    run_site(c, OpSubNorm<SpinorD, SpinorD, SpinorD>{b.d(), (*ax).d(), (*r).d(), c->d_scal}, 2);
+    CK(cudaMemcpyAsync(c->h_scal, c->d_scal, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    const double rr = c->h_scal[0];
+    const double bb = norm2_now(c, b);
+    return bb > 0 ? std::sqrt(rr / bb) : std::sqrt(rr);
+}
+
+// PreconditionedBiCGStab::solve (inverters/PreconditionedBiCGStab.cpp:33-100)
+int eo_bicgstab(lym_context *c, OpEntry &op, const Spinor &b, const Spinor &x, const Spinor *guess, double precision,
+                int max_steps, lym_solve_stats *st)
+{
+    const Geom &g = c->g;
+    const bool even = g.L[0] % 2 == 0 && g.L[1] % 2 == 0 && g.L[2] % 2 == 0 && g.L[3] % 2 == 0;
+    if (op.kind != LYM_OP_IMPROVED || !even) {
+        auto mv = [&](const Spinor &out, const Spinor &in, const int *skip) {
+            op_apply(c, op, PREC_D, out, in, nullptr, C2(0.0), skip);
+        };
+        return bicgstab_solve(c, mv, 2, b, x, guess, precision, max_steps, 0.0, st);
+    }
+    // the even-odd operators of the reference are default-constructed: gamma5 = true (DiracOperator.cpp:14)
+    OpEntry &eo = op;
+    Vec bp(c, PREC_D, 1), src(c, PREC_D, 1), te(c, PREC_D, 1), tmp(c, PREC_D, 1);
+    schur_source(c, op, b, *bp);
+    gamma5_inplace(c, *bp);  // odd_source = gamma5 (b_o + kappa H Tinv b_e)
+    apply_schur(c, eo, PREC_D, *src, *bp, *te, 1);  // odd_source_eo = gamma5 S odd_source
+    const double norm_even = norm2_now(c, b.parity(0));  // the reference's full-lattice source norm includes gamma5 b_e
+    auto mv = [&](const Spinor &out, const Spinor &in, const int *skip) {
+        apply_schur(c, eo, PREC_D, *tmp, in, *te, 1, nullptr, C2(0.0), skip);
+        apply_schur(c, eo, PREC_D, out, *tmp, *te, 1, nullptr, C2(0.0), skip);
+    };
+    Spinor go;
+    if (guess) go = guess->parity(1);
+    const int rc = bicgstab_solve(c, mv, 1, *src, x.parity(1), guess ? &go : nullptr, precision, max_steps,
+                                  norm_even, st);
+    schur_reconstruct(c, op, b, x);
+    return rc;
+}
+
+// Even-odd CG on (gamma5 S)^2 with reliable updates: D x = b to ||b - D x|| <= tol ||b||.
+// Inner iterations run in `sprec` (FP64, FP32 or FP16 spinors); x and the true
+// residual are FP64.  delta: reliable-update threshold on the recursive residual.
+int eo_cg(lym_context *c, OpEntry &op, int sprec, const Spinor &b, const Spinor &x, const Spinor *guess, double tol,
+          int max_steps, lym_solve_stats *st)
+{
+    const double delta = sprec == PREC_D ? 0.0 : 0.1;
+    OpEntry &eo = op;  // apply_schur takes gamma5 explicitly
+    if (kind_has_clover(op.kind)) ensure_clover(c, op);
+    Vec bp(c, PREC_D, 1), rS(c, PREC_D, 1), rN(c, PREC_D, 1), te(c, PREC_D, 1), t1(c, PREC_D, 1);
+    Vec xs(c, sprec == PREC_H ? PREC_F : sprec, 1), rs(c, sprec == PREC_H ? PREC_F : sprec, 1);
+    Vec ps(c, sprec, 1), aps(c, sprec, 1), tes(c, sprec, 1), tos(c, sprec, 1);
+    const Spinor xo = x.parity(1);
+    schur_source(c, op, b, *bp);
+    const double bb = norm2_now(c, b);
+    const double eps_S = tol * tol * bb;
+    if (guess) copy(c, xo, guess->parity(1));
+    else zero(c, xo);
+
+    // true residuals: r_S = b' - S x, r_N = g5 S g5 r_S ; returns |r_S|^2, |r_N|^2
+    auto true_res = [&](double &rrS, double &rrN) {
+        apply_schur(c, eo, PREC_D, *t1, xo, *te, 0);
+        run_site(c, OpSubNorm<SpinorD, SpinorD, SpinorD>{(*bp).d(), (*t1).d(), (*rS).d(), c->d_scal}, 1);
+        copy(c, *t1, *rS);
+        gamma5_inplace(c, *t1);
+        apply_schur(c, eo, PREC_D, *rN, *t1, *te, 1);
+        run_site(c, OpNorm<SpinorD>{(*rN).d(), c->d_scal + 1}, 1);
+        CK(cudaMemcpyAsync(c->h_scal, c->d_scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        rrS = c->h_scal[0];
+        rrN = c->h_scal[1];
+    };
+    double rrS, rrN;
+    true_res(rrS, rrN);
+    int iters = 0, updates = 0, rc = LYM_NOT_CONVERGED;
+    CGState *S = cg_state(c);
+    Gate gate{&S->pause, nullptr};
+    if (rrS < eps_S || bb == 0.0) {
+        rc = LYM_OK;
+    } else {
+        double eps_N = eps_S * (rrN / rrS);
+        copy(c, *rs, *rN);
+        copy(c, *ps, *rs);
+        zero(c, *xs);
+        CGState &H = cg_host(c);
+        memset(&H, 0, sizeof(H));
+        H.rr = rrN;
+        H.rr_max = rrN;
+        H.eps = eps_N;
+        H.delta2 = delta * delta;
+        H.max_iter = max_steps;
+        push_state(c, sizeof(CGState));
+        auto matvec = [&](const Spinor &out, const Spinor &in, const int *skip) {
+            apply_schur(c, eo, sprec, *tos, in, *tes, 1, nullptr, C2(0.0), skip);
+            apply_schur(c, eo, sprec, out, *tos, *tes, 1, nullptr, C2(0.0), skip);
+        };
+        auto step = [&]() {
+            matvec(*aps, *ps, &S->pause);
+            auto go = [&](auto P, auto AP, auto X, auto R) {
+                run_site(c, OpCGAlpha<decltype(P), decltype(AP)>{P, AP, S}, 1, gate);
+                run_site(c, OpCGUpdate<decltype(X), decltype(P), decltype(R), decltype(AP)>{X, P, R, AP, S}, 1, gate);
+                run_site(c, OpCGDirection<decltype(P), decltype(R)>{P, R, S}, 1, gate);
+            };
+            if (sprec == PREC_D) go((*ps).d(), (*aps).d(), (*xs).d(), (*rs).d());
+            else if (sprec == PREC_F) go((*ps).f(), (*aps).f(), (*xs).f(), (*rs).f());
+            else go((*ps).h(), (*aps).h(), (*xs).f(), (*rs).f());
+        };
+        for (int outer = 0; outer < 10000; ++outer) {
+            run_gated_state(c, S, step, 8, (long)max_steps - cg_host(c).iter + 8);
+            CGState R = cg_host(c);
+            iters = R.iter;
+            if (R.failed) fail(c, LYM_ERR_NUMERIC, "CG produced a non-finite residual");
+            // reliable update: x += x_sloppy, recompute the FP64 residuals
+            axpby(c, *xs, xo, C2(1.0), C2(1.0));
+            zero(c, *xs);
+            true_res(rrS, rrN);
+            ++updates;
+            if (rrS < eps_S) {
+                rc = LYM_OK;
+                break;
+            }
+            if (R.iter >= max_steps) break;
+            if (R.converged) {
+                // recursion converged but the true residual did not: tighten
+                eps_N = std::max(eps_N * 0.5 * eps_S / rrS, 1e-300);
+            }
+            copy(c, *rs, *rN);
+            CGState &W = cg_host(c);
+            W = R;
+            W.beta = rrN / R.rr_prev;
+            W.rr = rrN;
+            W.rr_max = rrN;
+            W.eps = eps_N;
+            W.pause = 0;
+            W.converged = 0;
+            W.need_update = 0;
+            push_state(c, sizeof(CGState));
+            // p = r + beta p with the true residual
+            if (sprec == PREC_D) run_site(c, OpCGDirection<SpinorD, SpinorD>{(*ps).d(), (*rs).d(), S}, 1);
+            else if (sprec == PREC_F) run_site(c, OpCGDirection<SpinorF, SpinorF>{(*ps).f(), (*rs).f(), S}, 1);
+            else run_site(c, OpCGDirection<SpinorH, SpinorF>{(*ps).h(), (*rs).f(), S}, 1);
+        }
+    }
+    schur_reconstruct(c, op, b, x);
+    if (st) {
+        st->iterations = iters;
+        st->steps = iters;
+        st->reliable_updates = updates;
+        st->converged = rc == LYM_OK;
+        st->last_error = rrS;
+    }
+    return rc;
+}
+
+// Multishift CG on (A + shift_i), A Hermitian positive definite (a Square* kind).
+int multishift_cg(lym_context *c, OpEntry &op, int nshift, const double *shifts, double eps, int max_steps,
+                  const Spinor &b, std::vector<Spinor> &xs, lym_solve_stats *st)
+{
+    if (nshift < 1 || nshift > kMaxShifts) fail(c, LYM_ERR_ARGUMENT, "multishift: 1..%d shifts", kMaxShifts);
+    int base = 0;
+    for (int i = 1; i < nshift; ++i)
+        if (shifts[i] < shifts[base]) base = i;
+    const double s0 = shifts[base];
+    std::vector<Vec *> ps;
+    for (int i = 0; i < nshift; ++i) ps.push_back(new Vec(c, PREC_D, 2));
+    Vec r(c, PREC_D, 2), ap(c, PREC_D, 2);
+    std::vector<SpinorD> hx(nshift), hp(nshift);
+    for (int i = 0; i < nshift; ++i) {
+        zero(c, xs[i]);
+        copy(c, **ps[i], b);
+        hx[i] = xs[i].d();
+        hp[i] = (**ps[i]).d();
+    }
+    copy(c, *r, b);
+    SpinorD *dviews = (SpinorD *)dev_alloc(c, 2 * kMaxShifts * sizeof(SpinorD));
+    CK(cudaMemcpyAsync(dviews, hx.data(), nshift * sizeof(SpinorD), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(dviews + kMaxShifts, hp.data(), nshift * sizeof(SpinorD), cudaMemcpyHostToDevice, c->st));
+    const double bb = norm2_now(c, b);
+    MultishiftState &H = *(MultishiftState *)c->h_state;
+    memset(&H, 0, sizeof(H));
+    H.nshift = nshift;
+    H.base = base;
+    for (int i = 0; i < nshift; ++i) {
+        H.sigma[i] = shifts[i] - s0;
+        H.zeta[i] = H.zeta_prev[i] = 1.0;
+        H.active[i] = 1;
+    }
+    H.rr = bb;
+    H.alpha = 1.0;
+    H.beta = 0.0;
+    H.eps = eps;
+    H.max_iter = max_steps;
+    CK(cudaMemcpyAsync(c->d_state, c->h_state, sizeof(MultishiftState), cudaMemcpyHostToDevice, c->st));
+    MultishiftState *S = (MultishiftState *)c->d_state;
+    Gate gate{&S->pause, nullptr};
+    const Spinor pb = **ps[base];
+    auto step = [&]() {
+        op_apply(c, op, PREC_D, *ap, pb, &pb, C2(s0), &S->pause);
+        run_site(c, OpMsAlpha<SpinorD, SpinorD>{pb.d(), (*ap).d(), S}, 2, gate);
+        run_site(c, OpMsResidual<SpinorD, SpinorD>{(*r).d(), (*ap).d(), S}, 2, gate);
+        run_site(c, OpMsUpdate<SpinorD>{dviews, dviews + kMaxShifts, (*r).d(), S, nshift}, 2, gate);
+    };
+    int rc = LYM_OK;
+    if (bb > 0 && max_steps > 0) {
+        run_gated_state(c, S, step, 4, max_steps);
+        MultishiftState &R = *(MultishiftState *)c->h_state;
+        rc = R.converged ? LYM_OK : LYM_NOT_CONVERGED;
+        if (st) {
+            st->iterations = R.iter;
+            st->steps = R.iter;
+            st->converged = R.converged;
+            st->last_error = R.rr;
+        }
+    }
+    for (auto v : ps) delete v;
+    dev_free(c, dviews, 2 * kMaxShifts * sizeof(SpinorD));
+    return rc;
+}
+
+}  // namespace
+
+// =============================================================== C ABI =====
+extern "C" {
+
+int lym_context_create(const int dims[4], int rep, int device, lym_context **out)
+{
+    if (!dims || !out) return LYM_ERR_ARGUMENT;
+    *out = nullptr;
+    for (int mu = 0; mu < 4; ++mu)
+        if (dims[mu] < 2) return LYM_ERR_ARGUMENT;
+    if (dims[3] % 2) return LYM_ERR_UNSUPPORTED;  // the even-odd half-site index needs an even L_t
+    if (rep != LYM_REP_SU3_FUNDAMENTAL && rep != LYM_REP_SU2_ADJOINT) return LYM_ERR_ARGUMENT;
+    const long long V = (long long)dims[0] * dims[1] * dims[2] * dims[3];
+    if (V > (1ll << 30)) return LYM_ERR_UNSUPPORTED;
+    lym_context *c = new lym_context();
+    c->device = device;
+    c->rep = rep;
+    for (int mu = 0; mu < 4; ++mu) c->g.L[mu] = dims[mu];
+    c->g.V = (int)V;
+    c->g.Vh = (int)(V / 2);
+    c->g.stride = (c->g.Vh + 63) / 64 * 64;
+    int rc = guarded(c, [&]() {
+        CK(cudaSetDevice(device));
+        CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+        c->partials = (double *)dev_alloc(c, (size_t)kBlasGridMax * kMaxRed * sizeof(double));
+        c->counter = (unsigned int *)dev_alloc(c, 64);
+        c->d_err = (int *)dev_alloc(c, 64);
+        c->d_state = dev_alloc(c, kStateBytes);
+        c->d_scal = (double *)dev_alloc(c, 64 * sizeof(double));
+        CK(cudaHostAlloc(&c->h_state, kStateBytes, cudaHostAllocDefault));
+        CK(cudaHostAlloc((void **)&c->h_scal, 64 * sizeof(double), cudaHostAllocDefault));
+        CK(cudaEventCreate(&c->ev0));
+        CK(cudaEventCreate(&c->ev1));
+        CK(cudaStreamSynchronize(c->st));
+        return LYM_OK;
+    });
+    if (rc != LYM_OK) {
+        lym_context_destroy(c);
+        return rc;
+    }
+    *out = c;
+    return LYM_OK;
+}
+
+void lym_context_destroy(lym_context *c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->st) cudaStreamSynchronize(c->st);
+    for (auto &kv : c->ops)
+        for (int p = 0; p < 3; ++p) {
+            cudaFree(kv.second.clover.T[p]);
+            cudaFree(kv.second.clover.Tinv[p]);
+        }
+    for (auto &kv : c->gauges) {
+        cudaFree(kv.second.dev.d64);
+        cudaFree(kv.second.dev.f32);
+        cudaFree(kv.second.dev.h16);
+        cudaFree(kv.second.dev.sign);
+    }
+    for (auto &s : c->pool) cudaFree(s.v);
+    for (int k = 0; k < 3; ++k) cudaFree(c->aos[k]);
+    cudaFree(c->partials);
+    cudaFree(c->counter);
+    cudaFree(c->d_err);
+    cudaFree(c->d_state);
+    cudaFree(c->d_scal);
+    if (c->h_state) cudaFreeHost(c->h_state);
+    if (c->h_scal) cudaFreeHost(c->h_scal);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+}
+
+const char *lym_last_error(lym_context *c) { return c ? c->err.c_str() : "no context"; }
+
+int lym_context_volume(lym_context *c) { return c ? c->g.V : 0; }
+
+size_t lym_context_device_bytes(lym_context *c) { return c ? c->bytes : 0; }
+
+int lym_synchronize(lym_context *c)
+{
+    return guarded(c, [&]() {
+        CK(cudaStreamSynchronize(c->st));
+        return LYM_OK;
+    });
+}
+
+static int gauge_store(lym_context *c, int id, const double *links, bool device_ptr)
+{
+    const Geom &g = c->g;
+    GaugeEntry *ge;
+    auto it = c->gauges.find(id);
+    if (it == c->gauges.end()) {
+        GaugeEntry e;
+        e.dev.rep = c->rep;
+        const size_t s = g.stride;
+        const size_t d64 = c->rep == REP_SU3 ? 2 * 4 * 9 * s * sizeof(double2) : 2 * 4 * 9 * s * sizeof(double);
+        const size_t f32 = c->rep == REP_SU3 ? 2 * 4 * 3 * s * sizeof(float4) : 2 * 4 * 3 * s * sizeof(float2);
+        const size_t h16 = c->rep == REP_SU3 ? 2 * 4 * 3 * s * sizeof(uint2) : 2 * 4 * 3 * s * sizeof(__half2);
+        e.dev.d64 = dev_alloc(c, d64);
+        e.dev.f32 = dev_alloc(c, f32);
+        e.dev.h16 = dev_alloc(c, h16);
+        e.dev.sign = (uint8_t *)dev_alloc(c, 2 * s);
+        ge = &(c->gauges[id] = e);
+    } else {
+        ge = &it->second;
+    }
+    const size_t per = c->rep == REP_SU3 ? 18 : 9;
+    const size_t bytes = (size_t)g.V * 4 * per * sizeof(double);
+    if (!device_ptr) {
+        double *buf = (double *)dev_alloc(c, bytes);
+        CK(cudaMemcpyAsync(buf, links, bytes, cudaMemcpyHostToDevice, c->st));
+        launch_upload_gauge(g, c->rep, buf, ge->dev, c->st);
+        CK(cudaStreamSynchronize(c->st));
+        dev_free(c, buf, bytes);
+    } else {
+        launch_upload_gauge(g, c->rep, links, ge->dev, c->st);
+    }
+    CK(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st));
+    launch_compress_gauge(g, ge->dev, c->d_err, c->st);
+    CK(cudaMemcpyAsync(c->h_scal, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaGetLastError());
+    memcpy(&ge->recon_err, c->h_scal, sizeof(int));
+    ge->dev.recon_ok = ge->recon_err == 0;
+    // operators on this gauge field need a new clover term
+    for (auto &kv : c->ops)
+        if (kv.second.gauge_id == id) kv.second.clover_ok = false;
+    return LYM_OK;
+}
+
+int lym_gauge_upload(lym_context *c, int id, const double *links)
+{
+    if (!links) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() { return gauge_store(c, id, links, false); });
+}
+
+int lym_gauge_upload_device(lym_context *c, int id, const double *links)
+{
+    if (!links) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() { return gauge_store(c, id, links, true); });
+}
+
+int lym_gauge_upload_fundamental(lym_context *c, int id, const double *gauge_links, int boundary)
+{
+    if (!gauge_links || (boundary != LYM_BC_PERIODIC && boundary != LYM_BC_ANTIPERIODIC)) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        const Geom &g = c->g;
+        const size_t in_per = c->rep == REP_SU3 ? 18 : 8, out_per = c->rep == REP_SU3 ? 18 : 9;
+        const size_t bin = (size_t)g.V * 4 * in_per * sizeof(double), bout = (size_t)g.V * 4 * out_per * sizeof(double);
+        double *din = (double *)dev_alloc(c, bin), *dout = (double *)dev_alloc(c, bout);
+        CK(cudaMemcpyAsync(din, gauge_links, bin, cudaMemcpyHostToDevice, c->st));
+        launch_fundamental_to_fermion(g, c->rep, boundary, din, dout, c->st);
+        int rc = gauge_store(c, id, dout, true);
+        CK(cudaStreamSynchronize(c->st));
+        dev_free(c, din, bin);
+        dev_free(c, dout, bout);
+        return rc;
+    });
+}
+
+int lym_gauge_evict(lym_context *c, int id)
+{
+    return guarded(c, [&]() {
+        auto it = c->gauges.find(id);
+        if (it == c->gauges.end()) fail(c, LYM_ERR_NOT_FOUND, "gauge field %d is not resident", id);
+        for (auto &kv : c->ops)
+            if (kv.second.gauge_id == id) fail(c, LYM_ERR_ARGUMENT, "gauge field %d is used by operator %d", id, kv.first);
+        CK(cudaStreamSynchronize(c->st));
+        const size_t s = c->g.stride;
+        const bool su3 = c->rep == REP_SU3;
+        dev_free(c, it->second.dev.d64, su3 ? 2 * 4 * 9 * s * sizeof(double2) : 2 * 4 * 9 * s * sizeof(double));
+        dev_free(c, it->second.dev.f32, su3 ? 2 * 4 * 3 * s * sizeof(float4) : 2 * 4 * 3 * s * sizeof(float2));
+        dev_free(c, it->second.dev.h16, su3 ? 2 * 4 * 3 * s * sizeof(uint2) : 2 * 4 * 3 * s * sizeof(__half2));
+        dev_free(c, it->second.dev.sign, 2 * s);
+        c->gauges.erase(it);
+        return LYM_OK;
+    });
+}
+
+int lym_operator_create(lym_context *c, int gauge_id, int kind, double kappa, double csw, int gamma5, int *op_id)
+{
+    if (!op_id || kind < 0 || kind > 5) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        gauge_of(c, gauge_id);
+        if (is_even_odd(kind) && c->rep != REP_SU3 && c->rep != REP_SU2ADJ)
+            fail(c, LYM_ERR_UNSUPPORTED, "even-odd operator needs diracVectorLength 3");
+        OpEntry e;
+        e.gauge_id = gauge_id;
+        e.kind = kind;
+        e.kappa = kappa;
+        e.csw = kind_has_clover(kind) ? csw : 0.0;
+        e.gamma5 = gamma5 ? 1 : 0;
+        const int id = c->next_op++;
+        c->ops[id] = e;
+        *op_id = id;
+        return LYM_OK;
+    });
+}
+
+int lym_operator_set_gamma5(lym_context *c, int op_id, int gamma5)
+{
+    return guarded(c, [&]() {
+        op_of(c, op_id).gamma5 = gamma5 ? 1 : 0;
+        return LYM_OK;
+    });
+}
+
+int lym_operator_set_kappa(lym_context *c, int op_id, double kappa)
+{
+    return guarded(c, [&]() {
+        OpEntry &o = op_of(c, op_id);
+        if (o.kappa != kappa) o.clover_ok = false;
+        o.kappa = kappa;
+        return LYM_OK;
+    });
+}
+
+int lym_operator_set_csw(lym_context *c, int op_id, double csw)
+{
+    return guarded(c, [&]() {
+        OpEntry &o = op_of(c, op_id);
+        if (o.csw != csw) o.clover_ok = false;
+        o.csw = kind_has_clover(o.kind) ? csw : 0.0;
+        return LYM_OK;
+    });
+}
+
+int lym_operator_set_gauge(lym_context *c, int op_id, int gauge_id)
+{
+    return guarded(c, [&]() {
+        gauge_of(c, gauge_id);
+        OpEntry &o = op_of(c, op_id);
+        o.gauge_id = gauge_id;
+        o.clover_ok = false;
+        return LYM_OK;
+    });
+}
+
+int lym_operator_destroy(lym_context *c, int op_id)
+{
+    return guarded(c, [&]() {
+        OpEntry &o = op_of(c, op_id);
+        CK(cudaStreamSynchronize(c->st));
+        free_clover(c, o);
+        c->ops.erase(op_id);
+        return LYM_OK;
+    });
+}
+
+static int do_multiply(lym_context *c, int op_id, int prec, double *out, const double *v1, const double *v2,
+                       double2 alpha, bool device_ptr)
+{
+    if (!out || !v1) return LYM_ERR_ARGUMENT;
+    if (prec < PREC_D || prec > PREC_H) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        OpEntry &op = op_of(c, op_id);
+        Vec a(c, prec, 2), o(c, prec, 2);
+        Vec *w = nullptr;
+        upload_vec(c, *a, v1, device_ptr, 0);
+        if (v2) {
+            w = new Vec(c, prec, 2);
+            upload_vec(c, **w, v2, device_ptr, 1);
+        }
+        try {
+            op_apply(c, op, prec, *o, *a, w ? &**w : nullptr, alpha);
+        } catch (...) {
+            delete w;
+            throw;
+        }
+        delete w;
+        download_vec(c, out, *o, device_ptr, 2);
+        CK(cudaStreamSynchronize(c->st));
+        CK(cudaGetLastError());
+        return LYM_OK;
+    });
+}
+
+int lym_multiply(lym_context *c, int op_id, double *out, const double *in)
+{
+    return do_multiply(c, op_id, PREC_D, out, in, nullptr, C2(0.0), false);
+}
+
+int lym_multiply_add(lym_context *c, int op_id, double *out, const double *v1, const double *v2, double are, double aim)
+{
+    if (!v2) return LYM_ERR_ARGUMENT;
+    return do_multiply(c, op_id, PREC_D, out, v1, v2, C2(are, aim), false);
+}
+
+int lym_multiply_device(lym_context *c, int op_id, double *out, const double *in)
+{
+    return do_multiply(c, op_id, PREC_D, out, in, nullptr, C2(0.0), true);
+}
+
+int lym_multiply_add_device(lym_context *c, int op_id, double *out, const double *v1, const double *v2, double are,
+                            double aim)
+{
+    if (!v2) return LYM_ERR_ARGUMENT;
+    return do_multiply(c, op_id, PREC_D, out, v1, v2, C2(are, aim), true);
+}
+
+int lym_multiply_precision(lym_context *c, int op_id, int prec, double *out, const double *in)
+{
+    return do_multiply(c, op_id, prec, out, in, nullptr, C2(0.0), false);
+}
+
+int lym_field_strength(lym_context *c, int op_id, double *F)
+{
+    if (!F) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        OpEntry &op = op_of(c, op_id);
+        const size_t b = (size_t)c->g.V * 6 * 9 * 2 * sizeof(double);
+        double *d = (double *)dev_alloc(c, b);
+        OpEntry tmp = op;
+        tmp.clover = CloverDev();
+        tmp.clover_ok = false;
+        try {
+            ensure_clover(c, tmp, d);
+        } catch (...) {
+            free_clover(c, tmp);
+            dev_free(c, d, b);
+            throw;
+        }
+        CK(cudaMemcpyAsync(F, d, b, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        free_clover(c, tmp);
+        dev_free(c, d, b);
+        if (c->rep == REP_SU2ADJ) {
+            // adjoint F is real: compact to the reference's real 3x3 layout
+            const size_t n = (size_t)c->g.V * 6 * 9;
+            for (size_t k = 0; k < n; ++k) F[k] = F[2 * k];
+        }
+        return LYM_OK;
+    });
+}
+
+static int do_solve(lym_context *c, int op_id, int solver, double precision, int max_steps, const double *source,
+                    double *solution, const double *guess, lym_solve_stats *stats, bool device_ptr, bool shifted,
+                    double2 shift)
+{
+    if (!source || !solution || max_steps < 0) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        OpEntry &op = op_of(c, op_id);
+        lym_solve_stats local;
+        memset(&local, 0, sizeof(local));
+        Vec b(c, PREC_D, 2), x(c, PREC_D, 2);
+        Vec *gs = nullptr;
+        upload_vec(c, *b, source, device_ptr, 0);
+        if (guess) {
+            gs = new Vec(c, PREC_D, 2);
+            upload_vec(c, **gs, guess, device_ptr, 1);
+        }
+        const Spinor *gp = gs ? &**gs : nullptr;
+        CK(cudaEventRecord(c->ev0, c->st));
+        int rc = LYM_OK;
+        try {
+            if (shifted) {
+                auto mv = [&](const Spinor &out, const Spinor &in, const int *skip) {
+                    op_apply(c, op, PREC_D, out, in, &in, shift, skip);
+                };
+                rc = bicgstab_solve(c, mv, 2, *b, *x, gp, precision, max_steps, 0.0, &local);
+            } else {
+                switch (solver) {
+                case LYM_SOLVER_CG: {
+                    auto mv = [&](const Spinor &out, const Spinor &in, const int *skip) {
+                        op_apply(c, op, PREC_D, out, in, nullptr, C2(0.0), skip);
+                    };
+                    rc = cg_solve(c, mv, 2, *b, *x, gp, precision, max_steps, &local);
+                    break;
+                }
+                case LYM_SOLVER_BICGSTAB: {
+                    auto mv = [&](const Spinor &out, const Spinor &in, const int *skip) {
+                        op_apply(c, op, PREC_D, out, in, nullptr, C2(0.0), skip);
+                    };
+                    rc = bicgstab_solve(c, mv, 2, *b, *x, gp, precision, max_steps, 0.0, &local);
+                    break;
+                }
+                case LYM_SOLVER_EO_BICGSTAB: rc = eo_bicgstab(c, op, *b, *x, gp, precision, max_steps, &local); break;
+                case LYM_SOLVER_EO_CG:
+                case LYM_SOLVER_EO_CG_MIXED_SINGLE:
+                case LYM_SOLVER_EO_CG_MIXED_HALF: {
+                    if (op.kind != LYM_OP_IMPROVED && op.kind != LYM_OP_DIRAC_WILSON)
+                        fail(c, LYM_ERR_UNSUPPORTED, "even-odd CG solves D x = b for a DiracWilson/Improved operator");
+                    const int sp = solver == LYM_SOLVER_EO_CG ? PREC_D
+                                   : solver == LYM_SOLVER_EO_CG_MIXED_SINGLE ? PREC_F : PREC_H;
+                    const double tol = precision <= 0.0 ? (precision == 0.0 ? 1e-10 : -precision)
+                                                        : std::sqrt(precision);
+                    rc = eo_cg(c, op, sp, *b, *x, gp, tol, max_steps, &local);
+                    local.true_residual = true_residual(c, op, *b, *x);
+                    break;
+                }
+                default: fail(c, LYM_ERR_ARGUMENT, "unknown solver %d", solver);
+                }
+            }
+        } catch (...) {
+            delete gs;
+            throw;
+        }
+        delete gs;
+        CK(cudaEventRecord(c->ev1, c->st));
+        download_vec(c, solution, *x, device_ptr, 2);
+        CK(cudaStreamSynchronize(c->st));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        local.seconds = ms * 1e-3;
+        if (stats) *stats = local;
+        CK(cudaGetLastError());
+        return rc;
+    });
+}
+
+int lym_solve(lym_context *c, int op_id, int solver, double precision, int max_steps, const double *source,
+              double *solution, const double *guess, lym_solve_stats *stats)
+{
+    return do_solve(c, op_id, solver, precision, max_steps, source, solution, guess, stats, false, false, C2(0.0));
+}
+
+int lym_solve_device(lym_context *c, int op_id, int solver, double precision, int max_steps, const double *source,
+                     double *solution, const double *guess, lym_solve_stats *stats)
+{
+    return do_solve(c, op_id, solver, precision, max_steps, source, solution, guess, stats, true, false, C2(0.0));
+}
+
+int lym_solve_shifted(lym_context *c, int op_id, double sre, double sim, double precision, int max_steps,
+                      const double *source, double *solution, const double *guess, lym_solve_stats *stats)
+{
+    return do_solve(c, op_id, LYM_SOLVER_BICGSTAB, precision, max_steps, source, solution, guess, stats, false, true,
+                    C2(sre, sim));
+}
+
+static int do_multishift(lym_context *c, int op_id, int algorithm, int nshift, const double *shifts, double precision,
+                         int max_steps, const double *source, double **solutions, lym_solve_stats *stats,
+                         bool device_ptr)
+{
+    if (!shifts || !source || !solutions || nshift < 1 || nshift > kMaxShifts) return LYM_ERR_ARGUMENT;
+    for (int i = 0; i < nshift; ++i)
+        if (!solutions[i]) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        OpEntry &op = op_of(c, op_id);
+        lym_solve_stats local;
+        memset(&local, 0, sizeof(local));
+        Vec b(c, PREC_D, 2);
+        upload_vec(c, *b, source, device_ptr, 0);
+        std::vector<Vec *> xs;
+        std::vector<Spinor> xv;
+        for (int i = 0; i < nshift; ++i) {
+            xs.push_back(new Vec(c, PREC_D, 2));
+            xv.push_back(**xs.back());
+        }
+        CK(cudaEventRecord(c->ev0, c->st));
+        int rc = LYM_OK;
+        try {
+            if (algorithm == LYM_MULTISHIFT_CG) {
+                rc = multishift_cg(c, op, nshift, shifts, precision, max_steps, *b, xv, &local);
+            } else if (algorithm == LYM_MULTISHIFT_ME) {
+                // MEMultishiftSolver::solve: CG per shift, warm-started from the previous shift
+                int total = 0;
+                bool ok = true;
+                for (int i = 0; i < nshift; ++i) {
+                    const double sh = shifts[i];
+                    auto mv = [&](const Spinor &out, const Spinor &in, const int *skip) {
+                        op_apply(c, op, PREC_D, out, in, &in, C2(sh), skip);
+                    };
+                    lym_solve_stats s1;
+                    memset(&s1, 0, sizeof(s1));
+                    if (i == 0) {
+                        Vec z(c, PREC_D, 2);
+                        zero(c, *z);
+                        rc = cg_solve(c, mv, 2, *b, xv[0], &*z, precision, max_steps, &s1);
+                    } else {
+                        rc = cg_solve(c, mv, 2, *b, xv[i], &xv[i - 1], precision, max_steps, &s1);
+                    }
+                    ok = ok && rc == LYM_OK;
+                    total += s1.iterations;
+                }
+                local.iterations = total;
+                local.steps = total;
+                local.converged = ok;
+                rc = ok ? LYM_OK : LYM_NOT_CONVERGED;
+            } else {
+                fail(c, LYM_ERR_UNSUPPORTED, "multishift algorithm %d", algorithm);
+            }
+        } catch (...) {
+            for (auto v : xs) delete v;
+            throw;
+        }
+        CK(cudaEventRecord(c->ev1, c->st));
+        for (int i = 0; i < nshift; ++i) download_vec(c, solutions[i], xv[i], device_ptr, 2), CK(cudaStreamSynchronize(c->st));
+        for (auto v : xs) delete v;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        local.seconds = ms * 1e-3;
+        if (stats) *stats = local;
+        CK(cudaGetLastError());
+        return rc;
+    });
+}
+
+int lym_multishift(lym_context *c, int op_id, int algorithm, int nshift, const double *shifts, double precision,
+                   int max_steps, const double *source, double **solutions, lym_solve_stats *stats)
+{
+    return do_multishift(c, op_id, algorithm, nshift, shifts, precision, max_steps, source, solutions, stats, false);
+}
+
+int lym_multishift_device(lym_context *c, int op_id, int algorithm, int nshift, const double *shifts, double precision,
+                          int max_steps, const double *source, double **solutions, lym_solve_stats *stats)
+{
+    return do_multishift(c, op_id, algorithm, nshift, shifts, precision, max_steps, source, solutions, stats, true);
+}
+
+int lym_neighbour_tables(lym_context *c, int *sup, int *sdn)
+{
+    if (!sup || !sdn) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        const size_t b = (size_t)c->g.V * 4 * sizeof(int);
+        int *d = (int *)dev_alloc(c, 2 * b);
+        launch_neighbour_tables(c->g, d, d + (size_t)c->g.V * 4, c->st);
+        CK(cudaMemcpyAsync(sup, d, b, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaMemcpyAsync(sdn, d + (size_t)c->g.V * 4, b, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        dev_free(c, d, 2 * b);
+        return LYM_OK;
+    });
+}
+
+int lym_stencil_indices(lym_context *c, int *out)
+{
+    if (!out) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        const size_t b = (size_t)c->g.V * 9 * sizeof(int);
+        int *d = (int *)dev_alloc(c, b);
+        launch_stencil_index_probe(c->g, d, c->st);
+        CK(cudaMemcpyAsync(out, d, b, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        dev_free(c, d, b);
+        return LYM_OK;
+    });
+}
+
+unsigned long long lym_context_kernel_launches(lym_context *c) { return c ? c->launches : 0ull; }
+
+int lym_time_stencil(lym_context *c, int op_id, int prec, int which, int iters, double *ms_per_launch)
+{
+    if (!ms_per_launch || iters < 1 || prec < PREC_D || prec > PREC_H || which < 0 || which > 1)
+        return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        OpEntry &op = op_of(c, op_id);
+        GaugeEntry &ge = gauge_of(c, op.gauge_id);
+        const bool clov = kind_has_clover(op.kind);
+        if (clov) ensure_clover(c, op);
+        require_recon(c, ge, prec);
+        Vec a(c, prec, 1), b(c, prec, 1), y(c, prec, 1);
+        DslashParams P;
+        P.g = c->g;
+        P.prec = prec;
+        P.rep = c->rep;
+        P.U = &ge.dev;
+        if (which == 0) {  // out_o = T_oo y_o - kappa^2 H_oe a_e  (second half of the Schur operator)
+            P.epi = EPI_XPAY_;
+            P.parity = 1;
+            P.clover = clov ? op.clover.T[prec] : nullptr;
+            P.b = -op.kappa * op.kappa;
+        } else {           // out_e = Tinv_ee H_eo a_o             (first half)
+            P.epi = clov ? EPI_CLOVINV_ : EPI_SCALE_;
+            P.parity = 0;
+            P.clover = clov ? op.clover.Tinv[prec] : nullptr;
+        }
+        P.in = *a;
+        P.out = *b;
+        P.y = *y;
+        P.v2 = *y;
+        for (int k = 0; k < 3; ++k) launch_dslash(P, c->st);
+        CK(cudaEventRecord(c->ev0, c->st));
+        for (int k = 0; k < iters; ++k) launch_dslash(P, c->st);
+        CK(cudaEventRecord(c->ev1, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        CK(cudaGetLastError());
+        count(c, iters + 3);
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        *ms_per_launch = (double)ms / iters;
+        return LYM_OK;
+    });
+}
+
+void *lym_host_alloc(size_t bytes)
+{
+    void *p = nullptr;
+    if (cudaHostAlloc(&p, bytes, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+void lym_host_free(void *p)
+{
+    if (p) cudaFreeHost(p);
+}
+
+}  // extern "C"

@@ -1,0 +1,82 @@
+// Host-side internal interfaces of the library (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "lym_common.cuh"
+
+namespace lym {
+
+enum Prec : int { PREC_D = 0, PREC_F = 1, PREC_H = 2 };
+enum Rep : int { REP_SU3 = 0, REP_SU2ADJ = 1 };
+
+// A device spinor: full lattice (nparity = 2) or one parity (nparity = 1).
+struct Spinor {
+    int prec = PREC_D;
+    int nparity = 0;
+    int stride = 0;
+    void *v = nullptr;
+    float *norm = nullptr;  // FP16 only
+    bool owned = false;
+
+    SpinorD d(int p = 0) const { return SpinorD{(double2 *)v, stride}.par(p); }
+    SpinorF f(int p = 0) const { return SpinorF{(float4 *)v, stride}.par(p); }
+    SpinorH h(int p = 0) const { return SpinorH{(int4 *)v, norm, stride}.par(p); }
+    size_t bytes_per_parity() const;
+    // view of one parity of a full spinor
+    Spinor parity(int p) const;
+};
+
+struct GaugeDev {
+    int rep = REP_SU3;
+    void *d64 = nullptr;       // FP64: double2[2][4][9][stride] (SU3) or double[2][4][9][stride] (adjoint)
+    void *f32 = nullptr;       // FP32 reconstructed: float4[2][4][3][stride] or float2[2][4][3][stride]
+    void *h16 = nullptr;       // FP16 reconstructed: uint2[2][4][3][stride] or half2[2][4][3][stride]
+    uint8_t *sign = nullptr;   // [2][stride]
+    bool recon_ok = false;
+};
+
+struct CloverDev {
+    void *T[3] = {nullptr, nullptr, nullptr};     // per precision, [2 parity][2 block][words][stride]
+    void *Tinv[3] = {nullptr, nullptr, nullptr};
+};
+
+enum Epi : int { EPI_SCALE_ = 0, EPI_CLOVINV_ = 1, EPI_XPAY_ = 2, EPI_XPAY_INV_ = 3 };
+
+struct DslashParams {
+    Geom g;
+    int prec = PREC_D;
+    int rep = REP_SU3;
+    int epi = EPI_SCALE_;
+    int parity = 0;          // output parity
+    Spinor in;               // view of the input parity (1 - parity)
+    Spinor out;              // view of the output parity
+    Spinor y;                // same-parity input (EPI_XPAY, EPI_XPAY_INV)
+    Spinor v2;               // optional added vector (EPI_XPAY)
+    int has_v2 = 0;
+    const GaugeDev *U = nullptr;
+    const void *clover = nullptr;  // T (EPI_XPAY) or Tinv (EPI_CLOVINV, EPI_XPAY_INV) of this precision
+    int gamma5 = 0;
+    double a = 1.0, b = 0.0, alpha_re = 0.0, alpha_im = 0.0;
+    const int *skip_if = nullptr;
+};
+
+// kernels (lym_kernels.cu)
+void launch_dslash(const DslashParams &P, cudaStream_t st);
+void launch_clover(const Geom &g, int prec, const Spinor &out, const Spinor &in, const void *clover, int parity,
+                   int gamma5, cudaStream_t st);
+void launch_pack(const Geom &g, const double *aos, const Spinor &full, cudaStream_t st);
+void launch_unpack(const Geom &g, const Spinor &full, double *aos, cudaStream_t st);
+void launch_upload_gauge(const Geom &g, int rep, const double *aos, GaugeDev &U, cudaStream_t st);
+void launch_compress_gauge(const Geom &g, GaugeDev &U, int *err, cudaStream_t st);
+void launch_fundamental_to_fermion(const Geom &g, int rep, int bc, const double *gauge_aos, double *fermion_aos,
+                                   cudaStream_t st);
+void launch_clover_build(const Geom &g, const GaugeDev &U, double kc, CloverDev &C, double *F_aos, int *err,
+                         cudaStream_t st);
+void launch_clover_compress(const Geom &g, CloverDev &C, cudaStream_t st);
+void launch_neighbour_tables(const Geom &g, int *sup, int *sdn, cudaStream_t st);
+void launch_stencil_index_probe(const Geom &g, int *out, cudaStream_t st);
+void launch_convert(const Geom &g, const Spinor &dst, const Spinor &src, cudaStream_t st);
+
+}  // namespace lym

@@ -1,0 +1,527 @@
+// Fused vector steps of the Krylov solvers.  Each functor is run by site_kernel
+// (lym_blas.cuh); finalize() runs once, in the last block, with the global sums
+// and advances the solver's FP64 scalar state held in device memory.
+#pragma once
+
+#include "lym_blas.cuh"
+
+namespace lym {
+
+// ------------------------------------------------------------------ state --
+struct CGState {
+    double rr;         // |r|^2 of the recursion
+    double rr_prev;    // |r|^2 before the last update (reliable-update beta)
+    double rr_max;     // max |r|^2 since the last reliable update
+    double eps;        // stop: rr < eps
+    double delta2;     // reliable update when rr < delta2 * rr_max (0: never)
+    double2 alpha;
+    double beta;
+    int iter;
+    int max_iter;
+    int pause;         // gates every captured kernel
+    int converged;
+    int need_update;
+    int failed;
+};
+
+struct BiCGState {
+    double2 rho;       // rho_{k-1}
+    double2 rho_next;
+    double2 alpha;
+    double2 omega;
+    double2 beta;
+    double norm;       // |r|^2
+    double precision;
+    double last_error;
+    int step;
+    int max_steps;
+    int pause;
+    int converged;
+    int breakdown;     // rho == 0 (BiConjugateGradient.cpp:381-384)
+    int degenerate;    // (t,t) == 0: solution = source (BiConjugateGradient.cpp:455-464)
+};
+
+// ------------------------------------------------------------ simple ops ---
+template <class SA, class SB> struct OpDot {  // sum conj(a) b -> out[0..1]
+    static constexpr int NRED = 2;
+    SA a;
+    SB b;
+    double *out;
+    LYM_D void site(int p, int h, double *acc) const
+    {
+        cx<double> x[12], y[12];
+        a.par(p).template load<double>(h, x);
+        b.par(p).template load<double>(h, y);
+        dotc(x, y, acc[0], acc[1]);
+    }
+    LYM_D void finalize(const double *t) const
+    {
+        out[0] = t[0];
+        out[1] = t[1];
+    }
+};
+
+template <class SA> struct OpNorm {
+    static constexpr int NRED = 1;
+    SA a;
+    double *out;
+    LYM_D void site(int p, int h, double *acc) const
+    {
+        cx<double> x[12];
+        a.par(p).template load<double>(h, x);
+        acc[0] += norm2(x);
+    }
+    LYM_D void finalize(const double *t) const { out[0] = t[0]; }
+};
+
+// y = a x + b y   (complex a, b from host constants)
+template <class SX, class SY> struct OpAxpby {
+    static constexpr int NRED = 0;
+    SX x;
+    SY y;
+    double2 a, b;
+    LYM_D void site(int p, int h, double *) const
+    {
+        cx<double> u[12], v[12];
+        x.par(p).template load<double>(h, u);
+        y.par(p).template load<double>(h, v);
+        const cx<double> A = {a.x, a.y}, B = {b.x, b.y};
+#pragma unroll
+        for (int k = 0; k < 12; ++k) v[k] = A * u[k] + B * v[k];
+        y.par(p).template store<double>(h, v);
+    }
+    LYM_D void finalize(const double *) const {}
+};
+
+// z = x - y,  out = |z|^2
+template <class SX, class SY, class SZ> struct OpSubNorm {
+    static constexpr int NRED = 1;
+    SX x;
+    SY y;
+    SZ z;
+    double *out;
+    LYM_D void site(int p, int h, double *acc) const
+    {
+        cx<double> u[12], v[12];
+        x.par(p).template load<double>(h, u);
+        y.par(p).template load<double>(h, v);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) u[k] = u[k] - v[k];
+        acc[0] += norm2(u);
+        z.par(p).template store<double>(h, u);
+    }
+    LYM_D void finalize(const double *t) const { out[0] = t[0]; }
+};
+
+// gamma5 in place on one view (lower spins negated)
+template <class SX> struct OpGamma5 {
+    static constexpr int NRED = 0;
+    SX x;
+    LYM_D void site(int p, int h, double *) const
+    {
+        cx<double> u[12];
+        x.par(p).template load<double>(h, u);
+#pragma unroll
+        for (int k = 6; k < 12; ++k) u[k] = -u[k];
+        x.par(p).template store<double>(h, u);
+    }
+    LYM_D void finalize(const double *) const {}
+};
+
+// ------------------------------------------------------------------- CG ----
+// alpha = rr / <p, Ap>  (ConjugateGradient.cpp:44-45)
+template <class SP, class SAp> struct OpCGAlpha {
+    static constexpr int NRED = 2;
+    SP p;
+    SAp ap;
+    CGState *s;
+    LYM_D void site(int q, int h, double *acc) const
+    {
+        cx<double> x[12], y[12];
+        p.par(q).template load<double>(h, x);
+        ap.par(q).template load<double>(h, y);
+        dotc(x, y, acc[0], acc[1]);
+    }
+    LYM_D void finalize(const double *t) const { s->alpha = cdiv(make_double2(s->rr, 0.0), make_double2(t[0], t[1])); }
+};
+
+// x += alpha p ; r -= alpha Ap ; rr_new = |r|^2 (ConjugateGradient.cpp:47-68)
+template <class SX, class SP, class SR, class SAp> struct OpCGUpdate {
+    static constexpr int NRED = 1;
+    SX x;
+    SP p;
+    SR r;
+    SAp ap;
+    CGState *s;
+    LYM_D void site(int q, int h, double *acc) const
+    {
+        const cx<double> al = {s->alpha.x, s->alpha.y};
+        cx<double> xv[12], pv[12], rv[12], av[12];
+        x.par(q).template load<double>(h, xv);
+        p.par(q).template load<double>(h, pv);
+        r.par(q).template load<double>(h, rv);
+        ap.par(q).template load<double>(h, av);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+            fma_c(xv[k], al, pv[k]);
+            rv[k] = rv[k] - al * av[k];
+        }
+        acc[0] += norm2(rv);
+        x.par(q).template store<double>(h, xv);
+        r.par(q).template store<double>(h, rv);
+    }
+    LYM_D void finalize(const double *t) const
+    {
+        const double rr_new = t[0];
+        s->iter += 1;
+        s->rr_prev = s->rr;
+        s->beta = rr_new / s->rr;
+        s->rr = rr_new;
+        if (rr_new > s->rr_max) s->rr_max = rr_new;
+        if (!(rr_new == rr_new)) {  // NaN
+            s->failed = 1;
+            s->pause = 1;
+        } else if (rr_new < s->eps) {
+            s->converged = 1;
+            s->need_update = 1;
+            s->pause = 1;
+        } else if (s->delta2 > 0.0 && rr_new < s->delta2 * s->rr_max) {
+            s->need_update = 1;
+            s->pause = 1;
+        } else if (s->iter >= s->max_iter) {
+            s->pause = 1;
+        }
+    }
+};
+
+// p = r + beta p
+template <class SP, class SR> struct OpCGDirection {
+    static constexpr int NRED = 0;
+    SP p;
+    SR r;
+    CGState *s;
+    LYM_D void site(int q, int h, double *) const
+    {
+        const double b = s->beta;
+        cx<double> pv[12], rv[12];
+        p.par(q).template load<double>(h, pv);
+        r.par(q).template load<double>(h, rv);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) pv[k] = rv[k] + b * pv[k];
+        p.par(q).template store<double>(h, pv);
+    }
+    LYM_D void finalize(const double *) const {}
+};
+
+// ------------------------------------------------------------- BiCGStab ----
+// rho_next = <rhat, r>; beta = (rho_next / rho)(alpha / omega)  (BiConjugateGradient.cpp:359-387)
+template <class SH, class SR> struct OpBiRho {
+    static constexpr int NRED = 2;
+    SH rhat;
+    SR r;
+    BiCGState *s;
+    LYM_D void site(int q, int h, double *acc) const
+    {
+        cx<double> a[12], b[12];
+        rhat.par(q).template load<double>(h, a);
+        r.par(q).template load<double>(h, b);
+        dotc(a, b, acc[0], acc[1]);
+    }
+    LYM_D void finalize(const double *t) const
+    {
+        const double2 rn = make_double2(t[0], t[1]);
+        s->rho_next = rn;
+        if (rn.x * rn.x + rn.y * rn.y == 0.0) {
+            s->breakdown = 1;
+            s->pause = 1;
+            return;
+        }
+        s->beta = cmul(cdiv(rn, s->rho), cdiv(s->alpha, s->omega));
+    }
+};
+
+// p = r + beta (p - omega nu)
+template <class SP, class SR, class SN> struct OpBiDirection {
+    static constexpr int NRED = 0;
+    SP p;
+    SR r;
+    SN nu;
+    BiCGState *s;
+    LYM_D void site(int q, int h, double *) const
+    {
+        const cx<double> be = {s->beta.x, s->beta.y}, om = {s->omega.x, s->omega.y};
+        cx<double> pv[12], rv[12], nv[12];
+        p.par(q).template load<double>(h, pv);
+        r.par(q).template load<double>(h, rv);
+        nu.par(q).template load<double>(h, nv);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) pv[k] = rv[k] + be * (pv[k] - om * nv[k]);
+        p.par(q).template store<double>(h, pv);
+    }
+    LYM_D void finalize(const double *) const {}
+};
+
+// alpha = rho_next / <rhat, nu>
+template <class SH, class SN> struct OpBiAlpha {
+    static constexpr int NRED = 2;
+    SH rhat;
+    SN nu;
+    BiCGState *s;
+    LYM_D void site(int q, int h, double *acc) const
+    {
+        cx<double> a[12], b[12];
+        rhat.par(q).template load<double>(h, a);
+        nu.par(q).template load<double>(h, b);
+        dotc(a, b, acc[0], acc[1]);
+    }
+    LYM_D void finalize(const double *t) const { s->alpha = cdiv(s->rho_next, make_double2(t[0], t[1])); }
+};
+
+// s = r - alpha nu
+template <class SS, class SR, class SN> struct OpBiS {
+    static constexpr int NRED = 0;
+    SS sv;
+    SR r;
+    SN nu;
+    BiCGState *s;
+    LYM_D void site(int q, int h, double *) const
+    {
+        const cx<double> al = {s->alpha.x, s->alpha.y};
+        cx<double> rv[12], nv[12];
+        r.par(q).template load<double>(h, rv);
+        nu.par(q).template load<double>(h, nv);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) rv[k] = rv[k] - al * nv[k];
+        sv.par(q).template store<double>(h, rv);
+    }
+    LYM_D void finalize(const double *) const {}
+};
+
+// omega = <t,s>/<t,t>
+template <class ST, class SS> struct OpBiOmega {
+    static constexpr int NRED = 4;
+    ST t;
+    SS sv;
+    BiCGState *s;
+    LYM_D void site(int q, int h, double *acc) const
+    {
+        cx<double> a[12], b[12];
+        t.par(q).template load<double>(h, a);
+        sv.par(q).template load<double>(h, b);
+        dotc(a, b, acc[0], acc[1]);
+        dotc(a, a, acc[2], acc[3]);
+    }
+    LYM_D void finalize(const double *t2) const
+    {
+        s->omega = cdiv(make_double2(t2[0], t2[1]), make_double2(t2[2], t2[3]));
+        if (t2[2] == 0.0) {
+            s->degenerate = 1;
+            s->converged = 1;
+            s->pause = 1;
+        }
+    }
+};
+
+// x += alpha p + omega s ; r = s - omega t ; norm = |r|^2 ; rho_next = <rhat, r> of the next step
+template <class SX, class SP, class SS, class ST, class SR, class SH> struct OpBiUpdate {
+    static constexpr int NRED = 3;
+    SX x;
+    SP p;
+    SS sv;
+    ST t;
+    SR r;
+    SH rhat;
+    BiCGState *s;
+    LYM_D void site(int q, int h, double *acc) const
+    {
+        const cx<double> al = {s->alpha.x, s->alpha.y}, om = {s->omega.x, s->omega.y};
+        cx<double> xv[12], pv[12], sv_[12], tv[12], hv[12];
+        x.par(q).template load<double>(h, xv);
+        p.par(q).template load<double>(h, pv);
+        sv.par(q).template load<double>(h, sv_);
+        t.par(q).template load<double>(h, tv);
+        rhat.par(q).template load<double>(h, hv);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+            xv[k] = xv[k] + (al * pv[k] + om * sv_[k]);
+            tv[k] = sv_[k] - om * tv[k];  // new residual
+        }
+        acc[0] += norm2(tv);
+        dotc(hv, tv, acc[1], acc[2]);
+        x.par(q).template store<double>(h, xv);
+        r.par(q).template store<double>(h, tv);
+    }
+    LYM_D void finalize(const double *t3) const
+    {
+        const double norm = t3[0];
+        s->norm = norm;
+        if (!(norm == norm)) {
+            s->breakdown = 1;
+            s->pause = 1;
+            return;
+        }
+        if (norm < s->precision) {
+            s->converged = 1;
+            s->pause = 1;
+            s->last_error = norm;
+            return;
+        }
+        s->rho = s->rho_next;
+        s->last_error = norm;
+        s->step += 1;
+        if (s->step >= s->max_steps) {
+            s->pause = 1;
+            return;
+        }
+        // next step's rho_next and beta (fused OpBiRho)
+        const double2 rn = make_double2(t3[1], t3[2]);
+        s->rho_next = rn;
+        if (rn.x * rn.x + rn.y * rn.y == 0.0) {
+            s->breakdown = 1;
+            s->pause = 1;
+            return;
+        }
+        s->beta = cmul(cdiv(rn, s->rho), cdiv(s->alpha, s->omega));
+    }
+};
+
+// ------------------------------------------------------ multishift CG ------
+constexpr int kMaxShifts = 32;
+
+struct MultishiftState {
+    int pause;                    // first word: gates every captured kernel
+    double sigma[kMaxShifts];     // shift relative to the base system: sigma_i - sigma_0
+    double zeta[kMaxShifts];      // zeta_k
+    double zeta_prev[kMaxShifts]; // zeta_{k-1}
+    double alpha_s[kMaxShifts];
+    double beta_s[kMaxShifts];
+    int active[kMaxShifts];
+    int nshift;
+    int base;                     // index of the base system (smallest shift)
+    double rr, rr_prev;
+    double alpha, alpha_prev, beta;
+    double eps;                   // per-shift stop: zeta_i^2 rr < eps
+    int iter, max_iter, converged, stop;
+};
+
+// base alpha = rr / <p, Ap>, then the shifted coefficients (Jegerlehner recursions)
+template <class SP, class SAp> struct OpMsAlpha {
+    static constexpr int NRED = 2;
+    SP p;
+    SAp ap;
+    MultishiftState *s;
+    LYM_D void site(int q, int h, double *acc) const
+    {
+        cx<double> x[12], y[12];
+        p.par(q).template load<double>(h, x);
+        ap.par(q).template load<double>(h, y);
+        dotc(x, y, acc[0], acc[1]);
+    }
+    // On entry s->alpha = alpha_{k-1}, s->beta = beta_k (p_k = r_k + beta_k p_{k-1}),
+    // zeta = zeta_k, zeta_prev = zeta_{k-1}.  For (A + sigma) with residuals
+    // r^sigma_k = zeta_k r_k the three-term recurrences give
+    //   zeta_{k+1} = zeta_k zeta_{k-1} a_{k-1} /
+    //                (zeta_{k-1} a_{k-1} (1 + sigma a_k) + a_k b_k (zeta_{k-1} - zeta_k))
+    //   a^sigma_k  = a_k zeta_{k+1} / zeta_k.
+    LYM_D void finalize(const double *t) const
+    {
+        const double a = s->rr / t[0];
+        const double am1 = s->alpha;
+        for (int i = 0; i < s->nshift; ++i) {
+            if (s->active[i] == 2) s->active[i] = 0;  // converged at the previous step
+            if (!s->active[i]) continue;
+            const double z = s->zeta[i], zp = s->zeta_prev[i];
+            const double den = zp * am1 * (1.0 + s->sigma[i] * a) + a * s->beta * (zp - z);
+            const double zn = (z * zp * am1) / den;
+            s->alpha_s[i] = a * zn / z;
+            s->zeta_prev[i] = z;
+            s->zeta[i] = zn;
+        }
+        s->alpha_prev = am1;
+        s->alpha = a;
+    }
+};
+
+// x_i += alpha_i p_i ; r -= alpha Ap ; rr_new
+template <class SR, class SAp> struct OpMsResidual {
+    static constexpr int NRED = 1;
+    SR r;
+    SAp ap;
+    MultishiftState *s;
+    LYM_D void site(int q, int h, double *acc) const
+    {
+        const double a = s->alpha;
+        cx<double> rv[12], av[12];
+        r.par(q).template load<double>(h, rv);
+        ap.par(q).template load<double>(h, av);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) rv[k] = rv[k] - a * av[k];
+        acc[0] += norm2(rv);
+        r.par(q).template store<double>(h, rv);
+    }
+    LYM_D void finalize(const double *t) const
+    {
+        const double rr_new = t[0];
+        s->iter += 1;
+        s->beta = rr_new / s->rr;
+        s->rr_prev = s->rr;
+        s->rr = rr_new;
+        int any = 0;
+        for (int i = 0; i < s->nshift; ++i) {
+            if (!s->active[i]) continue;
+            // residual of shift i after this step: zeta_{k+1} r_{k+1}
+            const double zr = s->zeta[i] * s->zeta[i] * rr_new;
+            s->beta_s[i] = s->beta * (s->zeta[i] / s->zeta_prev[i]) * (s->zeta[i] / s->zeta_prev[i]);
+            // converged: this step's x update still runs, then the shift is frozen.
+            // The base system (sigma 0, index base) keeps its direction p, which
+            // drives the recursion of all the others.
+            if (zr < s->eps && i != s->base) s->active[i] = 2;
+            else if (zr >= s->eps) any = 1;
+        }
+        // the x / p update of this step (OpMsUpdate) still runs; it turns stop into pause
+        if (!any) {
+            s->converged = 1;
+            s->stop = 1;
+        } else if (s->iter >= s->max_iter) {
+            s->stop = 1;
+        }
+    }
+};
+
+// per shift: x_i += alpha_i p_i ; p_i = zeta_i r + beta_i p_i  (one launch over all shifts)
+template <class SV> struct OpMsUpdate {
+    static constexpr int NRED = 1;  // no sum; finalize ends the step
+    SV *x;   // device array of nshift views
+    SV *ps;
+    SV r;
+    MultishiftState *s;
+    int nshift;
+    LYM_D void site(int q, int h, double *) const
+    {
+        cx<double> rv[12];
+        r.par(q).template load<double>(h, rv);
+        for (int i = 0; i < nshift; ++i) {
+            const int act = s->active[i];
+            if (!act) continue;
+            cx<double> xv[12], pv[12];
+            x[i].par(q).template load<double>(h, xv);
+            ps[i].par(q).template load<double>(h, pv);
+            const double ai = s->alpha_s[i];
+#pragma unroll
+            for (int k = 0; k < 12; ++k) fma_r(xv[k], ai, pv[k]);
+            x[i].par(q).template store<double>(h, xv);
+            if (act == 1) {
+                const double z = s->zeta[i], b = s->beta_s[i];
+#pragma unroll
+                for (int k = 0; k < 12; ++k) pv[k] = z * rv[k] + b * pv[k];
+                ps[i].par(q).template store<double>(h, pv);
+            }
+        }
+    }
+    LYM_D void finalize(const double *) const
+    {
+        if (s->stop) s->pause = 1;
+    }
+};
+
+}  // namespace lym

@@ -1,0 +1,231 @@
+"""ctypes bindings of the CPU oracle (liblym_oracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg as the checker.  The product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+KIND = {"DiracWilson": 0, "Improved": 1, "EvenOddImproved": 2,
+        "SquareDiracWilson": 3, "SquareImproved": 4, "SquareEvenOddImproved": 5}
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liblym_oracle.so")
+        if not os.path.exists(path):
+            build()
+        L = C.CDLL(path)
+        vp, ip, dp = C.c_void_p, C.POINTER(C.c_int), C.c_double
+        L.orc_geom_tables.argtypes = [ip, vp, vp, vp]
+        L.orc_op_init.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, vp, dp, dp, C.c_int]
+        L.orc_multiply.argtypes = [vp, vp, vp]
+        L.orc_multiply_add.argtypes = [vp, vp, vp, vp, dp, dp]
+        L.orc_cg.argtypes = [vp, vp, vp, vp, dp, C.c_int, ip]
+        L.orc_bicgstab.argtypes = [vp, vp, vp, vp, dp, C.c_int, ip, C.POINTER(C.c_double)]
+        L.orc_bicgstab_shifted.argtypes = [vp, vp, vp, dp, dp, vp, dp, C.c_int, ip, C.POINTER(C.c_double)]
+        L.orc_preconditioned_bicgstab.argtypes = [vp, vp, vp, vp, dp, C.c_int, ip]
+        L.orc_me_multishift.argtypes = [vp, vp, C.POINTER(C.c_void_p), C.POINTER(C.c_double), C.c_int, dp, C.c_int]
+        L.orc_mmmr_multishift.argtypes = [vp, vp, C.POINTER(C.c_void_p), C.POINTER(C.c_double), C.c_int, dp, C.c_int, ip]
+        L.orc_op_field_strength.argtypes = [vp]
+        L.orc_op_field_strength.restype = vp
+        L.orc_eo_multiply_even_odd.argtypes = [vp, vp, vp, C.c_int]
+        L.orc_eo_multiply_even_even_inverse.argtypes = [vp, vp]
+        L.orc_eo_multiply_odd_odd_minus_identity.argtypes = [vp, vp, vp, C.c_int]
+        L.orc_geom_init.argtypes = [vp, ip]
+        L.orc_geom_free.argtypes = [vp]
+        L.orc_op_free.argtypes = [vp]
+        L.orc_antiperiodic_bc.argtypes = [ip, vp, C.c_int, C.c_int]
+        L.orc_su2_to_adjoint.argtypes = [C.c_int, vp, vp]
+        _LIB = L
+    return _LIB
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _ints(v):
+    return (C.c_int * len(v))(*[int(x) for x in v])
+
+
+class _Geom(C.Structure):
+    _fields_ = [("dims", C.c_int * 4), ("V", C.c_int), ("sup", C.c_void_p),
+                ("sdn", C.c_void_p), ("coord", C.c_void_p)]
+
+
+class _Op(C.Structure):
+    _fields_ = [("g", C.c_void_p), ("nc", C.c_int), ("real_links", C.c_int), ("kind", C.c_int),
+                ("links", C.c_void_p), ("F", C.c_void_p), ("Tinv", C.c_void_p),
+                ("kappa", C.c_double), ("csw", C.c_double), ("gamma5", C.c_int)]
+
+
+def geom_tables(dims):
+    V = int(np.prod(dims))
+    sup = np.empty((V, 4), np.int32)
+    sdn = np.empty((V, 4), np.int32)
+    coord = np.empty((V, 4), np.int32)
+    lib().orc_geom_tables(_ints(dims), _ptr(sup), _ptr(sdn), _ptr(coord))
+    return sup, sdn, coord
+
+
+class Geometry:
+    def __init__(self, dims):
+        self.dims = tuple(int(d) for d in dims)
+        self._g = _Geom()
+        rc = lib().orc_geom_init(C.byref(self._g), _ints(self.dims))
+        if rc != 0:
+            raise RuntimeError(f"orc_geom_init failed: {rc}")
+        self.V = self._g.V
+
+    def __del__(self):
+        try:
+            lib().orc_geom_free(C.byref(self._g))
+        except Exception:
+            pass
+
+
+class Operator:
+    """Oracle operator of one kind over a fixed fermion-link field."""
+
+    def __init__(self, geom, links, kind, kappa, csw=0.0, gamma5=True):
+        self.geom = geom
+        self.links = np.ascontiguousarray(links)
+        self.real = not np.iscomplexobj(self.links)
+        self.nc = int(self.links.shape[-1])
+        self._op = _Op()
+        k = KIND[kind] if isinstance(kind, str) else int(kind)
+        rc = lib().orc_op_init(C.byref(self._op), C.byref(geom._g), self.nc, int(self.real), k,
+                               _ptr(self.links), float(kappa), float(csw), int(bool(gamma5)))
+        if rc != 0:
+            raise RuntimeError(f"orc_op_init failed: {rc}")
+
+    def __del__(self):
+        try:
+            lib().orc_op_free(C.byref(self._op))
+        except Exception:
+            pass
+
+    def _vec(self):
+        return np.zeros((self.geom.V, 4, self.nc), np.complex128)
+
+    def multiply(self, vin):
+        vin = np.ascontiguousarray(vin, dtype=np.complex128)
+        out = self._vec()
+        rc = lib().orc_multiply(C.byref(self._op), _ptr(out), _ptr(vin))
+        if rc != 0:
+            raise RuntimeError(f"orc_multiply failed: {rc}")
+        return out
+
+    def multiply_add(self, v1, v2, alpha):
+        v1 = np.ascontiguousarray(v1, dtype=np.complex128)
+        v2 = np.ascontiguousarray(v2, dtype=np.complex128)
+        out = self._vec()
+        a = complex(alpha)
+        rc = lib().orc_multiply_add(C.byref(self._op), _ptr(out), _ptr(v1), _ptr(v2), a.real, a.imag)
+        if rc != 0:
+            raise RuntimeError(f"orc_multiply_add failed: {rc}")
+        return out
+
+    def field_strength(self):
+        p = lib().orc_op_field_strength(C.byref(self._op))
+        n = self.geom.V * 6 * self.nc * self.nc
+        if self.real:
+            arr = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_double)), shape=(n,))
+            return arr.copy().reshape(self.geom.V, 6, self.nc, self.nc)
+        arr = np.ctypeslib.as_array(C.cast(p, C.POINTER(C.c_double)), shape=(2 * n,))
+        return arr.copy().view(np.complex128).reshape(self.geom.V, 6, self.nc, self.nc)
+
+    def even_odd(self, vin, part, out=None):
+        vin = np.ascontiguousarray(vin, dtype=np.complex128)
+        out = self._vec() if out is None else out
+        lib().orc_eo_multiply_even_odd(C.byref(self._op), _ptr(out), _ptr(vin), int(part))
+        return out
+
+    def even_even_inverse(self, v):
+        v = np.ascontiguousarray(v, dtype=np.complex128).copy()
+        lib().orc_eo_multiply_even_even_inverse(C.byref(self._op), _ptr(v))
+        return v
+
+    def odd_odd_minus_identity(self, out, vin, part):
+        out = np.ascontiguousarray(out, dtype=np.complex128).copy()
+        vin = np.ascontiguousarray(vin, dtype=np.complex128)
+        lib().orc_eo_multiply_odd_odd_minus_identity(C.byref(self._op), _ptr(out), _ptr(vin), int(part))
+        return out
+
+
+def cg(op, src, eps, max_steps=3000, guess=None):
+    src = np.ascontiguousarray(src, dtype=np.complex128)
+    sol = op._vec()
+    steps = C.c_int(0)
+    g = _ptr(np.ascontiguousarray(guess, dtype=np.complex128)) if guess is not None else None
+    rc = lib().orc_cg(C.byref(op._op), _ptr(src), _ptr(sol), g, float(eps), int(max_steps), C.byref(steps))
+    return rc, sol, steps.value
+
+
+def bicgstab(op, src, precision, max_steps=1000, guess=None, shift=None):
+    src = np.ascontiguousarray(src, dtype=np.complex128)
+    sol = op._vec()
+    steps = C.c_int(0)
+    last = C.c_double(0)
+    g = _ptr(np.ascontiguousarray(guess, dtype=np.complex128)) if guess is not None else None
+    if shift is None:
+        rc = lib().orc_bicgstab(C.byref(op._op), _ptr(src), _ptr(sol), g, float(precision), int(max_steps),
+                                C.byref(steps), C.byref(last))
+    else:
+        s = complex(shift)
+        rc = lib().orc_bicgstab_shifted(C.byref(op._op), _ptr(src), _ptr(sol), s.real, s.imag, g, float(precision),
+                                        int(max_steps), C.byref(steps), C.byref(last))
+    return rc, sol, steps.value
+
+
+def preconditioned_bicgstab(op, src, precision, max_steps=1000, guess=None):
+    src = np.ascontiguousarray(src, dtype=np.complex128)
+    sol = op._vec()
+    steps = C.c_int(0)
+    g = _ptr(np.ascontiguousarray(guess, dtype=np.complex128)) if guess is not None else None
+    rc = lib().orc_preconditioned_bicgstab(C.byref(op._op), _ptr(src), _ptr(sol), g, float(precision),
+                                           int(max_steps), C.byref(steps))
+    return rc, sol, steps.value
+
+
+def _multishift(fn, op, src, shifts, eps, max_steps, with_steps):
+    src = np.ascontiguousarray(src, dtype=np.complex128)
+    sols = [op._vec() for _ in shifts]
+    ptrs = (C.c_void_p * len(sols))(*[s.ctypes.data for s in sols])
+    sh = (C.c_double * len(shifts))(*[float(s) for s in shifts])
+    if with_steps:
+        steps = C.c_int(0)
+        rc = fn(C.byref(op._op), _ptr(src), ptrs, sh, len(shifts), float(eps), int(max_steps), C.byref(steps))
+        return rc, sols, steps.value
+    rc = fn(C.byref(op._op), _ptr(src), ptrs, sh, len(shifts), float(eps), int(max_steps))
+    return rc, sols, None
+
+
+def me_multishift(op, src, shifts, eps, max_steps=3000):
+    return _multishift(lib().orc_me_multishift, op, src, shifts, eps, max_steps, False)
+
+
+def mmmr_multishift(op, src, shifts, eps, max_steps=3000):
+    return _multishift(lib().orc_mmmr_multishift, op, src, shifts, eps, max_steps, True)
+
+
+def squared_norm(v):
+    return float(np.vdot(v, v).real)
+
+
+def dot(a, b):
+    return complex(np.vdot(a, b))

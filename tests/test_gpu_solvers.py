@@ -1,0 +1,161 @@
+"""GPU solvers through the C ABI against the oracle's restatement of the
+reference solvers.  Every solve's true residual ||b - A x|| / ||b|| is
+re-measured with the FP64 oracle operator."""
+import numpy as np
+import pytest
+
+import leonardym_b200 as L
+from leonardym_b200 import synth
+from tests.helpers import CONFIGS, links_for, rel
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", params=["su3", "su2adj"])
+def setup(request, oracle):
+    name = request.param
+    dims, rep, eps, kappa, csw = CONFIGS[name]
+    links = links_for(name)
+    lat = L.Lattice(dims, rep)
+    gid = lat.upload(links)
+    geom = oracle.Geometry(dims)
+    b = synth.gaussian_spinor(dims, 3, 21)
+    yield dict(dims=dims, rep=rep, kappa=kappa, csw=csw, links=links, lat=lat, gid=gid, geom=geom, b=b)
+    lat.close()
+
+
+def gpu_op(setup, cls, gamma5=True):
+    op = cls(setup["lat"], setup["kappa"])
+    if cls not in (L.DiracWilsonOperator, L.SquareDiracWilsonOperator):
+        op.setCSW(setup["csw"])
+    op.setGamma5(gamma5)
+    op.setLattice(setup["gid"])
+    return op
+
+
+def true_res(oracle_op, b, x, shift=None):
+    ax = oracle_op.multiply(x) if shift is None else oracle_op.multiply_add(x, x, shift)
+    return float(np.linalg.norm(b - ax) / np.linalg.norm(b))
+
+
+def test_cg_square_improved(setup, oracle):
+    # ConjugateGradient on D^+D (configs: CG on D^dagger D to 1e-10 relative)
+    b = setup["b"]
+    eps = (1e-10) ** 2 * float(np.vdot(b, b).real)
+    op = gpu_op(setup, L.SquareImprovedDiracWilsonOperator)
+    cg = L.ConjugateGradient()
+    cg.setPrecision(eps)
+    cg.setMaximumSteps(5000)
+    x = setup["lat"].new_vector()
+    assert cg.solve(op, b, x)
+    orc = oracle.Operator(setup["geom"], setup["links"], "SquareImproved", setup["kappa"], setup["csw"], True)
+    rc, xo, steps = oracle.cg(orc, b, eps, 5000)
+    assert rc == 1
+    assert abs(cg.getLastSteps() - steps) <= 2
+    assert true_res(orc, b, x) < 1.5e-10
+    assert rel(x, xo) < 1e-7
+
+
+def test_bicgstab_square_improved(setup, oracle):
+    b = setup["b"]
+    eps = (1e-10) ** 2 * float(np.vdot(b, b).real)
+    op = gpu_op(setup, L.SquareImprovedDiracWilsonOperator)
+    s = L.BiConjugateGradient()
+    s.setPrecision(eps)
+    s.setMaximumSteps(5000)
+    x = setup["lat"].new_vector()
+    assert s.solve(op, b, x)
+    orc = oracle.Operator(setup["geom"], setup["links"], "SquareImproved", setup["kappa"], setup["csw"], True)
+    rc, xo, steps = oracle.bicgstab(orc, b, eps, 5000)
+    assert rc == 1
+    assert abs(s.getLastSteps() - steps) <= 3
+    assert true_res(orc, b, x) < 1.5e-10
+    assert rel(x, xo) < 1e-7
+
+
+def test_bicgstab_shifted(setup, oracle):
+    b = setup["b"]
+    eps = (1e-10) ** 2 * float(np.vdot(b, b).real)
+    op = gpu_op(setup, L.SquareImprovedDiracWilsonOperator)
+    s = L.BiConjugateGradient()
+    s.setPrecision(eps)
+    s.setMaximumSteps(5000)
+    x = setup["lat"].new_vector()
+    assert s.solve(op, b, x, shift=0.05)
+    orc = oracle.Operator(setup["geom"], setup["links"], "SquareImproved", setup["kappa"], setup["csw"], True)
+    assert true_res(orc, b, x, 0.05) < 1.5e-10
+
+
+@pytest.mark.parametrize("gamma5", [False, True])
+def test_preconditioned_bicgstab(setup, gamma5, oracle):
+    b = setup["b"]
+    prec = (1e-10) ** 2 * float(np.vdot(b, b).real)
+    op = gpu_op(setup, L.ImprovedDiracWilsonOperator, gamma5)
+    s = L.PreconditionedBiCGStab()
+    s.setPrecision(prec)
+    s.setMaximumSteps(5000)
+    x = setup["lat"].new_vector()
+    assert s.solve(op, b, x)
+    orc = oracle.Operator(setup["geom"], setup["links"], "Improved", setup["kappa"], setup["csw"], gamma5)
+    rc, xo, steps = oracle.preconditioned_bicgstab(orc, b, prec, 5000)
+    assert rc == 1
+    assert abs(s.getLastSteps() - steps) <= 3
+    # the even-odd path solves D x = b (gamma5 = false operator) whatever the flag
+    D = oracle.Operator(setup["geom"], setup["links"], "Improved", setup["kappa"], setup["csw"], False)
+    assert true_res(D, b, x) < 1e-8
+    assert rel(x, xo) < 1e-7
+
+
+@pytest.mark.parametrize("mode", ["double", "single", "half"])
+def test_even_odd_cg_true_residual(setup, mode, oracle):
+    b = setup["b"]
+    op = gpu_op(setup, L.ImprovedDiracWilsonOperator, False)
+    s = L.EvenOddConjugateGradient(mode, 1e-10)
+    x = setup["lat"].new_vector()
+    assert s.solve(op, b, x)
+    D = oracle.Operator(setup["geom"], setup["links"], "Improved", setup["kappa"], setup["csw"], False)
+    r = true_res(D, b, x)
+    assert r <= 1e-10
+    assert s.stats.true_residual <= 1e-10
+    assert abs(s.stats.true_residual - r) < 1e-11
+
+
+def test_even_odd_cg_wilson(setup, oracle):
+    b = setup["b"]
+    op = gpu_op(setup, L.DiracWilsonOperator, False)
+    s = L.EvenOddConjugateGradient("single", 1e-10)
+    x = setup["lat"].new_vector()
+    assert s.solve(op, b, x)
+    D = oracle.Operator(setup["geom"], setup["links"], "DiracWilson", setup["kappa"], 0.0, False)
+    assert true_res(D, b, x) <= 1e-10
+
+
+def test_multishift_mass_estrapolation(setup, oracle):
+    b = setup["b"]
+    shifts = [0.5, 0.1, 0.01]
+    eps = (1e-10) ** 2 * float(np.vdot(b, b).real)
+    op = gpu_op(setup, L.SquareImprovedDiracWilsonOperator)
+    ms = L.MultishiftSolver.getInstance("mass_estrapolation")
+    ms.setPrecision(eps)
+    sols = []
+    assert ms.solve(op, b, sols, shifts)
+    orc = oracle.Operator(setup["geom"], setup["links"], "SquareImproved", setup["kappa"], setup["csw"], True)
+    rc, osols, _ = oracle.me_multishift(orc, b, shifts, eps)
+    for x, xo, s in zip(sols, osols, shifts):
+        assert true_res(orc, b, x, s) < 1.5e-10
+        assert rel(x, xo) < 1e-7
+
+
+def test_multishift_cg(setup, oracle):
+    b = setup["b"]
+    shifts = list(np.logspace(-4, 0, 12))
+    eps = (1e-10) ** 2 * float(np.vdot(b, b).real)
+    op = gpu_op(setup, L.SquareImprovedDiracWilsonOperator)
+    ms = L.MultishiftSolver.getInstance("multishift_cg")
+    ms.setPrecision(eps)
+    ms.setMaxSteps(10000)
+    sols = []
+    assert ms.solve(op, b, sols, shifts)
+    orc = oracle.Operator(setup["geom"], setup["links"], "SquareImproved", setup["kappa"], setup["csw"], True)
+    for x, s in zip(sols, shifts):
+        assert true_res(orc, b, x, s) < 3e-10
