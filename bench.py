@@ -1,0 +1,445 @@
+"""Benchmark: Wilson-clover propagator solves on one B200 (N GPUs = N replicas).
+
+Workload (the configuration the headline metric is quoted on): SU(3) fundamental
+Wilson-clover operator on a 24^3 x 48 lattice, kappa = 0.137, c_sw = 1.7, seeded
+near-unit links U = exp(i 0.25 H), antiperiodic in time; 44 right-hand sides
+(12 spin-colour point sources at the origin + 32 Z2 x Z2 noise sources).  One
+step solves all 44 systems D x = b to a true residual ||b - D x|| / ||b|| <= 1e-10
+with the even-odd mixed-precision CG (FP32 stencil, FP64 reliable updates,
+re-measured with the FP64 operator).
+
+Prints one JSON line (rank 0).  --impl reference times the reference algorithm on
+the host cores instead (see cpu_reference()).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DIMS = (24, 24, 24, 48)
+KAPPA, CSW, EPS, SEED = 0.137, 1.7, 0.25, 1237
+N_POINT, N_NOISE = 12, 32
+TOL = 1e-10
+METRIC = "solves/s @24^3x48 to res 1e-10 (mixed vs FP64); dslash HBM GB/s; p50/p99 ms"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "which": "fallback"}
+# algorithmic bytes per output half-site of the Schur stencil kernel that carries the
+# clover term (out_o = T_oo y_o - kappa^2 H_oe a_e): 8 links (+ 2 sign-table bytes for the
+# reconstructed formats), 1 neighbour spinor (each read once), the y spinor, T_oo, the output
+STENCIL_BYTES = {0: 8 * 144 + 3 * 192 + 576, 1: 8 * 48 + 2 + 3 * 96 + 288, 2: 8 * 24 + 2 + 3 * 52 + 144}
+STENCIL_FLOPS = 1320 + 504 + 48  # hopping + clover apply + xpay, per site
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": float(d["hbm_gbs"]), "which": "measured"}
+    return PEAKS_FALLBACK
+
+
+_LINKS = None
+
+
+def workload_links():
+    global _LINKS
+    if _LINKS is None:
+        from leonardym_b200 import synth
+        _LINKS = synth.fermion_links(DIMS, "su3", EPS, SEED)
+    return _LINKS
+
+
+def workload_sources(nc=3):
+    from leonardym_b200 import synth
+    srcs = []
+    for alpha in range(4):
+        for c in range(nc):
+            srcs.append(synth.point_source(DIMS, nc, alpha, c))
+    for k in range(N_NOISE):
+        srcs.append(synth.z2_source(DIMS, nc, SEED, stream=(1 << 21) + k))
+    return srcs
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"lym_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9 or parts[0] != str(self.index):
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def traffic_from_profiles(prec):
+    """DRAM bytes per launch of the stencil kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "stencil_schur_clover_24c48.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(rf"traffic_bytes_per_launch\[prec={prec}\]:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+def cpu_reference(sample_iters=(4, 8), threads=None):
+    """The reference's FP64 even-odd BiCGStab (PreconditionedBiCGStab.cpp:33-100) on the
+    host cores, on the benchmark's lattice and first source.  A bounded sample: the
+    solver runs twice with max_steps = 4 and 8; the difference gives the time per
+    iteration, the first run the set-up (field strength + 12x12 inverses).  Solves/s =
+    1 / (setup + iterations_to_converge x time_per_iteration), where the iteration count
+    is the reference algorithm's own (measured by its GPU mirror on the same system,
+    or by the oracle when no GPU is present)."""
+    import oracle as O
+    from leonardym_b200 import synth
+    kind = "reference" if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libleonard_ref.so")) else "port"
+    links = workload_links()
+    b = workload_sources()[N_POINT]
+    geom = O.Geometry(DIMS)
+    D = O.Operator(geom, links, "Improved", KAPPA, CSW, False)
+    prec = (TOL ** 2) * float(np.vdot(b, b).real)
+    ts = []
+    for n in sample_iters:
+        t0 = time.perf_counter()
+        O.preconditioned_bicgstab(D, b, prec, n)
+        ts.append(time.perf_counter() - t0)
+    t_iter = (ts[1] - ts[0]) / (sample_iters[1] - sample_iters[0])
+    setup = max(ts[0] - sample_iters[0] * t_iter, 0.0)
+    return {"t_iter": t_iter, "setup": setup, "kind": kind, "sample_seconds": sum(ts),
+            "cores": int(threads or os.environ.get("OMP_NUM_THREADS", os.cpu_count()))}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, x):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    steps = []
+    info = None
+    # solve iteration count of the reference algorithm on this system: the GPU mirror of
+    # PreconditionedBiCGStab when a GPU is present
+    n_iter = gpu_eo_bicgstab_iterations()
+    for s in range(args.warmup + args.steps):
+        info = cpu_reference()
+        per_solve = info["setup"] + n_iter * info["t_iter"]
+        if s >= args.warmup:
+            steps.append(per_solve)
+    per_solve = statistics.median(steps)
+    value = 1.0 / per_solve
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_solve * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)", "config": config_dict("reference-fp64-eo-bicgstab"),
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": info["cores"], "kind": info["kind"],
+                         "sample": (f"per step: the reference's FP64 even-odd BiCGStab run for 4 and 8 iterations on "
+                                    f"the 24^3x48 system (set-up {info['setup']:.2f} s, {info['t_iter']:.3f} s/iteration), "
+                                    f"extrapolated to its {n_iter} iterations to converge")},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def gpu_eo_bicgstab_iterations():
+    try:
+        import leonardym_b200 as L
+        links = workload_links()
+        lat = L.Lattice(DIMS, "su3", device=0)
+        op = L.ImprovedDiracWilsonOperator(lat, KAPPA, CSW, gamma5=False)
+        op.setLattice(links)
+        b = workload_sources()[N_POINT]
+        s = L.PreconditionedBiCGStab()
+        s.setPrecision((TOL ** 2) * float(np.vdot(b, b).real))
+        s.setMaximumSteps(5000)
+        x = lat.new_vector()
+        s.solve(op, b, x)
+        n = s.stats.iterations
+        lat.close()
+        return n
+    except Exception:
+        import oracle as O
+        links = workload_links()
+        b = workload_sources()[N_POINT]
+        D = O.Operator(O.Geometry(DIMS), links, "Improved", KAPPA, CSW, False)
+        _, _, n = O.preconditioned_bicgstab(D, b, (TOL ** 2) * float(np.vdot(b, b).real), 5000)
+        return n
+
+
+def config_dict(solver):
+    return {"workload": "su3-clover-24^3x48-kappa0.137-csw1.7-44rhs-tol1e-10", "lattice": "24x24x24x48",
+            "representation": "SU(3) fundamental", "kappa": KAPPA, "csw": CSW, "links": "exp(i 0.25 H), seeded",
+            "rhs": N_POINT + N_NOISE, "sources": "12 point + 32 Z2xZ2", "solver": solver, "tolerance": TOL,
+            "l2": "inputs larger than L2: FP64 links 382 MB + FP32 links 127 MB + clover resident",
+            "parallelism": "replicas (one independent solve stream per GPU)"}
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    import leonardym_b200 as L
+    from leonardym_b200 import synth
+    from leonardym_b200.solvers import SOLVER_EO_CG, SOLVER_EO_CG_MIXED_HALF, SOLVER_EO_CG_MIXED_SINGLE
+
+    lib = L.lib()
+    torch.cuda.set_device(local)
+    solver = {"single": SOLVER_EO_CG_MIXED_SINGLE, "half": SOLVER_EO_CG_MIXED_HALF}[args.precision]
+    sprec = 1 if args.precision == "single" else 2
+    links = workload_links()
+    srcs = workload_sources()
+    nrhs = len(srcs)
+    lat = L.Lattice(DIMS, "su3", device=local)
+    op = L.ImprovedDiracWilsonOperator(lat, KAPPA, CSW, gamma5=False)
+    op.setLattice(links)
+    ctx, opid = lat.handle, op.op_id
+    V = lat.V
+    dev_src = torch.from_numpy(np.stack(srcs).view(np.float64).reshape(nrhs, V * 24)).to(f"cuda:{local}")
+    dev_sol = torch.zeros_like(dev_src)
+    stats = L.SolveStats()
+
+    def solve_all(record=None):
+        for k in range(nrhs):
+            rc = lib.lym_solve_device(ctx, opid, solver, -TOL, 20000, C.c_void_p(dev_src[k].data_ptr()),
+                                      C.c_void_p(dev_sol[k].data_ptr()), None, C.byref(stats))
+            if rc != 0:
+                raise RuntimeError(f"solve {k} failed: {rc} {lib.lym_last_error(ctx)}")
+            if stats.true_residual > TOL:
+                raise RuntimeError(f"solve {k}: true residual {stats.true_residual:.3e} > {TOL}")
+            if record is not None:
+                record.append((stats.seconds, stats.iterations, stats.true_residual))
+
+    for _ in range(args.warmup):
+        solve_all()
+    sampler = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    lib.lym_synchronize(ctx)
+    launches0 = lib.lym_context_kernel_launches(ctx)
+    sampler.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    rec = []
+    for _ in range(args.steps):
+        solve_all(rec)
+    lib.lym_synchronize(ctx)
+    ev1.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = int(lib.lym_context_kernel_launches(ctx) - launches0)
+    elapsed = max_over_ranks(world, ev0.elapsed_time(ev1) / 1e3)
+    barrier(world)
+    value = world * nrhs * args.steps / elapsed
+    lat_ms = sorted(r[0] * 1e3 for r in rec)
+    iters = [r[1] for r in rec]
+
+    # end to end through the host-buffer API, pinned host memory, copies inside the region
+    nbytes = V * 24 * 8
+    hsrc = [lib.lym_host_alloc(nbytes) for _ in range(nrhs)]
+    hsol = [lib.lym_host_alloc(nbytes) for _ in range(nrhs)]
+    for k in range(nrhs):
+        C.memmove(hsrc[k], srcs[k].ctypes.data, nbytes)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        for k in range(nrhs):
+            rc = lib.lym_solve(ctx, opid, solver, -TOL, 20000, C.c_void_p(hsrc[k]), C.c_void_p(hsol[k]), None,
+                               C.byref(stats))
+            if rc != 0 or stats.true_residual > TOL:
+                raise RuntimeError(f"e2e solve {k} failed: rc {rc}, residual {stats.true_residual}")
+    lib.lym_synchronize(ctx)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_elapsed = max_over_ranks(world, e0.elapsed_time(e1) / 1e3)
+    for p in hsrc + hsol:
+        lib.lym_host_free(p)
+    e2e_value = world * nrhs * args.steps / e2e_elapsed
+
+    # plain FP64 single-RHS even-odd CG on the same systems (the comparison of the metric)
+    t64 = []
+    for k in (0, N_POINT):
+        rc = lib.lym_solve_device(ctx, opid, SOLVER_EO_CG, -TOL, 20000, C.c_void_p(dev_src[k].data_ptr()),
+                                  C.c_void_p(dev_sol[k].data_ptr()), None, C.byref(stats))
+        t64.append(stats.seconds)
+    fp64_value = world / statistics.mean(t64)
+
+    # stencil roofline: CUDA events around launches of the dominant kernel on the library stream
+    ms = C.c_double(0)
+    lib.lym_time_stencil(ctx, opid, sprec, 0, 50, C.byref(ms))
+    Vh = V // 2
+    bytes_launch = STENCIL_BYTES[sprec] * Vh
+    achieved = bytes_launch / (ms.value * 1e-3) / 1e9
+    pk = peaks()
+    traffic = traffic_from_profiles(sprec)
+    ms64 = C.c_double(0)
+    lib.lym_time_stencil(ctx, opid, 0, 0, 20, C.byref(ms64))
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        n_iter = None
+        s = L.PreconditionedBiCGStab()
+        b = srcs[N_POINT]
+        s.setPrecision((TOL ** 2) * float(np.vdot(b, b).real))
+        s.setMaximumSteps(5000)
+        x = lat.new_vector()
+        s.solve(op, b, x)
+        n_iter = s.stats.iterations
+        info = cpu_reference()
+        per_solve = info["setup"] + n_iter * info["t_iter"]
+        cpu = {"value": 1.0 / per_solve, "unit": "solves/s", "cores": info["cores"], "kind": info["kind"],
+               "sample": (f"the reference's FP64 even-odd BiCGStab on this lattice and source run for 4 and 8 "
+                          f"iterations (set-up {info['setup']:.2f} s, {info['t_iter']:.3f} s/iteration, "
+                          f"{info['sample_seconds']:.1f} s of CPU work), extrapolated to the {n_iter} iterations "
+                          f"its GPU mirror needs on the same system")}
+    lat.close()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if sprec == 1 else "f16",
+        "data": "synthetic (seeded links and sources)",
+        "config": config_dict(f"even-odd CG, {args.precision} stencil + FP64 reliable updates"),
+        "fp64_eo_cg_solves_per_s": fp64_value,
+        "mixed_over_fp64": value / world / (fp64_value / world),
+        "latency_ms": {"p50": lat_ms[len(lat_ms) // 2], "p99": lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))]},
+        "iterations": {"median": statistics.median(iters), "max": max(iters)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
+                     "kernel": f"Schur stencil with clover (prec {args.precision}), {ms.value * 1e3:.1f} us/launch",
+                     "algorithmic_bytes_per_launch": bytes_launch,
+                     "peak_source": f"{pk['which']} hbm_gbs",
+                     "fp64_kernel_gbs": STENCIL_BYTES[0] * Vh / (ms64.value * 1e-3) / 1e9,
+                     "gflops": STENCIL_FLOPS * Vh / (ms.value * 1e-3) / 1e9},
+        "clocks": clocks,
+        "gpu_launches": launches,
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": nrhs * nbytes,
+                "d2h_bytes_per_step": nrhs * nbytes},
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_profile(args):
+    """Small fixed case for ncu captures: one mixed-precision solve of the benchmark's
+    first noise source and 10 launches of the stencil kernel (about 1 GB on the device)."""
+    import leonardym_b200 as L
+    from leonardym_b200.solvers import SOLVER_EO_CG_MIXED_HALF, SOLVER_EO_CG_MIXED_SINGLE
+    lib = L.lib()
+    lat = L.Lattice(DIMS, "su3", device=0)
+    op = L.ImprovedDiracWilsonOperator(lat, KAPPA, CSW, gamma5=False)
+    op.setLattice(workload_links())
+    b = workload_sources()[N_POINT]
+    x = lat.new_vector()
+    solver = {"single": SOLVER_EO_CG_MIXED_SINGLE, "half": SOLVER_EO_CG_MIXED_HALF}[args.precision]
+    st = L.SolveStats()
+    rc = lib.lym_solve(lat.handle, op.op_id, solver, -TOL, 20000, b.ctypes.data_as(C.c_void_p),
+                       x.ctypes.data_as(C.c_void_p), None, C.byref(st))
+    ms = C.c_double(0)
+    lib.lym_time_stencil(lat.handle, op.op_id, 1 if args.precision == "single" else 2, 0, 10, C.byref(ms))
+    print(f"profile case: rc {rc}, iterations {st.iterations}, true residual {st.true_residual:.2e}, "
+          f"stencil {ms.value * 1e3:.1f} us")
+    lat.close()
+    if rc != 0:
+        sys.exit(1)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="single", choices=["single", "half"])
+    ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--profile", action="store_true", help="small fixed case for ncu captures")
+    args = ap.parse_args()
+    if args.profile:
+        run_profile(args)
+        return
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

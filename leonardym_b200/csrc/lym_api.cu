@@ -261,6 +261,7 @@ void free_clover(lym_context *c, OpEntry &op)
 void ensure_clover(lym_context *c, OpEntry &op, double *F_out = nullptr)
 {
     if (op.clover_ok && !F_out) return;
+    if (c->capturing) fail(c, LYM_ERR_ARGUMENT, "clover term must be built before graph capture");
     GaugeEntry &ge = gauge_of(c, op.gauge_id);
     for (int p = 0; p < 3; ++p) {
         if (!op.clover.T[p]) op.clover.T[p] = dev_alloc(c, clover_bytes(c->g, p));
@@ -844,6 +845,8 @@ int multishift_cg(lym_context *c, OpEntry &op, int nshift, const double *shifts,
     CK(cudaMemcpyAsync(dviews, hx.data(), nshift * sizeof(SpinorD), cudaMemcpyHostToDevice, c->st));
     CK(cudaMemcpyAsync(dviews + kMaxShifts, hp.data(), nshift * sizeof(SpinorD), cudaMemcpyHostToDevice, c->st));
     const double bb = norm2_now(c, b);
+    // build the clover term and pool the operator's temporaries before graph capture
+    op_apply(c, op, PREC_D, *ap, b, &b, C2(s0));
     MultishiftState &H = *(MultishiftState *)c->h_state;
     memset(&H, 0, sizeof(H));
     H.nshift = nshift;
@@ -882,6 +885,72 @@ int multishift_cg(lym_context *c, OpEntry &op, int nshift, const double *shifts,
     }
     for (auto v : ps) delete v;
     dev_free(c, dviews, 2 * kMaxShifts * sizeof(SpinorD));
+    return rc;
+}
+
+// MMMRMultishiftSolver::solve (inverters/MMMRMultishiftSolver.cpp:42-198): negative
+// shifts by separate CG, the rest by one minimal-residual Krylov space on the last shift.
+int multishift_mmmr(lym_context *c, OpEntry &op, int nshift, const double *shifts, double eps, int max_steps,
+                    const Spinor &b, std::vector<Spinor> &xs, lym_solve_stats *st)
+{
+    if (nshift < 1 || nshift > kMaxShifts) fail(c, LYM_ERR_ARGUMENT, "multishift: 1..%d shifts", kMaxShifts);
+    int first = 0, total = 0;
+    bool flag = true;
+    while (first < nshift && shifts[first] < 0) {
+        const double sh = shifts[first];
+        auto mv = [&](const Spinor &out, const Spinor &in, const int *skip) {
+            op_apply(c, op, PREC_D, out, in, &in, C2(sh), skip);
+        };
+        Vec z(c, PREC_D, 2);
+        zero(c, *z);
+        lym_solve_stats s1;
+        memset(&s1, 0, sizeof(s1));
+        flag = cg_solve(c, mv, 2, b, xs[first], &*z, eps, max_steps, &s1) == LYM_OK && flag;
+        total += s1.iterations;
+        ++first;
+    }
+    int rc = flag ? LYM_OK : LYM_NOT_CONVERGED;
+    if (first < nshift) {
+        const double last = shifts[nshift - 1];
+        Vec r(c, PREC_D, 2), p(c, PREC_D, 2);
+        for (int i = first; i < nshift; ++i) zero(c, xs[i]);
+        copy(c, *r, b);
+        std::vector<SpinorD> hx(nshift);
+        for (int i = 0; i < nshift; ++i) hx[i] = xs[i].d();
+        SpinorD *dviews = (SpinorD *)dev_alloc(c, kMaxShifts * sizeof(SpinorD));
+        CK(cudaMemcpyAsync(dviews, hx.data(), nshift * sizeof(SpinorD), cudaMemcpyHostToDevice, c->st));
+        op_apply(c, op, PREC_D, *p, *r, &*r, C2(last));  // clover and pooled temporaries before capture
+        MMMRState &H = *(MMMRState *)c->h_state;
+        memset(&H, 0, sizeof(H));
+        H.nshift = nshift;
+        H.first = first;
+        H.max_iter = max_steps;
+        H.omega = 0.95;
+        H.eps = eps;
+        for (int i = 0; i < nshift; ++i) {
+            H.sigma[i] = shifts[i] - last;
+            H.f[i] = C2(1.0);
+        }
+        CK(cudaMemcpyAsync(c->d_state, c->h_state, sizeof(MMMRState), cudaMemcpyHostToDevice, c->st));
+        MMMRState *S = (MMMRState *)c->d_state;
+        Gate gate{&S->pause, nullptr};
+        auto step = [&]() {
+            op_apply(c, op, PREC_D, *p, *r, &*r, C2(last), &S->pause);
+            run_site(c, OpMMMRAlpha<SpinorD, SpinorD>{(*p).d(), (*r).d(), S}, 2, gate);
+            run_site(c, OpMMMRUpdate<SpinorD>{dviews, (*r).d(), (*p).d(), S}, 2, gate);
+        };
+        if (max_steps > 0) run_gated_state(c, S, step, 4, max_steps);
+        MMMRState &R = *(MMMRState *)c->h_state;
+        total += R.iter;
+        if (!R.converged) rc = LYM_NOT_CONVERGED;
+        if (st) st->last_error = R.rr;
+        dev_free(c, dviews, kMaxShifts * sizeof(SpinorD));
+    }
+    if (st) {
+        st->iterations = total;
+        st->steps = total;
+        st->converged = rc == LYM_OK;
+    }
     return rc;
 }
 
@@ -1367,6 +1436,8 @@ static int do_multishift(lym_context *c, int op_id, int algorithm, int nshift, c
                 local.steps = total;
                 local.converged = ok;
                 rc = ok ? LYM_OK : LYM_NOT_CONVERGED;
+            } else if (algorithm == LYM_MULTISHIFT_MMMR) {
+                rc = multishift_mmmr(c, op, nshift, shifts, precision, max_steps, *b, xv, &local);
             } else {
                 fail(c, LYM_ERR_UNSUPPORTED, "multishift algorithm %d", algorithm);
             }

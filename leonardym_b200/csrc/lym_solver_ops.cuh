@@ -524,4 +524,84 @@ template <class SV> struct OpMsUpdate {
     }
 };
 
+// --------------------------------------------- multishift minimal residual --
+// MMMRMultishiftSolver::solve, non-ALIGNED_OPT branch (inverters/MMMRMultishiftSolver.cpp:123-198)
+struct MMMRState {
+    int pause;
+    int nshift, first, iter, max_iter, converged;
+    double sigma[kMaxShifts];   // shifts[i] - shifts.back()
+    double2 f[kMaxShifts];
+    double2 coef[kMaxShifts];   // x_i += coef_i r
+    double2 alpha;
+    double omega;               // over-relaxation 0.95 (MMMRMultishiftSolver.cpp:37)
+    double eps;
+    double rr;
+};
+
+// alpha = omega <p,r>/<p,p>; f_i = f_i / (1 + (s_i - s_last) alpha)
+template <class SP, class SR> struct OpMMMRAlpha {
+    static constexpr int NRED = 4;
+    SP p;
+    SR r;
+    MMMRState *s;
+    LYM_D void site(int q, int h, double *acc) const
+    {
+        cx<double> a[12], b[12];
+        p.par(q).template load<double>(h, a);
+        r.par(q).template load<double>(h, b);
+        dotc(a, b, acc[0], acc[1]);
+        dotc(a, a, acc[2], acc[3]);
+    }
+    LYM_D void finalize(const double *t) const
+    {
+        const double2 al = cscale(s->omega, cdiv(make_double2(t[0], t[1]), make_double2(t[2], t[3])));
+        s->alpha = al;
+        const int last = s->nshift - 1;
+        s->coef[last] = al;
+        for (int i = s->first; i < last; ++i) {
+            s->f[i] = cdiv(s->f[i], cadd(make_double2(1.0, 0.0), cscale(s->sigma[i], al)));
+            s->coef[i] = cmul(s->f[i], al);
+        }
+    }
+};
+
+// x_i += coef_i r (i >= first) ; r -= alpha p ; error = |r|^2
+template <class SV> struct OpMMMRUpdate {
+    static constexpr int NRED = 1;
+    SV *x;
+    SV r;
+    SV p;
+    MMMRState *s;
+    LYM_D void site(int q, int h, double *acc) const
+    {
+        cx<double> rv[12], pv[12];
+        r.par(q).template load<double>(h, rv);
+        p.par(q).template load<double>(h, pv);
+        for (int i = s->first; i < s->nshift; ++i) {
+            cx<double> xv[12];
+            x[i].par(q).template load<double>(h, xv);
+            const cx<double> cf = {s->coef[i].x, s->coef[i].y};
+#pragma unroll
+            for (int k = 0; k < 12; ++k) fma_c(xv[k], cf, rv[k]);
+            x[i].par(q).template store<double>(h, xv);
+        }
+        const cx<double> al = {s->alpha.x, s->alpha.y};
+#pragma unroll
+        for (int k = 0; k < 12; ++k) rv[k] = rv[k] - al * pv[k];
+        acc[0] += norm2(rv);
+        r.par(q).template store<double>(h, rv);
+    }
+    LYM_D void finalize(const double *t) const
+    {
+        s->rr = t[0];
+        s->iter += 1;
+        if (t[0] < s->eps) {
+            s->converged = 1;
+            s->pause = 1;
+        } else if (s->iter >= s->max_iter || !(t[0] == t[0])) {
+            s->pause = 1;
+        }
+    }
+};
+
 }  // namespace lym

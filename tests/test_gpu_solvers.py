@@ -159,3 +159,22 @@ def test_multishift_cg(setup, oracle):
     orc = oracle.Operator(setup["geom"], setup["links"], "SquareImproved", setup["kappa"], setup["csw"], True)
     for x, s in zip(sols, shifts):
         assert true_res(orc, b, x, s) < 3e-10
+
+
+def test_multishift_minimal_residual(setup, oracle):
+    # MMMRMultishiftSolver: base system = last shift; negative shifts by separate CG
+    b = setup["b"]
+    shifts = [-0.001, 0.5, 0.1, 0.02]
+    eps = (1e-10) ** 2 * float(np.vdot(b, b).real)
+    op = gpu_op(setup, L.SquareImprovedDiracWilsonOperator)
+    ms = L.MultishiftSolver.getInstance("minimal_residual")
+    ms.setPrecision(eps)
+    ms.setMaxSteps(10000)
+    sols = []
+    assert ms.solve(op, b, sols, shifts)
+    orc = oracle.Operator(setup["geom"], setup["links"], "SquareImproved", setup["kappa"], setup["csw"], True)
+    rc, osols, steps = oracle.mmmr_multishift(orc, b, shifts, eps, 10000)
+    assert rc == 1
+    for x, xo, s in zip(sols, osols, shifts):
+        assert true_res(orc, b, x, s) < 2e-10
+        assert rel(x, xo) < 1e-7
