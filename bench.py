@@ -128,31 +128,52 @@ def traffic_from_profiles(prec):
     return float(m.group(1)) if m else None
 
 
-def cpu_reference(sample_iters=(4, 8), threads=None):
+class quiet_stdout:
+    """Silences C-level stdout (the reference prints solver progress with std::cout)."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+
+    def __exit__(self, *a):
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
+def cpu_reference(sample_iters=(4, 8)):
     """The reference's FP64 even-odd BiCGStab (PreconditionedBiCGStab.cpp:33-100) on the
-    host cores, on the benchmark's lattice and first source.  A bounded sample: the
-    solver runs twice with max_steps = 4 and 8; the difference gives the time per
-    iteration, the first run the set-up (field strength + 12x12 inverses).  Solves/s =
-    1 / (setup + iterations_to_converge x time_per_iteration), where the iteration count
-    is the reference algorithm's own (measured by its GPU mirror on the same system,
-    or by the oracle when no GPU is present)."""
+    host cores (OpenMP, all threads), on the benchmark's lattice and first noise source.
+    A bounded sample: the solver runs with max_steps = 4 and 8; the difference gives the
+    time per iteration, the first run the set-up (field strength + 12x12 inverses).
+    Solves/s = 1 / (setup + iterations x time per iteration) with the iteration count the
+    reference algorithm needs on this system.  Runs the reference's own code compiled
+    from its sources (oracle/_ref) when present, else the oracle's restatement."""
     import oracle as O
-    from leonardym_b200 import synth
-    kind = "reference" if os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libleonard_ref.so")) else "port"
+    from oracle import ref as R
     links = workload_links()
     b = workload_sources()[N_POINT]
-    geom = O.Geometry(DIMS)
-    D = O.Operator(geom, links, "Improved", KAPPA, CSW, False)
     prec = (TOL ** 2) * float(np.vdot(b, b).real)
+    if R.available("su3"):
+        kind = "reference"
+        ref = R.Reference(DIMS, links, "su3")
+        run = lambda n: ref.solve("Improved", "preconditioned_bicgstab", b, prec, n, KAPPA, CSW, False)
+    else:
+        kind = "port"
+        D = O.Operator(O.Geometry(DIMS), links, "Improved", KAPPA, CSW, False)
+        run = lambda n: O.preconditioned_bicgstab(D, b, prec, n)
     ts = []
-    for n in sample_iters:
-        t0 = time.perf_counter()
-        O.preconditioned_bicgstab(D, b, prec, n)
-        ts.append(time.perf_counter() - t0)
+    with quiet_stdout():
+        for n in sample_iters:
+            t0 = time.perf_counter()
+            run(n)
+            ts.append(time.perf_counter() - t0)
     t_iter = (ts[1] - ts[0]) / (sample_iters[1] - sample_iters[0])
     setup = max(ts[0] - sample_iters[0] * t_iter, 0.0)
     return {"t_iter": t_iter, "setup": setup, "kind": kind, "sample_seconds": sum(ts),
-            "cores": int(threads or os.environ.get("OMP_NUM_THREADS", os.cpu_count()))}
+            "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))}
 
 
 def dist_setup():

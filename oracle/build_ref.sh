@@ -1,0 +1,52 @@
+#!/usr/bin/env bash
+# Compiles LeonardYM's own fermion hot path from its sources under /root/reference
+# (never copied into this repository) against the Eigen-API shim in
+# oracle/eigen_shim, plus oracle/ref_harness.cpp, into oracle/_ref/:
+#   libleonard_ref_su3.so     NUMCOLORS=3            (SU(3) fundamental)
+#   libleonard_ref_su2adj.so  NUMCOLORS=2 -DADJOINT  (SU(2) adjoint)
+# Flags follow the reference's Makefile.mth (-DEIGEN -DMULTITHREADING -fopenmp, the
+# MatrixBase plugin), with -std=c++17 because program_options uses <any>.
+set -euo pipefail
+REF=${LYM_REFERENCE:-/root/reference}/source
+HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
+OUT="$HERE/_ref"
+mkdir -p "$OUT"
+[ -d "$REF" ] || { echo "reference sources not found at $REF" >&2; exit 1; }
+TUS=(
+  MPILattice/LocalLayout.cpp
+  dirac_operators/DiracOperator.cpp dirac_operators/DiracWilsonOperator.cpp
+  dirac_operators/BasicDiracWilsonOperator.cpp dirac_operators/BasicSquareDiracWilsonOperator.cpp
+  dirac_operators/ImprovedDiracWilsonOperator.cpp dirac_operators/EvenOddImprovedDiracWilsonOperator.cpp
+  dirac_operators/SquareDiracWilsonOperator.cpp dirac_operators/SquareImprovedDiracWilsonOperator.cpp
+  dirac_operators/SquareEvenOddImprovedDiracWilsonOperator.cpp
+  dirac_operators/OverlapOperator.cpp dirac_operators/SquareOverlapOperator.cpp dirac_operators/ExactOverlapOperator.cpp
+  dirac_functions/Polynomial.cpp dirac_functions/ChebyshevRecursion.cpp fermion_measurements/DiracEigenSolver.cpp
+  inverters/ConjugateGradient.cpp inverters/BiConjugateGradient.cpp inverters/PreconditionedBiCGStab.cpp
+  inverters/MultishiftSolver.cpp inverters/MEMultishiftSolver.cpp inverters/MMMRMultishiftSolver.cpp
+  inverters/ChronologicalMultishiftSolver.cpp
+  algebra_utils/AlgebraUtils.cpp utils/RandomSeed.cpp utils/Gamma.cpp
+  program_options/StorageParameters.cpp
+  hmc_forces/Force.cpp hmc_forces/FermionForce.cpp hmc_forces/DiracWilsonFermionForce.cpp
+  hmc_forces/ImprovedFermionForce.cpp hmc_forces/OverlapFermionForce.cpp
+)
+build() {
+  local name=$1; shift
+  local flags=("$@")
+  local objdir="$OUT/obj_$name"
+  mkdir -p "$objdir"
+  local objs=()
+  for tu in "${TUS[@]}" ; do
+    local o="$objdir/$(echo "$tu" | tr '/' '_' | sed 's/\.cpp$/.o/')"
+    if [ ! -f "$o" ] || [ "$REF/$tu" -nt "$o" ] || [ "$HERE/eigen_shim/Eigen/Dense" -nt "$o" ]; then
+      g++ "${flags[@]}" -c "$REF/$tu" -o "$o" &
+    fi
+    objs+=("$o")
+  done
+  wait
+  g++ "${flags[@]}" -c "$HERE/ref_harness.cpp" -o "$objdir/ref_harness.o"
+  g++ -shared -fopenmp -o "$OUT/libleonard_ref_$name.so" "${objs[@]}" "$objdir/ref_harness.o"
+}
+COMMON=(-O2 -fPIC -fopenmp -std=c++17 -w -include ctime -include cstring -I"$HERE/eigen_shim" -I"$REF"
+        -DMBE="\"$REF/utils/MatrixBaseExtension.h\"" -DEIGEN -DMULTITHREADING)
+build su3 "${COMMON[@]}" -DNUMCOLORS=3
+build su2adj "${COMMON[@]}" -DNUMCOLORS=2 -DADJOINT

@@ -1,0 +1,129 @@
+"""ctypes bindings of the reference's own hot path compiled from its sources
+(oracle/build_ref.sh -> oracle/_ref/libleonard_ref_{su3,su2adj}.so).
+
+TEST INFRASTRUCTURE ONLY: used to pin the oracle restatement, to generate the
+golden fixtures, and as bench.py's CPU baseline ("kind": "reference").
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIBS = {}
+KIND = {"DiracWilson": 0, "Improved": 1, "EvenOddImproved": 2, "SquareDiracWilson": 3, "SquareImproved": 4,
+        "SquareEvenOddImproved": 5, "BasicDiracWilson": 6}
+SOLVER = {"cg": 0, "bicgstab": 1, "preconditioned_bicgstab": 2, "bicgstab_shifted": 3}
+
+
+def path(rep):
+    return os.path.join(_HERE, "_ref", f"libleonard_ref_{rep}.so")
+
+
+def available(rep="su3"):
+    return os.path.exists(path(rep))
+
+
+def lib(rep):
+    if rep not in _LIBS:
+        L = C.CDLL(path(rep))
+        vp, ip, dp, i = C.c_void_p, C.POINTER(C.c_int), C.c_double, C.c_int
+        L.ref_multiply.argtypes = [ip, i, dp, dp, i, vp, vp, vp]
+        L.ref_multiply_add.argtypes = [ip, i, dp, dp, i, vp, vp, vp, dp, dp, vp]
+        L.ref_field_strength.argtypes = [ip, dp, dp, vp, vp]
+        L.ref_solve.argtypes = [ip, i, dp, dp, i, vp, i, dp, i, dp, dp, vp, vp, ip]
+        L.ref_multishift.argtypes = [ip, i, dp, dp, i, vp, i, i, vp, dp, i, vp, C.POINTER(C.c_void_p)]
+        L.ref_neighbours.argtypes = [ip, ip, ip]
+        L.ref_antiperiodic.argtypes = [ip, vp]
+        if hasattr(L, "ref_to_adjoint"):
+            L.ref_to_adjoint.argtypes = [i, vp, vp]
+        _LIBS[rep] = L
+    return _LIBS[rep]
+
+
+def _d(dims):
+    return (C.c_int * 4)(*[int(x) for x in dims])
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Reference:
+    """The reference operators and solvers on one link field."""
+
+    def __init__(self, dims, links, rep=None):
+        self.dims = tuple(int(x) for x in dims)
+        self.links = np.ascontiguousarray(links)
+        self.rep = rep or ("su3" if np.iscomplexobj(self.links) else "su2adj")
+        self.L = lib(self.rep)
+        self.V = int(np.prod(self.dims))
+
+    def _vec(self):
+        return np.zeros((self.V, 4, 3), np.complex128)
+
+    def multiply(self, kind, x, kappa, csw=0.0, gamma5=True):
+        x = np.ascontiguousarray(x, np.complex128)
+        out = self._vec()
+        rc = self.L.ref_multiply(_d(self.dims), KIND[kind], kappa, csw, int(gamma5), _p(self.links), _p(x), _p(out))
+        assert rc == 0
+        return out
+
+    def multiply_add(self, kind, x, y, alpha, kappa, csw=0.0, gamma5=True):
+        x = np.ascontiguousarray(x, np.complex128)
+        y = np.ascontiguousarray(y, np.complex128)
+        out = self._vec()
+        a = complex(alpha)
+        rc = self.L.ref_multiply_add(_d(self.dims), KIND[kind], kappa, csw, int(gamma5), _p(self.links), _p(x), _p(y),
+                                     a.real, a.imag, _p(out))
+        assert rc == 0
+        return out
+
+    def field_strength(self, kappa, csw):
+        dt = np.complex128 if self.rep == "su3" else np.float64
+        F = np.zeros((self.V, 6, 3, 3), dt)
+        self.L.ref_field_strength(_d(self.dims), kappa, csw, _p(self.links), _p(F))
+        return F
+
+    def solve(self, kind, solver, b, precision, max_steps, kappa, csw=0.0, gamma5=True, shift=0.0):
+        b = np.ascontiguousarray(b, np.complex128)
+        x = self._vec()
+        steps = C.c_int(0)
+        s = complex(shift)
+        rc = self.L.ref_solve(_d(self.dims), KIND[kind], kappa, csw, int(gamma5), _p(self.links), SOLVER[solver],
+                              float(precision), int(max_steps), s.real, s.imag, _p(b), _p(x), C.byref(steps))
+        return rc, x, steps.value
+
+    def multishift(self, kind, algorithm, b, shifts, epsilon, max_steps, kappa, csw=0.0, gamma5=True):
+        b = np.ascontiguousarray(b, np.complex128)
+        sols = [self._vec() for _ in shifts]
+        ptrs = (C.c_void_p * len(sols))(*[s.ctypes.data for s in sols])
+        sh = np.ascontiguousarray(shifts, np.float64)
+        alg = {"mass_estrapolation": 0, "minimal_residual": 1}[algorithm]
+        rc = self.L.ref_multishift(_d(self.dims), KIND[kind], kappa, csw, int(gamma5), _p(self.links), alg,
+                                   len(shifts), _p(sh), float(epsilon), int(max_steps), _p(b), ptrs)
+        return rc, sols
+
+
+def neighbours(dims, rep="su3"):
+    V = int(np.prod(dims))
+    sup = np.zeros((V, 4), np.int32)
+    sdn = np.zeros((V, 4), np.int32)
+    lib(rep).ref_neighbours(_d(dims), sup.ctypes.data_as(C.POINTER(C.c_int)), sdn.ctypes.data_as(C.POINTER(C.c_int)))
+    return sup, sdn
+
+
+def antiperiodic(dims, links, rep):
+    out = np.ascontiguousarray(links).copy()
+    lib(rep).ref_antiperiodic(_d(dims), _p(out))
+    return out
+
+
+def to_adjoint(fund):
+    fund = np.ascontiguousarray(fund, np.complex128)
+    n = fund.size // 4
+    adj = np.zeros(fund.shape[:-2] + (3, 3), np.float64)
+    lib("su2adj").ref_to_adjoint(n, _p(fund), _p(adj))
+    return adj

@@ -1,0 +1,234 @@
+// C entry points around LeonardYM's own hot-path classes, compiled from the
+// reference sources by oracle/build_ref.sh into oracle/_ref/.  TEST
+// INFRASTRUCTURE ONLY: it pins the oracle restatement (tests/test_oracle_pins.py)
+// and generates the golden fixtures (tests/golden/make_golden.py).
+//
+// One library per representation: NUMCOLORS=3 (fundamental) and NUMCOLORS=2
+// with ADJOINT.  The layout is the reference's process-global LocalLayout, so
+// every entry point (re)initialises it for the requested extents.
+#include <cstring>
+#include <vector>
+
+#include "algebra_utils/AlgebraUtils.h"
+#include "dirac_operators/DiracWilsonOperator.h"
+#include "dirac_operators/EvenOddImprovedDiracWilsonOperator.h"
+#include "dirac_operators/ImprovedDiracWilsonOperator.h"
+#include "dirac_operators/SquareDiracWilsonOperator.h"
+#include "dirac_operators/SquareEvenOddImprovedDiracWilsonOperator.h"
+#include "dirac_operators/SquareImprovedDiracWilsonOperator.h"
+#include "dirac_operators/BasicDiracWilsonOperator.h"
+#include "inverters/BiConjugateGradient.h"
+#include "inverters/ConjugateGradient.h"
+#include "inverters/MEMultishiftSolver.h"
+#include "inverters/MMMRMultishiftSolver.h"
+#include "inverters/PreconditionedBiCGStab.h"
+#include "utils/ConvertLattice.h"
+
+using namespace Update;
+
+namespace {
+
+int g_dims[4] = {0, 0, 0, 0};
+
+void init_layout(const int d[4])
+{
+    if (g_dims[0] == d[0] && g_dims[1] == d[1] && g_dims[2] == d[2] && g_dims[3] == d[3]) return;
+    Lattice::LocalLayout::glob_x = d[0];
+    Lattice::LocalLayout::glob_y = d[1];
+    Lattice::LocalLayout::glob_z = d[2];
+    Lattice::LocalLayout::glob_t = d[3];
+    Lattice::LocalLayout::initialize();
+    for (int k = 0; k < 4; ++k) g_dims[k] = d[k];
+}
+
+template <class L> void load(L &lat, const double *raw)
+{
+    std::memcpy((void *)lat.getRawData(), raw, sizeof(typename L::TData) * lat.localsize);
+}
+template <class L> void store(const L &lat, double *raw)
+{
+    std::memcpy(raw, (const void *)lat.getRawData(), sizeof(typename L::TData) * lat.localsize);
+}
+
+// exposes the protected field strength of ImprovedDiracWilsonOperator
+struct FieldStrengthAccess : public ImprovedDiracWilsonOperator {
+    const reduced_field_strength_lattice_t &field() const { return F; }
+};
+
+DiracOperator *make_operator(int kind, double kappa, double csw, int gamma5, const extended_fermion_lattice_t &links)
+{
+    DiracOperator *op = nullptr;
+    switch (kind) {
+    case 0: op = new DiracWilsonOperator(); break;
+    case 1: op = new ImprovedDiracWilsonOperator(); break;
+    case 2: op = new EvenOddImprovedDiracWilsonOperator(); break;
+    case 3: op = new SquareDiracWilsonOperator(); break;
+    case 4: op = new SquareImprovedDiracWilsonOperator(); break;
+    case 5: op = new SquareEvenOddImprovedDiracWilsonOperator(); break;
+    case 6: op = new BasicDiracWilsonOperator(); break;
+    default: return nullptr;
+    }
+    op->setKappa(kappa);
+    if (kind == 1 || kind == 2) static_cast<ImprovedDiracWilsonOperator *>(op)->setCSW(csw);
+    if (kind == 4) static_cast<SquareImprovedDiracWilsonOperator *>(op)->setCSW(csw);
+    if (kind == 5) static_cast<SquareEvenOddImprovedDiracWilsonOperator *>(op)->setCSW(csw);
+    op->setLattice(links);
+    op->setGamma5(gamma5 != 0);
+    return op;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ref_dirac_vector_length() { return diracVectorLength; }
+int ref_link_doubles() { return (int)(sizeof(FermionicGroup) / sizeof(double)); }
+
+int ref_neighbours(const int dims[4], int *sup, int *sdn)
+{
+    init_layout(dims);
+    const int V = Lattice::LocalLayout::localsize;
+    for (int s = 0; s < V; ++s)
+        for (int mu = 0; mu < 4; ++mu) {
+            sup[s * 4 + mu] = reduced_dirac_vector_t::sup(s, mu);
+            sdn[s * 4 + mu] = reduced_dirac_vector_t::sdn(s, mu);
+        }
+    return 0;
+}
+
+// switchAntiperiodicBc on a fermion link field (in place)
+int ref_antiperiodic(const int dims[4], double *links)
+{
+    init_layout(dims);
+    extended_fermion_lattice_t L;
+    load(L, links);
+    switchAntiperiodicBc(L);
+    store(L, links);
+    return 0;
+}
+
+#ifdef ADJOINT
+// ConvertLattice::toAdjoint on nlinks SU(2) links (complex 2x2 column-major)
+int ref_to_adjoint(int nlinks, const double *fund, double *adj)
+{
+    for (int l = 0; l < nlinks; ++l) {
+        GaugeGroup U;
+        std::memcpy((void *)U.data(), fund + 8 * (size_t)l, sizeof(GaugeGroup));
+        AdjointGroup A;
+        ConvertLattice<extended_fermion_lattice_t, extended_gauge_lattice_t>::toAdjoint(U, A);
+        std::memcpy(adj + 9 * (size_t)l, (const void *)A.data(), sizeof(AdjointGroup));
+    }
+    return 0;
+}
+#endif
+
+int ref_multiply(const int dims[4], int kind, double kappa, double csw, int gamma5, const double *links,
+                 const double *in, double *out)
+{
+    init_layout(dims);
+    extended_fermion_lattice_t L;
+    load(L, links);
+    DiracOperator *op = make_operator(kind, kappa, csw, gamma5, L);
+    if (!op) return -1;
+    reduced_dirac_vector_t x, y;
+    load(x, in);
+    op->multiply(y, x);
+    store(y, out);
+    delete op;
+    return 0;
+}
+
+int ref_multiply_add(const int dims[4], int kind, double kappa, double csw, int gamma5, const double *links,
+                     const double *v1, const double *v2, double are, double aim, double *out)
+{
+    init_layout(dims);
+    extended_fermion_lattice_t L;
+    load(L, links);
+    DiracOperator *op = make_operator(kind, kappa, csw, gamma5, L);
+    if (!op) return -1;
+    reduced_dirac_vector_t a, b, y;
+    load(a, v1);
+    load(b, v2);
+    op->multiplyAdd(y, a, b, complex(are, aim));
+    store(y, out);
+    delete op;
+    return 0;
+}
+
+int ref_field_strength(const int dims[4], double kappa, double csw, const double *links, double *F)
+{
+    init_layout(dims);
+    extended_fermion_lattice_t L;
+    load(L, links);
+    FieldStrengthAccess op;
+    op.setKappa(kappa);
+    op.setCSW(csw);
+    op.setLattice(L);
+    store(op.field(), F);
+    return 0;
+}
+
+// solver = 0 ConjugateGradient, 1 BiConjugateGradient, 2 PreconditionedBiCGStab,
+// 3 BiConjugateGradient shifted by (are, aim)
+int ref_solve(const int dims[4], int kind, double kappa, double csw, int gamma5, const double *links, int solver,
+              double precision, int max_steps, double are, double aim, const double *src, double *sol, int *steps)
+{
+    init_layout(dims);
+    extended_fermion_lattice_t L;
+    load(L, links);
+    DiracOperator *op = make_operator(kind, kappa, csw, gamma5, L);
+    if (!op) return -1;
+    reduced_dirac_vector_t b, x;
+    load(b, src);
+    bool ok = false;
+    if (solver == 0) {
+        ConjugateGradient cg;
+        cg.setPrecision(precision);
+        cg.setMaximumSteps(max_steps);
+        ok = cg.solve(op, b, x);
+        *steps = cg.getLastSteps();
+    } else if (solver == 1 || solver == 3) {
+        BiConjugateGradient bi;
+        bi.setPrecision(precision);
+        bi.setMaximumSteps(max_steps);
+        ok = solver == 1 ? bi.solve(op, b, x) : bi.solve(op, b, x, complex(are, aim));
+        *steps = bi.getLastSteps();
+    } else if (solver == 2) {
+        PreconditionedBiCGStab pb;
+        pb.setPrecision(precision);
+        pb.setMaximumSteps(max_steps);
+        ok = pb.solve(op, b, x);
+        *steps = pb.getLastSteps();
+    } else {
+        delete op;
+        return -1;
+    }
+    store(x, sol);
+    delete op;
+    return ok ? 1 : 0;
+}
+
+// algorithm 0 MEMultishiftSolver, 1 MMMRMultishiftSolver
+int ref_multishift(const int dims[4], int kind, double kappa, double csw, int gamma5, const double *links,
+                   int algorithm, int nshift, const double *shifts, double epsilon, int max_steps, const double *src,
+                   double **sols)
+{
+    init_layout(dims);
+    extended_fermion_lattice_t L;
+    load(L, links);
+    DiracOperator *op = make_operator(kind, kappa, csw, gamma5, L);
+    if (!op) return -1;
+    extended_dirac_vector_t b;
+    load(b, src);
+    std::vector<extended_dirac_vector_t> xs(nshift);
+    std::vector<real_t> sh(shifts, shifts + nshift);
+    MultishiftSolver *ms = algorithm == 0 ? (MultishiftSolver *)new MEMultishiftSolver(epsilon, max_steps)
+                                          : (MultishiftSolver *)new MMMRMultishiftSolver(epsilon, max_steps);
+    const bool ok = ms->solve(op, b, xs, sh);
+    for (int i = 0; i < nshift; ++i) store(xs[i], sols[i]);
+    delete ms;
+    delete op;
+    return ok ? 1 : 0;
+}
+
+}  // extern "C"
