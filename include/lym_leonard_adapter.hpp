@@ -1,0 +1,211 @@
+// lym_leonard_adapter.hpp -- header-only binding of liblym_b200 (include/lym_b200.h)
+// into LeonardYM's own class hierarchy, for a maintainer to compile inside the
+// reference (it includes the reference's headers).  The classes subclass the
+// reference interfaces so existing callers (Solver::solve, MultishiftSolver::solve,
+// DiracOperator::multiply/multiplyAdd) keep working unchanged:
+//
+//   GpuDiracOperator<Base, Kind>   : Base  (DiracWilsonOperator, ImprovedDiracWilsonOperator,
+//                                           EvenOddImprovedDiracWilsonOperator and the Square* ones)
+//     setLattice -> lym_gauge_upload of the raw extended_fermion_lattice_t storage
+//     multiply / multiplyAdd -> lym_multiply / lym_multiply_add on the raw vector storage
+//   GpuSolver       : Solver            -> lym_solve     (inverters/Solver.h:13)
+//   GpuMultishiftSolver : MultishiftSolver -> lym_multishift (inverters/MultishiftSolver.h:28)
+//
+// Requirements: single process (no ENABLE_MPI), LocalLayout initialised, even glob_t.
+// Errors: the reference calls exit() on misuse; these adapters print the library's
+// message and return false (solvers) or leave the output untouched (operators).
+#ifndef LYM_LEONARD_ADAPTER_HPP
+#define LYM_LEONARD_ADAPTER_HPP
+
+#include <iostream>
+#include <vector>
+
+#include "dirac_operators/DiracWilsonOperator.h"
+#include "dirac_operators/EvenOddImprovedDiracWilsonOperator.h"
+#include "dirac_operators/ImprovedDiracWilsonOperator.h"
+#include "dirac_operators/SquareDiracWilsonOperator.h"
+#include "dirac_operators/SquareEvenOddImprovedDiracWilsonOperator.h"
+#include "dirac_operators/SquareImprovedDiracWilsonOperator.h"
+#include "inverters/MultishiftSolver.h"
+#include "inverters/Solver.h"
+#include "lym_b200.h"
+
+namespace Update {
+
+// One library context per process, for the geometry of the static LocalLayout.
+inline lym_context *lym_global_context()
+{
+    static lym_context *ctx = nullptr;
+    static int dims[4] = {0, 0, 0, 0};
+    typedef Lattice::LocalLayout LL;
+    const int want[4] = {LL::glob_x, LL::glob_y, LL::glob_z, LL::glob_t};
+    if (ctx && (dims[0] != want[0] || dims[1] != want[1] || dims[2] != want[2] || dims[3] != want[3])) {
+        lym_context_destroy(ctx);
+        ctx = nullptr;
+    }
+    if (!ctx) {
+#ifdef ADJOINT
+        const int rep = LYM_REP_SU2_ADJOINT;
+#else
+        const int rep = LYM_REP_SU3_FUNDAMENTAL;
+#endif
+        if (lym_context_create(want, rep, 0, &ctx) != LYM_OK) {
+            std::cerr << "lym_context_create failed" << std::endl;
+            return nullptr;
+        }
+        for (int k = 0; k < 4; ++k) dims[k] = want[k];
+    }
+    return ctx;
+}
+
+inline int lym_next_gauge_id()
+{
+    static int next = 1;
+    return next++;
+}
+
+template <class Base, int Kind> class GpuDiracOperator : public Base {
+public:
+    GpuDiracOperator() : Base(), op_(-1), gauge_(lym_next_gauge_id()) {}
+    ~GpuDiracOperator()
+    {
+        lym_context *c = lym_global_context();
+        if (c && op_ >= 0) lym_operator_destroy(c, op_);
+        if (c) lym_gauge_evict(c, gauge_);
+    }
+
+    virtual void setLattice(const extended_fermion_lattice_t &lat)
+    {
+        this->DiracOperator::setLattice(lat);  // keeps the host copy getLattice() returns
+        lym_context *c = lym_global_context();
+        if (!c) return;
+        if (lym_gauge_upload(c, gauge_, reinterpret_cast<const double *>(lat.getRawData())) != LYM_OK) report(c);
+        if (op_ < 0 && lym_operator_create(c, gauge_, Kind, this->kappa, csw_of(), this->gamma5, &op_) != LYM_OK)
+            report(c);
+        else if (op_ >= 0)
+            lym_operator_set_gauge(c, op_, gauge_);
+    }
+
+    virtual void multiply(reduced_dirac_vector_t &output, const reduced_dirac_vector_t &input)
+    {
+        lym_context *c = sync();
+        if (c && lym_multiply(c, op_, reinterpret_cast<double *>(output.getRawData()),
+                              reinterpret_cast<const double *>(input.getRawData())) != LYM_OK)
+            report(c);
+    }
+
+    virtual void multiplyAdd(reduced_dirac_vector_t &output, const reduced_dirac_vector_t &vector1,
+                             const reduced_dirac_vector_t &vector2, const complex &alpha)
+    {
+        lym_context *c = sync();
+        if (c && lym_multiply_add(c, op_, reinterpret_cast<double *>(output.getRawData()),
+                                  reinterpret_cast<const double *>(vector1.getRawData()),
+                                  reinterpret_cast<const double *>(vector2.getRawData()), alpha.real(),
+                                  alpha.imag()) != LYM_OK)
+            report(c);
+    }
+
+    int operatorId() { return sync() ? op_ : -1; }
+
+protected:
+    // kappa, csw and gamma5 are plain members of the reference classes (setGamma5 and
+    // setCSW are not virtual), so they are pushed to the library before every use.
+    lym_context *sync()
+    {
+        lym_context *c = lym_global_context();
+        if (!c || op_ < 0) return nullptr;
+        lym_operator_set_kappa(c, op_, this->kappa);
+        lym_operator_set_csw(c, op_, csw_of());
+        lym_operator_set_gamma5(c, op_, this->gamma5);
+        return c;
+    }
+    double csw_of() const { return csw_helper(this); }
+    static double csw_helper(const ImprovedDiracWilsonOperator *o) { return o->getCSW(); }
+    static double csw_helper(const SquareImprovedDiracWilsonOperator *o) { return o->getCSW(); }
+    static double csw_helper(const SquareEvenOddImprovedDiracWilsonOperator *o) { return o->getCSW(); }
+    static double csw_helper(const void *) { return 0.0; }
+    static void report(lym_context *c) { std::cerr << "liblym_b200: " << lym_last_error(c) << std::endl; }
+    int op_;
+    int gauge_;
+};
+
+typedef GpuDiracOperator<DiracWilsonOperator, LYM_OP_DIRAC_WILSON> GpuDiracWilsonOperator;
+typedef GpuDiracOperator<ImprovedDiracWilsonOperator, LYM_OP_IMPROVED> GpuImprovedDiracWilsonOperator;
+typedef GpuDiracOperator<EvenOddImprovedDiracWilsonOperator, LYM_OP_EVEN_ODD_IMPROVED> GpuEvenOddImprovedDiracWilsonOperator;
+typedef GpuDiracOperator<SquareDiracWilsonOperator, LYM_OP_SQUARE_DIRAC_WILSON> GpuSquareDiracWilsonOperator;
+typedef GpuDiracOperator<SquareImprovedDiracWilsonOperator, LYM_OP_SQUARE_IMPROVED> GpuSquareImprovedDiracWilsonOperator;
+typedef GpuDiracOperator<SquareEvenOddImprovedDiracWilsonOperator, LYM_OP_SQUARE_EVEN_ODD_IMPROVED>
+    GpuSquareEvenOddImprovedDiracWilsonOperator;
+
+// operator id of a Gpu* operator, -1 for any other DiracOperator
+inline int lym_operator_of(DiracOperator *d)
+{
+    if (auto o = dynamic_cast<GpuDiracWilsonOperator *>(d)) return o->operatorId();
+    if (auto o = dynamic_cast<GpuImprovedDiracWilsonOperator *>(d)) return o->operatorId();
+    if (auto o = dynamic_cast<GpuEvenOddImprovedDiracWilsonOperator *>(d)) return o->operatorId();
+    if (auto o = dynamic_cast<GpuSquareDiracWilsonOperator *>(d)) return o->operatorId();
+    if (auto o = dynamic_cast<GpuSquareImprovedDiracWilsonOperator *>(d)) return o->operatorId();
+    if (auto o = dynamic_cast<GpuSquareEvenOddImprovedDiracWilsonOperator *>(d)) return o->operatorId();
+    return -1;
+}
+
+// Solver::solve on the GPU; `algorithm` is a lym_solver value.
+class GpuSolver : public Solver {
+public:
+    explicit GpuSolver(int algorithm = LYM_SOLVER_EO_BICGSTAB) : Solver("GpuSolver"), algorithm_(algorithm) {}
+    using Solver::solve;
+    virtual bool solve(DiracOperator *dirac, const reduced_dirac_vector_t &source, reduced_dirac_vector_t &solution,
+                       reduced_dirac_vector_t const *initial_guess = 0)
+    {
+        lym_context *c = lym_global_context();
+        const int op = lym_operator_of(dirac);
+        if (!c || op < 0) {
+            std::cerr << "GpuSolver needs a Gpu* DiracOperator" << std::endl;
+            return false;
+        }
+        lym_solve_stats st;
+        const int rc = lym_solve(c, op, algorithm_, precision, (int)maxSteps,
+                                 reinterpret_cast<const double *>(source.getRawData()),
+                                 reinterpret_cast<double *>(solution.getRawData()),
+                                 initial_guess ? reinterpret_cast<const double *>(initial_guess->getRawData()) : 0, &st);
+        lastSteps = st.steps;
+        lastError = st.last_error;
+        if (rc < 0) std::cerr << "liblym_b200: " << lym_last_error(c) << std::endl;
+        return rc == LYM_OK;
+    }
+
+private:
+    int algorithm_;
+};
+
+// MultishiftSolver::solve on the GPU; `algorithm` is a lym_multishift_solver value.
+class GpuMultishiftSolver : public MultishiftSolver {
+public:
+    explicit GpuMultishiftSolver(int algorithm = LYM_MULTISHIFT_CG, real_t epsilon = 0.00000001,
+                                 unsigned int maxSteps = 3000)
+        : MultishiftSolver(epsilon, maxSteps), algorithm_(algorithm)
+    {
+    }
+    virtual bool solve(DiracOperator *dirac, const extended_dirac_vector_t &source,
+                       std::vector<extended_dirac_vector_t> &solutions, const std::vector<real_t> &shifts)
+    {
+        lym_context *c = lym_global_context();
+        const int op = lym_operator_of(dirac);
+        if (!c || op < 0) return false;
+        if (solutions.size() < shifts.size()) solutions.resize(shifts.size());
+        std::vector<double *> out(shifts.size());
+        for (size_t i = 0; i < shifts.size(); ++i) out[i] = reinterpret_cast<double *>(solutions[i].getRawData());
+        lym_solve_stats st;
+        const int rc = lym_multishift(c, op, algorithm_, (int)shifts.size(), shifts.data(), epsilon, (int)maxSteps,
+                                      reinterpret_cast<const double *>(source.getRawData()), out.data(), &st);
+        if (rc < 0) std::cerr << "liblym_b200: " << lym_last_error(c) << std::endl;
+        return rc == LYM_OK;
+    }
+
+private:
+    int algorithm_;
+};
+
+}  // namespace Update
+
+#endif
