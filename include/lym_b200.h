@@ -134,6 +134,22 @@ int lym_multiply_add(lym_context *ctx, int op_id, double *out, const double *v1,
 int lym_multiply_device(lym_context *ctx, int op_id, double *out, const double *in);
 int lym_multiply_add_device(lym_context *ctx, int op_id, double *out, const double *v1, const double *v2,
                             double alpha_re, double alpha_im);
+/* No counterpart in the reference.  Applies an EvenOddImproved operator like
+ * lym_multiply_device, but allocates no device memory: for callers that cannot call
+ * cudaMalloc, such as a process whose device memory all belongs to one pre-reserved arena
+ * or framework allocator, or a hot path that must not take the device-wide
+ * synchronisation of cudaMalloc / cudaFree.  `in` and `out` are caller-owned device
+ * vectors in the reference layout and must not overlap.  The operator's one intermediate
+ * vector (the even-site half spinor) lives in a fixed 12 MiB array inside the library,
+ * held by every GPU that loads it until exit, which limits the lattice to 131072 sites
+ * (for example 16^3 x 32); larger lattices get LYM_ERR_ARGUMENT.  The clover term must
+ * have been built by an earlier ordinary use of the operator (lym_multiply /
+ * lym_multiply_device), else LYM_ERR_ARGUMENT.  The first call on a device looks up the
+ * array's device address, so make that call before any stream capture.  All calls share
+ * the array (it keeps the last call's contents; nothing in it needs clearing): calls that
+ * overlap on the GPU, from several contexts on one device, race.  Returns after the result
+ * is complete. */
+int lym_multiply_device_noalloc(lym_context *ctx, int op_id, double *out, const double *in);
 /* storage precision of the single-precision / half-precision operator path, for
  * parity tests of the sloppy stencils: prec 0 FP64, 1 FP32 (12-real links), 2 FP16 */
 int lym_multiply_precision(lym_context *ctx, int op_id, int prec, double *out, const double *in);

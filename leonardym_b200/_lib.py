@@ -82,6 +82,7 @@ def lib():
         "lym_multiply_add": (i, [vp, i, vp, vp, vp, dp, dp]),
         "lym_multiply_device": (i, [vp, i, vp, vp]),
         "lym_multiply_add_device": (i, [vp, i, vp, vp, vp, dp, dp]),
+        "lym_multiply_device_noalloc": (i, [vp, i, vp, vp]),
         "lym_multiply_precision": (i, [vp, i, i, vp, vp]),
         "lym_field_strength": (i, [vp, i, vp]),
         "lym_solve": (i, [vp, i, i, dp, i, vp, vp, vp, sp]),

@@ -1560,3 +1560,32 @@ void lym_host_free(void *p)
 }
 
 }  // extern "C"
+
+// ------------------------------------------------- allocation-free variant --
+namespace lym {
+int noalloc_schur(const Geom &g, int rep, int device, cudaStream_t st, const GaugeDev &U, const CloverDev *C,
+                  double kappa, int gamma5, double *out, const double *in);
+}
+
+extern "C" int lym_multiply_device_noalloc(lym_context *c, int op_id, double *out, const double *in)
+{
+    if (!out || !in || out == in) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        OpEntry &op = op_of(c, op_id);
+        if (op.kind != LYM_OP_EVEN_ODD_IMPROVED)
+            fail(c, LYM_ERR_UNSUPPORTED, "lym_multiply_device_noalloc applies EvenOddImproved operators only");
+        if (c->g.Vh > 65536)
+            fail(c, LYM_ERR_ARGUMENT, "lym_multiply_device_noalloc: volume %d exceeds its maximum of 131072 sites",
+                 c->g.V);
+        if (!op.clover_ok)
+            fail(c, LYM_ERR_ARGUMENT,
+                 "lym_multiply_device_noalloc: the operator's clover term is not built yet (building it allocates); "
+                 "apply the operator once through lym_multiply or lym_multiply_device first");
+        GaugeEntry &ge = gauge_of(c, op.gauge_id);
+        const int rc = noalloc_schur(c->g, c->rep, c->device, c->st, ge.dev, &op.clover, op.kappa, op.gamma5, out, in);
+        if (rc != LYM_OK) fail(c, rc, "lym_multiply_device_noalloc: CUDA error %s", cudaGetErrorString(cudaGetLastError()));
+        CK(cudaStreamSynchronize(c->st));
+        count(c, 2);
+        return LYM_OK;
+    });
+}
