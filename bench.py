@@ -38,6 +38,10 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "which": "fallback"}
 # clover term (out_o = T_oo y_o - kappa^2 H_oe a_e): 8 links (+ 2 sign-table bytes for the
 # reconstructed formats), 1 neighbour spinor (each read once), the y spinor, T_oo, the output
 STENCIL_BYTES = {0: 8 * 144 + 3 * 192 + 576, 1: 8 * 48 + 2 + 3 * 96 + 288, 2: 8 * 24 + 2 + 3 * 52 + 144}
+# the batched kernel reads links, sign bytes and T once per site for the whole batch and
+# three spinors (neighbour, y, out) per right-hand side
+STENCIL_SITE_BYTES = {1: 8 * 48 + 2 + 288, 2: 8 * 24 + 2 + 144}
+STENCIL_RHS_BYTES = {1: 3 * 96, 2: 3 * 52}
 STENCIL_FLOPS = 1320 + 504 + 48  # hopping + clover apply + xpay, per site
 
 
@@ -119,12 +123,13 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def traffic_from_profiles(prec):
-    """DRAM bytes per launch of the stencil kernel from the committed ncu summary."""
+def traffic_from_profiles(prec, batch):
+    """DRAM bytes per launch of the batched stencil kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "stencil_schur_clover_24c48.md")
     if not os.path.exists(path):
         return None
-    m = re.search(rf"traffic_bytes_per_launch\[prec={prec}\]:\s*([0-9.eE+]+)", open(path).read())
+    m = re.search(rf"traffic_bytes_per_launch\[prec={prec},kernel=xpay,batch={batch}\]:\s*([0-9.eE+]+)",
+                  open(path).read())
     return float(m.group(1)) if m else None
 
 
@@ -288,17 +293,23 @@ def run_ours(args, world, rank, local):
     dev_src = torch.from_numpy(np.stack(srcs).view(np.float64).reshape(nrhs, V * 24)).to(f"cuda:{local}")
     dev_sol = torch.zeros_like(dev_src)
     stats = L.SolveStats()
+    bstats = (L.SolveStats * nrhs)()
+    src_ptrs = (C.c_void_p * nrhs)(*[dev_src[k].data_ptr() for k in range(nrhs)])
+    sol_ptrs = (C.c_void_p * nrhs)(*[dev_sol[k].data_ptr() for k in range(nrhs)])
+
+    def check_block(rc, tag):
+        if rc != 0:
+            raise RuntimeError(f"{tag} block solve failed: {rc} {lib.lym_last_error(ctx)}")
+        for k in range(nrhs):
+            if bstats[k].true_residual > TOL:
+                raise RuntimeError(f"{tag} solve {k}: true residual {bstats[k].true_residual:.3e} > {TOL}")
 
     def solve_all(record=None):
-        for k in range(nrhs):
-            rc = lib.lym_solve_device(ctx, opid, solver, -TOL, 20000, C.c_void_p(dev_src[k].data_ptr()),
-                                      C.c_void_p(dev_sol[k].data_ptr()), None, C.byref(stats))
-            if rc != 0:
-                raise RuntimeError(f"solve {k} failed: {rc} {lib.lym_last_error(ctx)}")
-            if stats.true_residual > TOL:
-                raise RuntimeError(f"solve {k}: true residual {stats.true_residual:.3e} > {TOL}")
-            if record is not None:
-                record.append((stats.seconds, stats.iterations, stats.true_residual))
+        rc = lib.lym_solve_block_device(ctx, opid, solver, -TOL, 20000, nrhs, src_ptrs, sol_ptrs, args.batch, bstats)
+        check_block(rc, "device")
+        if record is not None:
+            for k in range(nrhs):
+                record.append((bstats[k].seconds, bstats[k].iterations, bstats[k].true_residual))
 
     for _ in range(args.warmup):
         solve_all()
@@ -333,13 +344,12 @@ def run_ours(args, world, rank, local):
     barrier(world)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    hsrc_ptrs = (C.c_void_p * nrhs)(*hsrc)
+    hsol_ptrs = (C.c_void_p * nrhs)(*hsol)
     e0.record()
     for _ in range(args.steps):
-        for k in range(nrhs):
-            rc = lib.lym_solve(ctx, opid, solver, -TOL, 20000, C.c_void_p(hsrc[k]), C.c_void_p(hsol[k]), None,
-                               C.byref(stats))
-            if rc != 0 or stats.true_residual > TOL:
-                raise RuntimeError(f"e2e solve {k} failed: rc {rc}, residual {stats.true_residual}")
+        rc = lib.lym_solve_block(ctx, opid, solver, -TOL, 20000, nrhs, hsrc_ptrs, hsol_ptrs, args.batch, bstats)
+        check_block(rc, "e2e")
     lib.lym_synchronize(ctx)
     e1.record()
     torch.cuda.synchronize()
@@ -356,15 +366,17 @@ def run_ours(args, world, rank, local):
         t64.append(stats.seconds)
     fp64_value = world / statistics.mean(t64)
 
-    # stencil roofline: CUDA events around launches of the dominant kernel on the library stream
+    # stencil roofline: CUDA events around launches of the dominant kernel (the batched
+    # stencil of the block solve) on the library stream
     ms = C.c_double(0)
-    lib.lym_time_stencil(ctx, opid, sprec, 0, 50, C.byref(ms))
+    lib.lym_time_stencil_batch(ctx, opid, sprec, 0, args.batch, 30, C.byref(ms))
     Vh = V // 2
-    bytes_launch = STENCIL_BYTES[sprec] * Vh
+    bytes_launch = (STENCIL_SITE_BYTES[sprec] + args.batch * STENCIL_RHS_BYTES[sprec]) * Vh
     achieved = bytes_launch / (ms.value * 1e-3) / 1e9
     pk = peaks()
-    traffic = traffic_from_profiles(sprec)
-    ms64 = C.c_double(0)
+    traffic = traffic_from_profiles(sprec, args.batch)
+    ms1, ms64 = C.c_double(0), C.c_double(0)
+    lib.lym_time_stencil(ctx, opid, sprec, 0, 30, C.byref(ms1))
     lib.lym_time_stencil(ctx, opid, 0, 0, 20, C.byref(ms64))
 
     cpu = None
@@ -392,18 +404,21 @@ def run_ours(args, world, rank, local):
         "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32" if sprec == 1 else "f16",
         "data": "synthetic (seeded links and sources)",
-        "config": config_dict(f"even-odd CG, {args.precision} stencil + FP64 reliable updates"),
+        "config": config_dict(f"block even-odd CG, {args.batch} right-hand sides per batched stencil, "
+                              f"{args.precision} storage + FP64 reliable updates"),
         "fp64_eo_cg_solves_per_s": fp64_value,
         "mixed_over_fp64": value / world / (fp64_value / world),
         "latency_ms": {"p50": lat_ms[len(lat_ms) // 2], "p99": lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))]},
         "iterations": {"median": statistics.median(iters), "max": max(iters)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
-                     "kernel": f"Schur stencil with clover (prec {args.precision}), {ms.value * 1e3:.1f} us/launch",
+                     "kernel": (f"batched Schur stencil with clover, {args.batch} right-hand sides, "
+                                f"{args.precision} storage, {ms.value * 1e3:.1f} us/launch"),
                      "algorithmic_bytes_per_launch": bytes_launch,
                      "peak_source": f"{pk['which']} hbm_gbs",
-                     "fp64_kernel_gbs": STENCIL_BYTES[0] * Vh / (ms64.value * 1e-3) / 1e9,
-                     "gflops": STENCIL_FLOPS * Vh / (ms.value * 1e-3) / 1e9},
+                     "gflops": STENCIL_FLOPS * Vh * args.batch / (ms.value * 1e-3) / 1e9,
+                     "single_rhs_kernel_gbs": STENCIL_BYTES[sprec] * Vh / (ms1.value * 1e-3) / 1e9,
+                     "fp64_single_rhs_kernel_gbs": STENCIL_BYTES[0] * Vh / (ms64.value * 1e-3) / 1e9},
         "clocks": clocks,
         "gpu_launches": launches,
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": nrhs * nbytes,
@@ -414,24 +429,30 @@ def run_ours(args, world, rank, local):
 
 
 def run_profile(args):
-    """Small fixed case for ncu captures: one mixed-precision solve of the benchmark's
-    first noise source and 10 launches of the stencil kernel (about 1 GB on the device)."""
+    """Small fixed case for ncu captures: one block solve of the benchmark's first
+    `batch` noise sources, then 10 launches each of the single-RHS and the batched
+    stencil kernels (a few GB on the device)."""
     import leonardym_b200 as L
     from leonardym_b200.solvers import SOLVER_EO_CG_MIXED_HALF, SOLVER_EO_CG_MIXED_SINGLE
     lib = L.lib()
     lat = L.Lattice(DIMS, "su3", device=0)
     op = L.ImprovedDiracWilsonOperator(lat, KAPPA, CSW, gamma5=False)
     op.setLattice(workload_links())
-    b = workload_sources()[N_POINT]
-    x = lat.new_vector()
+    srcs = workload_sources()[N_POINT:N_POINT + args.batch]
+    xs = [lat.new_vector() for _ in srcs]
     solver = {"single": SOLVER_EO_CG_MIXED_SINGLE, "half": SOLVER_EO_CG_MIXED_HALF}[args.precision]
-    st = L.SolveStats()
-    rc = lib.lym_solve(lat.handle, op.op_id, solver, -TOL, 20000, b.ctypes.data_as(C.c_void_p),
-                       x.ctypes.data_as(C.c_void_p), None, C.byref(st))
+    bstats = (L.SolveStats * len(srcs))()
+    sp_ = (C.c_void_p * len(srcs))(*[s.ctypes.data for s in srcs])
+    xp_ = (C.c_void_p * len(srcs))(*[x.ctypes.data for x in xs])
+    rc = lib.lym_solve_block(lat.handle, op.op_id, solver, -TOL, 20000, len(srcs), sp_, xp_, args.batch, bstats)
+    st = bstats[0]
     ms = C.c_double(0)
-    lib.lym_time_stencil(lat.handle, op.op_id, 1 if args.precision == "single" else 2, 0, 10, C.byref(ms))
+    sp = 1 if args.precision == "single" else 2
+    lib.lym_time_stencil(lat.handle, op.op_id, sp, 0, 10, C.byref(ms))
+    msb = C.c_double(0)
+    lib.lym_time_stencil_batch(lat.handle, op.op_id, sp, 0, args.batch, 10, C.byref(msb))
     print(f"profile case: rc {rc}, iterations {st.iterations}, true residual {st.true_residual:.2e}, "
-          f"stencil {ms.value * 1e3:.1f} us")
+          f"stencil {ms.value * 1e3:.1f} us, batched stencil ({args.batch}) {msb.value * 1e3:.1f} us")
     lat.close()
     if rc != 0:
         sys.exit(1)
@@ -444,6 +465,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="single", choices=["single", "half"])
+    ap.add_argument("--batch", type=int, default=16, help="right-hand sides per batched stencil (power of 2 <= 32)")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--profile", action="store_true", help="small fixed case for ncu captures")
     args = ap.parse_args()

@@ -173,6 +173,21 @@ int lym_solve_device(lym_context *ctx, int op_id, int solver, double precision, 
 int lym_solve_shifted(lym_context *ctx, int op_id, double shift_re, double shift_im, double precision, int max_steps,
                       const double *source, double *solution, const double *guess, lym_solve_stats *stats);
 
+/* ---- many right-hand sides (no reference counterpart: the reference solves point and
+ * noise sources one by one, correlators/MesonCorrelator.cpp:92-98,
+ * fermion_measurements/ChiralCondensate.cpp:86-105) ----------------------------------
+ * Solves D x_j = b_j for nrhs sources with the mixed-precision even-odd CG
+ * (LYM_SOLVER_EO_CG_MIXED_SINGLE or _HALF), `batch` right-hand sides at a time (a power of
+ * two <= 32; 0 selects 16) through one batched stencil: links and clover are read once
+ * per site for the whole batch.  Each right-hand side keeps its own scalars, convergence
+ * mask and FP64 reliable updates, so its result does not depend on its batch mates beyond
+ * rounding.  stats (nrhs entries) may be NULL. */
+int lym_solve_block(lym_context *ctx, int op_id, int solver, double precision, int max_steps, int nrhs,
+                    const double *const *sources, double *const *solutions, int batch, lym_solve_stats *stats);
+int lym_solve_block_device(lym_context *ctx, int op_id, int solver, double precision, int max_steps, int nrhs,
+                           const double *const *sources, double *const *solutions, int batch,
+                           lym_solve_stats *stats);
+
 /* ---- multishift -------------------------------------------------------------------
  * MultishiftSolver::solve(dirac, source, solutions, shifts) -> bool
  * (inverters/MultishiftSolver.h:28); the operator must be Hermitian positive
@@ -196,6 +211,9 @@ int lym_stencil_indices(lym_context *ctx, int *out);
  * (second half of the Schur operator), 1 = even-parity output with T_ee^-1 (first half). */
 unsigned long long lym_context_kernel_launches(lym_context *ctx);
 int lym_time_stencil(lym_context *ctx, int op_id, int prec, int which, int iters, double *ms_per_launch);
+/* the same for the batched stencil of the block solves (prec 1 or 2, batch a power of 2 <= 32) */
+int lym_time_stencil_batch(lym_context *ctx, int op_id, int prec, int which, int batch, int iters,
+                           double *ms_per_launch);
 
 /* ---- pinned host memory for callers that want fast transfers ---------------------- */
 void *lym_host_alloc(size_t bytes);

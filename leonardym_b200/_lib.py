@@ -88,12 +88,15 @@ def lib():
         "lym_solve": (i, [vp, i, i, dp, i, vp, vp, vp, sp]),
         "lym_solve_device": (i, [vp, i, i, dp, i, vp, vp, vp, sp]),
         "lym_solve_shifted": (i, [vp, i, dp, dp, dp, i, vp, vp, vp, sp]),
+        "lym_solve_block": (i, [vp, i, i, dp, i, i, C.POINTER(vp), C.POINTER(vp), i, sp]),
+        "lym_solve_block_device": (i, [vp, i, i, dp, i, i, C.POINTER(vp), C.POINTER(vp), i, sp]),
         "lym_multishift": (i, [vp, i, i, i, vp, dp, i, vp, C.POINTER(vp), sp]),
         "lym_multishift_device": (i, [vp, i, i, i, vp, dp, i, vp, C.POINTER(vp), sp]),
         "lym_neighbour_tables": (i, [vp, ip, ip]),
         "lym_stencil_indices": (i, [vp, ip]),
         "lym_context_kernel_launches": (C.c_ulonglong, [vp]),
         "lym_time_stencil": (i, [vp, i, i, i, i, C.POINTER(C.c_double)]),
+        "lym_time_stencil_batch": (i, [vp, i, i, i, i, i, C.POINTER(C.c_double)]),
         "lym_host_alloc": (vp, [C.c_size_t]),
         "lym_host_free": (None, [vp]),
     }

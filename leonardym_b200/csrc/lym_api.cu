@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/lym_b200.h"
+#include "lym_batch.cuh"
 #include "lym_internal.h"
 #include "lym_solver_ops.cuh"
 
@@ -52,6 +53,7 @@ struct lym_context {
     int next_op = 1;
     // reductions
     double *partials = nullptr;
+    double *bpartials = nullptr;  // per-RHS partial sums of the batched reductions
     unsigned int *counter = nullptr;
     int *d_err = nullptr;
     void *d_state = nullptr;      // solver state (device)
@@ -954,6 +956,230 @@ int multishift_mmmr(lym_context *c, OpEntry &op, int nshift, const double *shift
     return rc;
 }
 
+// ------------------------------------------------------ multi-RHS (batched) --
+size_t batch_bytes(const Geom &g, int prec, int nb)
+{
+    const size_t s = g.stride;
+    return prec == PREC_F ? 6 * s * nb * sizeof(float4) : 3 * s * nb * sizeof(int4) + s * nb * sizeof(float);
+}
+
+struct BVec {
+    lym_context *c;
+    SpinorBatch s;
+    size_t bytes;
+    BVec(lym_context *ctx, int prec, int nb) : c(ctx)
+    {
+        s.prec = prec;
+        s.nb = nb;
+        s.lognb = 0;
+        while ((1 << s.lognb) < nb) ++s.lognb;
+        s.stride = c->g.stride;
+        bytes = batch_bytes(c->g, prec, nb);
+        char *base = (char *)dev_alloc(c, bytes);
+        s.v = base;
+        if (prec == PREC_H) s.norm = (float *)(base + (size_t)3 * s.stride * nb * sizeof(int4));
+    }
+    ~BVec() { dev_free(c, s.v, bytes); }
+    BVec(const BVec &) = delete;
+    BVec &operator=(const BVec &) = delete;
+    SpinorFB f() const { return SpinorFB{(float4 *)s.v, s.stride, s.lognb}; }
+    SpinorHB h() const { return SpinorHB{(int4 *)s.v, s.norm, s.stride, s.lognb}; }
+};
+
+template <class Op> void run_batch(lym_context *c, const Op &op, int lognb, Gate gate = Gate{nullptr, nullptr})
+{
+    count(c, 1);
+    const long threads = (long)c->g.Vh << lognb;
+    const int grid = (int)std::min<long>((threads + kBlasThreads - 1) / kBlasThreads, kBlasGridMax);
+    site_batch_kernel<Op><<<grid, kBlasThreads, 0, c->st>>>(op, c->g.Vh, lognb, c->bpartials, c->counter, gate);
+}
+
+// Schur complement on a batch: out_r = G5^g (T_oo in_r - kappa^2 H_oe T_ee^-1 H_eo in_r)
+void apply_schur_batch(lym_context *c, OpEntry &op, int prec, const SpinorBatch &out, const SpinorBatch &in,
+                       const SpinorBatch &tmp, int gamma5, const int *skip, const int *active)
+{
+    GaugeEntry &ge = gauge_of(c, op.gauge_id);
+    const bool clov = kind_has_clover(op.kind);
+    DslashBatchParams P;
+    P.g = c->g;
+    P.prec = prec;
+    P.rep = c->rep;
+    P.U = &ge.dev;
+    P.skip_if = skip;
+    P.active = active;
+    P.epi = clov ? EPI_CLOVINV_ : EPI_SCALE_;
+    P.parity = 0;
+    P.in = in;
+    P.out = tmp;
+    P.y = tmp;
+    P.clover = clov ? op.clover.Tinv[prec] : nullptr;
+    P.a = 1.0;
+    launch_dslash_batch(P, c->st);
+    P.epi = EPI_XPAY_;
+    P.parity = 1;
+    P.in = tmp;
+    P.out = out;
+    P.y = in;
+    P.clover = clov ? op.clover.T[prec] : nullptr;
+    P.b = -op.kappa * op.kappa;
+    P.gamma5 = gamma5;
+    launch_dslash_batch(P, c->st);
+    count(c, 2);
+}
+
+// y = a x + b y between a slot of a batch and a single FP64 half spinor (either way)
+template <class X, class Y> void axpby_views(lym_context *c, const X &x, const Y &y, double2 a, double2 b)
+{
+    run_site(c, OpAxpby<X, Y>{x, y, a, b}, 1);
+}
+
+// Even-odd CG on (gamma5 S)^2 for m <= nb right-hand sides at once (chunk of a block
+// solve): one batched stencil serves every RHS, each RHS keeps its own FP64 scalars,
+// convergence mask and FP64 reliable updates.  B: full FP64 sources, X: full FP64
+// solutions (odd sites are the CG unknowns; even sites reconstructed).
+int eo_cg_chunk(lym_context *c, OpEntry &op, int sprec, int nb, int m, const std::vector<Spinor> &B,
+                const std::vector<Spinor> &X, double tol, int max_steps, lym_solve_stats *st)
+{
+    const double delta = 0.1;
+    if (kind_has_clover(op.kind)) ensure_clover(c, op);
+    require_recon(c, gauge_of(c, op.gauge_id), sprec);
+    Vec te(c, PREC_D, 1), t1(c, PREC_D, 1), rS(c, PREC_D, 1), rN(c, PREC_D, 1);
+    BVec xs(c, PREC_F, nb), rs(c, PREC_F, nb), ps(c, sprec, nb), aps(c, sprec, nb), tes(c, sprec, nb),
+        tos(c, sprec, nb);
+    std::vector<Vec *> bp(m);
+    std::vector<double> epsS(m), bb(m);
+    for (int j = 0; j < m; ++j) {
+        bp[j] = new Vec(c, PREC_D, 1);
+        schur_source(c, op, B[j], **bp[j]);
+        bb[j] = norm2_now(c, B[j]);
+        epsS[j] = tol * tol * bb[j];
+        zero(c, X[j].parity(1));
+    }
+    auto true_res = [&](int j, double &rrS, double &rrN) {
+        const Spinor xo = X[j].parity(1);
+        apply_schur(c, op, PREC_D, *t1, xo, *te, 0);
+        run_site(c, OpSubNorm<SpinorD, SpinorD, SpinorD>{(**bp[j]).d(), (*t1).d(), (*rS).d(), c->d_scal}, 1);
+        copy(c, *t1, *rS);
+        gamma5_inplace(c, *t1);
+        apply_schur(c, op, PREC_D, *rN, *t1, *te, 1);
+        run_site(c, OpNorm<SpinorD>{(*rN).d(), c->d_scal + 1}, 1);
+        CK(cudaMemcpyAsync(c->h_scal, c->d_scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        rrS = c->h_scal[0];
+        rrN = c->h_scal[1];
+    };
+    auto slot_f = [&](const BVec &v, int j) { return v.f().bind(j); };
+    // p_j = a r_j + b p_j, in the precision of p
+    auto set_direction = [&](int j, double b) {
+        if (sprec == PREC_F) axpby_views(c, slot_f(rs, j), ps.f().bind(j), C2(1.0), C2(b));
+        else axpby_views(c, slot_f(rs, j), ps.h().bind(j), C2(1.0), C2(b));
+    };
+    CK(cudaMemsetAsync(xs.s.v, 0, xs.bytes, c->st));
+    CK(cudaMemsetAsync(rs.s.v, 0, rs.bytes, c->st));
+    CK(cudaMemsetAsync(ps.s.v, 0, ps.bytes, c->st));
+    BatchCGState &H = *(BatchCGState *)c->h_state;
+    static_assert(sizeof(BatchCGState) <= kStateBytes, "state buffer too small");
+    memset(&H, 0, sizeof(H));
+    H.nb = nb;
+    H.max_iter = max_steps;
+    H.delta2 = delta * delta;
+    std::vector<int> iters(m, 0), updates(m, 0), done(m, 0);
+    for (int j = 0; j < m; ++j) {
+        double rrS, rrN;
+        true_res(j, rrS, rrN);
+        if (rrS < epsS[j] || bb[j] == 0.0) {
+            done[j] = 1;
+            continue;
+        }
+        axpby_views(c, (*rN).d(), slot_f(rs, j), C2(1.0), C2(0.0));
+        set_direction(j, 0.0);
+        BatchCGState &W = *(BatchCGState *)c->h_state;
+        W.active[j] = 1;
+        W.rr[j] = W.rr_max[j] = rrN;
+        W.eps[j] = epsS[j] * (rrN / rrS);
+    }
+    CK(cudaMemcpyAsync(c->d_state, c->h_state, sizeof(BatchCGState), cudaMemcpyHostToDevice, c->st));
+    BatchCGState *S = (BatchCGState *)c->d_state;
+    Gate gate{&S->pause, nullptr};
+    const int lognb = xs.s.lognb;
+    auto step = [&]() {
+        apply_schur_batch(c, op, sprec, tos.s, ps.s, tes.s, 1, &S->pause, S->active);
+        apply_schur_batch(c, op, sprec, aps.s, tos.s, tes.s, 1, &S->pause, S->active);
+        if (sprec == PREC_F) {
+            run_batch(c, OpBAlpha<SpinorFB, SpinorFB>{ps.f(), aps.f(), S}, lognb, gate);
+            run_batch(c, OpBUpdate<SpinorFB, SpinorFB, SpinorFB, SpinorFB>{xs.f(), ps.f(), rs.f(), aps.f(), S}, lognb,
+                      gate);
+            run_batch(c, OpBDirection<SpinorFB, SpinorFB>{ps.f(), rs.f(), S}, lognb, gate);
+        } else {
+            run_batch(c, OpBAlpha<SpinorHB, SpinorHB>{ps.h(), aps.h(), S}, lognb, gate);
+            run_batch(c, OpBUpdate<SpinorFB, SpinorHB, SpinorFB, SpinorHB>{xs.f(), ps.h(), rs.f(), aps.h(), S}, lognb,
+                      gate);
+            run_batch(c, OpBDirection<SpinorHB, SpinorFB>{ps.h(), rs.f(), S}, lognb, gate);
+        }
+    };
+    auto direction_rest = [&]() {  // the direction update the pause skipped, for RHS without an update
+        if (sprec == PREC_F) run_batch(c, OpBDirection<SpinorFB, SpinorFB>{ps.f(), rs.f(), S}, lognb);
+        else run_batch(c, OpBDirection<SpinorHB, SpinorFB>{ps.h(), rs.f(), S}, lognb);
+    };
+    auto any_active = [&]() {
+        for (int j = 0; j < m; ++j)
+            if (((BatchCGState *)c->h_state)->active[j]) return true;
+        return false;
+    };
+    for (int outer = 0; outer < 100000 && any_active(); ++outer) {
+        const int left = max_steps - ((BatchCGState *)c->h_state)->iter;
+        if (left <= 0) break;
+        run_gated_state(c, S, step, 8, (long)left + 8);
+        BatchCGState R = *(BatchCGState *)c->h_state;
+        if (R.failed) fail(c, LYM_ERR_NUMERIC, "block CG produced a non-finite residual");
+        direction_rest();
+        for (int j = 0; j < m; ++j) {
+            if (!R.active[j] || !R.need_update[j]) continue;
+            // reliable update: x_j += x_sloppy_j in FP64, recompute the true residuals
+            axpby_views(c, slot_f(xs, j), X[j].parity(1).d(), C2(1.0), C2(1.0));
+            axpby_views(c, slot_f(xs, j), slot_f(xs, j), C2(0.0), C2(0.0));
+            double rrS, rrN;
+            true_res(j, rrS, rrN);
+            ++updates[j];
+            if (rrS < epsS[j]) {
+                R.active[j] = 0;
+                done[j] = 1;
+                iters[j] = R.iter;
+            } else {
+                if (R.converged[j]) R.eps[j] = std::max(R.eps[j] * 0.5 * epsS[j] / rrS, 1e-300);
+                axpby_views(c, (*rN).d(), slot_f(rs, j), C2(1.0), C2(0.0));
+                set_direction(j, rrN / R.rr_prev[j]);
+                R.rr[j] = R.rr_max[j] = rrN;
+            }
+            R.converged[j] = 0;
+            R.need_update[j] = 0;
+        }
+        R.pause = 0;
+        *(BatchCGState *)c->h_state = R;
+        CK(cudaMemcpyAsync(c->d_state, c->h_state, sizeof(BatchCGState), cudaMemcpyHostToDevice, c->st));
+        if (R.iter >= max_steps) break;
+    }
+    BatchCGState R = *(BatchCGState *)c->h_state;
+    int rc = LYM_OK;
+    for (int j = 0; j < m; ++j) {
+        if (R.active[j]) {  // out of iterations: keep the progress of the sloppy solution
+            axpby_views(c, slot_f(xs, j), X[j].parity(1).d(), C2(1.0), C2(1.0));
+            iters[j] = R.iter;
+            rc = LYM_NOT_CONVERGED;
+        }
+        schur_reconstruct(c, op, B[j], X[j]);
+        if (st) {
+            st[j].iterations = iters[j];
+            st[j].steps = iters[j];
+            st[j].reliable_updates = updates[j];
+            st[j].converged = done[j];
+            st[j].true_residual = true_residual(c, op, B[j], X[j]);
+        }
+        delete bp[j];
+    }
+    return rc;
+}
+
 }  // namespace
 
 // =============================================================== C ABI =====
@@ -980,6 +1206,7 @@ int lym_context_create(const int dims[4], int rep, int device, lym_context **out
         CK(cudaSetDevice(device));
         CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
         c->partials = (double *)dev_alloc(c, (size_t)kBlasGridMax * kMaxRed * sizeof(double));
+        c->bpartials = (double *)dev_alloc(c, (size_t)kBlasGridMax * kMaxBatch * 4 * sizeof(double));
         c->counter = (unsigned int *)dev_alloc(c, 64);
         c->d_err = (int *)dev_alloc(c, 64);
         c->d_state = dev_alloc(c, kStateBytes);
@@ -1018,6 +1245,7 @@ void lym_context_destroy(lym_context *c)
     for (auto &s : c->pool) cudaFree(s.v);
     for (int k = 0; k < 3; ++k) cudaFree(c->aos[k]);
     cudaFree(c->partials);
+    cudaFree(c->bpartials);
     cudaFree(c->counter);
     cudaFree(c->d_err);
     cudaFree(c->d_state);
@@ -1380,6 +1608,79 @@ int lym_solve_device(lym_context *c, int op_id, int solver, double precision, in
     return do_solve(c, op_id, solver, precision, max_steps, source, solution, guess, stats, true, false, C2(0.0));
 }
 
+static int do_solve_block(lym_context *c, int op_id, int solver, double precision, int max_steps, int nrhs,
+                          const double *const *sources, double *const *solutions, int batch, lym_solve_stats *stats,
+                          bool device_ptr)
+{
+    if (!sources || !solutions || nrhs < 1 || max_steps < 0) return LYM_ERR_ARGUMENT;
+    if (batch == 0) batch = 16;
+    if (batch < 1 || batch > kMaxBatch || (batch & (batch - 1))) return LYM_ERR_ARGUMENT;
+    for (int j = 0; j < nrhs; ++j)
+        if (!sources[j] || !solutions[j]) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        OpEntry &op = op_of(c, op_id);
+        if (op.kind != LYM_OP_IMPROVED && op.kind != LYM_OP_DIRAC_WILSON)
+            fail(c, LYM_ERR_UNSUPPORTED, "block solves solve D x = b for a DiracWilson/Improved operator");
+        if (solver != LYM_SOLVER_EO_CG_MIXED_SINGLE && solver != LYM_SOLVER_EO_CG_MIXED_HALF)
+            fail(c, LYM_ERR_UNSUPPORTED, "block solves use LYM_SOLVER_EO_CG_MIXED_SINGLE or _HALF");
+        const int sp = solver == LYM_SOLVER_EO_CG_MIXED_SINGLE ? PREC_F : PREC_H;
+        const double tol = precision <= 0.0 ? (precision == 0.0 ? 1e-10 : -precision) : std::sqrt(precision);
+        int rc_all = LYM_OK;
+        for (int c0 = 0; c0 < nrhs; c0 += batch) {
+            const int m = std::min(batch, nrhs - c0);
+            std::vector<Vec *> bv, xv;
+            std::vector<Spinor> B, X;
+            for (int j = 0; j < m; ++j) {
+                bv.push_back(new Vec(c, PREC_D, 2));
+                xv.push_back(new Vec(c, PREC_D, 2));
+                B.push_back(**bv.back());
+                X.push_back(**xv.back());
+                upload_vec(c, B[j], sources[c0 + j], device_ptr, 0);
+                if (!device_ptr) CK(cudaStreamSynchronize(c->st));  // the staging buffer is reused
+            }
+            CK(cudaEventRecord(c->ev0, c->st));
+            int rc;
+            try {
+                rc = eo_cg_chunk(c, op, sp, batch, m, B, X, tol, max_steps, stats ? stats + c0 : nullptr);
+            } catch (...) {
+                for (auto v : bv) delete v;
+                for (auto v : xv) delete v;
+                throw;
+            }
+            CK(cudaEventRecord(c->ev1, c->st));
+            for (int j = 0; j < m; ++j) {
+                download_vec(c, solutions[c0 + j], X[j], device_ptr, 2);
+                if (!device_ptr) CK(cudaStreamSynchronize(c->st));
+            }
+            CK(cudaStreamSynchronize(c->st));
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+            if (stats)
+                for (int j = 0; j < m; ++j) {
+                    stats[c0 + j].seconds = ms * 1e-3;
+                    stats[c0 + j].last_error = 0.0;
+                }
+            for (auto v : bv) delete v;
+            for (auto v : xv) delete v;
+            if (rc != LYM_OK) rc_all = rc;
+        }
+        CK(cudaGetLastError());
+        return rc_all;
+    });
+}
+
+int lym_solve_block(lym_context *c, int op_id, int solver, double precision, int max_steps, int nrhs,
+                    const double *const *sources, double *const *solutions, int batch, lym_solve_stats *stats)
+{
+    return do_solve_block(c, op_id, solver, precision, max_steps, nrhs, sources, solutions, batch, stats, false);
+}
+
+int lym_solve_block_device(lym_context *c, int op_id, int solver, double precision, int max_steps, int nrhs,
+                           const double *const *sources, double *const *solutions, int batch, lym_solve_stats *stats)
+{
+    return do_solve_block(c, op_id, solver, precision, max_steps, nrhs, sources, solutions, batch, stats, true);
+}
+
 int lym_solve_shifted(lym_context *c, int op_id, double sre, double sim, double precision, int max_steps,
                       const double *source, double *solution, const double *guess, lym_solve_stats *stats)
 {
@@ -1533,6 +1834,51 @@ int lym_time_stencil(lym_context *c, int op_id, int prec, int which, int iters, 
         for (int k = 0; k < 3; ++k) launch_dslash(P, c->st);
         CK(cudaEventRecord(c->ev0, c->st));
         for (int k = 0; k < iters; ++k) launch_dslash(P, c->st);
+        CK(cudaEventRecord(c->ev1, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        CK(cudaGetLastError());
+        count(c, iters + 3);
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+        *ms_per_launch = (double)ms / iters;
+        return LYM_OK;
+    });
+}
+
+int lym_time_stencil_batch(lym_context *c, int op_id, int prec, int which, int batch, int iters,
+                           double *ms_per_launch)
+{
+    if (!ms_per_launch || iters < 1 || (prec != PREC_F && prec != PREC_H) || which < 0 || which > 1 ||
+        batch < 1 || batch > kMaxBatch || (batch & (batch - 1)))
+        return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        OpEntry &op = op_of(c, op_id);
+        GaugeEntry &ge = gauge_of(c, op.gauge_id);
+        const bool clov = kind_has_clover(op.kind);
+        if (clov) ensure_clover(c, op);
+        require_recon(c, ge, prec);
+        BVec a(c, prec, batch), b(c, prec, batch), y(c, prec, batch);
+        DslashBatchParams P;
+        P.g = c->g;
+        P.prec = prec;
+        P.rep = c->rep;
+        P.U = &ge.dev;
+        if (which == 0) {
+            P.epi = EPI_XPAY_;
+            P.parity = 1;
+            P.clover = clov ? op.clover.T[prec] : nullptr;
+            P.b = -op.kappa * op.kappa;
+        } else {
+            P.epi = clov ? EPI_CLOVINV_ : EPI_SCALE_;
+            P.parity = 0;
+            P.clover = clov ? op.clover.Tinv[prec] : nullptr;
+        }
+        P.in = a.s;
+        P.out = b.s;
+        P.y = y.s;
+        for (int k = 0; k < 3; ++k) launch_dslash_batch(P, c->st);
+        CK(cudaEventRecord(c->ev0, c->st));
+        for (int k = 0; k < iters; ++k) launch_dslash_batch(P, c->st);
         CK(cudaEventRecord(c->ev1, c->st));
         CK(cudaStreamSynchronize(c->st));
         CK(cudaGetLastError());

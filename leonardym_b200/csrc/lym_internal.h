@@ -80,3 +80,26 @@ void launch_stencil_index_probe(const Geom &g, int *out, cudaStream_t st);
 void launch_convert(const Geom &g, const Spinor &dst, const Spinor &src, cudaStream_t st);
 
 }  // namespace lym
+
+namespace lym {
+// A batch of nb right-hand sides of one parity, interleaved (see lym_batch.cuh).
+struct SpinorBatch {
+    int prec = PREC_F;   // PREC_F or PREC_H
+    int nb = 0, lognb = 0, stride = 0;
+    void *v = nullptr;
+    float *norm = nullptr;
+};
+
+struct DslashBatchParams {
+    Geom g;
+    int prec = PREC_F, rep = REP_SU3, epi = EPI_SCALE_, parity = 0, gamma5 = 0;
+    SpinorBatch in, out, y;
+    const GaugeDev *U = nullptr;
+    const void *clover = nullptr;
+    double a = 1.0, b = 0.0;
+    const int *skip_if = nullptr;
+    const int *active = nullptr;
+};
+
+void launch_dslash_batch(const DslashBatchParams &P, cudaStream_t st);
+}  // namespace lym

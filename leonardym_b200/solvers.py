@@ -142,6 +142,26 @@ class EvenOddConjugateGradient(Solver):
     def solve(self, dirac, source, solution, initial_guess=None):
         return self._run(dirac, source, solution, initial_guess, self.MODES[self.mode], -self.tolerance)
 
+    def solve_block(self, dirac, sources, solutions=None, batch=16):
+        """Solve D x_j = b_j for many sources through the batched stencil (lym_solve_block).
+        Returns (all_converged, solutions); per-source statistics land in self.block_stats."""
+        if self.mode == "double":
+            raise LymError(-4, "block solves run the mixed-precision inner iterations ('single' or 'half')")
+        lat = dirac.lattice
+        srcs = [dirac._vec(s) for s in sources]
+        if solutions is None:
+            solutions = [lat.new_vector() for _ in srcs]
+        n = len(srcs)
+        sp = (C.c_void_p * n)(*[s.ctypes.data for s in srcs])
+        xp = (C.c_void_p * n)(*[x.ctypes.data for x in solutions])
+        stats = (SolveStats * n)()
+        rc = lib().lym_solve_block(lat.handle, dirac.op_id, self.MODES[self.mode], -self.tolerance,
+                                   int(self.maxSteps), n, sp, xp, int(batch), stats)
+        if rc < 0:
+            raise LymError(rc, lib().lym_last_error(lat.handle).decode())
+        self.block_stats = [stats[j] for j in range(n)]
+        return rc == 0, solutions
+
 
 class MultishiftSolver:
     """inverters/MultishiftSolver.h:11-44; epsilon 1e-8, 3000 steps by default

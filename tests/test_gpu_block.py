@@ -1,0 +1,48 @@
+"""Many right-hand sides through the batched stencil (lym_solve_block): every result
+meets the 1e-10 true residual re-measured with the FP64 oracle operator, and equals
+the same source solved alone within what the 1e-10 residual allows."""
+import numpy as np
+import pytest
+
+import leonardym_b200 as L
+from leonardym_b200 import synth
+from tests.helpers import CONFIGS, links_for, rel
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", params=["su3", "su2adj"])
+def setup(request, oracle):
+    dims, rep, eps, kappa, csw = CONFIGS[request.param]
+    links = links_for(request.param)
+    lat = L.Lattice(dims, rep)
+    op = L.ImprovedDiracWilsonOperator(lat, kappa, csw, gamma5=False)
+    op.setLattice(links)
+    D = oracle.Operator(oracle.Geometry(dims), links, "Improved", kappa, csw, False)
+    srcs = [synth.point_source(dims, 3, a, 1) for a in range(2)] + \
+           [synth.z2_source(dims, 3, 5, stream=(1 << 21) + k) for k in range(2)] + \
+           [synth.gaussian_spinor(dims, 3, 40 + k) for k in range(2)]
+    yield dict(lat=lat, op=op, D=D, srcs=srcs)
+    lat.close()
+
+
+@pytest.mark.parametrize("mode", ["single", "half"])
+@pytest.mark.parametrize("batch", [4, 8])
+def test_block_solve_alone_and_in_the_mix(setup, mode, batch):
+    s = L.EvenOddConjugateGradient(mode, 1e-10)
+    ok, sols = s.solve_block(setup["op"], setup["srcs"], batch=batch)
+    assert ok
+    for j, (b, x) in enumerate(zip(setup["srcs"], sols)):
+        r = np.linalg.norm(b - setup["D"].multiply(x)) / np.linalg.norm(b)
+        assert r <= 1e-10, (j, r)
+        assert s.block_stats[j].true_residual <= 1e-10
+        alone = setup["lat"].new_vector()
+        single = L.EvenOddConjugateGradient(mode, 1e-10)
+        assert single.solve(setup["op"], b, alone)
+        assert rel(x, alone) < 1e-8
+
+
+def test_block_rejects_bad_batch(setup):
+    s = L.EvenOddConjugateGradient("single", 1e-10)
+    with pytest.raises(L.LymError):
+        s.solve_block(setup["op"], setup["srcs"], batch=3)
