@@ -198,6 +198,36 @@ int lym_multishift_device(lym_context *ctx, int op_id, int algorithm, int nshift
                           double precision, int max_steps, const double *source, double **solutions,
                           lym_solve_stats *stats);
 
+/* ---- solve server (no reference counterpart: the reference has no serving mode) -------
+ * Keeps gauge fields resident by key (one context, CUDA stream and worker thread per
+ * field, so work on different fields overlaps on the device) and serves solve requests
+ * D x_k = b_k (an Improved operator: kappa, c_sw; 1..n sources; relative tolerance on the
+ * true residual) with the block mixed-precision even-odd CG.  Sources of all requests on a
+ * field are continuously batched: they enter free slots of the running batch as earlier
+ * ones finish, whatever their kappa.  A request's clover term is built when its first
+ * source is admitted and freed with its last; a new clover term is admitted only while
+ * the server's device memory stays within hbm_budget_bytes (0 = no limit).  Host source /
+ * solution buffers must stay valid until lym_server_wait returns for the ticket. */
+typedef struct lym_server lym_server;
+typedef struct {
+    double latency_s;          /* submit -> last solution written                   */
+    double queue_s;            /* submit -> first source admitted into a slot       */
+    int nsrc;
+    int max_iterations;        /* over the request's sources                        */
+    double max_true_residual;  /* ||b - D x|| / ||b|| re-measured in FP64, worst source */
+    int converged;
+    int status;                /* lym_status of the request                         */
+} lym_request_stats;
+int lym_server_create(int device, size_t hbm_budget_bytes, int batch, int precision, lym_server **server);
+void lym_server_destroy(lym_server *server);
+const char *lym_server_last_error(lym_server *server);
+size_t lym_server_device_bytes(lym_server *server);
+int lym_server_add_gauge(lym_server *server, int key, const int dims[4], int rep, const double *fermion_links);
+int lym_server_submit(lym_server *server, int key, double kappa, double csw, int nsrc, const double *const *sources,
+                      double *const *solutions, double tol, int max_steps, long long *ticket);
+int lym_server_wait(lym_server *server, long long ticket, double timeout_s, lym_request_stats *stats);
+int lym_server_poll(lym_server *server, long long ticket, int *done);
+
 /* ---- layout self-checks (no reference counterpart: test hooks for the layout) --------
  * reference-order neighbour tables sup/sdn [V][4] (LocalLayout.h:34-110, Lattice.h:201-207)
  * and the stencil's computed indices [2][V/2][9] (own site, 8 neighbour half-indices). */

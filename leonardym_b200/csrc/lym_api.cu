@@ -1,6 +1,7 @@
 // C ABI of the library: contexts, resident gauge fields, operators, operator
 // application and the Krylov solvers.  See include/lym_b200.h for the contract.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -54,6 +55,7 @@ struct lym_context {
     // reductions
     double *partials = nullptr;
     double *bpartials = nullptr;  // per-RHS partial sums of the batched reductions
+    int *nbr = nullptr;           // neighbour half-site table [2][8][stride] (batched stencil)
     unsigned int *counter = nullptr;
     int *d_err = nullptr;
     void *d_state = nullptr;      // solver state (device)
@@ -994,25 +996,28 @@ template <class Op> void run_batch(lym_context *c, const Op &op, int lognb, Gate
     site_batch_kernel<Op><<<grid, kBlasThreads, 0, c->st>>>(op, c->g.Vh, lognb, c->bpartials, c->counter, gate);
 }
 
-// Schur complement on a batch: out_r = G5^g (T_oo in_r - kappa^2 H_oe T_ee^-1 H_eo in_r)
-void apply_schur_batch(lym_context *c, OpEntry &op, int prec, const SpinorBatch &out, const SpinorBatch &in,
-                       const SpinorBatch &tmp, int gamma5, const int *skip, const int *active)
+// Schur complement on a batch whose slots share the gauge field and may carry their own
+// kappa and clover terms (per-slot tables b_slot = -kappa^2, T, Tinv in device memory):
+//   out_r = G5^g (T_oo,r in_r - kappa_r^2 H_oe T_ee,r^-1 H_eo in_r)
+void apply_schur_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, const SpinorBatch &out,
+                       const SpinorBatch &in, const SpinorBatch &tmp, int gamma5, const int *skip, const int *active,
+                       const double *b_slot, const void *const *T_slot, const void *const *Ti_slot)
 {
-    GaugeEntry &ge = gauge_of(c, op.gauge_id);
-    const bool clov = kind_has_clover(op.kind);
     DslashBatchParams P;
     P.g = c->g;
     P.prec = prec;
     P.rep = c->rep;
-    P.U = &ge.dev;
+    P.U = &U;
     P.skip_if = skip;
     P.active = active;
+    P.nbr = c->nbr;
     P.epi = clov ? EPI_CLOVINV_ : EPI_SCALE_;
     P.parity = 0;
     P.in = in;
     P.out = tmp;
     P.y = tmp;
-    P.clover = clov ? op.clover.Tinv[prec] : nullptr;
+    P.clover = clov ? Ti_slot : nullptr;  // non-null marks "has clover"; the bases come from the table
+    P.clover_slot = clov ? Ti_slot : nullptr;
     P.a = 1.0;
     launch_dslash_batch(P, c->st);
     P.epi = EPI_XPAY_;
@@ -1020,8 +1025,9 @@ void apply_schur_batch(lym_context *c, OpEntry &op, int prec, const SpinorBatch 
     P.in = tmp;
     P.out = out;
     P.y = in;
-    P.clover = clov ? op.clover.T[prec] : nullptr;
-    P.b = -op.kappa * op.kappa;
+    P.clover = clov ? T_slot : nullptr;
+    P.clover_slot = clov ? T_slot : nullptr;
+    P.b_slot = b_slot;
     P.gamma5 = gamma5;
     launch_dslash_batch(P, c->st);
     count(c, 2);
@@ -1033,78 +1039,228 @@ template <class X, class Y> void axpby_views(lym_context *c, const X &x, const Y
     run_site(c, OpAxpby<X, Y>{x, y, a, b}, 1);
 }
 
-// Even-odd CG on (gamma5 S)^2 for m <= nb right-hand sides at once (chunk of a block
-// solve): one batched stencil serves every RHS, each RHS keeps its own FP64 scalars,
-// convergence mask and FP64 reliable updates.  B: full FP64 sources, X: full FP64
-// solutions (odd sites are the CG unknowns; even sites reconstructed).
-int eo_cg_chunk(lym_context *c, OpEntry &op, int sprec, int nb, int m, const std::vector<Spinor> &B,
-                const std::vector<Spinor> &X, double tol, int max_steps, lym_solve_stats *st)
-{
-    const double delta = 0.1;
-    if (kind_has_clover(op.kind)) ensure_clover(c, op);
-    require_recon(c, gauge_of(c, op.gauge_id), sprec);
-    Vec te(c, PREC_D, 1), t1(c, PREC_D, 1), rS(c, PREC_D, 1), rN(c, PREC_D, 1);
-    BVec xs(c, PREC_F, nb), rs(c, PREC_F, nb), ps(c, sprec, nb), aps(c, sprec, nb), tes(c, sprec, nb),
-        tos(c, sprec, nb);
-    std::vector<Vec *> bp(m);
-    std::vector<double> epsS(m), bb(m);
-    for (int j = 0; j < m; ++j) {
-        bp[j] = new Vec(c, PREC_D, 1);
-        schur_source(c, op, B[j], **bp[j]);
-        bb[j] = norm2_now(c, B[j]);
-        epsS[j] = tol * tol * bb[j];
-        zero(c, X[j].parity(1));
+// Block even-odd CG engine: nb slots on one resident gauge field.  Every slot solves its
+// own D_slot x = b (its own kappa / clover term) by CG on (gamma5 S)^2 with its own FP64
+// scalars, convergence mask and FP64 reliable updates; one batched stencil serves all
+// slots.  Slots are filled with add(), advanced together with advance(), and can be
+// refilled as soon as they finish (continuous batching).  The engine uses the context's
+// device solver state exclusively while it lives.
+class BlockEngine {
+public:
+    struct Slot {
+        bool busy = false, finished = false;
+        OpEntry *op = nullptr;
+        Spinor B, X;
+        Vec *bp = nullptr;
+        double epsS = 0.0, bb = 0.0;
+        int start_iter = 0, iters = 0, updates = 0, max_iter = 0, converged = 0;
+        long long tag = -1;
+    };
+
+    BlockEngine(lym_context *ctx, int sprec_, int nb_)
+        : c(ctx), sprec(sprec_), nb(nb_), te(ctx, PREC_D, 1), t1(ctx, PREC_D, 1), rS(ctx, PREC_D, 1),
+          rN(ctx, PREC_D, 1), xs(ctx, PREC_F, nb_), rs(ctx, PREC_F, nb_), ps(ctx, sprec_, nb_), aps(ctx, sprec_, nb_),
+          tes(ctx, sprec_, nb_), tos(ctx, sprec_, nb_)
+    {
+        tables = (char *)dev_alloc(c, 3 * kMaxBatch * sizeof(double));
+        d_b = (double *)tables;
+        d_T = (const void **)(tables + kMaxBatch * sizeof(double));
+        d_Ti = (const void **)(tables + 2 * kMaxBatch * sizeof(double));
+        CK(cudaMemsetAsync(xs.s.v, 0, xs.bytes, c->st));
+        CK(cudaMemsetAsync(rs.s.v, 0, rs.bytes, c->st));
+        CK(cudaMemsetAsync(ps.s.v, 0, ps.bytes, c->st));
+        memset(&hs, 0, sizeof(hs));
+        hs.nb = nb;
+        hs.delta2 = 0.01;  // reliable update when the recursive residual fell by 10x
+        static_assert(sizeof(BatchCGState) <= kStateBytes, "state buffer too small");
     }
-    auto true_res = [&](int j, double &rrS, double &rrN) {
-        const Spinor xo = X[j].parity(1);
-        apply_schur(c, op, PREC_D, *t1, xo, *te, 0);
-        run_site(c, OpSubNorm<SpinorD, SpinorD, SpinorD>{(**bp[j]).d(), (*t1).d(), (*rS).d(), c->d_scal}, 1);
+    ~BlockEngine()
+    {
+        for (int j = 0; j < nb; ++j) delete slot[j].bp;
+        dev_free(c, tables, 3 * kMaxBatch * sizeof(double));
+    }
+
+    int free_slot() const
+    {
+        for (int j = 0; j < nb; ++j)
+            if (!slot[j].busy) return j;
+        return -1;
+    }
+    bool working() const
+    {
+        for (int j = 0; j < nb; ++j)
+            if (slot[j].busy && !slot[j].finished) return true;
+        return false;
+    }
+    const Slot &info(int j) const { return slot[j]; }
+
+    // Puts D x = b in slot j.  B, X: full FP64 spinors that stay alive until release(j).
+    void add(int j, OpEntry &op, const Spinor &B, const Spinor &X, double tol, int max_iter, long long tag)
+    {
+        const bool clov = kind_has_clover(op.kind);
+        if (gauge_id < 0) {
+            gauge_id = op.gauge_id;
+            has_clover = clov;
+        } else if (op.gauge_id != gauge_id || clov != has_clover) {
+            fail(c, LYM_ERR_ARGUMENT, "the slots of one batch share the gauge field and operator kind");
+        }
+        if (clov) ensure_clover(c, op);
+        require_recon(c, gauge_of(c, op.gauge_id), sprec);
+        Slot &s = slot[j];
+        delete s.bp;
+        s = Slot();
+        s.busy = true;
+        s.op = &op;
+        s.B = B;
+        s.X = X;
+        s.tag = tag;
+        s.max_iter = max_iter;
+        s.start_iter = hs.iter;
+        s.bp = new Vec(c, PREC_D, 1);
+        schur_source(c, op, B, **s.bp);
+        s.bb = norm2_now(c, B);
+        s.epsS = tol * tol * s.bb;
+        zero(c, X.parity(1));
+        const double b = -op.kappa * op.kappa;
+        const void *T = clov ? op.clover.T[sprec] : nullptr, *Ti = clov ? op.clover.Tinv[sprec] : nullptr;
+        CK(cudaMemcpyAsync(d_b + j, &b, sizeof(double), cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(d_T + j, &T, sizeof(void *), cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(d_Ti + j, &Ti, sizeof(void *), cudaMemcpyHostToDevice, c->st));
+        axpby_views(c, xs.f().bind(j), xs.f().bind(j), C2(0.0), C2(0.0));
+        double rrS, rrN;
+        true_res(j, rrS, rrN);  // synchronises: the host values above were consumed
+        if (rrS < s.epsS || s.bb == 0.0) {
+            s.converged = 1;
+            finish(j);
+            return;
+        }
+        axpby_views(c, (*rN).d(), rs.f().bind(j), C2(1.0), C2(0.0));
+        set_direction(j, 0.0);
+        hs.active[j] = 1;
+        hs.rr[j] = hs.rr_max[j] = rrN;
+        hs.eps[j] = s.epsS * (rrN / rrS);
+        hs.converged[j] = hs.need_update[j] = 0;
+    }
+
+    // Iterates all working slots until some slot needs the host (reliable update, done,
+    // iteration limit).  Returns the slots that finished since the last call.
+    std::vector<int> advance()
+    {
+        if (working() && any_active()) {
+            int left = 1 << 30;
+            for (int j = 0; j < nb; ++j)
+                if (slot[j].busy && !slot[j].finished && hs.active[j])
+                    left = std::min(left, slot[j].max_iter - (hs.iter - slot[j].start_iter));
+            left = std::max(left, 1);
+            hs.max_iter = hs.iter + left;
+            hs.pause = 0;
+            *(BatchCGState *)c->h_state = hs;
+            CK(cudaMemcpyAsync(c->d_state, c->h_state, sizeof(BatchCGState), cudaMemcpyHostToDevice, c->st));
+            BatchCGState *S = (BatchCGState *)c->d_state;
+            run_gated_state(c, S, [&]() { step(S); }, 8, (long)left + 8);
+            hs = *(BatchCGState *)c->h_state;
+            if (hs.failed) fail(c, LYM_ERR_NUMERIC, "block CG produced a non-finite residual");
+            direction_rest(S);
+            for (int j = 0; j < nb; ++j) {
+                Slot &s = slot[j];
+                if (!s.busy || s.finished || !hs.active[j]) continue;
+                if (hs.need_update[j]) reliable_update(j);
+                if (!s.finished && hs.iter - s.start_iter >= s.max_iter) {
+                    axpby_views(c, xs.f().bind(j), s.X.parity(1).d(), C2(1.0), C2(1.0));
+                    finish(j);
+                }
+            }
+        }
+        std::vector<int> out;
+        out.swap(done_list);
+        return out;
+    }
+
+    // forget a finished slot (its B and X are the caller's again)
+    void release(int j)
+    {
+        delete slot[j].bp;
+        slot[j] = Slot();
+        hs.active[j] = 0;
+    }
+
+private:
+    lym_context *c;
+    int sprec, nb;
+    Vec te, t1, rS, rN;
+    BVec xs, rs, ps, aps, tes, tos;
+    char *tables = nullptr;
+    double *d_b = nullptr;
+    const void **d_T = nullptr, **d_Ti = nullptr;
+    int gauge_id = -1;
+    bool has_clover = false;
+    Slot slot[kMaxBatch];
+    BatchCGState hs;
+    std::vector<int> done_list;
+
+    bool any_active() const
+    {
+        for (int j = 0; j < nb; ++j)
+            if (hs.active[j]) return true;
+        return false;
+    }
+    void true_res(int j, double &rrS, double &rrN)
+    {
+        Slot &s = slot[j];
+        const Spinor xo = s.X.parity(1);
+        apply_schur(c, *s.op, PREC_D, *t1, xo, *te, 0);
+        run_site(c, OpSubNorm<SpinorD, SpinorD, SpinorD>{(**s.bp).d(), (*t1).d(), (*rS).d(), c->d_scal}, 1);
         copy(c, *t1, *rS);
         gamma5_inplace(c, *t1);
-        apply_schur(c, op, PREC_D, *rN, *t1, *te, 1);
+        apply_schur(c, *s.op, PREC_D, *rN, *t1, *te, 1);
         run_site(c, OpNorm<SpinorD>{(*rN).d(), c->d_scal + 1}, 1);
         CK(cudaMemcpyAsync(c->h_scal, c->d_scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
         CK(cudaStreamSynchronize(c->st));
         rrS = c->h_scal[0];
         rrN = c->h_scal[1];
-    };
-    auto slot_f = [&](const BVec &v, int j) { return v.f().bind(j); };
-    // p_j = a r_j + b p_j, in the precision of p
-    auto set_direction = [&](int j, double b) {
-        if (sprec == PREC_F) axpby_views(c, slot_f(rs, j), ps.f().bind(j), C2(1.0), C2(b));
-        else axpby_views(c, slot_f(rs, j), ps.h().bind(j), C2(1.0), C2(b));
-    };
-    CK(cudaMemsetAsync(xs.s.v, 0, xs.bytes, c->st));
-    CK(cudaMemsetAsync(rs.s.v, 0, rs.bytes, c->st));
-    CK(cudaMemsetAsync(ps.s.v, 0, ps.bytes, c->st));
-    BatchCGState &H = *(BatchCGState *)c->h_state;
-    static_assert(sizeof(BatchCGState) <= kStateBytes, "state buffer too small");
-    memset(&H, 0, sizeof(H));
-    H.nb = nb;
-    H.max_iter = max_steps;
-    H.delta2 = delta * delta;
-    std::vector<int> iters(m, 0), updates(m, 0), done(m, 0);
-    for (int j = 0; j < m; ++j) {
+    }
+    void set_direction(int j, double b)  // p_j = r_j + b p_j in the precision of p
+    {
+        if (sprec == PREC_F) axpby_views(c, rs.f().bind(j), ps.f().bind(j), C2(1.0), C2(b));
+        else axpby_views(c, rs.f().bind(j), ps.h().bind(j), C2(1.0), C2(b));
+    }
+    void reliable_update(int j)
+    {
+        Slot &s = slot[j];
+        axpby_views(c, xs.f().bind(j), s.X.parity(1).d(), C2(1.0), C2(1.0));
+        axpby_views(c, xs.f().bind(j), xs.f().bind(j), C2(0.0), C2(0.0));
         double rrS, rrN;
         true_res(j, rrS, rrN);
-        if (rrS < epsS[j] || bb[j] == 0.0) {
-            done[j] = 1;
-            continue;
+        ++s.updates;
+        if (rrS < s.epsS) {
+            s.converged = 1;
+            finish(j);
+        } else {
+            if (hs.converged[j]) hs.eps[j] = std::max(hs.eps[j] * 0.5 * s.epsS / rrS, 1e-300);
+            axpby_views(c, (*rN).d(), rs.f().bind(j), C2(1.0), C2(0.0));
+            set_direction(j, rrN / hs.rr_prev[j]);
+            hs.rr[j] = hs.rr_max[j] = rrN;
         }
-        axpby_views(c, (*rN).d(), slot_f(rs, j), C2(1.0), C2(0.0));
-        set_direction(j, 0.0);
-        BatchCGState &W = *(BatchCGState *)c->h_state;
-        W.active[j] = 1;
-        W.rr[j] = W.rr_max[j] = rrN;
-        W.eps[j] = epsS[j] * (rrN / rrS);
+        hs.converged[j] = 0;
+        hs.need_update[j] = 0;
     }
-    CK(cudaMemcpyAsync(c->d_state, c->h_state, sizeof(BatchCGState), cudaMemcpyHostToDevice, c->st));
-    BatchCGState *S = (BatchCGState *)c->d_state;
-    Gate gate{&S->pause, nullptr};
-    const int lognb = xs.s.lognb;
-    auto step = [&]() {
-        apply_schur_batch(c, op, sprec, tos.s, ps.s, tes.s, 1, &S->pause, S->active);
-        apply_schur_batch(c, op, sprec, aps.s, tos.s, tes.s, 1, &S->pause, S->active);
+    void finish(int j)
+    {
+        Slot &s = slot[j];
+        s.finished = true;
+        s.iters = hs.iter - s.start_iter;
+        hs.active[j] = 0;
+        hs.need_update[j] = 0;
+        schur_reconstruct(c, *s.op, s.B, s.X);
+        done_list.push_back(j);
+    }
+    void step(BatchCGState *S)
+    {
+        const GaugeDev &U = gauge_of(c, gauge_id).dev;
+        Gate gate{&S->pause, nullptr};
+        const int lognb = xs.s.lognb;
+        apply_schur_batch(c, U, has_clover, sprec, tos.s, ps.s, tes.s, 1, &S->pause, S->active, d_b, d_T, d_Ti);
+        apply_schur_batch(c, U, has_clover, sprec, aps.s, tos.s, tes.s, 1, &S->pause, S->active, d_b, d_T, d_Ti);
         if (sprec == PREC_F) {
             run_batch(c, OpBAlpha<SpinorFB, SpinorFB>{ps.f(), aps.f(), S}, lognb, gate);
             run_batch(c, OpBUpdate<SpinorFB, SpinorFB, SpinorFB, SpinorFB>{xs.f(), ps.f(), rs.f(), aps.f(), S}, lognb,
@@ -1116,69 +1272,13 @@ int eo_cg_chunk(lym_context *c, OpEntry &op, int sprec, int nb, int m, const std
                       gate);
             run_batch(c, OpBDirection<SpinorHB, SpinorFB>{ps.h(), rs.f(), S}, lognb, gate);
         }
-    };
-    auto direction_rest = [&]() {  // the direction update the pause skipped, for RHS without an update
-        if (sprec == PREC_F) run_batch(c, OpBDirection<SpinorFB, SpinorFB>{ps.f(), rs.f(), S}, lognb);
-        else run_batch(c, OpBDirection<SpinorHB, SpinorFB>{ps.h(), rs.f(), S}, lognb);
-    };
-    auto any_active = [&]() {
-        for (int j = 0; j < m; ++j)
-            if (((BatchCGState *)c->h_state)->active[j]) return true;
-        return false;
-    };
-    for (int outer = 0; outer < 100000 && any_active(); ++outer) {
-        const int left = max_steps - ((BatchCGState *)c->h_state)->iter;
-        if (left <= 0) break;
-        run_gated_state(c, S, step, 8, (long)left + 8);
-        BatchCGState R = *(BatchCGState *)c->h_state;
-        if (R.failed) fail(c, LYM_ERR_NUMERIC, "block CG produced a non-finite residual");
-        direction_rest();
-        for (int j = 0; j < m; ++j) {
-            if (!R.active[j] || !R.need_update[j]) continue;
-            // reliable update: x_j += x_sloppy_j in FP64, recompute the true residuals
-            axpby_views(c, slot_f(xs, j), X[j].parity(1).d(), C2(1.0), C2(1.0));
-            axpby_views(c, slot_f(xs, j), slot_f(xs, j), C2(0.0), C2(0.0));
-            double rrS, rrN;
-            true_res(j, rrS, rrN);
-            ++updates[j];
-            if (rrS < epsS[j]) {
-                R.active[j] = 0;
-                done[j] = 1;
-                iters[j] = R.iter;
-            } else {
-                if (R.converged[j]) R.eps[j] = std::max(R.eps[j] * 0.5 * epsS[j] / rrS, 1e-300);
-                axpby_views(c, (*rN).d(), slot_f(rs, j), C2(1.0), C2(0.0));
-                set_direction(j, rrN / R.rr_prev[j]);
-                R.rr[j] = R.rr_max[j] = rrN;
-            }
-            R.converged[j] = 0;
-            R.need_update[j] = 0;
-        }
-        R.pause = 0;
-        *(BatchCGState *)c->h_state = R;
-        CK(cudaMemcpyAsync(c->d_state, c->h_state, sizeof(BatchCGState), cudaMemcpyHostToDevice, c->st));
-        if (R.iter >= max_steps) break;
     }
-    BatchCGState R = *(BatchCGState *)c->h_state;
-    int rc = LYM_OK;
-    for (int j = 0; j < m; ++j) {
-        if (R.active[j]) {  // out of iterations: keep the progress of the sloppy solution
-            axpby_views(c, slot_f(xs, j), X[j].parity(1).d(), C2(1.0), C2(1.0));
-            iters[j] = R.iter;
-            rc = LYM_NOT_CONVERGED;
-        }
-        schur_reconstruct(c, op, B[j], X[j]);
-        if (st) {
-            st[j].iterations = iters[j];
-            st[j].steps = iters[j];
-            st[j].reliable_updates = updates[j];
-            st[j].converged = done[j];
-            st[j].true_residual = true_residual(c, op, B[j], X[j]);
-        }
-        delete bp[j];
+    void direction_rest(BatchCGState *S)  // the direction update the pause skipped, for slots without an update
+    {
+        if (sprec == PREC_F) run_batch(c, OpBDirection<SpinorFB, SpinorFB>{ps.f(), rs.f(), S}, xs.s.lognb);
+        else run_batch(c, OpBDirection<SpinorHB, SpinorFB>{ps.h(), rs.f(), S}, xs.s.lognb);
     }
-    return rc;
-}
+};
 
 }  // namespace
 
@@ -1207,6 +1307,8 @@ int lym_context_create(const int dims[4], int rep, int device, lym_context **out
         CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
         c->partials = (double *)dev_alloc(c, (size_t)kBlasGridMax * kMaxRed * sizeof(double));
         c->bpartials = (double *)dev_alloc(c, (size_t)kBlasGridMax * kMaxBatch * 4 * sizeof(double));
+        c->nbr = (int *)dev_alloc(c, (size_t)16 * c->g.stride * sizeof(int));
+        launch_nbr_table(c->g, c->nbr, c->st);
         c->counter = (unsigned int *)dev_alloc(c, 64);
         c->d_err = (int *)dev_alloc(c, 64);
         c->d_state = dev_alloc(c, kStateBytes);
@@ -1241,11 +1343,13 @@ void lym_context_destroy(lym_context *c)
         cudaFree(kv.second.dev.f32);
         cudaFree(kv.second.dev.h16);
         cudaFree(kv.second.dev.sign);
+        cudaFree(kv.second.dev.f32full);
     }
     for (auto &s : c->pool) cudaFree(s.v);
     for (int k = 0; k < 3; ++k) cudaFree(c->aos[k]);
     cudaFree(c->partials);
     cudaFree(c->bpartials);
+    cudaFree(c->nbr);
     cudaFree(c->counter);
     cudaFree(c->d_err);
     cudaFree(c->d_state);
@@ -1288,6 +1392,7 @@ static int gauge_store(lym_context *c, int id, const double *links, bool device_
         e.dev.f32 = dev_alloc(c, f32);
         e.dev.h16 = dev_alloc(c, h16);
         e.dev.sign = (uint8_t *)dev_alloc(c, 2 * s);
+        e.dev.f32full = dev_alloc(c, c->rep == REP_SU3 ? 2 * 4 * 9 * s * sizeof(float2) : 2 * 4 * 9 * s * sizeof(float));
         ge = &(c->gauges[id] = e);
     } else {
         ge = &it->second;
@@ -1360,6 +1465,7 @@ int lym_gauge_evict(lym_context *c, int id)
         dev_free(c, it->second.dev.f32, su3 ? 2 * 4 * 3 * s * sizeof(float4) : 2 * 4 * 3 * s * sizeof(float2));
         dev_free(c, it->second.dev.h16, su3 ? 2 * 4 * 3 * s * sizeof(uint2) : 2 * 4 * 3 * s * sizeof(__half2));
         dev_free(c, it->second.dev.sign, 2 * s);
+        dev_free(c, it->second.dev.f32full, su3 ? 2 * 4 * 9 * s * sizeof(float2) : 2 * 4 * 9 * s * sizeof(float));
         c->gauges.erase(it);
         return LYM_OK;
     });
@@ -1625,45 +1731,63 @@ static int do_solve_block(lym_context *c, int op_id, int solver, double precisio
             fail(c, LYM_ERR_UNSUPPORTED, "block solves use LYM_SOLVER_EO_CG_MIXED_SINGLE or _HALF");
         const int sp = solver == LYM_SOLVER_EO_CG_MIXED_SINGLE ? PREC_F : PREC_H;
         const double tol = precision <= 0.0 ? (precision == 0.0 ? 1e-10 : -precision) : std::sqrt(precision);
-        int rc_all = LYM_OK;
-        for (int c0 = 0; c0 < nrhs; c0 += batch) {
-            const int m = std::min(batch, nrhs - c0);
-            std::vector<Vec *> bv, xv;
-            std::vector<Spinor> B, X;
-            for (int j = 0; j < m; ++j) {
-                bv.push_back(new Vec(c, PREC_D, 2));
-                xv.push_back(new Vec(c, PREC_D, 2));
-                B.push_back(**bv.back());
-                X.push_back(**xv.back());
-                upload_vec(c, B[j], sources[c0 + j], device_ptr, 0);
-                if (!device_ptr) CK(cudaStreamSynchronize(c->st));  // the staging buffer is reused
-            }
-            CK(cudaEventRecord(c->ev0, c->st));
-            int rc;
-            try {
-                rc = eo_cg_chunk(c, op, sp, batch, m, B, X, tol, max_steps, stats ? stats + c0 : nullptr);
-            } catch (...) {
-                for (auto v : bv) delete v;
-                for (auto v : xv) delete v;
-                throw;
-            }
-            CK(cudaEventRecord(c->ev1, c->st));
-            for (int j = 0; j < m; ++j) {
-                download_vec(c, solutions[c0 + j], X[j], device_ptr, 2);
-                if (!device_ptr) CK(cudaStreamSynchronize(c->st));
-            }
-            CK(cudaStreamSynchronize(c->st));
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-            if (stats)
-                for (int j = 0; j < m; ++j) {
-                    stats[c0 + j].seconds = ms * 1e-3;
-                    stats[c0 + j].last_error = 0.0;
+        const int width = std::min(batch, 1 << (int)std::ceil(std::log2((double)nrhs)));
+        BlockEngine engine(c, sp, std::max(width, 1));
+        std::vector<Vec *> bufs;  // two full FP64 spinors per slot
+        for (int j = 0; j < 2 * width; ++j) bufs.push_back(new Vec(c, PREC_D, 2));
+        int next = 0, rc_all = LYM_OK;
+        std::vector<double> t_start(nrhs, 0.0);
+        auto now = []() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
+        try {
+            for (;;) {
+                // continuous batching: refill every free slot with the next right-hand side
+                int j;
+                while (next < nrhs && (j = engine.free_slot()) >= 0) {
+                    const Spinor B = **bufs[2 * j], X = **bufs[2 * j + 1];
+                    upload_vec(c, B, sources[next], device_ptr, 0);
+                    t_start[next] = now();
+                    engine.add(j, op, B, X, tol, max_steps, next);
+                    ++next;
                 }
-            for (auto v : bv) delete v;
-            for (auto v : xv) delete v;
-            if (rc != LYM_OK) rc_all = rc;
+                if (!engine.working() && next >= nrhs) {
+                    // flush what add() finished at once
+                    for (int f : engine.advance()) {
+                        const auto &s = engine.info(f);
+                        download_vec(c, solutions[s.tag], s.X, device_ptr, 2);
+                        CK(cudaStreamSynchronize(c->st));
+                        if (stats) {
+                            stats[s.tag].iterations = stats[s.tag].steps = s.iters;
+                            stats[s.tag].reliable_updates = s.updates;
+                            stats[s.tag].converged = s.converged;
+                            stats[s.tag].true_residual = true_residual(c, *s.op, s.B, s.X);
+                            stats[s.tag].seconds = now() - t_start[s.tag];
+                        }
+                        if (!s.converged) rc_all = LYM_NOT_CONVERGED;
+                        engine.release(f);
+                    }
+                    if (!engine.working()) break;
+                    continue;
+                }
+                for (int f : engine.advance()) {
+                    const auto &s = engine.info(f);
+                    if (stats) {
+                        stats[s.tag].iterations = stats[s.tag].steps = s.iters;
+                        stats[s.tag].reliable_updates = s.updates;
+                        stats[s.tag].converged = s.converged;
+                        stats[s.tag].true_residual = true_residual(c, *s.op, s.B, s.X);
+                    }
+                    download_vec(c, solutions[s.tag], s.X, device_ptr, 2);
+                    CK(cudaStreamSynchronize(c->st));
+                    if (stats) stats[s.tag].seconds = now() - t_start[s.tag];
+                    if (!s.converged) rc_all = LYM_NOT_CONVERGED;
+                    engine.release(f);
+                }
+            }
+        } catch (...) {
+            for (auto v : bufs) delete v;
+            throw;
         }
+        for (auto v : bufs) delete v;
         CK(cudaGetLastError());
         return rc_all;
     });
@@ -1863,6 +1987,7 @@ int lym_time_stencil_batch(lym_context *c, int op_id, int prec, int which, int b
         P.prec = prec;
         P.rep = c->rep;
         P.U = &ge.dev;
+        P.nbr = c->nbr;
         if (which == 0) {
             P.epi = EPI_XPAY_;
             P.parity = 1;
@@ -1935,3 +2060,5 @@ extern "C" int lym_multiply_device_noalloc(lym_context *c, int op_id, double *ou
         return LYM_OK;
     });
 }
+
+#include "lym_server.inc"

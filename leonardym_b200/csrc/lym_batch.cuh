@@ -3,9 +3,10 @@
 // A batch of nb right-hand sides (nb a power of two <= 32) is stored interleaved with
 // the RHS index innermost: word k of RHS r at half-site h is v[(k*stride + h)*nb + r].
 // One thread handles one (h, r) pair with r fastest, so the nb lanes of a site load the
-// same link and clover words (one broadcast transaction) while their spinor words are
-// nb consecutive vectors (fully coalesced).  Link and clover traffic per site is
-// therefore shared by the whole batch.
+// same neighbour-index, link and clover words (one broadcast transaction) while their
+// spinor words are nb consecutive vectors (fully coalesced).  Link, clover and index
+// traffic per site is therefore shared by the whole batch, which is why this path reads
+// uncompressed 18-real links and a neighbour table instead of recomputing them per lane.
 #pragma once
 
 #include "lym_blas.cuh"
@@ -102,8 +103,13 @@ template <class SB, class GaugeT, class CloverT> struct DslashBatchArg {
     CloverT T;
     int parity, gamma5, has_clover, lognb;
     double a, b;
+    NbrTable nbr;        // precomputed neighbour half-site indices
     const int *skip_if;  // skip the launch when *skip_if != 0
     const int *active;   // per-RHS mask (nullptr: all active)
+    // per-RHS operator (nullptr: the shared a/b and T above): slots of one batch share the
+    // gauge field but may carry different kappa, hence different b and clover terms
+    const double *b_slot;
+    const void *const *clover_slot;
 };
 
 // out_r = a H in_r (EPI_SCALE), Tinv (a H in_r) (EPI_CLOVINV) or
@@ -117,25 +123,27 @@ __global__ void __launch_bounds__(128) dslash_batch_kernel(const DslashBatchArg<
     if (h >= arg.g.Vh) return;
     if (arg.active && !arg.active[r]) return;
     const auto in = arg.in.bind(r);
+    CloverT T = arg.T;
+    if (arg.clover_slot) T.c = (decltype(T.c))arg.clover_slot[r];
     cx<R> acc[12], res[12];
-    hopping<R>(arg.g, in, arg.U, arg.parity, h, acc);
+    hopping_table<R>(arg.nbr, in, arg.U, arg.parity, h, acc);
     if (EPI == EPI_SCALE) {
 #pragma unroll
         for (int k = 0; k < 12; ++k) res[k] = (R)arg.a * acc[k];
     } else if (EPI == EPI_CLOVINV) {
 #pragma unroll
         for (int k = 0; k < 12; ++k) acc[k] = (R)arg.a * acc[k];
-        clover_apply<R>(arg.T, arg.parity, h, acc, res);
+        clover_apply<R>(T, arg.parity, h, acc, res);
     } else {
         cx<R> yv[12];
         arg.y.bind(r).template load<R>(h, yv);
         if (arg.has_clover) {
-            clover_apply<R>(arg.T, arg.parity, h, yv, res);
+            clover_apply<R>(T, arg.parity, h, yv, res);
         } else {
 #pragma unroll
             for (int k = 0; k < 12; ++k) res[k] = yv[k];
         }
-        const R b = (R)arg.b;
+        const R b = arg.b_slot ? (R)arg.b_slot[r] : (R)arg.b;
 #pragma unroll
         for (int k = 0; k < 12; ++k) fma_r(res[k], b, acc[k]);
         if (arg.gamma5) {

@@ -271,6 +271,43 @@ struct GaugeD9 {
     }
 };
 
+// FP32 complex, 18 reals (no reconstruction; the batched stencil)
+struct GaugeF18 {
+    typedef LinkC<float> Link;
+    const float2 *u;
+    int stride;
+    LYM_D void load(int p, int mu, int h, Link &U) const
+    {
+        const float2 *b = u + ((size_t)(p * 4 + mu) * 9) * stride + h;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            const float2 w = __ldg(b + (size_t)k * stride);
+            U.u[k / 3][k % 3] = cx<float>{w.x, w.y};
+        }
+    }
+};
+
+// FP32 real, 9 reals (adjoint, no reconstruction; the batched stencil)
+struct GaugeF9 {
+    typedef LinkR<float> Link;
+    const float *u;
+    int stride;
+    LYM_D void load(int p, int mu, int h, Link &U) const
+    {
+        const float *b = u + ((size_t)(p * 4 + mu) * 9) * stride + h;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) U.u[k / 3][k % 3] = __ldg(b + (size_t)k * stride);
+    }
+};
+
+// Precomputed half-site indices of the 8 neighbours: nbr[(p*8 + 2 mu + dir)*stride + h],
+// dir 0 = +mu, 1 = -mu (the same values neighbour_h computes; tested bit-exact).
+struct NbrTable {
+    const int *n;
+    int stride;
+    LYM_D int get(int p, int mu, int dir, int h) const { return __ldg(n + (size_t)(p * 8 + 2 * mu + dir) * stride + h); }
+};
+
 // FP32 complex, 12 reals: rows 0 and 1; row 2 = sign * conj(row0 x row1)
 struct GaugeF12 {
     typedef LinkC<float> Link;

@@ -86,6 +86,58 @@ LYM_D void hopping(const Geom &g, const SpinorT &in, const GaugeT &U, int p, int
     }
 }
 
+// The same accumulation with the neighbour indices read from a table.
+template <typename R, class SpinorT, class GaugeT>
+LYM_D void hopping_table(const NbrTable &nbr, const SpinorT &in, const GaugeT &U, int p, int h, cx<R> acc[12])
+{
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc[k] = cx<R>{0, 0};
+    const int q = 1 - p;
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) {
+        {
+            const int hf = nbr.get(p, mu, 0, h);
+            cx<R> x[12];
+            in.template load<R>(hf, x);
+            typename GaugeT::Link L;
+            U.load(p, mu, h, L);
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int code = proj_code(mu, k), pk = proj_partner(mu, k);
+                cx<R> hv[3], w[3];
+#pragma unroll
+                for (int m = 0; m < 3; ++m) hv[m] = x[3 * k + m] - mul_code(code, x[3 * pk + m]);
+                mul_u(L, hv, w);
+#pragma unroll
+                for (int m = 0; m < 3; ++m) {
+                    acc[3 * k + m] = acc[3 * k + m] + w[m];
+                    acc[3 * pk + m] = acc[3 * pk + m] - mul_code(conj_code(code), w[m]);
+                }
+            }
+        }
+        {
+            const int hb = nbr.get(p, mu, 1, h);
+            cx<R> x[12];
+            in.template load<R>(hb, x);
+            typename GaugeT::Link L;
+            U.load(q, mu, hb, L);
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int code = proj_code(mu, k), pk = proj_partner(mu, k);
+                cx<R> hv[3], w[3];
+#pragma unroll
+                for (int m = 0; m < 3; ++m) hv[m] = x[3 * k + m] + mul_code(code, x[3 * pk + m]);
+                mul_ud(L, hv, w);
+#pragma unroll
+                for (int m = 0; m < 3; ++m) {
+                    acc[3 * k + m] = acc[3 * k + m] + w[m];
+                    acc[3 * pk + m] = acc[3 * pk + m] + mul_code(conj_code(code), w[m]);
+                }
+            }
+        }
+    }
+}
+
 template <typename R, class CloverT>
 LYM_D void clover_apply(const CloverT &T, int p, int h, const cx<R> x[12], cx<R> y[12])
 {

@@ -35,6 +35,10 @@ struct GaugeDev {
     void *h16 = nullptr;       // FP16 reconstructed: uint2[2][4][3][stride] or half2[2][4][3][stride]
     uint8_t *sign = nullptr;   // [2][stride]
     bool recon_ok = false;
+    // FP32 without reconstruction, for the batched stencil (link bytes are shared by the
+    // batch, the reconstruction arithmetic would not be): float2[2][4][9][stride] (SU3)
+    // or float[2][4][9][stride] (adjoint)
+    void *f32full = nullptr;
 };
 
 struct CloverDev {
@@ -99,7 +103,11 @@ struct DslashBatchParams {
     double a = 1.0, b = 0.0;
     const int *skip_if = nullptr;
     const int *active = nullptr;
+    const int *nbr = nullptr;                  // neighbour table [2][8][stride]
+    const double *b_slot = nullptr;            // device array [nb] or nullptr
+    const void *const *clover_slot = nullptr;  // device array [nb] of clover bases or nullptr
 };
 
 void launch_dslash_batch(const DslashBatchParams &P, cudaStream_t st);
+void launch_nbr_table(const Geom &g, int *nbr, cudaStream_t st);
 }  // namespace lym

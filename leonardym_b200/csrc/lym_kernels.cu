@@ -161,7 +161,8 @@ LYM_D void load_link_d(const Geom &g, int rep, const void *d64, int p, int mu, i
 // Compress the FP64 links to the reconstructed FP32 / FP16 formats.  A link is
 // accepted when it is +-V with V special unitary (SU(3)) or special orthogonal
 // (adjoint); the sign goes to the sign table.
-__global__ void compress_gauge_kernel(Geom g, int rep, const void *d64, void *f32, void *h16, uint8_t *sign, int *err)
+__global__ void compress_gauge_kernel(Geom g, int rep, const void *d64, void *f32, void *h16, uint8_t *sign, int *err,
+                                      void *f32full)
 {
     const int h = blockIdx.x * blockDim.x + threadIdx.x;
     const int p = blockIdx.y;
@@ -187,6 +188,11 @@ __global__ void compress_gauge_kernel(Geom g, int rep, const void *d64, void *f3
         else atomicOr(err, 1);
         if (dev > 1e-8) atomicOr(err, 2);
         bits |= (uint8_t)(neg << mu);
+        for (int kk = 0; kk < 9; ++kk) {
+            const size_t wf = ((size_t)(p * 4 + mu) * 9 + kk) * g.stride + h;
+            if (rep == REP_SU3) ((float2 *)f32full)[wf] = make_float2(u[kk / 3][kk % 3].re, u[kk / 3][kk % 3].im);
+            else ((float *)f32full)[wf] = (float)u[kk / 3][kk % 3].re;
+        }
         const size_t w0 = (size_t)(p * 4 + mu) * 3 * g.stride + h;
         if (rep == REP_SU3) {
             float4 *F = (float4 *)f32;
@@ -220,7 +226,7 @@ __global__ void compress_gauge_kernel(Geom g, int rep, const void *d64, void *f3
 void launch_compress_gauge(const Geom &g, GaugeDev &U, int *err, cudaStream_t st)
 {
     dim3 grid(nblocks(g.Vh, 128), 2);
-    compress_gauge_kernel<<<grid, 128, 0, st>>>(g, U.rep, U.d64, U.f32, U.h16, U.sign, err);
+    compress_gauge_kernel<<<grid, 128, 0, st>>>(g, U.rep, U.d64, U.f32, U.h16, U.sign, err, U.f32full);
 }
 
 // Fundamental gauge links -> fermion links: the adjoint map for SU(2)
@@ -546,6 +552,25 @@ __global__ void stencil_index_probe_kernel(Geom g, int *out)
         o[1 + 2 * mu] = neighbour_h(g, c, mu, +1);
         o[2 + 2 * mu] = neighbour_h(g, c, mu, -1);
     }
+}
+
+__global__ void nbr_table_kernel(Geom g, int *nbr)
+{
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    const int p = blockIdx.y;
+    if (h >= g.Vh) return;
+    int c[4];
+    site_coords(g, h, p, c);
+    for (int mu = 0; mu < 4; ++mu) {
+        nbr[(size_t)(p * 8 + 2 * mu) * g.stride + h] = neighbour_h(g, c, mu, +1);
+        nbr[(size_t)(p * 8 + 2 * mu + 1) * g.stride + h] = neighbour_h(g, c, mu, -1);
+    }
+}
+
+void launch_nbr_table(const Geom &g, int *nbr, cudaStream_t st)
+{
+    dim3 grid(nblocks(g.Vh, 128), 2);
+    nbr_table_kernel<<<grid, 128, 0, st>>>(g, nbr);
 }
 
 void launch_stencil_index_probe(const Geom &g, int *out, cudaStream_t st)
