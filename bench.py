@@ -441,6 +441,9 @@ def run_profile(args):
     srcs = workload_sources()[N_POINT:N_POINT + args.batch]
     xs = [lat.new_vector() for _ in srcs]
     solver = {"single": SOLVER_EO_CG_MIXED_SINGLE, "half": SOLVER_EO_CG_MIXED_HALF}[args.precision]
+    if args.tile:  # a fixed batched-stencil configuration instead of the autotuner's
+        by, bz, minb = (int(v) for v in args.tile.split(","))
+        lib.lym_set_batch_tile(lat.handle, by, bz, minb)
     bstats = (L.SolveStats * len(srcs))()
     sp_ = (C.c_void_p * len(srcs))(*[s.ctypes.data for s in srcs])
     xp_ = (C.c_void_p * len(srcs))(*[x.ctypes.data for x in xs])
@@ -468,6 +471,7 @@ def main():
     ap.add_argument("--batch", type=int, default=16, help="right-hand sides per batched stencil (power of 2 <= 32)")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--profile", action="store_true", help="small fixed case for ncu captures")
+    ap.add_argument("--tile", default="", help="with --profile: batched stencil column and variant 'by,bz,minb'")
     args = ap.parse_args()
     if args.profile:
         run_profile(args)

@@ -241,9 +241,30 @@ int lym_stencil_indices(lym_context *ctx, int *out);
  * (second half of the Schur operator), 1 = even-parity output with T_ee^-1 (first half). */
 unsigned long long lym_context_kernel_launches(lym_context *ctx);
 int lym_time_stencil(lym_context *ctx, int op_id, int prec, int which, int iters, double *ms_per_launch);
-/* the same for the batched stencil of the block solves (prec 1 or 2, batch a power of 2 <= 32) */
+/* the same for the batched stencil of the block solves (prec 1 or 2, batch a power of 2,
+ * 2 <= batch <= 32), in the configuration the autotuner picks (tuned on first use) */
 int lym_time_stencil_batch(lym_context *ctx, int op_id, int prec, int which, int batch, int iters,
                            double *ms_per_launch);
+
+/* ---- batched stencil, one application (no reference counterpart: a test and tuning
+ * hook) ---------------------------------------------------------------------------
+ * out[j] = EvenOddImprovedDiracWilsonOperator::multiply(in[j]) of operator op_ids[j]
+ * (EvenOddImprovedDiracWilsonOperator.cpp:26-47) for nrhs <= 32 full host spinors at
+ * once, through the batched stencil with prec 1 (FP32) or 2 (FP16 + norms) storage.
+ * The operators share the gauge field and the gamma5 flag; kappa and c_sw may differ. */
+int lym_multiply_batch(lym_context *ctx, int prec, int nrhs, const int *op_ids, const double *const *in,
+                       double *const *out);
+
+/* ---- batched-stencil autotuner (no reference counterpart) --------------------------
+ * The block solves time every traversal column and kernel variant of the batched
+ * stencil on first use per (precision, batch width, clover) and keep the fastest.  A
+ * column is by * bz sites of the (y, z) plane, walked x first and t fastest inside
+ * (by = 0: plain half-site order, x slowest); minb is the kernel's register budget as
+ * minimum resident blocks per SM (1, 3 or 4).  lym_set_batch_tile forces a
+ * configuration for the context (by < 0 returns to tuning); lym_get_batch_tile reports
+ * the one in use (LYM_ERR_NOT_FOUND before the first tuning of that key). */
+int lym_set_batch_tile(lym_context *ctx, int by, int bz, int minb);
+int lym_get_batch_tile(lym_context *ctx, int prec, int batch, int has_clover, int *by, int *bz, int *minb);
 
 /* ---- pinned host memory for callers that want fast transfers ---------------------- */
 void *lym_host_alloc(size_t bytes);

@@ -97,6 +97,9 @@ def lib():
         "lym_context_kernel_launches": (C.c_ulonglong, [vp]),
         "lym_time_stencil": (i, [vp, i, i, i, i, C.POINTER(C.c_double)]),
         "lym_time_stencil_batch": (i, [vp, i, i, i, i, i, C.POINTER(C.c_double)]),
+        "lym_multiply_batch": (i, [vp, i, i, C.POINTER(C.c_int), C.POINTER(vp), C.POINTER(vp)]),
+        "lym_set_batch_tile": (i, [vp, i, i, i]),
+        "lym_get_batch_tile": (i, [vp, i, i, i, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "lym_host_alloc": (vp, [C.c_size_t]),
         "lym_host_free": (None, [vp]),
     }

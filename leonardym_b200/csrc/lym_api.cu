@@ -42,6 +42,13 @@ struct LymError {
 
 }  // namespace
 
+// Batched stencil configuration picked by the autotuner: traversal column (by, bz) of
+// the (y, z) plane (by = 0: plain half-site order) and the kernel variant (minimum
+// resident blocks per SM).
+struct BatchTile {
+    int by = 0, bz = 0, minb = 1;
+};
+
 struct lym_context {
     Geom g;
     int rep = REP_SU3;
@@ -56,6 +63,10 @@ struct lym_context {
     double *partials = nullptr;
     double *bpartials = nullptr;  // per-RHS partial sums of the batched reductions
     int *nbr = nullptr;           // neighbour half-site table [2][8][stride] (batched stencil)
+    std::map<int, int *> orders;  // traversal tables [stride] by column by * 4096 + bz
+    std::map<int, BatchTile> tiles;  // tuned configuration by (precision, batch, clover)
+    BatchTile forced_tile;
+    bool tile_forced = false;
     unsigned int *counter = nullptr;
     int *d_err = nullptr;
     void *d_state = nullptr;      // solver state (device)
@@ -971,6 +982,9 @@ struct BVec {
     size_t bytes;
     BVec(lym_context *ctx, int prec, int nb) : c(ctx)
     {
+        if (nb < 2 || nb > kMaxBatch || (nb & (nb - 1))) fail(c, LYM_ERR_ARGUMENT, "batch width %d", nb);
+        if ((double)12 * c->g.stride * nb / 2 >= 4294967296.0 || (double)72 * c->g.stride >= 4294967296.0)
+            fail(c, LYM_ERR_UNSUPPORTED, "lattice too large for the batched stencil's 32-bit word indices");
         s.prec = prec;
         s.nb = nb;
         s.lognb = 0;
@@ -984,16 +998,49 @@ struct BVec {
     ~BVec() { dev_free(c, s.v, bytes); }
     BVec(const BVec &) = delete;
     BVec &operator=(const BVec &) = delete;
-    SpinorFB f() const { return SpinorFB{(float4 *)s.v, s.stride, s.lognb}; }
-    SpinorHB h() const { return SpinorHB{(int4 *)s.v, s.norm, s.stride, s.lognb}; }
+    BatchF f() const { return BatchF{(float4 *)s.v, s.stride, s.lognb - 1}; }
+    BatchH h() const { return BatchH{(int4 *)s.v, (float2 *)s.norm, s.stride, s.lognb - 1}; }
 };
 
 template <class Op> void run_batch(lym_context *c, const Op &op, int lognb, Gate gate = Gate{nullptr, nullptr})
 {
     count(c, 1);
-    const long threads = (long)c->g.Vh << lognb;
+    const int lognp = lognb - 1;
+    const long threads = (long)c->g.Vh << lognp;
     const int grid = (int)std::min<long>((threads + kBlasThreads - 1) / kBlasThreads, kBlasGridMax);
-    site_batch_kernel<Op><<<grid, kBlasThreads, 0, c->st>>>(op, c->g.Vh, lognb, c->bpartials, c->counter, gate);
+    site_batch_kernel<Op><<<grid, kBlasThreads, 0, c->st>>>(op, c->g.Vh, lognp, c->bpartials, c->counter, gate);
+}
+
+const int *order_table(lym_context *c, int by, int bz)
+{
+    if (by == 0) return nullptr;
+    const int key = by * 4096 + bz;
+    auto it = c->orders.find(key);
+    if (it != c->orders.end()) return it->second;
+    if (c->capturing) fail(c, LYM_ERR_ARGUMENT, "traversal tables must be built before graph capture");
+    int *t = (int *)dev_alloc(c, (size_t)c->g.stride * sizeof(int));
+    launch_order_table(c->g, by, bz, t, c->st);
+    count(c, 1);
+    c->orders[key] = t;
+    return t;
+}
+
+// Traversal columns worth timing: plain half-site order (x slowest), columns of 2, 4, 8
+// and 12 y-rows spanning z, and square (y, z) columns of 4 and 8.
+std::vector<BatchTile> tile_candidates(const Geom &g)
+{
+    std::vector<BatchTile> out;
+    out.push_back(BatchTile{0, 0, 1});
+    const int Ly = g.L[1], Lz = g.L[2];
+    auto add = [&](int by, int bz) {
+        if (by < 1 || bz < 1 || Ly % by || Lz % bz || (by == Ly && bz == Lz)) return;
+        for (auto &t : out)
+            if (t.by == by && t.bz == bz) return;
+        out.push_back(BatchTile{by, bz, 1});
+    };
+    for (int by : {2, 4, 8, 12}) add(by, Lz);
+    for (int b : {4, 8}) add(b, b);
+    return out;
 }
 
 // Schur complement on a batch whose slots share the gauge field and may carry their own
@@ -1001,7 +1048,8 @@ template <class Op> void run_batch(lym_context *c, const Op &op, int lognb, Gate
 //   out_r = G5^g (T_oo,r in_r - kappa_r^2 H_oe T_ee,r^-1 H_eo in_r)
 void apply_schur_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, const SpinorBatch &out,
                        const SpinorBatch &in, const SpinorBatch &tmp, int gamma5, const int *skip, const int *active,
-                       const double *b_slot, const void *const *T_slot, const void *const *Ti_slot)
+                       const double *b_slot, const void *const *T_slot, const void *const *Ti_slot,
+                       const BatchTile &tile)
 {
     DslashBatchParams P;
     P.g = c->g;
@@ -1011,12 +1059,14 @@ void apply_schur_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, c
     P.skip_if = skip;
     P.active = active;
     P.nbr = c->nbr;
+    P.order = order_table(c, tile.by, tile.bz);
+    P.minb = tile.minb;
+    P.has_clover = clov;
     P.epi = clov ? EPI_CLOVINV_ : EPI_SCALE_;
     P.parity = 0;
     P.in = in;
     P.out = tmp;
     P.y = tmp;
-    P.clover = clov ? Ti_slot : nullptr;  // non-null marks "has clover"; the bases come from the table
     P.clover_slot = clov ? Ti_slot : nullptr;
     P.a = 1.0;
     launch_dslash_batch(P, c->st);
@@ -1025,7 +1075,6 @@ void apply_schur_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, c
     P.in = tmp;
     P.out = out;
     P.y = in;
-    P.clover = clov ? T_slot : nullptr;
     P.clover_slot = clov ? T_slot : nullptr;
     P.b_slot = b_slot;
     P.gamma5 = gamma5;
@@ -1033,11 +1082,80 @@ void apply_schur_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, c
     count(c, 2);
 }
 
+// Autotuner of the batched stencil: times one batched Schur application for every
+// traversal column and kernel variant on the caller's fields (in is read, tmp and out
+// are overwritten) and keeps the fastest per (precision, batch width, clover).
+BatchTile tune_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, const SpinorBatch &out,
+                     const SpinorBatch &in, const SpinorBatch &tmp, const double *b_slot, const void *const *T_slot,
+                     const void *const *Ti_slot)
+{
+    if (c->tile_forced) return c->forced_tile;
+    const int key = (prec * 64 + in.nb) * 2 + (clov ? 1 : 0);
+    auto it = c->tiles.find(key);
+    if (it != c->tiles.end()) return it->second;
+    if (c->capturing) fail(c, LYM_ERR_ARGUMENT, "the batched stencil must be tuned before graph capture");
+    BatchTile best;
+    float best_ms = 1e30f;
+    for (BatchTile t : tile_candidates(c->g)) {
+        for (int k = 0; k < kBatchMinBlocksCount; ++k) {
+            t.minb = kBatchMinBlocks[k];
+            apply_schur_batch(c, U, clov, prec, out, in, tmp, 1, nullptr, nullptr, b_slot, T_slot, Ti_slot, t);
+            CK(cudaEventRecord(c->ev0, c->st));
+            for (int r = 0; r < 3; ++r)
+                apply_schur_batch(c, U, clov, prec, out, in, tmp, 1, nullptr, nullptr, b_slot, T_slot, Ti_slot, t);
+            CK(cudaEventRecord(c->ev1, c->st));
+            CK(cudaEventSynchronize(c->ev1));
+            CK(cudaGetLastError());
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+            if (ms < best_ms) best_ms = ms, best = t;
+        }
+    }
+    c->tiles[key] = best;
+    return best;
+}
+
 // y = a x + b y between a slot of a batch and a single FP64 half spinor (either way)
 template <class X, class Y> void axpby_views(lym_context *c, const X &x, const Y &y, double2 a, double2 b)
 {
     run_site(c, OpAxpby<X, Y>{x, y, a, b}, 1);
 }
+
+// Per-slot operator tables of a batch in device memory: b = -kappa^2 and the FP32
+// clover bases T / Tinv of every slot (freed with the object).
+struct SlotTables {
+    lym_context *c;
+    char *mem;
+    double *b;
+    const void **T, **Ti;
+    SlotTables(lym_context *ctx, const std::vector<const OpEntry *> &ops) : c(ctx)
+    {
+        mem = (char *)dev_alloc(c, 3 * kMaxBatch * sizeof(double));
+        b = (double *)mem;
+        T = (const void **)(mem + kMaxBatch * sizeof(double));
+        Ti = (const void **)(mem + 2 * kMaxBatch * sizeof(double));
+        std::vector<double> hb(ops.size());
+        std::vector<const void *> hT(ops.size()), hTi(ops.size());
+        for (size_t j = 0; j < ops.size(); ++j) {
+            const bool clov = kind_has_clover(ops[j]->kind);
+            hb[j] = -ops[j]->kappa * ops[j]->kappa;
+            hT[j] = clov ? ops[j]->clover.T[PREC_F] : nullptr;
+            hTi[j] = clov ? ops[j]->clover.Tinv[PREC_F] : nullptr;
+        }
+        try {
+            CK(cudaMemcpyAsync(b, hb.data(), ops.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
+            CK(cudaMemcpyAsync(T, hT.data(), ops.size() * sizeof(void *), cudaMemcpyHostToDevice, c->st));
+            CK(cudaMemcpyAsync(Ti, hTi.data(), ops.size() * sizeof(void *), cudaMemcpyHostToDevice, c->st));
+            CK(cudaStreamSynchronize(c->st));
+        } catch (...) {
+            dev_free(c, mem, 3 * kMaxBatch * sizeof(double));
+            throw;
+        }
+    }
+    ~SlotTables() { dev_free(c, mem, 3 * kMaxBatch * sizeof(double)); }
+    SlotTables(const SlotTables &) = delete;
+    SlotTables &operator=(const SlotTables &) = delete;
+};
 
 // Block even-odd CG engine: nb slots on one resident gauge field.  Every slot solves its
 // own D_slot x = b (its own kappa / clover term) by CG on (gamma5 S)^2 with its own FP64
@@ -1066,9 +1184,8 @@ public:
         d_b = (double *)tables;
         d_T = (const void **)(tables + kMaxBatch * sizeof(double));
         d_Ti = (const void **)(tables + 2 * kMaxBatch * sizeof(double));
-        CK(cudaMemsetAsync(xs.s.v, 0, xs.bytes, c->st));
-        CK(cudaMemsetAsync(rs.s.v, 0, rs.bytes, c->st));
-        CK(cudaMemsetAsync(ps.s.v, 0, ps.bytes, c->st));
+        CK(cudaMemsetAsync(tables, 0, 3 * kMaxBatch * sizeof(double), c->st));
+        for (BVec *v : {&xs, &rs, &ps, &aps, &tes, &tos}) CK(cudaMemsetAsync(v->s.v, 0, v->bytes, c->st));
         memset(&hs, 0, sizeof(hs));
         hs.nb = nb;
         hs.delta2 = 0.01;  // reliable update when the recursive residual fell by 10x
@@ -1098,14 +1215,19 @@ public:
     void add(int j, OpEntry &op, const Spinor &B, const Spinor &X, double tol, int max_iter, long long tag)
     {
         const bool clov = kind_has_clover(op.kind);
+        if (gauge_id >= 0 && (op.gauge_id != gauge_id || clov != has_clover))
+            fail(c, LYM_ERR_ARGUMENT, "the slots of one batch share the gauge field and operator kind");
+        if (clov) ensure_clover(c, op);
+        const double b = -op.kappa * op.kappa;
+        const void *T = clov ? op.clover.T[PREC_F] : nullptr, *Ti = clov ? op.clover.Tinv[PREC_F] : nullptr;
         if (gauge_id < 0) {
+            // first operator: every slot's table entry points at it (an idle lane of a pair
+            // borrows valid operator data), then the batched stencil is tuned on it
             gauge_id = op.gauge_id;
             has_clover = clov;
-        } else if (op.gauge_id != gauge_id || clov != has_clover) {
-            fail(c, LYM_ERR_ARGUMENT, "the slots of one batch share the gauge field and operator kind");
+            for (int k = 0; k < nb; ++k) set_tables(k, b, T, Ti);
+            tile = tune_batch(c, gauge_of(c, gauge_id).dev, clov, sprec, tos.s, ps.s, tes.s, d_b, d_T, d_Ti);
         }
-        if (clov) ensure_clover(c, op);
-        require_recon(c, gauge_of(c, op.gauge_id), sprec);
         Slot &s = slot[j];
         delete s.bp;
         s = Slot();
@@ -1121,12 +1243,8 @@ public:
         s.bb = norm2_now(c, B);
         s.epsS = tol * tol * s.bb;
         zero(c, X.parity(1));
-        const double b = -op.kappa * op.kappa;
-        const void *T = clov ? op.clover.T[sprec] : nullptr, *Ti = clov ? op.clover.Tinv[sprec] : nullptr;
-        CK(cudaMemcpyAsync(d_b + j, &b, sizeof(double), cudaMemcpyHostToDevice, c->st));
-        CK(cudaMemcpyAsync(d_T + j, &T, sizeof(void *), cudaMemcpyHostToDevice, c->st));
-        CK(cudaMemcpyAsync(d_Ti + j, &Ti, sizeof(void *), cudaMemcpyHostToDevice, c->st));
-        axpby_views(c, xs.f().bind(j), xs.f().bind(j), C2(0.0), C2(0.0));
+        set_tables(j, b, T, Ti);
+        axpby_views(c, xs.f().slot(j), xs.f().slot(j), C2(0.0), C2(0.0));
         double rrS, rrN;
         true_res(j, rrS, rrN);  // synchronises: the host values above were consumed
         if (rrS < s.epsS || s.bb == 0.0) {
@@ -1134,7 +1252,7 @@ public:
             finish(j);
             return;
         }
-        axpby_views(c, (*rN).d(), rs.f().bind(j), C2(1.0), C2(0.0));
+        axpby_views(c, (*rN).d(), rs.f().slot(j), C2(1.0), C2(0.0));
         set_direction(j, 0.0);
         hs.active[j] = 1;
         hs.rr[j] = hs.rr_max[j] = rrN;
@@ -1166,7 +1284,7 @@ public:
                 if (!s.busy || s.finished || !hs.active[j]) continue;
                 if (hs.need_update[j]) reliable_update(j);
                 if (!s.finished && hs.iter - s.start_iter >= s.max_iter) {
-                    axpby_views(c, xs.f().bind(j), s.X.parity(1).d(), C2(1.0), C2(1.0));
+                    axpby_views(c, xs.f().slot(j), s.X.parity(1).d(), C2(1.0), C2(1.0));
                     finish(j);
                 }
             }
@@ -1194,7 +1312,17 @@ private:
     const void **d_T = nullptr, **d_Ti = nullptr;
     int gauge_id = -1;
     bool has_clover = false;
+    BatchTile tile;
     Slot slot[kMaxBatch];
+
+    // the operator of slot j in the device tables: b = -kappa^2 and the FP32 T / Tinv bases
+    void set_tables(int j, double b, const void *T, const void *Ti)
+    {
+        CK(cudaMemcpyAsync(d_b + j, &b, sizeof(double), cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(d_T + j, &T, sizeof(void *), cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(d_Ti + j, &Ti, sizeof(void *), cudaMemcpyHostToDevice, c->st));
+        CK(cudaStreamSynchronize(c->st));
+    }
     BatchCGState hs;
     std::vector<int> done_list;
 
@@ -1221,14 +1349,14 @@ private:
     }
     void set_direction(int j, double b)  // p_j = r_j + b p_j in the precision of p
     {
-        if (sprec == PREC_F) axpby_views(c, rs.f().bind(j), ps.f().bind(j), C2(1.0), C2(b));
-        else axpby_views(c, rs.f().bind(j), ps.h().bind(j), C2(1.0), C2(b));
+        if (sprec == PREC_F) axpby_views(c, rs.f().slot(j), ps.f().slot(j), C2(1.0), C2(b));
+        else axpby_views(c, rs.f().slot(j), ps.h().slot(j), C2(1.0), C2(b));
     }
     void reliable_update(int j)
     {
         Slot &s = slot[j];
-        axpby_views(c, xs.f().bind(j), s.X.parity(1).d(), C2(1.0), C2(1.0));
-        axpby_views(c, xs.f().bind(j), xs.f().bind(j), C2(0.0), C2(0.0));
+        axpby_views(c, xs.f().slot(j), s.X.parity(1).d(), C2(1.0), C2(1.0));
+        axpby_views(c, xs.f().slot(j), xs.f().slot(j), C2(0.0), C2(0.0));
         double rrS, rrN;
         true_res(j, rrS, rrN);
         ++s.updates;
@@ -1237,7 +1365,7 @@ private:
             finish(j);
         } else {
             if (hs.converged[j]) hs.eps[j] = std::max(hs.eps[j] * 0.5 * s.epsS / rrS, 1e-300);
-            axpby_views(c, (*rN).d(), rs.f().bind(j), C2(1.0), C2(0.0));
+            axpby_views(c, (*rN).d(), rs.f().slot(j), C2(1.0), C2(0.0));
             set_direction(j, rrN / hs.rr_prev[j]);
             hs.rr[j] = hs.rr_max[j] = rrN;
         }
@@ -1259,24 +1387,24 @@ private:
         const GaugeDev &U = gauge_of(c, gauge_id).dev;
         Gate gate{&S->pause, nullptr};
         const int lognb = xs.s.lognb;
-        apply_schur_batch(c, U, has_clover, sprec, tos.s, ps.s, tes.s, 1, &S->pause, S->active, d_b, d_T, d_Ti);
-        apply_schur_batch(c, U, has_clover, sprec, aps.s, tos.s, tes.s, 1, &S->pause, S->active, d_b, d_T, d_Ti);
+        apply_schur_batch(c, U, has_clover, sprec, tos.s, ps.s, tes.s, 1, &S->pause, S->active, d_b, d_T, d_Ti, tile);
+        apply_schur_batch(c, U, has_clover, sprec, aps.s, tos.s, tes.s, 1, &S->pause, S->active, d_b, d_T, d_Ti, tile);
         if (sprec == PREC_F) {
-            run_batch(c, OpBAlpha<SpinorFB, SpinorFB>{ps.f(), aps.f(), S}, lognb, gate);
-            run_batch(c, OpBUpdate<SpinorFB, SpinorFB, SpinorFB, SpinorFB>{xs.f(), ps.f(), rs.f(), aps.f(), S}, lognb,
+            run_batch(c, OpBAlpha<BatchF, BatchF>{ps.f(), aps.f(), S}, lognb, gate);
+            run_batch(c, OpBUpdate<BatchF, BatchF, BatchF, BatchF>{xs.f(), ps.f(), rs.f(), aps.f(), S}, lognb,
                       gate);
-            run_batch(c, OpBDirection<SpinorFB, SpinorFB>{ps.f(), rs.f(), S}, lognb, gate);
+            run_batch(c, OpBDirection<BatchF, BatchF>{ps.f(), rs.f(), S}, lognb, gate);
         } else {
-            run_batch(c, OpBAlpha<SpinorHB, SpinorHB>{ps.h(), aps.h(), S}, lognb, gate);
-            run_batch(c, OpBUpdate<SpinorFB, SpinorHB, SpinorFB, SpinorHB>{xs.f(), ps.h(), rs.f(), aps.h(), S}, lognb,
+            run_batch(c, OpBAlpha<BatchH, BatchH>{ps.h(), aps.h(), S}, lognb, gate);
+            run_batch(c, OpBUpdate<BatchF, BatchH, BatchF, BatchH>{xs.f(), ps.h(), rs.f(), aps.h(), S}, lognb,
                       gate);
-            run_batch(c, OpBDirection<SpinorHB, SpinorFB>{ps.h(), rs.f(), S}, lognb, gate);
+            run_batch(c, OpBDirection<BatchH, BatchF>{ps.h(), rs.f(), S}, lognb, gate);
         }
     }
     void direction_rest(BatchCGState *S)  // the direction update the pause skipped, for slots without an update
     {
-        if (sprec == PREC_F) run_batch(c, OpBDirection<SpinorFB, SpinorFB>{ps.f(), rs.f(), S}, xs.s.lognb);
-        else run_batch(c, OpBDirection<SpinorHB, SpinorFB>{ps.h(), rs.f(), S}, xs.s.lognb);
+        if (sprec == PREC_F) run_batch(c, OpBDirection<BatchF, BatchF>{ps.f(), rs.f(), S}, xs.s.lognb);
+        else run_batch(c, OpBDirection<BatchH, BatchF>{ps.h(), rs.f(), S}, xs.s.lognb);
     }
 };
 
@@ -1343,13 +1471,14 @@ void lym_context_destroy(lym_context *c)
         cudaFree(kv.second.dev.f32);
         cudaFree(kv.second.dev.h16);
         cudaFree(kv.second.dev.sign);
-        cudaFree(kv.second.dev.f32full);
+        cudaFree(kv.second.dev.f32dup);
     }
     for (auto &s : c->pool) cudaFree(s.v);
     for (int k = 0; k < 3; ++k) cudaFree(c->aos[k]);
     cudaFree(c->partials);
     cudaFree(c->bpartials);
     cudaFree(c->nbr);
+    for (auto &kv : c->orders) cudaFree(kv.second);
     cudaFree(c->counter);
     cudaFree(c->d_err);
     cudaFree(c->d_state);
@@ -1392,7 +1521,7 @@ static int gauge_store(lym_context *c, int id, const double *links, bool device_
         e.dev.f32 = dev_alloc(c, f32);
         e.dev.h16 = dev_alloc(c, h16);
         e.dev.sign = (uint8_t *)dev_alloc(c, 2 * s);
-        e.dev.f32full = dev_alloc(c, c->rep == REP_SU3 ? 2 * 4 * 9 * s * sizeof(float2) : 2 * 4 * 9 * s * sizeof(float));
+        e.dev.f32dup = dev_alloc(c, c->rep == REP_SU3 ? 2 * 4 * 9 * s * sizeof(float4) : 2 * 4 * 9 * s * sizeof(float2));
         ge = &(c->gauges[id] = e);
     } else {
         ge = &it->second;
@@ -1465,7 +1594,7 @@ int lym_gauge_evict(lym_context *c, int id)
         dev_free(c, it->second.dev.f32, su3 ? 2 * 4 * 3 * s * sizeof(float4) : 2 * 4 * 3 * s * sizeof(float2));
         dev_free(c, it->second.dev.h16, su3 ? 2 * 4 * 3 * s * sizeof(uint2) : 2 * 4 * 3 * s * sizeof(__half2));
         dev_free(c, it->second.dev.sign, 2 * s);
-        dev_free(c, it->second.dev.f32full, su3 ? 2 * 4 * 9 * s * sizeof(float2) : 2 * 4 * 9 * s * sizeof(float));
+        dev_free(c, it->second.dev.f32dup, su3 ? 2 * 4 * 9 * s * sizeof(float4) : 2 * 4 * 9 * s * sizeof(float2));
         c->gauges.erase(it);
         return LYM_OK;
     });
@@ -1731,8 +1860,8 @@ static int do_solve_block(lym_context *c, int op_id, int solver, double precisio
             fail(c, LYM_ERR_UNSUPPORTED, "block solves use LYM_SOLVER_EO_CG_MIXED_SINGLE or _HALF");
         const int sp = solver == LYM_SOLVER_EO_CG_MIXED_SINGLE ? PREC_F : PREC_H;
         const double tol = precision <= 0.0 ? (precision == 0.0 ? 1e-10 : -precision) : std::sqrt(precision);
-        const int width = std::min(batch, 1 << (int)std::ceil(std::log2((double)nrhs)));
-        BlockEngine engine(c, sp, std::max(width, 1));
+        const int width = std::max(2, std::min(batch, 1 << (int)std::ceil(std::log2((double)nrhs))));
+        BlockEngine engine(c, sp, width);
         std::vector<Vec *> bufs;  // two full FP64 spinors per slot
         for (int j = 0; j < 2 * width; ++j) bufs.push_back(new Vec(c, PREC_D, 2));
         int next = 0, rc_all = LYM_OK;
@@ -1973,30 +2102,35 @@ int lym_time_stencil_batch(lym_context *c, int op_id, int prec, int which, int b
                            double *ms_per_launch)
 {
     if (!ms_per_launch || iters < 1 || (prec != PREC_F && prec != PREC_H) || which < 0 || which > 1 ||
-        batch < 1 || batch > kMaxBatch || (batch & (batch - 1)))
+        batch < 2 || batch > kMaxBatch || (batch & (batch - 1)))
         return LYM_ERR_ARGUMENT;
     return guarded(c, [&]() {
         OpEntry &op = op_of(c, op_id);
         GaugeEntry &ge = gauge_of(c, op.gauge_id);
         const bool clov = kind_has_clover(op.kind);
         if (clov) ensure_clover(c, op);
-        require_recon(c, ge, prec);
         BVec a(c, prec, batch), b(c, prec, batch), y(c, prec, batch);
+        for (BVec *v : {&a, &b, &y}) CK(cudaMemsetAsync(v->s.v, 0, v->bytes, c->st));
+        SlotTables tab(c, std::vector<const OpEntry *>(batch, &op));  // every slot on this operator
+        const BatchTile tile = tune_batch(c, ge.dev, clov, prec, b.s, a.s, y.s, tab.b, tab.T, tab.Ti);
         DslashBatchParams P;
         P.g = c->g;
         P.prec = prec;
         P.rep = c->rep;
         P.U = &ge.dev;
         P.nbr = c->nbr;
+        P.order = order_table(c, tile.by, tile.bz);
+        P.minb = tile.minb;
+        P.has_clover = clov;
         if (which == 0) {
             P.epi = EPI_XPAY_;
             P.parity = 1;
-            P.clover = clov ? op.clover.T[prec] : nullptr;
-            P.b = -op.kappa * op.kappa;
+            P.clover_slot = clov ? tab.T : nullptr;
+            P.b_slot = tab.b;
         } else {
             P.epi = clov ? EPI_CLOVINV_ : EPI_SCALE_;
             P.parity = 0;
-            P.clover = clov ? op.clover.Tinv[prec] : nullptr;
+            P.clover_slot = clov ? tab.Ti : nullptr;
         }
         P.in = a.s;
         P.out = b.s;
@@ -2011,6 +2145,91 @@ int lym_time_stencil_batch(lym_context *c, int op_id, int prec, int which, int b
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
         *ms_per_launch = (double)ms / iters;
+        return LYM_OK;
+    });
+}
+
+int lym_multiply_batch(lym_context *c, int prec, int nrhs, const int *op_ids, const double *const *in,
+                       double *const *out)
+{
+    if (!op_ids || !in || !out || nrhs < 1 || nrhs > kMaxBatch || (prec != PREC_F && prec != PREC_H))
+        return LYM_ERR_ARGUMENT;
+    for (int j = 0; j < nrhs; ++j)
+        if (!in[j] || !out[j]) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        std::vector<const OpEntry *> ops;
+        for (int j = 0; j < nrhs; ++j) {
+            OpEntry &op = op_of(c, op_ids[j]);
+            if (op.kind != LYM_OP_EVEN_ODD_IMPROVED)
+                fail(c, LYM_ERR_UNSUPPORTED, "lym_multiply_batch applies EvenOddImproved operators");
+            if (j && (op.gauge_id != ops[0]->gauge_id || op.gamma5 != ops[0]->gamma5))
+                fail(c, LYM_ERR_ARGUMENT, "the operators of one batch share the gauge field and the gamma5 flag");
+            ensure_clover(c, op);
+            ops.push_back(&op);
+        }
+        int nb = 2;
+        while (nb < nrhs) nb *= 2;
+        BVec bin(c, prec, nb), btmp(c, prec, nb), bout(c, prec, nb);
+        for (BVec *v : {&bin, &btmp, &bout}) CK(cudaMemsetAsync(v->s.v, 0, v->bytes, c->st));
+        std::vector<const OpEntry *> slot_ops(nb, ops[0]);  // unused slots borrow the first operator
+        for (int j = 0; j < nrhs; ++j) slot_ops[j] = ops[j];
+        SlotTables tab(c, slot_ops);
+        Vec full(c, PREC_D, 2);
+        for (int j = 0; j < nrhs; ++j) {
+            upload_vec(c, *full, in[j], false, 0);
+            if (prec == PREC_F) axpby_views(c, (*full).parity(1).d(), bin.f().slot(j), C2(1.0), C2(0.0));
+            else axpby_views(c, (*full).parity(1).d(), bin.h().slot(j), C2(1.0), C2(0.0));
+        }
+        const GaugeDev &U = gauge_of(c, ops[0]->gauge_id).dev;
+        const BatchTile tile = tune_batch(c, U, true, prec, btmp.s, bin.s, bout.s, tab.b, tab.T, tab.Ti);
+        apply_schur_batch(c, U, true, prec, bout.s, bin.s, btmp.s, ops[0]->gamma5, nullptr, nullptr, tab.b, tab.T,
+                          tab.Ti, tile);
+        for (int j = 0; j < nrhs; ++j) {
+            upload_vec(c, *full, in[j], false, 0);  // the even parity passes through
+            if (prec == PREC_F) axpby_views(c, bout.f().slot(j), (*full).parity(1).d(), C2(1.0), C2(0.0));
+            else axpby_views(c, bout.h().slot(j), (*full).parity(1).d(), C2(1.0), C2(0.0));
+            download_vec(c, out[j], *full, false, 0);
+            CK(cudaStreamSynchronize(c->st));
+        }
+        CK(cudaGetLastError());
+        return LYM_OK;
+    });
+}
+
+int lym_set_batch_tile(lym_context *c, int by, int bz, int minb)
+{
+    return guarded(c, [&]() {
+        if (by < 0) {
+            c->tile_forced = false;
+            return LYM_OK;
+        }
+        bool known = false;
+        for (int k = 0; k < kBatchMinBlocksCount; ++k) known |= kBatchMinBlocks[k] == minb;
+        const Geom &g = c->g;
+        if (!known || (by != 0 && (g.L[1] % by || bz < 1 || g.L[2] % bz)))
+            fail(c, LYM_ERR_ARGUMENT, "batch tile (%d, %d, %d) does not fit the lattice or the compiled variants", by,
+                 bz, minb);
+        c->forced_tile = BatchTile{by, by ? bz : 0, minb};
+        c->tile_forced = true;
+        return LYM_OK;
+    });
+}
+
+int lym_get_batch_tile(lym_context *c, int prec, int batch, int has_clover, int *by, int *bz, int *minb)
+{
+    if (!by || !bz || !minb) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        BatchTile t;
+        if (c->tile_forced) {
+            t = c->forced_tile;
+        } else {
+            auto it = c->tiles.find((prec * 64 + batch) * 2 + (has_clover ? 1 : 0));
+            if (it == c->tiles.end()) fail(c, LYM_ERR_NOT_FOUND, "no tuned batch configuration for this key yet");
+            t = it->second;
+        }
+        *by = t.by;
+        *bz = t.bz;
+        *minb = t.minb;
         return LYM_OK;
     });
 }

@@ -1,27 +1,41 @@
-// Dispatcher over the batched stencil instantiations (lym_batch.cuh).  The batched path
-// reads FP32 links without reconstruction whatever the spinor storage (FP32 or FP16):
-// link bytes are shared by the batch.
+// Dispatcher over the batched stencil instantiations (lym_batch.cuh) and the traversal
+// tables the autotuner chooses between.
 #include "lym_batch.cuh"
 #include "lym_internal.h"
 
 namespace lym {
 
-static SpinorFB fview(const SpinorBatch &s) { return SpinorFB{(float4 *)s.v, s.stride, s.lognb}; }
-static SpinorHB hview(const SpinorBatch &s) { return SpinorHB{(int4 *)s.v, s.norm, s.stride, s.lognb}; }
+// Variants of the batched stencil by the register budget the compiler is held to
+// (__launch_bounds__(128, minb)); the autotuner times them.
+const int kBatchMinBlocks[] = {1, 3, 4};
+const int kBatchMinBlocksCount = 3;
 
-template <typename R, class SB, class G, class C>
-static void run(const DslashBatchParams &P, const SB &in, const SB &out, const SB &y, const G &U, const C &T,
-                cudaStream_t st)
+static BatchF fview(const SpinorBatch &s) { return BatchF{(float4 *)s.v, s.stride, s.lognb - 1}; }
+static BatchH hview(const SpinorBatch &s) { return BatchH{(int4 *)s.v, (float2 *)s.norm, s.stride, s.lognb - 1}; }
+
+template <int EPI, class SB, class G>
+static void launch_minb(const DslashBatchParams &P, const DslashBatchArg<SB, G> &a, cudaStream_t st)
 {
-    DslashBatchArg<SB, G, C> a{P.g,       in,        out,       y,          U,         T,       P.parity, P.gamma5,
-                               P.clover != nullptr,  in.lognb,  P.a,        P.b,       NbrTable{P.nbr, P.g.stride},
-                               P.skip_if, P.active,  P.b_slot,  P.clover_slot};
-    const long threads = (long)P.g.Vh << in.lognb;
+    const long threads = (long)P.g.Vh << a.lognp;
     const int nb = (int)((threads + 127) / 128);
+    switch (P.minb) {
+    case 3: dslash_batch_kernel<EPI, 3><<<nb, 128, 0, st>>>(a); break;
+    case 4: dslash_batch_kernel<EPI, 4><<<nb, 128, 0, st>>>(a); break;
+    default: dslash_batch_kernel<EPI, 1><<<nb, 128, 0, st>>>(a); break;
+    }
+}
+
+template <class SB, class G>
+static void run(const DslashBatchParams &P, const SB &in, const SB &out, const SB &y, const G &U, cudaStream_t st)
+{
+    DslashBatchArg<SB, G> a{P.g,       in,          out,       y,         U,
+                            P.parity,  P.gamma5,    P.has_clover, in.lognp, (float)P.a,
+                            (float)P.b, NbrTable{P.nbr, P.g.stride}, P.order, P.skip_if, P.active,
+                            P.b_slot,  P.clover_slot};
     switch (P.epi) {
-    case EPI_SCALE_: dslash_batch_kernel<R, EPI_SCALE><<<nb, 128, 0, st>>>(a); break;
-    case EPI_CLOVINV_: dslash_batch_kernel<R, EPI_CLOVINV><<<nb, 128, 0, st>>>(a); break;
-    default: dslash_batch_kernel<R, EPI_XPAY><<<nb, 128, 0, st>>>(a); break;
+    case EPI_SCALE_: launch_minb<EPI_SCALE>(P, a, st); break;
+    case EPI_CLOVINV_: launch_minb<EPI_CLOVINV>(P, a, st); break;
+    default: launch_minb<EPI_XPAY>(P, a, st); break;
     }
 }
 
@@ -30,18 +44,44 @@ void launch_dslash_batch(const DslashBatchParams &P, cudaStream_t st)
     const GaugeDev &U = *P.U;
     const int s = P.g.stride;
     if (P.prec == PREC_F) {
-        CloverF T{(const float4 *)P.clover, s};
-        if (P.rep == REP_SU3)
-            run<float>(P, fview(P.in), fview(P.out), fview(P.y), GaugeF18{(const float2 *)U.f32full, s}, T, st);
-        else
-            run<float>(P, fview(P.in), fview(P.out), fview(P.y), GaugeF9{(const float *)U.f32full, s}, T, st);
+        if (P.rep == REP_SU3) run(P, fview(P.in), fview(P.out), fview(P.y), GaugeDupC{(const float4 *)U.f32dup, s}, st);
+        else run(P, fview(P.in), fview(P.out), fview(P.y), GaugeDupR{(const float2 *)U.f32dup, s}, st);
     } else {
-        CloverH T{(const uint2 *)P.clover, s};
-        if (P.rep == REP_SU3)
-            run<float>(P, hview(P.in), hview(P.out), hview(P.y), GaugeF18{(const float2 *)U.f32full, s}, T, st);
-        else
-            run<float>(P, hview(P.in), hview(P.out), hview(P.y), GaugeF9{(const float *)U.f32full, s}, T, st);
+        if (P.rep == REP_SU3) run(P, hview(P.in), hview(P.out), hview(P.y), GaugeDupC{(const float4 *)U.f32dup, s}, st);
+        else run(P, hview(P.in), hview(P.out), hview(P.y), GaugeDupR{(const float2 *)U.f32dup, s}, st);
     }
+}
+
+// Work item w -> half-site h for a column (by, bz): the lattice is walked in columns of
+// by * bz sites of the (y, z) plane, each column with x, then y, z inside the column
+// and t fastest, i.e. in the order (y block, z block, x, y, z, t / 2).  Consecutive
+// items are consecutive half-sites along t (coalesced), and the x neighbours of a site
+// are by * bz * Lt / 2 items away, so they are still in L2 when they are read again.
+// The half-site index h = t / 2 + Lt / 2 * (z + Lz * (y + Ly * x)) does not depend on
+// the parity, so one table serves both.
+__global__ void order_table_kernel(Geom g, int by, int bz, int *order)
+{
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= g.Vh) return;
+    const int lth = g.L[3] / 2;
+    int u = w;
+    const int th = u % lth;
+    u /= lth;
+    const int zi = u % bz;
+    u /= bz;
+    const int yi = u % by;
+    u /= by;
+    const int x = u % g.L[0];
+    u /= g.L[0];
+    const int nzb = g.L[2] / bz;
+    const int zb = u % nzb, yb = u / nzb;
+    const int y = yb * by + yi, z = zb * bz + zi;
+    order[w] = th + lth * (z + g.L[2] * (y + g.L[1] * x));
+}
+
+void launch_order_table(const Geom &g, int by, int bz, int *order, cudaStream_t st)
+{
+    order_table_kernel<<<(g.Vh + 127) / 128, 128, 0, st>>>(g, by, bz, order);
 }
 
 }  // namespace lym

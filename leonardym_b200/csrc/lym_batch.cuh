@@ -1,12 +1,24 @@
 // Multi-right-hand-side (batched) fields and kernels.
 //
-// A batch of nb right-hand sides (nb a power of two <= 32) is stored interleaved with
-// the RHS index innermost: word k of RHS r at half-site h is v[(k*stride + h)*nb + r].
-// One thread handles one (h, r) pair with r fastest, so the nb lanes of a site load the
-// same neighbour-index, link and clover words (one broadcast transaction) while their
-// spinor words are nb consecutive vectors (fully coalesced).  Link, clover and index
-// traffic per site is therefore shared by the whole batch, which is why this path reads
-// uncompressed 18-real links and a neighbour table instead of recomputing them per lane.
+// A batch holds nb right-hand sides (nb a power of two, 2 <= nb <= 32) of one parity.
+// The RHS are taken in pairs (2q, 2q+1), q < np = nb / 2, and a pair is the unit of
+// work of one thread: every arithmetic step runs on float2 registers whose two lanes
+// are the two RHS of the pair, with the packed FP32 instructions of sm_100
+// (__ffma2_rn / __fadd2_rn / __fmul2_rn, sub.rn.f32x2), which halves the issued
+// arithmetic.
+//
+// Storage, with the pair index innermost so that the np threads of a half-site read
+// consecutive 16-byte words:
+//   FP32: float4 v[(c * stride + h) * np + q] = (re_2q, re_2q+1, im_2q, im_2q+1)
+//         for complex component c = spin * 3 + colour (12 per site);
+//   FP16: int4 v[(w * stride + h) * np + q] = halves (re_a, re_b, im_a, im_b) of
+//         component 2w followed by those of component 2w+1 (w < 6), and a float2
+//         norm n[h * np + q] = (max |.| of RHS 2q, of RHS 2q+1).
+// Link, clover and neighbour-index words of a half-site are read by all np threads
+// of that half-site (broadcast), so their bytes are shared by the whole batch; the
+// batched stencil therefore reads links stored without reconstruction and with each
+// component duplicated into both lanes, (re, re, im, im), ready for the packed
+// multiply.
 #pragma once
 
 #include "lym_blas.cuh"
@@ -16,53 +28,138 @@ namespace lym {
 
 constexpr int kMaxBatch = 32;
 
-// ------------------------------------------------------------ batch views --
-struct SpinorFBr {  // FP32, one RHS of a batch
-    float4 *v;
-    int stride, lognb, r;
-    LYM_HD SpinorFBr par(int) const { return *this; }  // one parity per batch view
+// ------------------------------------------------------- pair arithmetic ---
+struct c2 {  // one complex component of the two RHS of a pair
+    float2 re, im;
+};
+
+LYM_D float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+LYM_D float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+LYM_D float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+LYM_D float2 sub2(float2 a, float2 b)  // a - b in one packed instruction (no negated copy of b)
+{
+    float2 d;
+    asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\t"
+        "mov.b64 rb, {%4, %5};\n\t"
+        "sub.rn.f32x2 rd, ra, rb;\n\t"
+        "mov.b64 {%0, %1}, rd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+
+// a + s * code * z with code 0: +1, 1: -1, 2: +i, 3: -i (s = +1 or -1, compile time)
+template <int S> LYM_D c2 add_code(c2 a, int code, c2 z)
+{
+    const bool plus = (S > 0) == (code == 0 || code == 3);
+    switch (code) {
+    case 0:
+    case 1: return plus ? c2{add2(a.re, z.re), add2(a.im, z.im)} : c2{sub2(a.re, z.re), sub2(a.im, z.im)};
+    case 2:  // +i z = (-z.im, z.re)
+        return S > 0 ? c2{sub2(a.re, z.im), add2(a.im, z.re)} : c2{add2(a.re, z.im), sub2(a.im, z.re)};
+    default:  // -i z = (z.im, -z.re)
+        return S > 0 ? c2{add2(a.re, z.im), sub2(a.im, z.re)} : c2{sub2(a.re, z.im), add2(a.im, z.re)};
+    }
+}
+
+// ------------------------------------------------------------- batch views --
+// One RHS r of a FP32 pair-layout batch, as a single half-spinor view (slot set-up and
+// extraction; not on the iteration path).
+struct SlotF {
+    float *f;
+    int stride, lognp, r;
+    LYM_HD SlotF par(int) const { return *this; }
+    LYM_D size_t base(int c, int h) const
+    {
+        return (((((size_t)c * stride + h) << lognp) + (r >> 1)) << 2) + (r & 1);
+    }
     template <typename R> LYM_D void load(int h, cx<R> s[12]) const
     {
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            const float4 w = __ldg(v + (((size_t)k * stride + h) << lognb) + r);
-            s[2 * k] = cx<R>{(R)w.x, (R)w.y};
-            s[2 * k + 1] = cx<R>{(R)w.z, (R)w.w};
+        for (int c = 0; c < 12; ++c) {
+            const size_t b = base(c, h);
+            s[c] = cx<R>{(R)f[b], (R)f[b + 2]};
         }
     }
     template <typename R> LYM_D void store(int h, const cx<R> s[12]) const
     {
 #pragma unroll
-        for (int k = 0; k < 6; ++k)
-            v[(((size_t)k * stride + h) << lognb) + r] =
-                make_float4((float)s[2 * k].re, (float)s[2 * k].im, (float)s[2 * k + 1].re, (float)s[2 * k + 1].im);
+        for (int c = 0; c < 12; ++c) {
+            const size_t b = base(c, h);
+            f[b] = (float)s[c].re;
+            f[b + 2] = (float)s[c].im;
+        }
     }
 };
 
-struct SpinorFB {
+struct BatchF {
     float4 *v;
-    int stride, lognb;
-    LYM_HD SpinorFB par(int p) const { return SpinorFB{v + ((size_t)p * 6 * stride << lognb), stride, lognb}; }
-    LYM_HD SpinorFBr bind(int r) const { return SpinorFBr{v, stride, lognb, r}; }
+    int stride, lognp;
+    // word index; a batch holds at most 2^32 words (checked when it is allocated)
+    LYM_D unsigned at(int c, int h, int q) const { return (((unsigned)c * stride + h) << lognp) + q; }
+    LYM_D void load(int h, int q, c2 x[12]) const
+    {
+        const unsigned b = at(0, h, q), s = (unsigned)stride << lognp;
+#pragma unroll
+        for (int c = 0; c < 12; ++c) {
+            const float4 w = __ldg(v + b + c * s);
+            x[c] = c2{make_float2(w.x, w.y), make_float2(w.z, w.w)};
+        }
+    }
+    // streaming read (a field read once per launch)
+    LYM_D void load_cs(int h, int q, c2 x[12]) const
+    {
+        const unsigned b = at(0, h, q), s = (unsigned)stride << lognp;
+#pragma unroll
+        for (int c = 0; c < 12; ++c) {
+            const float4 w = __ldcs(v + b + c * s);
+            x[c] = c2{make_float2(w.x, w.y), make_float2(w.z, w.w)};
+        }
+    }
+    LYM_D void store(int h, int q, const c2 x[12]) const
+    {
+        const unsigned b = at(0, h, q), s = (unsigned)stride << lognp;
+#pragma unroll
+        for (int c = 0; c < 12; ++c) __stcs(v + b + c * s, make_float4(x[c].re.x, x[c].re.y, x[c].im.x, x[c].im.y));
+    }
+    // FP64 values of both RHS of the pair (vector algebra)
+    LYM_D void load_d(int h, int q, cx<double> a[12], cx<double> b[12]) const
+    {
+#pragma unroll
+        for (int c = 0; c < 12; ++c) {
+            const float4 w = __ldg(v + at(c, h, q));
+            a[c] = cx<double>{(double)w.x, (double)w.z};
+            b[c] = cx<double>{(double)w.y, (double)w.w};
+        }
+    }
+    LYM_D void store_d(int h, int q, const cx<double> a[12], const cx<double> b[12]) const
+    {
+#pragma unroll
+        for (int c = 0; c < 12; ++c)
+            v[at(c, h, q)] = make_float4((float)a[c].re, (float)b[c].re, (float)a[c].im, (float)b[c].im);
+    }
+    LYM_HD SlotF slot(int r) const { return SlotF{(float *)v, stride, lognp, r}; }
 };
 
-struct SpinorHBr {  // FP16 with a per-(site, RHS) norm, one RHS of a batch
-    int4 *v;
+// One RHS r of a FP16 pair-layout batch, as a single half-spinor view.
+struct SlotH {
+    __half *hv;
     float *norm;
-    int stride, lognb, r;
-    LYM_HD SpinorHBr par(int) const { return *this; }
+    int stride, lognp, r;
+    LYM_HD SlotH par(int) const { return *this; }
+    LYM_D size_t base(int w, int h) const
+    {
+        return (((((size_t)w * stride + h) << lognp) + (r >> 1)) << 3) + (r & 1);
+    }
     template <typename R> LYM_D void load(int h, cx<R> s[12]) const
     {
-        const float nrm = __ldg(norm + ((size_t)h << lognb) + r);
+        const float n = norm[((size_t)h << (lognp + 1)) + r];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            int4 w = __ldg(v + (((size_t)k * stride + h) << lognb) + r);
-            const __half2 *hp = reinterpret_cast<const __half2 *>(&w);
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const float2 f = __half22float2(hp[j]);
-                s[4 * k + j] = cx<R>{(R)(f.x * nrm), (R)(f.y * nrm)};
-            }
+        for (int w = 0; w < 6; ++w) {
+            const size_t b = base(w, h);
+            s[2 * w] = cx<R>{(R)(__half2float(hv[b]) * n), (R)(__half2float(hv[b + 2]) * n)};
+            s[2 * w + 1] = cx<R>{(R)(__half2float(hv[b + 4]) * n), (R)(__half2float(hv[b + 6]) * n)};
         }
     }
     template <typename R> LYM_D void store(int h, const cx<R> s[12]) const
@@ -71,120 +168,427 @@ struct SpinorHBr {  // FP16 with a per-(site, RHS) norm, one RHS of a batch
 #pragma unroll
         for (int k = 0; k < 12; ++k) m = fmaxf(m, fmaxf(fabsf((float)s[k].re), fabsf((float)s[k].im)));
         const float inv = m > 0.f ? 1.0f / m : 0.f;
-        norm[((size_t)h << lognb) + r] = m;
+        norm[((size_t)h << (lognp + 1)) + r] = m;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            int4 w;
-            __half2 *hp = reinterpret_cast<__half2 *>(&w);
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-                hp[j] = __floats2half2_rn((float)s[4 * k + j].re * inv, (float)s[4 * k + j].im * inv);
-            v[(((size_t)k * stride + h) << lognb) + r] = w;
+        for (int w = 0; w < 6; ++w) {
+            const size_t b = base(w, h);
+            hv[b] = __float2half_rn((float)s[2 * w].re * inv);
+            hv[b + 2] = __float2half_rn((float)s[2 * w].im * inv);
+            hv[b + 4] = __float2half_rn((float)s[2 * w + 1].re * inv);
+            hv[b + 6] = __float2half_rn((float)s[2 * w + 1].im * inv);
         }
     }
 };
 
-struct SpinorHB {
+struct BatchH {
     int4 *v;
-    float *norm;
-    int stride, lognb;
-    LYM_HD SpinorHB par(int p) const
+    float2 *norm;
+    int stride, lognp;
+    LYM_D unsigned at(int w, int h, int q) const { return (((unsigned)w * stride + h) << lognp) + q; }
+    LYM_D void load(int h, int q, c2 x[12]) const
     {
-        return SpinorHB{v + ((size_t)p * 3 * stride << lognb), norm + ((size_t)p * stride << lognb), stride, lognb};
+        const float2 n = __ldg(norm + ((unsigned)h << lognp) + q);
+        const unsigned b = at(0, h, q), s = (unsigned)stride << lognp;
+#pragma unroll
+        for (int w = 0; w < 6; ++w) {
+            int4 u = __ldg(v + b + w * s);
+            const __half2 *hp = reinterpret_cast<const __half2 *>(&u);
+            x[2 * w] = c2{mul2(__half22float2(hp[0]), n), mul2(__half22float2(hp[1]), n)};
+            x[2 * w + 1] = c2{mul2(__half22float2(hp[2]), n), mul2(__half22float2(hp[3]), n)};
+        }
     }
-    LYM_HD SpinorHBr bind(int r) const { return SpinorHBr{v, norm, stride, lognb, r}; }
+    LYM_D void load_cs(int h, int q, c2 x[12]) const { load(h, q, x); }
+    LYM_D void store(int h, int q, const c2 x[12]) const
+    {
+        float ma = 0.f, mb = 0.f;
+#pragma unroll
+        for (int c = 0; c < 12; ++c) {
+            ma = fmaxf(ma, fmaxf(fabsf(x[c].re.x), fabsf(x[c].im.x)));
+            mb = fmaxf(mb, fmaxf(fabsf(x[c].re.y), fabsf(x[c].im.y)));
+        }
+        const float2 inv = make_float2(ma > 0.f ? 1.0f / ma : 0.f, mb > 0.f ? 1.0f / mb : 0.f);
+        norm[((unsigned)h << lognp) + q] = make_float2(ma, mb);
+        const unsigned b = at(0, h, q), s = (unsigned)stride << lognp;
+#pragma unroll
+        for (int w = 0; w < 6; ++w) {
+            int4 u;
+            __half2 *hp = reinterpret_cast<__half2 *>(&u);
+            hp[0] = __float22half2_rn(mul2(x[2 * w].re, inv));
+            hp[1] = __float22half2_rn(mul2(x[2 * w].im, inv));
+            hp[2] = __float22half2_rn(mul2(x[2 * w + 1].re, inv));
+            hp[3] = __float22half2_rn(mul2(x[2 * w + 1].im, inv));
+            v[b + w * s] = u;
+        }
+    }
+    LYM_D void load_d(int h, int q, cx<double> a[12], cx<double> b[12]) const
+    {
+        c2 x[12];
+        load(h, q, x);
+#pragma unroll
+        for (int c = 0; c < 12; ++c) {
+            a[c] = cx<double>{(double)x[c].re.x, (double)x[c].im.x};
+            b[c] = cx<double>{(double)x[c].re.y, (double)x[c].im.y};
+        }
+    }
+    LYM_D void store_d(int h, int q, const cx<double> a[12], const cx<double> b[12]) const
+    {
+        c2 x[12];
+#pragma unroll
+        for (int c = 0; c < 12; ++c)
+            x[c] = c2{make_float2((float)a[c].re, (float)b[c].re), make_float2((float)a[c].im, (float)b[c].im)};
+        store(h, q, x);
+    }
+    LYM_HD SlotH slot(int r) const { return SlotH{(__half *)v, (float *)norm, stride, lognp, r}; }
 };
 
+// ---------------------------------------------------------- links, clover --
+struct LinkP {  // a link with every component duplicated into both lanes
+    float2 ur[3][3], ui[3][3];
+};
+
+// Links and clover words are read by exactly one warp instruction per launch (all np
+// lanes of the half-site at once), so they are loaded with the evict-first hint and
+// leave L2 to the neighbour spinors, which are read eight times.
+struct GaugeDupC {  // SU(3): float4 (re, re, im, im) per component, [parity][mu][9][stride]
+    static constexpr bool kReal = false;
+    const float4 *u;
+    int stride;
+    LYM_D void load(int p, int mu, int h, LinkP &L) const
+    {
+        const float4 *b = u + ((unsigned)(p * 4 + mu) * 9 * stride + h);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            const float4 w = __ldcs(b + k * stride);
+            L.ur[k / 3][k % 3] = make_float2(w.x, w.y);
+            L.ui[k / 3][k % 3] = make_float2(w.z, w.w);
+        }
+    }
+};
+
+struct GaugeDupR {  // real adjoint links: float2 (u, u) per component, [parity][mu][9][stride]
+    static constexpr bool kReal = true;
+    const float2 *u;
+    int stride;
+    LYM_D void load(int p, int mu, int h, LinkP &L) const
+    {
+        const float2 *b = u + ((unsigned)(p * 4 + mu) * 9 * stride + h);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) L.ur[k / 3][k % 3] = __ldcs(b + k * stride);
+    }
+};
+
+// w = U h.  Re w_i = sum_j Ur_ij Re h_j - sum_j Ui_ij Im h_j: the subtracted sum is
+// accumulated on its own and taken off once per row, so no negated operand is needed.
+template <bool REAL> LYM_D void mul_u2(const LinkP &L, const c2 h[3], c2 w[3])
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float2 re = mul2(L.ur[i][0], h[0].re), im = mul2(L.ur[i][0], h[0].im);
+#pragma unroll
+        for (int j = 1; j < 3; ++j) {
+            re = fma2(L.ur[i][j], h[j].re, re);
+            im = fma2(L.ur[i][j], h[j].im, im);
+        }
+        if (!REAL) {
+            float2 t = mul2(L.ui[i][0], h[0].im);
+#pragma unroll
+            for (int j = 1; j < 3; ++j) t = fma2(L.ui[i][j], h[j].im, t);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) im = fma2(L.ui[i][j], h[j].re, im);
+            re = sub2(re, t);
+        }
+        w[i] = c2{re, im};
+    }
+}
+
+// w = U^+ h.  Im w_i = sum_j Ur_ji Im h_j - sum_j Ui_ji Re h_j.
+template <bool REAL> LYM_D void mul_ud2(const LinkP &L, const c2 h[3], c2 w[3])
+{
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float2 re = mul2(L.ur[0][i], h[0].re), im = mul2(L.ur[0][i], h[0].im);
+#pragma unroll
+        for (int j = 1; j < 3; ++j) {
+            re = fma2(L.ur[j][i], h[j].re, re);
+            im = fma2(L.ur[j][i], h[j].im, im);
+        }
+        if (!REAL) {
+            float2 t = mul2(L.ui[0][i], h[0].re);
+#pragma unroll
+            for (int j = 1; j < 3; ++j) t = fma2(L.ui[j][i], h[j].re, t);
+#pragma unroll
+            for (int j = 0; j < 3; ++j) re = fma2(L.ui[j][i], h[j].im, re);
+            im = sub2(im, t);
+        }
+        w[i] = c2{re, im};
+    }
+}
+
+// The 36 words of one clover block for the pair: SAME (both lanes on one operator) reads
+// them once and duplicates each into both lanes, otherwise each lane reads its own.
+template <bool SAME>
+LYM_D void clover_words(const float4 *ta, const float4 *tb, unsigned off, int stride, float2 v[36])
+{
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        const float4 wa = __ldcs(ta + off + k * stride);
+        const float4 wb = SAME ? wa : __ldcs(tb + off + k * stride);
+        v[4 * k] = make_float2(wa.x, wb.x);
+        v[4 * k + 1] = make_float2(wa.y, wb.y);
+        v[4 * k + 2] = make_float2(wa.z, wb.z);
+        v[4 * k + 3] = make_float2(wa.w, wb.w);
+    }
+}
+
+// y = A x for one Hermitian 6x6 block of the FP32 clover term (packed as in CloverF: 6
+// real diagonal entries, then the 15 entries below the diagonal, row-major), for the two
+// RHS of a pair.  A_ij = a (i > j), A_ji = conj(a); the products entering with a minus
+// sign are summed apart (nre, nim) and subtracted once per row.
+template <bool SAME>
+LYM_D void clover_pair_block(const float4 *ta, const float4 *tb, int stride, int p, int blk, int h, const c2 x[6],
+                             c2 y[6])
+{
+    float2 v[36];
+    clover_words<SAME>(ta, tb, (unsigned)(p * 2 + blk) * 9 * stride + h, stride, v);
+    float2 pre[6], pim[6], nre[6], nim[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        pre[i] = mul2(v[i], x[i].re);
+        pim[i] = mul2(v[i], x[i].im);
+    }
+#pragma unroll
+    for (int i = 1; i < 6; ++i)
+#pragma unroll
+        for (int j = 0; j < i; ++j) {
+            const int t = tri_index(i, j);
+            const float2 are = v[6 + 2 * t], aim = v[7 + 2 * t];
+            // y_i += a x_j
+            pre[i] = fma2(are, x[j].re, pre[i]);
+            nre[i] = j == 0 ? mul2(aim, x[j].im) : fma2(aim, x[j].im, nre[i]);
+            pim[i] = fma2(are, x[j].im, pim[i]);
+            pim[i] = fma2(aim, x[j].re, pim[i]);
+            // y_j += conj(a) x_i
+            pre[j] = fma2(are, x[i].re, pre[j]);
+            pre[j] = fma2(aim, x[i].im, pre[j]);
+            pim[j] = fma2(are, x[i].im, pim[j]);
+            nim[j] = i == j + 1 ? mul2(aim, x[i].re) : fma2(aim, x[i].re, nim[j]);
+        }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        y[i].re = i == 0 ? pre[0] : sub2(pre[i], nre[i]);
+        y[i].im = i == 5 ? pim[5] : sub2(pim[i], nim[i]);
+    }
+}
+
+template <bool SAME>
+LYM_D void clover_pair(const float4 *ta, const float4 *tb, int stride, int p, int h, const c2 x[12], c2 y[12])
+{
+    clover_pair_block<SAME>(ta, tb, stride, p, 0, h, x, y);
+    clover_pair_block<SAME>(ta, tb, stride, p, 1, h, x + 6, y + 6);
+}
+
 // ---------------------------------------------------------- batch stencil --
-template <class SB, class GaugeT, class CloverT> struct DslashBatchArg {
+// One term of H x for the pair: DIR 0 adds U_mu(s) (1 - g_mu) x(s + mu), DIR 1 adds
+// U_mu(s - mu)^+ (1 + g_mu) x(s - mu), through the half-spinor projections of the
+// chiral basis (see lym_dslash.cuh).
+template <bool REAL, int MU, int DIR> LYM_D void accumulate_dir(const c2 x[12], const LinkP &L, c2 acc[12])
+{
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int code = proj_code(MU, k), pk = proj_partner(MU, k);
+        c2 hv[3], w[3];
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+            hv[m] = DIR == 0 ? add_code<-1>(x[3 * k + m], code, x[3 * pk + m])
+                             : add_code<+1>(x[3 * k + m], code, x[3 * pk + m]);
+        if (DIR == 0) mul_u2<REAL>(L, hv, w);
+        else mul_ud2<REAL>(L, hv, w);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            acc[3 * k + m] = c2{add2(acc[3 * k + m].re, w[m].re), add2(acc[3 * k + m].im, w[m].im)};
+            acc[3 * pk + m] = DIR == 0 ? add_code<-1>(acc[3 * pk + m], conj_code(code), w[m])
+                                       : add_code<+1>(acc[3 * pk + m], conj_code(code), w[m]);
+        }
+    }
+}
+
+template <bool REAL, int MU, class SB, class GaugeT>
+LYM_D void hopping_mu(const int nf[4], const int nbk[4], const SB &in, const GaugeT &U, int p, int h, int q,
+                      c2 acc[12])
+{
+    {
+        c2 x[12];
+        in.load(nf[MU], q, x);
+        LinkP L;
+        U.load(p, MU, h, L);
+        accumulate_dir<REAL, MU, 0>(x, L, acc);
+    }
+    {
+        c2 x[12];
+        in.load(nbk[MU], q, x);
+        LinkP L;
+        U.load(1 - p, MU, nbk[MU], L);
+        accumulate_dir<REAL, MU, 1>(x, L, acc);
+    }
+}
+
+// H x at half-site h of output parity p for the pair q; nf / nbk: the forward and
+// backward neighbour half-sites, read from the table before the first spinor load.
+template <bool REAL, class SB, class GaugeT>
+LYM_D void hopping_pair(const int nf[4], const int nbk[4], const SB &in, const GaugeT &U, int p, int h, int q,
+                        c2 acc[12])
+{
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc[k] = c2{make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+    hopping_mu<REAL, 0>(nf, nbk, in, U, p, h, q, acc);
+    hopping_mu<REAL, 1>(nf, nbk, in, U, p, h, q, acc);
+    hopping_mu<REAL, 2>(nf, nbk, in, U, p, h, q, acc);
+    hopping_mu<REAL, 3>(nf, nbk, in, U, p, h, q, acc);
+}
+
+template <class SB, class GaugeT> struct DslashBatchArg {
     Geom g;
     SB in, out, y;
     GaugeT U;
-    CloverT T;
-    int parity, gamma5, has_clover, lognb;
-    double a, b;
+    int parity, gamma5, has_clover, lognp;
+    float a, b;
     NbrTable nbr;        // precomputed neighbour half-site indices
+    const int *order;    // work item -> half-site ([stride], both parities) or nullptr
     const int *skip_if;  // skip the launch when *skip_if != 0
     const int *active;   // per-RHS mask (nullptr: all active)
-    // per-RHS operator (nullptr: the shared a/b and T above): slots of one batch share the
-    // gauge field but may carry different kappa, hence different b and clover terms
+    // per-RHS operator: slots of one batch share the gauge field but may carry different
+    // kappa, hence different b (nullptr: the shared b) and clover terms (FP32 bases)
     const double *b_slot;
     const void *const *clover_slot;
 };
 
-// out_r = a H in_r (EPI_SCALE), Tinv (a H in_r) (EPI_CLOVINV) or
-// G5^g (T y_r + b H in_r) (EPI_XPAY), for every active RHS r
-template <typename R, int EPI, class SB, class GaugeT, class CloverT>
-__global__ void __launch_bounds__(128) dslash_batch_kernel(const DslashBatchArg<SB, GaugeT, CloverT> arg)
+// The epilogue on H x (acc) for the pair q at half-site h; yv: the same-parity input
+// (EPI_XPAY only).
+template <int EPI, class SB, class GaugeT>
+LYM_D void batch_epilogue(const DslashBatchArg<SB, GaugeT> &arg, int h, int q, bool act_a, bool act_b, c2 acc[12],
+                          const c2 yv[12])
+{
+    const int ra = 2 * q, rb = 2 * q + 1;
+    c2 res[12];
+    const float4 *ta = nullptr, *tb = nullptr;
+    if (EPI != EPI_SCALE && arg.has_clover) {  // an inactive lane borrows its partner's operator
+        ta = (const float4 *)arg.clover_slot[act_a ? ra : rb];
+        tb = (const float4 *)arg.clover_slot[act_b ? rb : ra];
+    }
+    if (EPI == EPI_SCALE) {
+        const float2 a = make_float2(arg.a, arg.a);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) res[k] = c2{mul2(a, acc[k].re), mul2(a, acc[k].im)};
+    } else if (EPI == EPI_CLOVINV) {
+        const float2 a = make_float2(arg.a, arg.a);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) acc[k] = c2{mul2(a, acc[k].re), mul2(a, acc[k].im)};
+        if (!arg.has_clover) {
+#pragma unroll
+            for (int k = 0; k < 12; ++k) res[k] = acc[k];
+        } else if (ta == tb) {
+            clover_pair<true>(ta, tb, arg.g.stride, arg.parity, h, acc, res);
+        } else {
+            clover_pair<false>(ta, tb, arg.g.stride, arg.parity, h, acc, res);
+        }
+    } else {
+        if (!arg.has_clover) {
+#pragma unroll
+            for (int k = 0; k < 12; ++k) res[k] = yv[k];
+        } else if (ta == tb) {
+            clover_pair<true>(ta, tb, arg.g.stride, arg.parity, h, yv, res);
+        } else {
+            clover_pair<false>(ta, tb, arg.g.stride, arg.parity, h, yv, res);
+        }
+        float ba = arg.b, bb = arg.b;
+        if (arg.b_slot) {
+            ba = (float)arg.b_slot[act_a ? ra : rb];
+            bb = (float)arg.b_slot[act_b ? rb : ra];
+        }
+        const float2 b = make_float2(ba, bb);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) res[k] = c2{fma2(b, acc[k].re, res[k].re), fma2(b, acc[k].im, res[k].im)};
+        if (arg.gamma5) {  // lower spins: -(T y + b H x) = (-b) H x - T y
+            const float2 nb = make_float2(-ba, -bb);
+#pragma unroll
+            for (int k = 6; k < 12; ++k)
+                res[k] = c2{sub2(mul2(nb, acc[k].re), res[k].re), sub2(mul2(nb, acc[k].im), res[k].im)};
+        } else {
+#pragma unroll
+            for (int k = 6; k < 12; ++k) res[k] = c2{fma2(b, acc[k].re, res[k].re), fma2(b, acc[k].im, res[k].im)};
+        }
+    }
+    arg.out.store(h, q, res);
+}
+
+// out_r = a H in_r (EPI_SCALE), Tinv_r (a H in_r) (EPI_CLOVINV) or
+// G5^g (T_r y_r + b_r H in_r) (EPI_XPAY), for both RHS of every pair with an active RHS
+template <int EPI, int MINB, class SB, class GaugeT>
+__global__ void __launch_bounds__(128, MINB) dslash_batch_kernel(const DslashBatchArg<SB, GaugeT> arg)
 {
     if (arg.skip_if && *arg.skip_if) return;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int h = tid >> arg.lognb, r = tid & ((1 << arg.lognb) - 1);
-    if (h >= arg.g.Vh) return;
-    if (arg.active && !arg.active[r]) return;
-    const auto in = arg.in.bind(r);
-    CloverT T = arg.T;
-    if (arg.clover_slot) T.c = (decltype(T.c))arg.clover_slot[r];
-    cx<R> acc[12], res[12];
-    hopping_table<R>(arg.nbr, in, arg.U, arg.parity, h, acc);
-    if (EPI == EPI_SCALE) {
-#pragma unroll
-        for (int k = 0; k < 12; ++k) res[k] = (R)arg.a * acc[k];
-    } else if (EPI == EPI_CLOVINV) {
-#pragma unroll
-        for (int k = 0; k < 12; ++k) acc[k] = (R)arg.a * acc[k];
-        clover_apply<R>(T, arg.parity, h, acc, res);
-    } else {
-        cx<R> yv[12];
-        arg.y.bind(r).template load<R>(h, yv);
-        if (arg.has_clover) {
-            clover_apply<R>(T, arg.parity, h, yv, res);
-        } else {
-#pragma unroll
-            for (int k = 0; k < 12; ++k) res[k] = yv[k];
-        }
-        const R b = arg.b_slot ? (R)arg.b_slot[r] : (R)arg.b;
-#pragma unroll
-        for (int k = 0; k < 12; ++k) fma_r(res[k], b, acc[k]);
-        if (arg.gamma5) {
-#pragma unroll
-            for (int k = 6; k < 12; ++k) res[k] = -res[k];
-        }
+    const int wi = tid >> arg.lognp, q = tid & ((1 << arg.lognp) - 1);
+    if (wi >= arg.g.Vh) return;
+    bool act_a = true, act_b = true;
+    if (arg.active) {
+        act_a = arg.active[2 * q] != 0;
+        act_b = arg.active[2 * q + 1] != 0;
+        if (!act_a && !act_b) return;
     }
-    arg.out.bind(r).template store<R>(h, res);
+    const int h = arg.order ? __ldg(arg.order + wi) : wi;
+    int nf[4], nbk[4];
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) {
+        nf[mu] = arg.nbr.get(arg.parity, mu, 0, h);
+        nbk[mu] = arg.nbr.get(arg.parity, mu, 1, h);
+    }
+    c2 acc[12];
+    hopping_pair<GaugeT::kReal>(nf, nbk, arg.in, arg.U, arg.parity, h, q, acc);
+    if (EPI == EPI_XPAY) {
+        c2 yv[12];
+        arg.y.load_cs(h, q, yv);
+        batch_epilogue<EPI>(arg, h, q, act_a, act_b, acc, yv);
+    } else {
+        batch_epilogue<EPI>(arg, h, q, act_a, act_b, acc, acc);
+    }
 }
 
 // --------------------------------------------------- batch site kernels ----
-// Like site_kernel, over (h, r) pairs; each thread keeps one r (the grid stride is a
-// multiple of nb), reductions are per RHS: partials[block][r][k], and the last block
-// runs Op::finalize(r, totals) for every r in parallel (thread r).
+// Like site_kernel, over (h, pair) items with the pair index fastest; each thread keeps
+// one pair (the grid stride is a multiple of np), its FP64 partial sums are per RHS,
+// acc[lane * NRED + k], and the last block runs Op::finalize(r, totals) for every r in
+// parallel (thread r), then Op::finalize_all().
 template <class Op>
-__global__ void __launch_bounds__(kBlasThreads) site_batch_kernel(Op op, int vh, int lognb, double *partials,
+__global__ void __launch_bounds__(kBlasThreads) site_batch_kernel(Op op, int vh, int lognp, double *partials,
                                                                   unsigned int *counter, Gate gate)
 {
     if (gate.closed()) return;
     constexpr int NR = Op::NRED > 0 ? Op::NRED : 1;
-    const int nb = 1 << lognb;
+    const int np = 1 << lognp, nb = 2 * np;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int r = tid & (nb - 1);
-    double acc[NR];
+    const int q = tid & (np - 1);
+    double acc[2 * NR];
 #pragma unroll
-    for (int k = 0; k < NR; ++k) acc[k] = 0.0;
-    const long total = (long)vh << lognb;
-    for (long i = tid; i < total; i += (long)gridDim.x * blockDim.x) op.site((int)(i >> lognb), r, acc);
+    for (int k = 0; k < 2 * NR; ++k) acc[k] = 0.0;
+    const long total = (long)vh << lognp;
+    for (long i = tid; i < total; i += (long)gridDim.x * blockDim.x) op.site((int)(i >> lognp), q, acc);
     if constexpr (Op::NRED > 0) {
         __shared__ double smem[kBlasThreads / 32][kMaxBatch][NR];
         __shared__ bool last;
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-        for (int k = 0; k < NR; ++k) {
+        for (int k = 0; k < 2 * NR; ++k) {
             double x = acc[k];
-            for (int o = 16; o >= nb; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            for (int o = 16; o >= np; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
             acc[k] = x;
         }
-        if (lane < nb)
+        if (lane < np)
 #pragma unroll
-            for (int k = 0; k < NR; ++k) smem[warp][lane][k] = acc[k];
+            for (int k = 0; k < NR; ++k) {
+                smem[warp][2 * lane][k] = acc[k];
+                smem[warp][2 * lane + 1][k] = acc[NR + k];
+            }
         __syncthreads();
         if (threadIdx.x < nb) {
             for (int k = 0; k < NR; ++k) {
@@ -234,18 +638,21 @@ struct BatchCGState {
     int failed;
 };
 
+// alpha_r = rr_r / <p_r, A p_r>
 template <class SP, class SAp> struct OpBAlpha {
     static constexpr int NRED = 2;
     SP p;
     SAp ap;
     BatchCGState *s;
-    LYM_D void site(int h, int r, double *acc) const
+    LYM_D void site(int h, int q, double *acc) const
     {
-        if (!s->active[r]) return;
-        cx<double> x[12], y[12];
-        p.bind(r).template load<double>(h, x);
-        ap.bind(r).template load<double>(h, y);
-        dotc(x, y, acc[0], acc[1]);
+        const bool a0 = s->active[2 * q] != 0, a1 = s->active[2 * q + 1] != 0;
+        if (!a0 && !a1) return;
+        cx<double> x0[12], x1[12], y0[12], y1[12];
+        p.load_d(h, q, x0, x1);
+        ap.load_d(h, q, y0, y1);
+        if (a0) dotc(x0, y0, acc[0], acc[1]);
+        if (a1) dotc(x1, y1, acc[2], acc[3]);
     }
     LYM_D void finalize(int r, const double *t) const
     {
@@ -254,6 +661,8 @@ template <class SP, class SAp> struct OpBAlpha {
     LYM_D void finalize_all() const {}
 };
 
+// x_r += alpha_r p_r, res_r -= alpha_r A p_r, rr_r = |res_r|^2 and the convergence /
+// reliable-update decisions
 template <class SX, class SP, class SR, class SAp> struct OpBUpdate {
     static constexpr int NRED = 1;
     SX x;
@@ -261,23 +670,28 @@ template <class SX, class SP, class SR, class SAp> struct OpBUpdate {
     SR rv;
     SAp ap;
     BatchCGState *s;
-    LYM_D void site(int h, int r, double *acc) const
+    LYM_D void site(int h, int q, double *acc) const
     {
-        if (!s->active[r]) return;
-        const cx<double> al = {s->alpha[r].x, s->alpha[r].y};
-        cx<double> xv[12], pv[12], res[12], av[12];
-        x.bind(r).template load<double>(h, xv);
-        p.bind(r).template load<double>(h, pv);
-        rv.bind(r).template load<double>(h, res);
-        ap.bind(r).template load<double>(h, av);
+        const bool act[2] = {s->active[2 * q] != 0, s->active[2 * q + 1] != 0};
+        if (!act[0] && !act[1]) return;
+        cx<double> xv[2][12], pv[2][12], res[2][12], av[2][12];
+        x.load_d(h, q, xv[0], xv[1]);
+        p.load_d(h, q, pv[0], pv[1]);
+        rv.load_d(h, q, res[0], res[1]);
+        ap.load_d(h, q, av[0], av[1]);
 #pragma unroll
-        for (int k = 0; k < 12; ++k) {
-            fma_c(xv[k], al, pv[k]);
-            res[k] = res[k] - al * av[k];
+        for (int l = 0; l < 2; ++l) {
+            if (!act[l]) continue;
+            const cx<double> al = {s->alpha[2 * q + l].x, s->alpha[2 * q + l].y};
+#pragma unroll
+            for (int k = 0; k < 12; ++k) {
+                fma_c(xv[l][k], al, pv[l][k]);
+                res[l][k] = res[l][k] - al * av[l][k];
+            }
+            acc[l] += norm2(res[l]);
         }
-        acc[0] += norm2(res);
-        x.bind(r).template store<double>(h, xv);
-        rv.bind(r).template store<double>(h, res);
+        x.store_d(h, q, xv[0], xv[1]);
+        rv.store_d(h, q, res[0], res[1]);
     }
     LYM_D void finalize(int r, const double *t) const
     {
@@ -306,21 +720,29 @@ template <class SX, class SP, class SR, class SAp> struct OpBUpdate {
     }
 };
 
+// p_r = res_r + beta_r p_r for the active RHS that need no reliable update
 template <class SP, class SR> struct OpBDirection {
     static constexpr int NRED = 0;
     SP p;
     SR rv;
     BatchCGState *s;
-    LYM_D void site(int h, int r, double *) const
+    LYM_D void site(int h, int q, double *) const
     {
-        if (!s->active[r] || s->need_update[r]) return;
-        const double b = s->beta[r];
-        cx<double> pv[12], res[12];
-        p.bind(r).template load<double>(h, pv);
-        rv.bind(r).template load<double>(h, res);
+        bool go[2];
 #pragma unroll
-        for (int k = 0; k < 12; ++k) pv[k] = res[k] + b * pv[k];
-        p.bind(r).template store<double>(h, pv);
+        for (int l = 0; l < 2; ++l) go[l] = s->active[2 * q + l] && !s->need_update[2 * q + l];
+        if (!go[0] && !go[1]) return;
+        cx<double> pv[2][12], res[2][12];
+        p.load_d(h, q, pv[0], pv[1]);
+        rv.load_d(h, q, res[0], res[1]);
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+            if (!go[l]) continue;
+            const double b = s->beta[2 * q + l];
+#pragma unroll
+            for (int k = 0; k < 12; ++k) pv[l][k] = res[l][k] + b * pv[l][k];
+        }
+        p.store_d(h, q, pv[0], pv[1]);
     }
     LYM_D void finalize(int, const double *) const {}
     LYM_D void finalize_all() const {}

@@ -305,7 +305,7 @@ struct GaugeF9 {
 struct NbrTable {
     const int *n;
     int stride;
-    LYM_D int get(int p, int mu, int dir, int h) const { return __ldg(n + (size_t)(p * 8 + 2 * mu + dir) * stride + h); }
+    LYM_D int get(int p, int mu, int dir, int h) const { return __ldg(n + ((unsigned)(p * 8 + 2 * mu + dir) * stride + h)); }
 };
 
 // FP32 complex, 12 reals: rows 0 and 1; row 2 = sign * conj(row0 x row1)

@@ -35,10 +35,11 @@ struct GaugeDev {
     void *h16 = nullptr;       // FP16 reconstructed: uint2[2][4][3][stride] or half2[2][4][3][stride]
     uint8_t *sign = nullptr;   // [2][stride]
     bool recon_ok = false;
-    // FP32 without reconstruction, for the batched stencil (link bytes are shared by the
-    // batch, the reconstruction arithmetic would not be): float2[2][4][9][stride] (SU3)
-    // or float[2][4][9][stride] (adjoint)
-    void *f32full = nullptr;
+    // FP32 without reconstruction and with every component duplicated into both lanes of
+    // a float2 pair, for the batched stencil (link bytes are shared by the batch, the
+    // reconstruction arithmetic would not be): float4 (re, re, im, im)[2][4][9][stride]
+    // (SU3) or float2 (u, u)[2][4][9][stride] (adjoint)
+    void *f32dup = nullptr;
 };
 
 struct CloverDev {
@@ -99,15 +100,22 @@ struct DslashBatchParams {
     int prec = PREC_F, rep = REP_SU3, epi = EPI_SCALE_, parity = 0, gamma5 = 0;
     SpinorBatch in, out, y;
     const GaugeDev *U = nullptr;
-    const void *clover = nullptr;
+    int has_clover = 0;
     double a = 1.0, b = 0.0;
     const int *skip_if = nullptr;
     const int *active = nullptr;
     const int *nbr = nullptr;                  // neighbour table [2][8][stride]
+    const int *order = nullptr;                // traversal table [stride] or nullptr (h order)
+    int minb = 1;                              // kernel variant: minimum resident blocks per SM
     const double *b_slot = nullptr;            // device array [nb] or nullptr
-    const void *const *clover_slot = nullptr;  // device array [nb] of clover bases or nullptr
+    const void *const *clover_slot = nullptr;  // device array [nb] of FP32 clover bases (T or Tinv)
 };
 
 void launch_dslash_batch(const DslashBatchParams &P, cudaStream_t st);
 void launch_nbr_table(const Geom &g, int *nbr, cudaStream_t st);
+// traversal of the half-sites in by * bz columns of the (y, z) plane, t fastest
+// (by | Ly, bz | Lz)
+void launch_order_table(const Geom &g, int by, int bz, int *order, cudaStream_t st);
+extern const int kBatchMinBlocks[];  // the compiled variants of the batched stencil
+extern const int kBatchMinBlocksCount;
 }  // namespace lym

@@ -162,7 +162,7 @@ LYM_D void load_link_d(const Geom &g, int rep, const void *d64, int p, int mu, i
 // accepted when it is +-V with V special unitary (SU(3)) or special orthogonal
 // (adjoint); the sign goes to the sign table.
 __global__ void compress_gauge_kernel(Geom g, int rep, const void *d64, void *f32, void *h16, uint8_t *sign, int *err,
-                                      void *f32full)
+                                      void *f32dup)
 {
     const int h = blockIdx.x * blockDim.x + threadIdx.x;
     const int p = blockIdx.y;
@@ -190,8 +190,9 @@ __global__ void compress_gauge_kernel(Geom g, int rep, const void *d64, void *f3
         bits |= (uint8_t)(neg << mu);
         for (int kk = 0; kk < 9; ++kk) {
             const size_t wf = ((size_t)(p * 4 + mu) * 9 + kk) * g.stride + h;
-            if (rep == REP_SU3) ((float2 *)f32full)[wf] = make_float2(u[kk / 3][kk % 3].re, u[kk / 3][kk % 3].im);
-            else ((float *)f32full)[wf] = (float)u[kk / 3][kk % 3].re;
+            const float ure = (float)u[kk / 3][kk % 3].re, uim = (float)u[kk / 3][kk % 3].im;
+            if (rep == REP_SU3) ((float4 *)f32dup)[wf] = make_float4(ure, ure, uim, uim);
+            else ((float2 *)f32dup)[wf] = make_float2(ure, ure);
         }
         const size_t w0 = (size_t)(p * 4 + mu) * 3 * g.stride + h;
         if (rep == REP_SU3) {
@@ -226,7 +227,7 @@ __global__ void compress_gauge_kernel(Geom g, int rep, const void *d64, void *f3
 void launch_compress_gauge(const Geom &g, GaugeDev &U, int *err, cudaStream_t st)
 {
     dim3 grid(nblocks(g.Vh, 128), 2);
-    compress_gauge_kernel<<<grid, 128, 0, st>>>(g, U.rep, U.d64, U.f32, U.h16, U.sign, err, U.f32full);
+    compress_gauge_kernel<<<grid, 128, 0, st>>>(g, U.rep, U.d64, U.f32, U.h16, U.sign, err, U.f32dup);
 }
 
 // Fundamental gauge links -> fermion links: the adjoint map for SU(2)

@@ -298,3 +298,33 @@ class SquareEvenOddImprovedDiracWilsonOperator(DiracOperator):
 
     def __init__(self, lattice, kappa=0.0, csw=1.0, gamma5=True):
         super().__init__(lattice, kappa, csw, gamma5)
+
+
+def multiply_batch(operators, inputs, precision="single"):
+    """EvenOddImprovedDiracWilsonOperator::multiply of operators[j] applied to inputs[j]
+    for up to 32 inputs in one batched stencil (FP32 or FP16 storage).  The operators
+    share the lattice, the gauge field and the gamma5 flag; kappa and c_sw may differ."""
+    if len(operators) != len(inputs) or not inputs:
+        raise ValueError("one operator per input")
+    lat = operators[0].lattice
+    xs = [operators[0]._vec(x) for x in inputs]
+    outs = [lat.new_vector() for _ in xs]
+    ids = (C.c_int * len(xs))(*[op.op_id for op in operators])
+    ip = (C.c_void_p * len(xs))(*[x.ctypes.data for x in xs])
+    op_ = (C.c_void_p * len(xs))(*[o.ctypes.data for o in outs])
+    _check(lat.handle, lib().lym_multiply_batch(lat.handle, PRECISIONS[precision], len(xs), ids, ip, op_))
+    return outs
+
+
+def set_batch_tile(lattice, by, bz, minb=1):
+    """Force the batched stencil's traversal column (by * bz sites of the (y, z) plane;
+    by = 0: plain half-site order) and kernel variant (by < 0: autotune)."""
+    _check(lattice.handle, lib().lym_set_batch_tile(lattice.handle, by, bz, minb))
+
+
+def batch_tile(lattice, precision, batch, clover=True):
+    """The (by, bz, minb) configuration the batched stencil uses for this key."""
+    by, bz, mb = C.c_int(), C.c_int(), C.c_int()
+    _check(lattice.handle, lib().lym_get_batch_tile(lattice.handle, PRECISIONS[precision], batch, int(clover),
+                                                    C.byref(by), C.byref(bz), C.byref(mb)))
+    return by.value, bz.value, mb.value
