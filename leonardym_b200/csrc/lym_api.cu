@@ -1089,7 +1089,10 @@ BatchTile tune_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, con
                      const SpinorBatch &in, const SpinorBatch &tmp, const double *b_slot, const void *const *T_slot,
                      const void *const *Ti_slot)
 {
-    if (c->tile_forced) return c->forced_tile;
+    if (c->tile_forced) {
+        order_table(c, c->forced_tile.by, c->forced_tile.bz);  // built now, before any capture
+        return c->forced_tile;
+    }
     const int key = (prec * 64 + in.nb) * 2 + (clov ? 1 : 0);
     auto it = c->tiles.find(key);
     if (it != c->tiles.end()) return it->second;

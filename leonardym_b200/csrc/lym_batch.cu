@@ -5,10 +5,25 @@
 
 namespace lym {
 
-// Variants of the batched stencil by the register budget the compiler is held to
-// (__launch_bounds__(128, minb)); the autotuner times them.
-const int kBatchMinBlocks[] = {1, 3, 4};
-const int kBatchMinBlocksCount = 3;
+// Variants of the batched stencil the autotuner times: the register budget the compiler
+// is held to (__launch_bounds__(128, minb)) for the direct-load kernel (codes 1, 3, 4),
+// and the same for the kernel that stages neighbour spinors in shared memory (codes
+// 16 + minb: 19, 20).
+const int kBatchMinBlocks[] = {1, 3, 4, 19, 20};
+const int kBatchMinBlocksCount = 5;
+
+template <int EPI, int MINB, class SB, class G>
+static void launch_staged(const DslashBatchArg<SB, G> &a, int nblk, cudaStream_t st)
+{
+    static bool attr = false;  // the shared-memory limit above 48 KB, once per instantiation
+    const int bytes = staged_smem_bytes(a.lognp);
+    if (!attr) {
+        cudaFuncSetAttribute(dslash_batch_staged_kernel<EPI, MINB, SB, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             staged_smem_bytes(0));
+        attr = true;
+    }
+    dslash_batch_staged_kernel<EPI, MINB><<<nblk, kStagedThreads, bytes, st>>>(a);
+}
 
 static BatchF fview(const SpinorBatch &s) { return BatchF{(float4 *)s.v, s.stride, s.lognb - 1}; }
 static BatchH hview(const SpinorBatch &s) { return BatchH{(int4 *)s.v, (float2 *)s.norm, s.stride, s.lognb - 1}; }
@@ -21,6 +36,8 @@ static void launch_minb(const DslashBatchParams &P, const DslashBatchArg<SB, G> 
     switch (P.minb) {
     case 3: dslash_batch_kernel<EPI, 3><<<nb, 128, 0, st>>>(a); break;
     case 4: dslash_batch_kernel<EPI, 4><<<nb, 128, 0, st>>>(a); break;
+    case 19: launch_staged<EPI, 3>(a, nb, st); break;
+    case 20: launch_staged<EPI, 4>(a, nb, st); break;
     default: dslash_batch_kernel<EPI, 1><<<nb, 128, 0, st>>>(a); break;
     }
 }

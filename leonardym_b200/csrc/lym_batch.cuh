@@ -63,6 +63,19 @@ template <int S> LYM_D c2 add_code(c2 a, int code, c2 z)
     }
 }
 
+// ----------------------------------------------------- asynchronous copies --
+LYM_D unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+LYM_D void cp_async16(unsigned saddr, const void *g)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(saddr), "l"(g) : "memory");
+}
+LYM_D void cp_async8(unsigned saddr, const void *g)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(saddr), "l"(g) : "memory");
+}
+LYM_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> LYM_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // ------------------------------------------------------------- batch views --
 // One RHS r of a FP32 pair-layout batch, as a single half-spinor view (slot set-up and
 // extraction; not on the iteration path).
@@ -138,6 +151,22 @@ struct BatchF {
 #pragma unroll
         for (int c = 0; c < 12; ++c)
             v[at(c, h, q)] = make_float4((float)a[c].re, (float)b[c].re, (float)a[c].im, (float)b[c].im);
+    }
+    // asynchronous copy of the pair's 12 words into shared memory (word c at s0 + c * sstep
+    // bytes) and the read back from there (word c at p0[c * step])
+    LYM_D void stage(unsigned s0, unsigned sstep, int h, int q) const
+    {
+        const unsigned b = at(0, h, q), s = (unsigned)stride << lognp;
+#pragma unroll
+        for (int c = 0; c < 12; ++c) cp_async16(s0 + c * sstep, v + b + c * s);
+    }
+    LYM_D void unstage(const float4 *p0, int step, c2 x[12]) const
+    {
+#pragma unroll
+        for (int c = 0; c < 12; ++c) {
+            const float4 w = p0[c * step];
+            x[c] = c2{make_float2(w.x, w.y), make_float2(w.z, w.w)};
+        }
     }
     LYM_HD SlotF slot(int r) const { return SlotF{(float *)v, stride, lognp, r}; }
 };
@@ -238,6 +267,26 @@ struct BatchH {
             x[c] = c2{make_float2((float)a[c].re, (float)b[c].re), make_float2((float)a[c].im, (float)b[c].im)};
         store(h, q, x);
     }
+    // the 6 words and the norm (word 6) through shared memory, as BatchF::stage / unstage
+    LYM_D void stage(unsigned s0, unsigned sstep, int h, int q) const
+    {
+        const unsigned b = at(0, h, q), s = (unsigned)stride << lognp;
+#pragma unroll
+        for (int w = 0; w < 6; ++w) cp_async16(s0 + w * sstep, v + b + w * s);
+        cp_async8(s0 + 6 * sstep, norm + ((unsigned)h << lognp) + q);
+    }
+    LYM_D void unstage(const float4 *p0, int step, c2 x[12]) const
+    {
+        const float4 nw = p0[6 * step];
+        const float2 n = make_float2(nw.x, nw.y);
+#pragma unroll
+        for (int w = 0; w < 6; ++w) {
+            const int4 u = *reinterpret_cast<const int4 *>(p0 + w * step);
+            const __half2 *hp = reinterpret_cast<const __half2 *>(&u);
+            x[2 * w] = c2{mul2(__half22float2(hp[0]), n), mul2(__half22float2(hp[1]), n)};
+            x[2 * w + 1] = c2{mul2(__half22float2(hp[2]), n), mul2(__half22float2(hp[3]), n)};
+        }
+    }
     LYM_HD SlotH slot(int r) const { return SlotH{(__half *)v, (float *)norm, stride, lognp, r}; }
 };
 
@@ -263,6 +312,20 @@ struct GaugeDupC {  // SU(3): float4 (re, re, im, im) per component, [parity][mu
             L.ui[k / 3][k % 3] = make_float2(w.z, w.w);
         }
     }
+    // word k of link (p, mu, h) copied to shared memory / a link read from 9 staged words
+    LYM_D void stage(int p, int mu, int k, int h, unsigned saddr) const
+    {
+        cp_async16(saddr, u + ((unsigned)((p * 4 + mu) * 9 + k) * stride + h));
+    }
+    LYM_D void unstage(const float4 *w9, LinkP &L) const
+    {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            const float4 w = w9[k];
+            L.ur[k / 3][k % 3] = make_float2(w.x, w.y);
+            L.ui[k / 3][k % 3] = make_float2(w.z, w.w);
+        }
+    }
 };
 
 struct GaugeDupR {  // real adjoint links: float2 (u, u) per component, [parity][mu][9][stride]
@@ -274,6 +337,18 @@ struct GaugeDupR {  // real adjoint links: float2 (u, u) per component, [parity]
         const float2 *b = u + ((unsigned)(p * 4 + mu) * 9 * stride + h);
 #pragma unroll
         for (int k = 0; k < 9; ++k) L.ur[k / 3][k % 3] = __ldcs(b + k * stride);
+    }
+    LYM_D void stage(int p, int mu, int k, int h, unsigned saddr) const
+    {
+        cp_async8(saddr, u + ((unsigned)((p * 4 + mu) * 9 + k) * stride + h));
+    }
+    LYM_D void unstage(const float4 *w9, LinkP &L) const
+    {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            const float4 w = w9[k];
+            L.ur[k / 3][k % 3] = make_float2(w.x, w.y);
+        }
     }
 };
 
@@ -551,6 +626,116 @@ __global__ void __launch_bounds__(128, MINB) dslash_batch_kernel(const DslashBat
         batch_epilogue<EPI>(arg, h, q, act_a, act_b, acc, yv);
     } else {
         batch_epilogue<EPI>(arg, h, q, act_a, act_b, acc, acc);
+    }
+}
+
+// ------------------------------------------------------ staged batch stencil --
+// The same stencil with the neighbour spinors and links of direction d + 1 copied into
+// shared memory (cp.async) while direction d is computed, so the loads of the next
+// term overlap the arithmetic of this one without holding registers.  Shared memory
+// per block of 128 threads: two buffers of 12 words per thread (the thread's own
+// spinor words) and two buffers of 9 link words per half-site; the np threads of a
+// half-site copy its link words between them and meet at __syncwarp before reading.
+constexpr int kStagedThreads = 128;
+LYM_HD int staged_smem_bytes(int lognp)
+{
+    return (2 * 12 * kStagedThreads + 2 * (kStagedThreads >> lognp) * 9) * 16;
+}
+
+template <bool STAGE_Y, class SB, class GaugeT> struct StagedHop {
+    const DslashBatchArg<SB, GaugeT> &arg;
+    float4 *smem;
+    int h, q, np, site, lane_in;
+    int nf[4], nbk[4];
+    bool live;
+    unsigned vmask;
+
+    LYM_D float4 *sx(int buf) const { return smem + buf * 12 * kStagedThreads + threadIdx.x; }
+    LYM_D float4 *sl(int buf) const
+    {
+        return smem + 2 * 12 * kStagedThreads + (buf * (kStagedThreads / np) + site) * 9;
+    }
+    template <int D> LYM_D void issue() const
+    {
+        constexpr int MU = D / 2, DIR = D % 2;
+        const int n = DIR == 0 ? nf[MU] : nbk[MU];
+        if (live) arg.in.stage(smem_u32(sx(D & 1)), kStagedThreads * 16, n, q);
+        const int lp = DIR == 0 ? arg.parity : 1 - arg.parity, lh = DIR == 0 ? h : n;
+        float4 *L = sl(D & 1);
+        for (int k = lane_in; k < 9; k += np) arg.U.stage(lp, MU, k, lh, smem_u32(L + k));
+    }
+    template <int D> LYM_D void step(c2 acc[12]) const
+    {
+        if constexpr (D < 7) {
+            issue<D + 1>();
+        } else if constexpr (STAGE_Y) {
+            if (live) arg.y.stage(smem_u32(sx(0)), kStagedThreads * 16, h, q);
+        }
+        cp_async_commit();
+        cp_async_wait<1>();  // the copies of direction D (this thread's)
+        __syncwarp(vmask);   // ... and those of the other lanes of the half-site
+        if (live) {
+            c2 x[12];
+            arg.in.unstage(sx(D & 1), kStagedThreads, x);
+            LinkP L;
+            arg.U.unstage(sl(D & 1), L);
+            accumulate_dir<GaugeT::kReal, D / 2, D % 2>(x, L, acc);
+        }
+        __syncwarp(vmask);  // every lane is done with buffer D & 1 before it is refilled
+    }
+};
+
+template <int EPI, int MINB, class SB, class GaugeT>
+__global__ void __launch_bounds__(kStagedThreads, MINB)
+    dslash_batch_staged_kernel(const DslashBatchArg<SB, GaugeT> arg)
+{
+    extern __shared__ float4 stage_smem[];
+    if (arg.skip_if && *arg.skip_if) return;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int wi = tid >> arg.lognp, q = tid & ((1 << arg.lognp) - 1);
+    const bool valid = wi < arg.g.Vh;  // equal for all lanes of a half-site
+    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+    if (!valid) return;
+    bool act_a = true, act_b = true;
+    if (arg.active) {
+        act_a = arg.active[2 * q] != 0;
+        act_b = arg.active[2 * q + 1] != 0;
+    }
+    const int np = 1 << arg.lognp;
+    StagedHop<EPI == EPI_XPAY, SB, GaugeT> s{arg, stage_smem, 0, q, np, (int)threadIdx.x >> arg.lognp,
+                                             (int)threadIdx.x & (np - 1)};
+    s.h = arg.order ? __ldg(arg.order + wi) : wi;
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) {
+        s.nf[mu] = arg.nbr.get(arg.parity, mu, 0, s.h);
+        s.nbk[mu] = arg.nbr.get(arg.parity, mu, 1, s.h);
+    }
+    s.live = act_a || act_b;  // idle pairs still copy their share of the link words
+    s.vmask = vmask;
+    c2 acc[12];
+#pragma unroll
+    for (int k = 0; k < 12; ++k) acc[k] = c2{make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+    s.template issue<0>();
+    cp_async_commit();
+    s.template step<0>(acc);
+    s.template step<1>(acc);
+    s.template step<2>(acc);
+    s.template step<3>(acc);
+    s.template step<4>(acc);
+    s.template step<5>(acc);
+    s.template step<6>(acc);
+    s.template step<7>(acc);
+    if (!s.live) {
+        cp_async_wait<0>();
+        return;
+    }
+    if (EPI == EPI_XPAY) {
+        cp_async_wait<0>();
+        c2 yv[12];
+        arg.y.unstage(s.sx(0), kStagedThreads, yv);
+        batch_epilogue<EPI>(arg, s.h, q, act_a, act_b, acc, yv);
+    } else {
+        batch_epilogue<EPI>(arg, s.h, q, act_a, act_b, acc, acc);
     }
 }
 
