@@ -263,6 +263,18 @@ def gpu_eo_bicgstab_iterations():
         return n
 
 
+def block_solver(args):
+    """The solver id of the block solves: mixed-precision even-odd CG on (gamma5 S)^2 or
+    BiCGStab on S, with single (FP32) or half (FP16 + norms) inner storage."""
+    from leonardym_b200 import solvers as S
+    return {("cg", "single"): S.SOLVER_EO_CG_MIXED_SINGLE, ("cg", "half"): S.SOLVER_EO_CG_MIXED_HALF,
+            ("bicgstab", "single"): S.SOLVER_EO_BICGSTAB_MIXED_SINGLE,
+            ("bicgstab", "half"): S.SOLVER_EO_BICGSTAB_MIXED_HALF}[(args.solver, args.precision)]
+
+
+SOLVER_NAMES = {"cg": "block even-odd CG on (gamma5 S)^2", "bicgstab": "block even-odd BiCGStab on S"}
+
+
 def config_dict(solver):
     return {"workload": "su3-clover-24^3x48-kappa0.137-csw1.7-44rhs-tol1e-10", "lattice": "24x24x24x48",
             "representation": "SU(3) fundamental", "kappa": KAPPA, "csw": CSW, "links": "exp(i 0.25 H), seeded",
@@ -276,11 +288,11 @@ def run_ours(args, world, rank, local):
 
     import leonardym_b200 as L
     from leonardym_b200 import synth
-    from leonardym_b200.solvers import SOLVER_EO_CG, SOLVER_EO_CG_MIXED_HALF, SOLVER_EO_CG_MIXED_SINGLE
+    from leonardym_b200.solvers import SOLVER_EO_CG
 
     lib = L.lib()
     torch.cuda.set_device(local)
-    solver = {"single": SOLVER_EO_CG_MIXED_SINGLE, "half": SOLVER_EO_CG_MIXED_HALF}[args.precision]
+    solver = block_solver(args)
     sprec = 1 if args.precision == "single" else 2
     links = workload_links()
     srcs = workload_sources()
@@ -404,7 +416,7 @@ def run_ours(args, world, rank, local):
         "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32" if sprec == 1 else "f16",
         "data": "synthetic (seeded links and sources)",
-        "config": config_dict(f"block even-odd CG, {args.batch} right-hand sides per batched stencil, "
+        "config": config_dict(f"{SOLVER_NAMES[args.solver]}, {args.batch} right-hand sides per batched stencil, "
                               f"{args.precision} storage + FP64 reliable updates"),
         "fp64_eo_cg_solves_per_s": fp64_value,
         "mixed_over_fp64": value / world / (fp64_value / world),
@@ -433,28 +445,30 @@ def run_profile(args):
     `batch` noise sources, then 10 launches each of the single-RHS and the batched
     stencil kernels (a few GB on the device)."""
     import leonardym_b200 as L
-    from leonardym_b200.solvers import SOLVER_EO_CG_MIXED_HALF, SOLVER_EO_CG_MIXED_SINGLE
     lib = L.lib()
     lat = L.Lattice(DIMS, "su3", device=0)
     op = L.ImprovedDiracWilsonOperator(lat, KAPPA, CSW, gamma5=False)
     op.setLattice(workload_links())
     srcs = workload_sources()[N_POINT:N_POINT + args.batch]
     xs = [lat.new_vector() for _ in srcs]
-    solver = {"single": SOLVER_EO_CG_MIXED_SINGLE, "half": SOLVER_EO_CG_MIXED_HALF}[args.precision]
+    solver = block_solver(args)
     if args.tile:  # a fixed batched-stencil configuration instead of the autotuner's
         by, bz, minb = (int(v) for v in args.tile.split(","))
         lib.lym_set_batch_tile(lat.handle, by, bz, minb)
     bstats = (L.SolveStats * len(srcs))()
     sp_ = (C.c_void_p * len(srcs))(*[s.ctypes.data for s in srcs])
     xp_ = (C.c_void_p * len(srcs))(*[x.ctypes.data for x in xs])
+    t0 = time.perf_counter()
     rc = lib.lym_solve_block(lat.handle, op.op_id, solver, -TOL, 20000, len(srcs), sp_, xp_, args.batch, bstats)
+    t_solve = time.perf_counter() - t0
     st = bstats[0]
     ms = C.c_double(0)
     sp = 1 if args.precision == "single" else 2
     lib.lym_time_stencil(lat.handle, op.op_id, sp, 0, 10, C.byref(ms))
     msb = C.c_double(0)
     lib.lym_time_stencil_batch(lat.handle, op.op_id, sp, 0, args.batch, 10, C.byref(msb))
-    print(f"profile case: rc {rc}, iterations {st.iterations}, true residual {st.true_residual:.2e}, "
+    print(f"profile case: rc {rc}, block solve {t_solve:.3f} s, updates {st.reliable_updates}, "
+          f"iterations {st.iterations}, true residual {st.true_residual:.2e}, "
           f"stencil {ms.value * 1e3:.1f} us, batched stencil ({args.batch}) {msb.value * 1e3:.1f} us")
     lat.close()
     if rc != 0:
@@ -468,6 +482,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="single", choices=["single", "half"])
+    ap.add_argument("--solver", default="cg", choices=["cg", "bicgstab"], help="the block solver of the timed solves")
     ap.add_argument("--batch", type=int, default=16, help="right-hand sides per batched stencil (power of 2 <= 32)")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--profile", action="store_true", help="small fixed case for ncu captures")

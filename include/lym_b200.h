@@ -69,7 +69,12 @@ enum lym_solver {
     LYM_SOLVER_EO_BICGSTAB = 2,      /* PreconditionedBiCGStab::solve (inverters/PreconditionedBiCGStab.cpp:33-100) */
     LYM_SOLVER_EO_CG = 3,            /* even-odd Schur CG on (g5 S)^2, D x = b, FP64 throughout          */
     LYM_SOLVER_EO_CG_MIXED_SINGLE = 4, /* same, FP32 stencil inner iterations, FP64 reliable updates     */
-    LYM_SOLVER_EO_CG_MIXED_HALF = 5    /* same, FP16 spinor storage (per-site norm) inner iterations     */
+    LYM_SOLVER_EO_CG_MIXED_HALF = 5,   /* same, FP16 spinor storage (per-site norm) inner iterations     */
+    /* BiCGStab (inverters/BiConjugateGradient.cpp:321-507) on the even-odd Schur operator S
+     * itself (not squared): D x = b, FP32 or FP16 inner iterations, FP64 reliable updates that
+     * restart from the true residual; no initial guess */
+    LYM_SOLVER_EO_BICGSTAB_MIXED_SINGLE = 6,
+    LYM_SOLVER_EO_BICGSTAB_MIXED_HALF = 7
 };
 
 enum lym_multishift_solver {
@@ -177,8 +182,9 @@ int lym_solve_shifted(lym_context *ctx, int op_id, double shift_re, double shift
  * noise sources one by one, correlators/MesonCorrelator.cpp:92-98,
  * fermion_measurements/ChiralCondensate.cpp:86-105) ----------------------------------
  * Solves D x_j = b_j for nrhs sources with the mixed-precision even-odd CG
- * (LYM_SOLVER_EO_CG_MIXED_SINGLE or _HALF), `batch` right-hand sides at a time (a power of
- * two <= 32; 0 selects 16) through one batched stencil: links and clover are read once
+ * (LYM_SOLVER_EO_CG_MIXED_SINGLE or _HALF) or BiCGStab (LYM_SOLVER_EO_BICGSTAB_MIXED_SINGLE
+ * or _HALF), `batch` right-hand sides at a time (a power of two <= 32, at least 2; 0 selects
+ * 16) through one batched stencil: links and clover are read once
  * per site for the whole batch.  Each right-hand side keeps its own scalars, convergence
  * mask and FP64 reliable updates, so its result does not depend on its batch mates beyond
  * rounding.  stats (nrhs entries) may be NULL. */

@@ -8,13 +8,14 @@ from ._lib import LymError, SolveStats, build, declared_symbols, lib
 from .dirac import (DiracOperator, DiracWilsonOperator, EvenOddImprovedDiracWilsonOperator,
                     ImprovedDiracWilsonOperator, Lattice, SquareDiracWilsonOperator,
                     SquareEvenOddImprovedDiracWilsonOperator, SquareImprovedDiracWilsonOperator)
-from .solvers import (BiConjugateGradient, ConjugateGradient, EvenOddConjugateGradient, MultishiftSolver,
-                      PreconditionedBiCGStab, Solver)
+from .solvers import (BiConjugateGradient, ConjugateGradient, EvenOddBiCGStab, EvenOddConjugateGradient,
+                      MultishiftSolver, PreconditionedBiCGStab, Solver)
 
 __all__ = [
     "LymError", "SolveStats", "build", "declared_symbols", "lib", "Lattice", "DiracOperator",
     "DiracWilsonOperator", "ImprovedDiracWilsonOperator", "EvenOddImprovedDiracWilsonOperator",
     "SquareDiracWilsonOperator", "SquareImprovedDiracWilsonOperator", "SquareEvenOddImprovedDiracWilsonOperator",
     "Solver", "ConjugateGradient", "BiConjugateGradient", "PreconditionedBiCGStab", "EvenOddConjugateGradient",
+    "EvenOddBiCGStab",
     "MultishiftSolver",
 ]

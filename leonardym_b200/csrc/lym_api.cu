@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -1160,6 +1161,8 @@ struct SlotTables {
     SlotTables &operator=(const SlotTables &) = delete;
 };
 
+enum BlockAlgo : int { ALGO_CG = 0, ALGO_BICGSTAB = 1 };
+
 // Block even-odd CG engine: nb slots on one resident gauge field.  Every slot solves its
 // own D_slot x = b (its own kappa / clover term) by CG on (gamma5 S)^2 with its own FP64
 // scalars, convergence mask and FP64 reliable updates; one batched stencil serves all
@@ -1176,13 +1179,26 @@ public:
         double epsS = 0.0, bb = 0.0;
         int start_iter = 0, iters = 0, updates = 0, max_iter = 0, converged = 0;
         long long tag = -1;
+        // BiCGStab progress: the best true residual so far, updates without a halving of it,
+        // breakdown restarts; gave_up: stopped without convergence for another solver
+        double best_rr = 0.0;
+        int stalls = 0, restarts = 0;
+        bool gave_up = false;
     };
 
-    BlockEngine(lym_context *ctx, int sprec_, int nb_)
-        : c(ctx), sprec(sprec_), nb(nb_), te(ctx, PREC_D, 1), t1(ctx, PREC_D, 1), rS(ctx, PREC_D, 1),
+    // algo ALGO_CG: CG on (gamma5 S)^2 (per iteration S^+ S p); ALGO_BICGSTAB: BiCGStab on S
+    // itself (per iteration S p and S s), both with FP64 reliable updates
+    BlockEngine(lym_context *ctx, int sprec_, int nb_, int algo_ = ALGO_CG)
+        : c(ctx), sprec(sprec_), nb(nb_), algo(algo_), te(ctx, PREC_D, 1), t1(ctx, PREC_D, 1), rS(ctx, PREC_D, 1),
           rN(ctx, PREC_D, 1), xs(ctx, PREC_F, nb_), rs(ctx, PREC_F, nb_), ps(ctx, sprec_, nb_), aps(ctx, sprec_, nb_),
           tes(ctx, sprec_, nb_), tos(ctx, sprec_, nb_)
     {
+        if (algo == ALGO_BICGSTAB) {
+            svec.reset(new BVec(c, sprec, nb));
+            rhat.reset(new BVec(c, PREC_F, nb));
+            CK(cudaMemsetAsync(svec->s.v, 0, svec->bytes, c->st));
+            CK(cudaMemsetAsync(rhat->s.v, 0, rhat->bytes, c->st));
+        }
         tables = (char *)dev_alloc(c, 3 * kMaxBatch * sizeof(double));
         d_b = (double *)tables;
         d_T = (const void **)(tables + kMaxBatch * sizeof(double));
@@ -1196,6 +1212,7 @@ public:
     }
     ~BlockEngine()
     {
+        if (exec) cudaGraphExecDestroy(exec);
         for (int j = 0; j < nb; ++j) delete slot[j].bp;
         dev_free(c, tables, 3 * kMaxBatch * sizeof(double));
     }
@@ -1235,6 +1252,7 @@ public:
         delete s.bp;
         s = Slot();
         s.busy = true;
+        hs.its[j] = 0;
         s.op = &op;
         s.B = B;
         s.X = X;
@@ -1248,49 +1266,61 @@ public:
         zero(c, X.parity(1));
         set_tables(j, b, T, Ti);
         axpby_views(c, xs.f().slot(j), xs.f().slot(j), C2(0.0), C2(0.0));
-        double rrS, rrN;
-        true_res(j, rrS, rrN);  // synchronises: the host values above were consumed
+        double rrS, rrN = 0.0;
+        if (algo == ALGO_BICGSTAB) true_res_S(j, rrS);  // synchronises: the host values above were consumed
+        else true_res(j, rrS, rrN);
         if (rrS < s.epsS || s.bb == 0.0) {
             s.converged = 1;
             finish(j);
             return;
         }
-        axpby_views(c, (*rN).d(), rs.f().slot(j), C2(1.0), C2(0.0));
-        set_direction(j, 0.0);
-        hs.active[j] = 1;
-        hs.rr[j] = hs.rr_max[j] = rrN;
-        hs.eps[j] = s.epsS * (rrN / rrS);
         hs.converged[j] = hs.need_update[j] = 0;
+        hs.last_update_its[j] = 0;
+        if (algo == ALGO_BICGSTAB) {
+            s.best_rr = rrS;
+            restart_bicg(j, rrS);
+            hs.eps[j] = s.epsS;
+        } else {
+            axpby_views(c, (*rN).d(), rs.f().slot(j), C2(1.0), C2(0.0));
+            set_direction(j, 0.0);
+            hs.active[j] = 1;
+            hs.rr[j] = hs.rr_max[j] = rrN;
+            hs.eps[j] = s.epsS * (rrN / rrS);
+        }
     }
 
-    // Iterates all working slots until some slot needs the host (reliable update, done,
-    // iteration limit).  Returns the slots that finished since the last call.
+    // Iterates the running slots until the captured loop pauses (slots parked for their
+    // FP64 reliable update, iteration limit, nothing left running), then services the
+    // parked slots.  Returns the slots that finished since the last call.
     std::vector<int> advance()
     {
-        if (working() && any_active()) {
-            int left = 1 << 30;
+        service();
+        if (any_active()) {
+            int left = 1 << 30, busy = 0;
             for (int j = 0; j < nb; ++j)
-                if (slot[j].busy && !slot[j].finished && hs.active[j])
-                    left = std::min(left, slot[j].max_iter - (hs.iter - slot[j].start_iter));
+                if (slot[j].busy && !slot[j].finished) {
+                    ++busy;
+                    if (hs.active[j]) left = std::min(left, slot[j].max_iter - hs.its[j]);
+                }
             left = std::max(left, 1);
             hs.max_iter = hs.iter + left;
+            hs.park_limit = std::max(1, busy / kParkFraction);
             hs.pause = 0;
             *(BatchCGState *)c->h_state = hs;
             CK(cudaMemcpyAsync(c->d_state, c->h_state, sizeof(BatchCGState), cudaMemcpyHostToDevice, c->st));
             BatchCGState *S = (BatchCGState *)c->d_state;
-            run_gated_state(c, S, [&]() { step(S); }, 8, (long)left + 8);
+            run_loop(S, (long)left + kGraphIters);
             hs = *(BatchCGState *)c->h_state;
             if (hs.failed) fail(c, LYM_ERR_NUMERIC, "block CG produced a non-finite residual");
             direction_rest(S);
             for (int j = 0; j < nb; ++j) {
                 Slot &s = slot[j];
-                if (!s.busy || s.finished || !hs.active[j]) continue;
-                if (hs.need_update[j]) reliable_update(j);
-                if (!s.finished && hs.iter - s.start_iter >= s.max_iter) {
+                if (s.busy && !s.finished && hs.active[j] && hs.its[j] >= s.max_iter) {
                     axpby_views(c, xs.f().slot(j), s.X.parity(1).d(), C2(1.0), C2(1.0));
                     finish(j);
                 }
             }
+            service();
         }
         std::vector<int> out;
         out.swap(done_list);
@@ -1307,15 +1337,24 @@ public:
 
 private:
     lym_context *c;
-    int sprec, nb;
+    int sprec, nb, algo;
     Vec te, t1, rS, rN;
-    BVec xs, rs, ps, aps, tes, tos;
+    BVec xs, rs, ps, aps, tes, tos;       // CG: p, S^+S p (aps), tmp, S p (tos); BiCGStab: p, v, tmp, t
+    std::unique_ptr<BVec> svec, rhat;     // BiCGStab only: s and the shadow residual
     char *tables = nullptr;
     double *d_b = nullptr;
     const void **d_T = nullptr, **d_Ti = nullptr;
     int gauge_id = -1;
     bool has_clover = false;
     BatchTile tile;
+    cudaGraphExec_t exec = nullptr;  // kGraphIters captured iterations, replayed
+    size_t nodes = 0;
+    static constexpr int kGraphIters = 8;
+    // the loop pauses once a kParkFraction-th of the busy slots waits for its update
+    static constexpr int kParkFraction = 8;
+    // BiCGStab gives a source up after kMaxStalls reliable updates in a row that did not
+    // halve its best true residual, or after kMaxRestarts breakdowns
+    static constexpr int kMaxStalls = 3, kMaxRestarts = 3;
     Slot slot[kMaxBatch];
 
     // the operator of slot j in the device tables: b = -kappa^2 and the FP32 T / Tinv bases
@@ -1350,13 +1389,130 @@ private:
         rrS = c->h_scal[0];
         rrN = c->h_scal[1];
     }
+    // |b' - S x|^2 of slot j, the residual left in rS
+    void true_res_S(int j, double &rrS)
+    {
+        Slot &s = slot[j];
+        apply_schur(c, *s.op, PREC_D, *t1, s.X.parity(1), *te, 0);
+        run_site(c, OpSubNorm<SpinorD, SpinorD, SpinorD>{(**s.bp).d(), (*t1).d(), (*rS).d(), c->d_scal}, 1);
+        CK(cudaMemcpyAsync(c->h_scal, c->d_scal, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        rrS = c->h_scal[0];
+    }
+    // BiCGStab (re)start of slot j from the true residual in rS: r = rhat = p = rS
+    void restart_bicg(int j, double rrS)
+    {
+        axpby_views(c, (*rS).d(), rs.f().slot(j), C2(1.0), C2(0.0));
+        axpby_views(c, (*rS).d(), rhat->f().slot(j), C2(1.0), C2(0.0));
+        set_direction(j, 0.0);
+        hs.rho[j] = make_double2(rrS, 0.0);
+        hs.rr[j] = hs.rr_max[j] = rrS;
+        hs.restart[j] = 0;
+        hs.active[j] = 1;
+    }
+    void reliable_update_bicg(int j)
+    {
+        Slot &s = slot[j];
+        axpby_views(c, xs.f().slot(j), s.X.parity(1).d(), C2(1.0), C2(1.0));
+        axpby_views(c, xs.f().slot(j), xs.f().slot(j), C2(0.0), C2(0.0));
+        double rrS;
+        true_res_S(j, rrS);
+        ++s.updates;
+        hs.last_update_its[j] = hs.its[j];
+        if (rrS < 0.5 * s.best_rr) {
+            s.best_rr = rrS;
+            s.stalls = 0;
+        } else {
+            ++s.stalls;
+        }
+        if (hs.restart[j]) ++s.restarts;
+        if (rrS < s.epsS) {
+            s.converged = 1;
+            finish(j);
+        } else if (s.stalls >= kMaxStalls || s.restarts >= kMaxRestarts) {
+            s.gave_up = true;  // BiCGStab does not converge on this source
+            finish(j);
+        } else {
+            if (hs.converged[j]) hs.eps[j] = std::max(hs.eps[j] * 0.5 * s.epsS / rrS, 1e-300);
+            if (hs.restart[j]) {
+                restart_bicg(j, rrS);
+            } else {
+                // the recursion goes on with the true residual in place of the recursive
+                // one: rho = <rhat, r>, then the direction update the pause held back
+                axpby_views(c, (*rS).d(), rs.f().slot(j), C2(1.0), C2(0.0));
+                run_site(c, OpDot<SlotF, SpinorD>{rhat->f().slot(j), (*rS).d(), c->d_scal}, 1);
+                CK(cudaMemcpyAsync(c->h_scal, c->d_scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+                CK(cudaStreamSynchronize(c->st));
+                hs.rho[j] = make_double2(c->h_scal[0], c->h_scal[1]);
+                const double2 be = hs.alpha[j], bo = cmul(be, hs.omega[j]);
+                if (sprec == PREC_F) {
+                    axpby_views(c, aps.f().slot(j), ps.f().slot(j), make_double2(-bo.x, -bo.y), be);
+                    axpby_views(c, rs.f().slot(j), ps.f().slot(j), C2(1.0), C2(1.0));
+                } else {
+                    axpby_views(c, aps.h().slot(j), ps.h().slot(j), make_double2(-bo.x, -bo.y), be);
+                    axpby_views(c, rs.f().slot(j), ps.h().slot(j), C2(1.0), C2(1.0));
+                }
+                hs.rr[j] = hs.rr_max[j] = rrS;
+                hs.active[j] = 1;
+            }
+        }
+        hs.restart[j] = 0;
+        hs.converged[j] = 0;
+        hs.need_update[j] = 0;
+    }
     void set_direction(int j, double b)  // p_j = r_j + b p_j in the precision of p
     {
         if (sprec == PREC_F) axpby_views(c, rs.f().slot(j), ps.f().slot(j), C2(1.0), C2(b));
         else axpby_views(c, rs.f().slot(j), ps.h().slot(j), C2(1.0), C2(b));
     }
+    // the reliable updates of the parked slots; a slot past its iteration limit finishes
+    void service()
+    {
+        for (int j = 0; j < nb; ++j) {
+            Slot &s = slot[j];
+            if (!s.busy || s.finished || !hs.need_update[j]) continue;
+            reliable_update(j);
+            if (!s.finished && hs.its[j] >= s.max_iter) finish(j);
+        }
+    }
+    // captures kGraphIters iterations once, then replays them until the state pauses
+    void run_loop(BatchCGState *S, long max_iterations)
+    {
+        if (!exec) {
+            cudaGraph_t graph = nullptr;
+            CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeRelaxed));
+            c->capturing = true;
+            try {
+                for (int k = 0; k < kGraphIters; ++k) step(S);
+            } catch (...) {
+                c->capturing = false;
+                cudaStreamEndCapture(c->st, &graph);
+                if (graph) cudaGraphDestroy(graph);
+                throw;
+            }
+            c->capturing = false;
+            CK(cudaStreamEndCapture(c->st, &graph));
+            const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphGetNodes(graph, nullptr, &nodes);
+            cudaGraphDestroy(graph);
+            CK(e);
+        }
+        const long max_launches = max_iterations / kGraphIters + 4;
+        for (long l = 0; l < max_launches; ++l) {
+            CK(cudaGraphLaunch(exec, c->st));
+            c->launches += nodes;
+            CK(cudaMemcpyAsync(c->h_state, S, sizeof(BatchCGState), cudaMemcpyDeviceToHost, c->st));
+            CK(cudaStreamSynchronize(c->st));
+            if (((BatchCGState *)c->h_state)->pause) return;
+        }
+        fail(c, LYM_ERR_TIMEOUT, "block CG state did not pause within %ld iterations", max_iterations);
+    }
     void reliable_update(int j)
     {
+        if (algo == ALGO_BICGSTAB) {
+            reliable_update_bicg(j);
+            return;
+        }
         Slot &s = slot[j];
         axpby_views(c, xs.f().slot(j), s.X.parity(1).d(), C2(1.0), C2(1.0));
         axpby_views(c, xs.f().slot(j), xs.f().slot(j), C2(0.0), C2(0.0));
@@ -1371,6 +1527,7 @@ private:
             axpby_views(c, (*rN).d(), rs.f().slot(j), C2(1.0), C2(0.0));
             set_direction(j, rrN / hs.rr_prev[j]);
             hs.rr[j] = hs.rr_max[j] = rrN;
+            hs.active[j] = 1;  // back into the iteration
         }
         hs.converged[j] = 0;
         hs.need_update[j] = 0;
@@ -1379,14 +1536,41 @@ private:
     {
         Slot &s = slot[j];
         s.finished = true;
-        s.iters = hs.iter - s.start_iter;
+        if (s.gave_up) {  // nothing to reconstruct: the source is solved again elsewhere
+            s.iters = hs.its[j];
+            hs.active[j] = 0;
+            hs.need_update[j] = 0;
+            done_list.push_back(j);
+            return;
+        }
+        s.iters = hs.its[j];
         hs.active[j] = 0;
         hs.need_update[j] = 0;
         schur_reconstruct(c, *s.op, s.B, s.X);
         done_list.push_back(j);
     }
+    template <class SP> void step_bicg(BatchCGState *S, const SP &p, const SP &v, const SP &sv, const SP &t)
+    {
+        const GaugeDev &U = gauge_of(c, gauge_id).dev;
+        Gate gate{&S->pause, nullptr};
+        const int lognb = xs.s.lognb;
+        apply_schur_batch(c, U, has_clover, sprec, aps.s, ps.s, tes.s, 0, &S->pause, S->active, d_b, d_T, d_Ti, tile);
+        run_batch(c, OpBBAlpha<BatchF, SP>{rhat->f(), v, S}, lognb, gate);
+        run_batch(c, OpBBResidualS<BatchF, SP, SP>{rs.f(), v, sv, S}, lognb, gate);
+        apply_schur_batch(c, U, has_clover, sprec, tos.s, svec->s, tes.s, 0, &S->pause, S->active, d_b, d_T, d_Ti,
+                          tile);
+        run_batch(c, OpBBOmega<SP, SP>{t, sv, S}, lognb, gate);
+        run_batch(c, OpBBUpdate<BatchF, SP, SP, SP, BatchF, BatchF>{xs.f(), p, sv, t, rs.f(), rhat->f(), S}, lognb,
+                  gate);
+        run_batch(c, OpBBDirection<SP, BatchF, SP>{p, rs.f(), v, S}, lognb, gate);
+    }
     void step(BatchCGState *S)
     {
+        if (algo == ALGO_BICGSTAB) {
+            if (sprec == PREC_F) step_bicg(S, ps.f(), aps.f(), svec->f(), tos.f());
+            else step_bicg(S, ps.h(), aps.h(), svec->h(), tos.h());
+            return;
+        }
         const GaugeDev &U = gauge_of(c, gauge_id).dev;
         Gate gate{&S->pause, nullptr};
         const int lognb = xs.s.lognb;
@@ -1406,6 +1590,12 @@ private:
     }
     void direction_rest(BatchCGState *S)  // the direction update the pause skipped, for slots without an update
     {
+        if (algo == ALGO_BICGSTAB) {
+            if (sprec == PREC_F)
+                run_batch(c, OpBBDirection<BatchF, BatchF, BatchF>{ps.f(), rs.f(), aps.f(), S}, xs.s.lognb);
+            else run_batch(c, OpBBDirection<BatchH, BatchF, BatchH>{ps.h(), rs.f(), aps.h(), S}, xs.s.lognb);
+            return;
+        }
         if (sprec == PREC_F) run_batch(c, OpBDirection<BatchF, BatchF>{ps.f(), rs.f(), S}, xs.s.lognb);
         else run_batch(c, OpBDirection<BatchH, BatchF>{ps.h(), rs.f(), S}, xs.s.lognb);
     }
@@ -1814,6 +2004,38 @@ static int do_solve(lym_context *c, int op_id, int solver, double precision, int
                     local.true_residual = true_residual(c, op, *b, *x);
                     break;
                 }
+                case LYM_SOLVER_EO_BICGSTAB_MIXED_SINGLE:
+                case LYM_SOLVER_EO_BICGSTAB_MIXED_HALF: {
+                    if (op.kind != LYM_OP_IMPROVED && op.kind != LYM_OP_DIRAC_WILSON)
+                        fail(c, LYM_ERR_UNSUPPORTED, "even-odd BiCGStab solves D x = b for a DiracWilson/Improved operator");
+                    if (gp) fail(c, LYM_ERR_UNSUPPORTED, "the mixed-precision BiCGStab starts from x = 0 (no guess)");
+                    const int sp = solver == LYM_SOLVER_EO_BICGSTAB_MIXED_SINGLE ? PREC_F : PREC_H;
+                    const double tol = precision <= 0.0 ? (precision == 0.0 ? 1e-10 : -precision)
+                                                        : std::sqrt(precision);
+                    // the block engine with one busy slot (the batched stencil's smallest width)
+                    bool gave_up = false;
+                    {
+                        BlockEngine engine(c, sp, 2, ALGO_BICGSTAB);
+                        engine.add(0, op, *b, *x, tol, max_steps, 0);
+                        while (engine.working()) engine.advance();
+                        engine.advance();
+                        const auto &s = engine.info(0);
+                        local.iterations = local.steps = s.iters;
+                        local.reliable_updates = s.updates;
+                        local.converged = s.converged;
+                        gave_up = s.gave_up;
+                        rc = s.converged ? LYM_OK : LYM_NOT_CONVERGED;
+                    }
+                    if (gave_up) {  // BiCGStab breaks down on this source: CG on (gamma5 S)^2
+                        const int its = local.iterations, ups = local.reliable_updates;
+                        rc = eo_cg(c, op, sp, *b, *x, nullptr, tol, max_steps, &local);
+                        local.iterations += its;
+                        local.steps = local.iterations;
+                        local.reliable_updates += ups;
+                    }
+                    local.true_residual = true_residual(c, op, *b, *x);
+                    break;
+                }
                 default: fail(c, LYM_ERR_ARGUMENT, "unknown solver %d", solver);
                 }
             }
@@ -1846,6 +2068,63 @@ int lym_solve_device(lym_context *c, int op_id, int solver, double precision, in
     return do_solve(c, op_id, solver, precision, max_steps, source, solution, guess, stats, true, false, C2(0.0));
 }
 
+// Solves the sources listed in `tags` with one block engine, refilling its slots as they
+// finish (continuous batching).  Sources on which BiCGStab gave up (breakdown or no
+// progress) are returned in gave_up, without statistics.
+static int run_block(lym_context *c, OpEntry &op, int sp, int algo, double tol, int max_steps,
+                     const std::vector<int> &tags, const double *const *sources, double *const *solutions, int width,
+                     lym_solve_stats *stats, bool device_ptr, std::vector<int> &gave_up)
+{
+    BlockEngine engine(c, sp, width, algo);
+    std::vector<Vec *> bufs;  // two full FP64 spinors per slot
+    int rc_all = LYM_OK;
+    auto now = []() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
+    std::vector<double> t_start(tags.size(), 0.0);
+    auto collect = [&](int f) {
+        const auto &s = engine.info(f);
+        const int tag = tags[s.tag];
+        if (s.gave_up) {
+            gave_up.push_back(tag);
+        } else {
+            download_vec(c, solutions[tag], s.X, device_ptr, 2);
+            CK(cudaStreamSynchronize(c->st));
+            if (stats) {
+                stats[tag].iterations = stats[tag].steps = s.iters;
+                stats[tag].reliable_updates = s.updates;
+                stats[tag].converged = s.converged;
+                stats[tag].true_residual = true_residual(c, *s.op, s.B, s.X);
+                stats[tag].seconds = now() - t_start[s.tag];
+            }
+            if (!s.converged) rc_all = LYM_NOT_CONVERGED;
+        }
+        engine.release(f);
+    };
+    try {
+        for (int j = 0; j < 2 * width; ++j) bufs.push_back(new Vec(c, PREC_D, 2));
+        size_t next = 0;
+        for (;;) {
+            int j;
+            while (next < tags.size() && (j = engine.free_slot()) >= 0) {
+                const Spinor B = **bufs[2 * j], X = **bufs[2 * j + 1];
+                upload_vec(c, B, sources[tags[next]], device_ptr, 0);
+                t_start[next] = now();
+                engine.add(j, op, B, X, tol, max_steps, (long long)next);
+                ++next;
+            }
+            for (int f : engine.advance()) collect(f);
+            if (!engine.working() && next >= tags.size()) {
+                for (int f : engine.advance()) collect(f);
+                if (!engine.working()) break;
+            }
+        }
+    } catch (...) {
+        for (auto v : bufs) delete v;
+        throw;
+    }
+    for (auto v : bufs) delete v;
+    return rc_all;
+}
+
 static int do_solve_block(lym_context *c, int op_id, int solver, double precision, int max_steps, int nrhs,
                           const double *const *sources, double *const *solutions, int batch, lym_solve_stats *stats,
                           bool device_ptr)
@@ -1859,69 +2138,31 @@ static int do_solve_block(lym_context *c, int op_id, int solver, double precisio
         OpEntry &op = op_of(c, op_id);
         if (op.kind != LYM_OP_IMPROVED && op.kind != LYM_OP_DIRAC_WILSON)
             fail(c, LYM_ERR_UNSUPPORTED, "block solves solve D x = b for a DiracWilson/Improved operator");
-        if (solver != LYM_SOLVER_EO_CG_MIXED_SINGLE && solver != LYM_SOLVER_EO_CG_MIXED_HALF)
-            fail(c, LYM_ERR_UNSUPPORTED, "block solves use LYM_SOLVER_EO_CG_MIXED_SINGLE or _HALF");
-        const int sp = solver == LYM_SOLVER_EO_CG_MIXED_SINGLE ? PREC_F : PREC_H;
+        if (solver != LYM_SOLVER_EO_CG_MIXED_SINGLE && solver != LYM_SOLVER_EO_CG_MIXED_HALF &&
+            solver != LYM_SOLVER_EO_BICGSTAB_MIXED_SINGLE && solver != LYM_SOLVER_EO_BICGSTAB_MIXED_HALF)
+            fail(c, LYM_ERR_UNSUPPORTED, "block solves use the mixed-precision even-odd CG or BiCGStab solvers");
+        const int sp = (solver == LYM_SOLVER_EO_CG_MIXED_SINGLE || solver == LYM_SOLVER_EO_BICGSTAB_MIXED_SINGLE)
+                           ? PREC_F
+                           : PREC_H;
+        const int algo = (solver == LYM_SOLVER_EO_BICGSTAB_MIXED_SINGLE || solver == LYM_SOLVER_EO_BICGSTAB_MIXED_HALF)
+                             ? ALGO_BICGSTAB
+                             : ALGO_CG;
         const double tol = precision <= 0.0 ? (precision == 0.0 ? 1e-10 : -precision) : std::sqrt(precision);
         const int width = std::max(2, std::min(batch, 1 << (int)std::ceil(std::log2((double)nrhs))));
-        BlockEngine engine(c, sp, width);
-        std::vector<Vec *> bufs;  // two full FP64 spinors per slot
-        for (int j = 0; j < 2 * width; ++j) bufs.push_back(new Vec(c, PREC_D, 2));
-        int next = 0, rc_all = LYM_OK;
-        std::vector<double> t_start(nrhs, 0.0);
-        auto now = []() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
-        try {
-            for (;;) {
-                // continuous batching: refill every free slot with the next right-hand side
-                int j;
-                while (next < nrhs && (j = engine.free_slot()) >= 0) {
-                    const Spinor B = **bufs[2 * j], X = **bufs[2 * j + 1];
-                    upload_vec(c, B, sources[next], device_ptr, 0);
-                    t_start[next] = now();
-                    engine.add(j, op, B, X, tol, max_steps, next);
-                    ++next;
-                }
-                if (!engine.working() && next >= nrhs) {
-                    // flush what add() finished at once
-                    for (int f : engine.advance()) {
-                        const auto &s = engine.info(f);
-                        download_vec(c, solutions[s.tag], s.X, device_ptr, 2);
-                        CK(cudaStreamSynchronize(c->st));
-                        if (stats) {
-                            stats[s.tag].iterations = stats[s.tag].steps = s.iters;
-                            stats[s.tag].reliable_updates = s.updates;
-                            stats[s.tag].converged = s.converged;
-                            stats[s.tag].true_residual = true_residual(c, *s.op, s.B, s.X);
-                            stats[s.tag].seconds = now() - t_start[s.tag];
-                        }
-                        if (!s.converged) rc_all = LYM_NOT_CONVERGED;
-                        engine.release(f);
-                    }
-                    if (!engine.working()) break;
-                    continue;
-                }
-                for (int f : engine.advance()) {
-                    const auto &s = engine.info(f);
-                    if (stats) {
-                        stats[s.tag].iterations = stats[s.tag].steps = s.iters;
-                        stats[s.tag].reliable_updates = s.updates;
-                        stats[s.tag].converged = s.converged;
-                        stats[s.tag].true_residual = true_residual(c, *s.op, s.B, s.X);
-                    }
-                    download_vec(c, solutions[s.tag], s.X, device_ptr, 2);
-                    CK(cudaStreamSynchronize(c->st));
-                    if (stats) stats[s.tag].seconds = now() - t_start[s.tag];
-                    if (!s.converged) rc_all = LYM_NOT_CONVERGED;
-                    engine.release(f);
-                }
-            }
-        } catch (...) {
-            for (auto v : bufs) delete v;
-            throw;
+        std::vector<int> tags(nrhs), gave_up;
+        for (int j = 0; j < nrhs; ++j) tags[j] = j;
+        int rc = run_block(c, op, sp, algo, tol, max_steps, tags, sources, solutions, width, stats, device_ptr, gave_up);
+        if (!gave_up.empty()) {
+            // BiCGStab broke down or stopped making progress on these sources (an indefinite
+            // Schur operator): they are solved again with CG on (gamma5 S)^2
+            std::vector<int> again;
+            const int w2 = std::max(2, std::min(width, 1 << (int)std::ceil(std::log2((double)gave_up.size()))));
+            const int rc2 = run_block(c, op, sp, ALGO_CG, tol, max_steps, gave_up, sources, solutions, w2, stats,
+                                      device_ptr, again);
+            if (rc2 != LYM_OK) rc = rc2;
         }
-        for (auto v : bufs) delete v;
         CK(cudaGetLastError());
-        return rc_all;
+        return rc;
     });
 }
 

@@ -811,17 +811,44 @@ __global__ void __launch_bounds__(kBlasThreads) site_batch_kernel(Op op, int vh,
 }
 
 // ------------------------------------------------------ batched CG state ---
+// A slot whose recursive residual fell by delta2 (or reached eps) parks: it leaves the
+// iteration (active = 0, need_update = 1) while the others go on, and the captured
+// loop pauses for the host's FP64 reliable updates once park_limit slots are parked or
+// none is left running.
 struct BatchCGState {
     int pause;                 // gates every captured kernel
     int iter, max_iter, nb;
+    int park_limit;
     double delta2;
     double rr[kMaxBatch], rr_prev[kMaxBatch], rr_max[kMaxBatch], eps[kMaxBatch], beta[kMaxBatch];
     double2 alpha[kMaxBatch];
     int active[kMaxBatch];     // 0: converged and frozen
     int converged[kMaxBatch];  // the recursion's residual reached eps
     int need_update[kMaxBatch];
+    int its[kMaxBatch];        // iterations each slot took part in
     int failed;
+    double2 rho[kMaxBatch], omega[kMaxBatch];  // BiCGStab only
+    int restart[kMaxBatch];                    // BiCGStab broke down: restart at the update
+    int last_update_its[kMaxBatch];            // its at the last reliable update
 };
+
+// a slot gets a reliable update at least every kForcedUpdateIts of its iterations, so a
+// stagnating recursion still reaches the host's progress check
+constexpr int kForcedUpdateIts = 200;
+
+// finalize_all of the step that closes an iteration: counts it and pauses the captured
+// loop at the iteration limit, when no slot is left running, or when park_limit slots
+// wait for their reliable update
+LYM_D void batch_iteration_done(BatchCGState *s)
+{
+    s->iter += 1;
+    int parked = 0, running = 0;
+    for (int r = 0; r < s->nb; ++r) {
+        parked += s->need_update[r];
+        running += s->active[r];
+    }
+    if (s->iter >= s->max_iter || running == 0 || parked >= s->park_limit) s->pause = 1;
+}
 
 // alpha_r = rr_r / <p_r, A p_r>
 template <class SP, class SAp> struct OpBAlpha {
@@ -881,6 +908,7 @@ template <class SX, class SP, class SR, class SAp> struct OpBUpdate {
     LYM_D void finalize(int r, const double *t) const
     {
         if (!s->active[r]) return;
+        s->its[r] += 1;
         const double rr_new = t[0];
         s->rr_prev[r] = s->rr[r];
         s->beta[r] = rr_new / s->rr[r];
@@ -892,17 +920,13 @@ template <class SX, class SP, class SR, class SAp> struct OpBUpdate {
         } else if (rr_new < s->eps[r]) {
             s->converged[r] = 1;
             s->need_update[r] = 1;
-            s->pause = 1;
+            s->active[r] = 0;
         } else if (rr_new < s->delta2 * s->rr_max[r]) {
             s->need_update[r] = 1;
-            s->pause = 1;
+            s->active[r] = 0;
         }
     }
-    LYM_D void finalize_all() const
-    {
-        s->iter += 1;
-        if (s->iter >= s->max_iter) s->pause = 1;
-    }
+    LYM_D void finalize_all() const { batch_iteration_done(s); }
 };
 
 // p_r = res_r + beta_r p_r for the active RHS that need no reliable update
@@ -926,6 +950,206 @@ template <class SP, class SR> struct OpBDirection {
             const double b = s->beta[2 * q + l];
 #pragma unroll
             for (int k = 0; k < 12; ++k) pv[l][k] = res[l][k] + b * pv[l][k];
+        }
+        p.store_d(h, q, pv[0], pv[1]);
+    }
+    LYM_D void finalize(int, const double *) const {}
+    LYM_D void finalize_all() const {}
+};
+
+// -------------------------------------------------- batched BiCGStab ops ---
+// One iteration of BiCGStab on the Schur operator S (no gamma5), per RHS r:
+//   v = S p;  alpha = rho / <rhat, v>;  s = r - alpha v;  t = S s;
+//   omega = <t, s> / |t|^2;  x += alpha p + omega s;  r = s - omega t;
+//   rho' = <rhat, r>;  beta = (rho' / rho) (alpha / omega);  p = r + beta (p - omega v)
+// (BiConjugateGradient::solve, inverters/BiConjugateGradient.cpp:321-507, with the
+// scalars kept per RHS in FP64 and the vectors in the batch precisions).
+
+LYM_D double2 as_d2(cx<double> z) { return make_double2(z.re, z.im); }
+LYM_D cx<double> as_cx(double2 z) { return cx<double>{z.x, z.y}; }
+
+// alpha_r = rho_r / <rhat_r, v_r>
+template <class SRh, class SV> struct OpBBAlpha {
+    static constexpr int NRED = 2;
+    SRh rh;
+    SV v;
+    BatchCGState *s;
+    LYM_D void site(int h, int q, double *acc) const
+    {
+        const bool a0 = s->active[2 * q] != 0, a1 = s->active[2 * q + 1] != 0;
+        if (!a0 && !a1) return;
+        cx<double> x0[12], x1[12], y0[12], y1[12];
+        rh.load_d(h, q, x0, x1);
+        v.load_d(h, q, y0, y1);
+        if (a0) dotc(x0, y0, acc[0], acc[1]);
+        if (a1) dotc(x1, y1, acc[2], acc[3]);
+    }
+    LYM_D void finalize(int r, const double *t) const
+    {
+        if (!s->active[r]) return;
+        if (t[0] == 0.0 && t[1] == 0.0) {  // breakdown: restart from the true residual
+            s->need_update[r] = 1;
+            s->restart[r] = 1;
+            s->active[r] = 0;
+            return;
+        }
+        s->alpha[r] = cdiv(s->rho[r], make_double2(t[0], t[1]));
+    }
+    LYM_D void finalize_all() const {}
+};
+
+// s_r = r_r - alpha_r v_r
+template <class SR, class SV, class SS> struct OpBBResidualS {
+    static constexpr int NRED = 0;
+    SR rv;
+    SV v;
+    SS sv;
+    BatchCGState *s;
+    LYM_D void site(int h, int q, double *) const
+    {
+        const bool act[2] = {s->active[2 * q] != 0, s->active[2 * q + 1] != 0};
+        if (!act[0] && !act[1]) return;
+        cx<double> r[2][12], w[2][12];
+        rv.load_d(h, q, r[0], r[1]);
+        v.load_d(h, q, w[0], w[1]);
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+            if (!act[l]) continue;
+            const cx<double> al = as_cx(s->alpha[2 * q + l]);
+#pragma unroll
+            for (int k = 0; k < 12; ++k) r[l][k] = r[l][k] - al * w[l][k];
+        }
+        sv.store_d(h, q, r[0], r[1]);
+    }
+    LYM_D void finalize(int, const double *) const {}
+    LYM_D void finalize_all() const {}
+};
+
+// omega_r = <t_r, s_r> / |t_r|^2
+template <class ST, class SS> struct OpBBOmega {
+    static constexpr int NRED = 3;
+    ST tv;
+    SS sv;
+    BatchCGState *s;
+    LYM_D void site(int h, int q, double *acc) const
+    {
+        const bool a0 = s->active[2 * q] != 0, a1 = s->active[2 * q + 1] != 0;
+        if (!a0 && !a1) return;
+        cx<double> t0[12], t1[12], s0[12], s1[12];
+        tv.load_d(h, q, t0, t1);
+        sv.load_d(h, q, s0, s1);
+        if (a0) {
+            dotc(t0, s0, acc[0], acc[1]);
+            acc[2] += norm2(t0);
+        }
+        if (a1) {
+            dotc(t1, s1, acc[3], acc[4]);
+            acc[5] += norm2(t1);
+        }
+    }
+    LYM_D void finalize(int r, const double *t) const
+    {
+        if (!s->active[r]) return;
+        if (t[2] == 0.0) {  // s = 0: alpha p already solved this RHS; the update decides
+            s->omega[r] = make_double2(0.0, 0.0);
+            return;
+        }
+        s->omega[r] = make_double2(t[0] / t[2], t[1] / t[2]);
+    }
+    LYM_D void finalize_all() const {}
+};
+
+// x_r += alpha_r p_r + omega_r s_r, r_r = s_r - omega_r t_r, rho' = <rhat_r, r_r>,
+// |r_r|^2, and the convergence / reliable-update decisions
+template <class SX, class SP, class SS, class ST, class SR, class SRh> struct OpBBUpdate {
+    static constexpr int NRED = 3;
+    SX x;
+    SP p;
+    SS sv;
+    ST tv;
+    SR rv;
+    SRh rh;
+    BatchCGState *s;
+    LYM_D void site(int h, int q, double *acc) const
+    {
+        const bool act[2] = {s->active[2 * q] != 0, s->active[2 * q + 1] != 0};
+        if (!act[0] && !act[1]) return;
+        cx<double> xv[2][12], pv[2][12], sw[2][12], tw[2][12], rr[2][12], hv[2][12];
+        x.load_d(h, q, xv[0], xv[1]);
+        p.load_d(h, q, pv[0], pv[1]);
+        sv.load_d(h, q, sw[0], sw[1]);
+        tv.load_d(h, q, tw[0], tw[1]);
+        rv.load_d(h, q, rr[0], rr[1]);
+        rh.load_d(h, q, hv[0], hv[1]);
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+            if (!act[l]) continue;
+            const cx<double> al = as_cx(s->alpha[2 * q + l]), om = as_cx(s->omega[2 * q + l]);
+#pragma unroll
+            for (int k = 0; k < 12; ++k) {
+                fma_c(xv[l][k], al, pv[l][k]);
+                fma_c(xv[l][k], om, sw[l][k]);
+                rr[l][k] = sw[l][k] - om * tw[l][k];
+            }
+            dotc(hv[l], rr[l], acc[3 * l], acc[3 * l + 1]);
+            acc[3 * l + 2] += norm2(rr[l]);
+        }
+        x.store_d(h, q, xv[0], xv[1]);
+        rv.store_d(h, q, rr[0], rr[1]);
+    }
+    LYM_D void finalize(int r, const double *t) const
+    {
+        if (!s->active[r]) return;
+        s->its[r] += 1;
+        const double rr_new = t[2];
+        const double2 rho_new = make_double2(t[0], t[1]);
+        const double2 om = s->omega[r];
+        s->rr_prev[r] = s->rr[r];
+        s->rr[r] = rr_new;
+        if (rr_new > s->rr_max[r]) s->rr_max[r] = rr_new;
+        const bool stalled = (om.x == 0.0 && om.y == 0.0) || (rho_new.x == 0.0 && rho_new.y == 0.0);
+        if (!stalled) s->alpha[r] = cmul(cdiv(rho_new, s->rho[r]), cdiv(s->alpha[r], om));  // beta, kept in alpha
+        s->rho[r] = rho_new;
+        if (!(rr_new == rr_new)) {
+            s->failed = 1;
+            s->pause = 1;
+        } else if (rr_new < s->eps[r]) {
+            s->converged[r] = 1;
+            s->need_update[r] = 1;
+            s->active[r] = 0;
+        } else if (stalled || rr_new < s->delta2 * s->rr_max[r] ||
+                   s->its[r] - s->last_update_its[r] >= kForcedUpdateIts) {
+            s->need_update[r] = 1;
+            s->restart[r] = stalled;
+            s->active[r] = 0;
+        }
+    }
+    LYM_D void finalize_all() const { batch_iteration_done(s); }
+};
+
+// p_r = r_r + beta_r (p_r - omega_r v_r) for the running RHS (beta is in alpha)
+template <class SP, class SR, class SV> struct OpBBDirection {
+    static constexpr int NRED = 0;
+    SP p;
+    SR rv;
+    SV v;
+    BatchCGState *s;
+    LYM_D void site(int h, int q, double *) const
+    {
+        bool go[2];
+#pragma unroll
+        for (int l = 0; l < 2; ++l) go[l] = s->active[2 * q + l] && !s->need_update[2 * q + l];
+        if (!go[0] && !go[1]) return;
+        cx<double> pv[2][12], rr[2][12], w[2][12];
+        p.load_d(h, q, pv[0], pv[1]);
+        rv.load_d(h, q, rr[0], rr[1]);
+        v.load_d(h, q, w[0], w[1]);
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+            if (!go[l]) continue;
+            const cx<double> be = as_cx(s->alpha[2 * q + l]), om = as_cx(s->omega[2 * q + l]);
+#pragma unroll
+            for (int k = 0; k < 12; ++k) pv[l][k] = rr[l][k] + be * (pv[l][k] - om * w[l][k]);
         }
         p.store_d(h, q, pv[0], pv[1]);
     }

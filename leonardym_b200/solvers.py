@@ -19,6 +19,7 @@ from ._lib import LymError, SolveStats, lib
 
 SOLVER_CG, SOLVER_BICGSTAB, SOLVER_EO_BICGSTAB = 0, 1, 2
 SOLVER_EO_CG, SOLVER_EO_CG_MIXED_SINGLE, SOLVER_EO_CG_MIXED_HALF = 3, 4, 5
+SOLVER_EO_BICGSTAB_MIXED_SINGLE, SOLVER_EO_BICGSTAB_MIXED_HALF = 6, 7
 MULTISHIFT = {"mass_estrapolation": 0, "minimal_residual": 1, "multishift_cg": 2}
 
 
@@ -161,6 +162,19 @@ class EvenOddConjugateGradient(Solver):
             raise LymError(rc, lib().lym_last_error(lat.handle).decode())
         self.block_stats = [stats[j] for j in range(n)]
         return rc == 0, solutions
+
+
+class EvenOddBiCGStab(EvenOddConjugateGradient):
+    """Mixed-precision BiCGStab (inverters/BiConjugateGradient.cpp:321-507) on the even-odd
+    Schur operator S itself, solving D x = b; "single" (FP32) or "half" (FP16 + norms)
+    inner iterations with FP64 reliable updates that restart from the true residual.
+    The same interface as EvenOddConjugateGradient, one or many sources; no guess."""
+
+    MODES = {"single": SOLVER_EO_BICGSTAB_MIXED_SINGLE, "half": SOLVER_EO_BICGSTAB_MIXED_HALF}
+
+    def __init__(self, precision_mode="single", tolerance=1e-10):
+        super().__init__(precision_mode, tolerance)
+        self.name = "EvenOddBiCGStab"
 
 
 class MultishiftSolver:

@@ -26,10 +26,14 @@ def setup(request, oracle):
     lat.close()
 
 
+SOLVERS = {"cg": L.EvenOddConjugateGradient, "bicgstab": L.EvenOddBiCGStab}
+
+
+@pytest.mark.parametrize("algo", ["cg", "bicgstab"])
 @pytest.mark.parametrize("mode", ["single", "half"])
-@pytest.mark.parametrize("batch", [4, 8])
-def test_block_solve_alone_and_in_the_mix(setup, mode, batch):
-    s = L.EvenOddConjugateGradient(mode, 1e-10)
+@pytest.mark.parametrize("batch", [2, 8])
+def test_block_solve_alone_and_in_the_mix(setup, algo, mode, batch):
+    s = SOLVERS[algo](mode, 1e-10)
     ok, sols = s.solve_block(setup["op"], setup["srcs"], batch=batch)
     assert ok
     for j, (b, x) in enumerate(zip(setup["srcs"], sols)):
@@ -37,7 +41,7 @@ def test_block_solve_alone_and_in_the_mix(setup, mode, batch):
         assert r <= 1e-10, (j, r)
         assert s.block_stats[j].true_residual <= 1e-10
         alone = setup["lat"].new_vector()
-        single = L.EvenOddConjugateGradient(mode, 1e-10)
+        single = SOLVERS[algo](mode, 1e-10)
         assert single.solve(setup["op"], b, alone)
         assert rel(x, alone) < 1e-8
 

@@ -122,6 +122,31 @@ def test_even_odd_cg_true_residual(setup, mode, oracle):
     assert abs(s.stats.true_residual - r) < 1e-11
 
 
+@pytest.mark.parametrize("mode", ["single", "half"])
+@pytest.mark.parametrize("cls", ["Improved", "DiracWilson"])
+def test_even_odd_bicgstab_mixed_true_residual(setup, mode, cls, oracle):
+    b = setup["b"]
+    gcls = L.ImprovedDiracWilsonOperator if cls == "Improved" else L.DiracWilsonOperator
+    op = gpu_op(setup, gcls, False)
+    s = L.EvenOddBiCGStab(mode, 1e-10)
+    x = setup["lat"].new_vector()
+    assert s.solve(op, b, x), s.stats.as_dict()
+    csw = setup["csw"] if cls == "Improved" else 0.0
+    D = oracle.Operator(setup["geom"], setup["links"], cls, setup["kappa"], csw, False)
+    r = true_res(D, b, x)
+    assert r <= 1e-10
+    assert abs(s.stats.true_residual - r) < 1e-11
+    assert s.stats.reliable_updates >= 1
+
+
+def test_even_odd_bicgstab_rejects_guess(setup):
+    op = gpu_op(setup, L.ImprovedDiracWilsonOperator, False)
+    s = L.EvenOddBiCGStab("single", 1e-10)
+    x = setup["lat"].new_vector()
+    with pytest.raises(L.LymError):
+        s.solve(op, setup["b"], x, initial_guess=setup["b"])
+
+
 def test_even_odd_cg_wilson(setup, oracle):
     b = setup["b"]
     op = gpu_op(setup, L.DiracWilsonOperator, False)
