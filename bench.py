@@ -125,12 +125,12 @@ class ClockSampler:
 
 def traffic_from_profiles(prec, batch):
     """DRAM bytes per launch of the batched stencil kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "stencil_schur_clover_24c48.md")
-    if not os.path.exists(path):
-        return None
-    m = re.search(rf"traffic_bytes_per_launch\[prec={prec},kernel=xpay,batch={batch}\]:\s*([0-9.eE+]+)",
-                  open(path).read())
-    return float(m.group(1)) if m else None
+    for name in sorted(os.listdir(os.path.join(ROOT, "profiles"))):
+        m = re.search(rf"traffic_bytes_per_launch\[prec={prec},kernel=xpay,batch={batch}\]:\s*([0-9.eE+]+)",
+                      open(os.path.join(ROOT, "profiles", name)).read())
+        if m:
+            return float(m.group(1))
+    return None
 
 
 class quiet_stdout:
@@ -482,7 +482,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="single", choices=["single", "half"])
-    ap.add_argument("--solver", default="cg", choices=["cg", "bicgstab"], help="the block solver of the timed solves")
+    ap.add_argument("--solver", default="bicgstab", choices=["cg", "bicgstab"],
+                    help="the block solver of the timed solves")
     ap.add_argument("--batch", type=int, default=16, help="right-hand sides per batched stencil (power of 2 <= 32)")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--profile", action="store_true", help="small fixed case for ncu captures")
