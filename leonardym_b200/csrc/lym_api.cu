@@ -1050,7 +1050,7 @@ std::vector<BatchTile> tile_candidates(const Geom &g)
 void apply_schur_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, const SpinorBatch &out,
                        const SpinorBatch &in, const SpinorBatch &tmp, int gamma5, const int *skip, const int *active,
                        const double *b_slot, const void *const *T_slot, const void *const *Ti_slot,
-                       const BatchTile &tile)
+                       const BatchTile &tile, const int *uniform)
 {
     DslashBatchParams P;
     P.g = c->g;
@@ -1063,6 +1063,7 @@ void apply_schur_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, c
     P.order = order_table(c, tile.by, tile.bz);
     P.minb = tile.minb;
     P.has_clover = clov;
+    P.uniform = uniform;
     P.epi = clov ? EPI_CLOVINV_ : EPI_SCALE_;
     P.parity = 0;
     P.in = in;
@@ -1088,7 +1089,7 @@ void apply_schur_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, c
 // are overwritten) and keeps the fastest per (precision, batch width, clover).
 BatchTile tune_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, const SpinorBatch &out,
                      const SpinorBatch &in, const SpinorBatch &tmp, const double *b_slot, const void *const *T_slot,
-                     const void *const *Ti_slot)
+                     const void *const *Ti_slot, const int *uniform)
 {
     if (c->tile_forced) {
         order_table(c, c->forced_tile.by, c->forced_tile.bz);  // built now, before any capture
@@ -1103,10 +1104,10 @@ BatchTile tune_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, con
     for (BatchTile t : tile_candidates(c->g)) {
         for (int k = 0; k < kBatchMinBlocksCount; ++k) {
             t.minb = kBatchMinBlocks[k];
-            apply_schur_batch(c, U, clov, prec, out, in, tmp, 1, nullptr, nullptr, b_slot, T_slot, Ti_slot, t);
+            apply_schur_batch(c, U, clov, prec, out, in, tmp, 1, nullptr, nullptr, b_slot, T_slot, Ti_slot, t, uniform);
             CK(cudaEventRecord(c->ev0, c->st));
             for (int r = 0; r < 3; ++r)
-                apply_schur_batch(c, U, clov, prec, out, in, tmp, 1, nullptr, nullptr, b_slot, T_slot, Ti_slot, t);
+                apply_schur_batch(c, U, clov, prec, out, in, tmp, 1, nullptr, nullptr, b_slot, T_slot, Ti_slot, t, uniform);
             CK(cudaEventRecord(c->ev1, c->st));
             CK(cudaEventSynchronize(c->ev1));
             CK(cudaGetLastError());
@@ -1132,12 +1133,15 @@ struct SlotTables {
     char *mem;
     double *b;
     const void **T, **Ti;
+    int *uniform;
+    static constexpr size_t kBytes = 3 * kMaxBatch * sizeof(double) + 16;
     SlotTables(lym_context *ctx, const std::vector<const OpEntry *> &ops) : c(ctx)
     {
-        mem = (char *)dev_alloc(c, 3 * kMaxBatch * sizeof(double));
+        mem = (char *)dev_alloc(c, kBytes);
         b = (double *)mem;
         T = (const void **)(mem + kMaxBatch * sizeof(double));
         Ti = (const void **)(mem + 2 * kMaxBatch * sizeof(double));
+        uniform = (int *)(mem + 3 * kMaxBatch * sizeof(double));
         std::vector<double> hb(ops.size());
         std::vector<const void *> hT(ops.size()), hTi(ops.size());
         for (size_t j = 0; j < ops.size(); ++j) {
@@ -1150,13 +1154,16 @@ struct SlotTables {
             CK(cudaMemcpyAsync(b, hb.data(), ops.size() * sizeof(double), cudaMemcpyHostToDevice, c->st));
             CK(cudaMemcpyAsync(T, hT.data(), ops.size() * sizeof(void *), cudaMemcpyHostToDevice, c->st));
             CK(cudaMemcpyAsync(Ti, hTi.data(), ops.size() * sizeof(void *), cudaMemcpyHostToDevice, c->st));
+            int uni = 1;
+            for (size_t j = 1; j < ops.size(); ++j) uni &= hT[j] == hT[0];
+            CK(cudaMemcpyAsync(uniform, &uni, sizeof(int), cudaMemcpyHostToDevice, c->st));
             CK(cudaStreamSynchronize(c->st));
         } catch (...) {
-            dev_free(c, mem, 3 * kMaxBatch * sizeof(double));
+            dev_free(c, mem, kBytes);
             throw;
         }
     }
-    ~SlotTables() { dev_free(c, mem, 3 * kMaxBatch * sizeof(double)); }
+    ~SlotTables() { dev_free(c, mem, kBytes); }
     SlotTables(const SlotTables &) = delete;
     SlotTables &operator=(const SlotTables &) = delete;
 };
@@ -1199,11 +1206,12 @@ public:
             CK(cudaMemsetAsync(svec->s.v, 0, svec->bytes, c->st));
             CK(cudaMemsetAsync(rhat->s.v, 0, rhat->bytes, c->st));
         }
-        tables = (char *)dev_alloc(c, 3 * kMaxBatch * sizeof(double));
+        tables = (char *)dev_alloc(c, kTableBytes);
         d_b = (double *)tables;
         d_T = (const void **)(tables + kMaxBatch * sizeof(double));
         d_Ti = (const void **)(tables + 2 * kMaxBatch * sizeof(double));
-        CK(cudaMemsetAsync(tables, 0, 3 * kMaxBatch * sizeof(double), c->st));
+        d_uniform = (int *)(tables + 3 * kMaxBatch * sizeof(double));
+        CK(cudaMemsetAsync(tables, 0, kTableBytes, c->st));
         for (BVec *v : {&xs, &rs, &ps, &aps, &tes, &tos}) CK(cudaMemsetAsync(v->s.v, 0, v->bytes, c->st));
         memset(&hs, 0, sizeof(hs));
         hs.nb = nb;
@@ -1214,7 +1222,7 @@ public:
     {
         if (exec) cudaGraphExecDestroy(exec);
         for (int j = 0; j < nb; ++j) delete slot[j].bp;
-        dev_free(c, tables, 3 * kMaxBatch * sizeof(double));
+        dev_free(c, tables, kTableBytes);
     }
 
     int free_slot() const
@@ -1246,7 +1254,7 @@ public:
             gauge_id = op.gauge_id;
             has_clover = clov;
             for (int k = 0; k < nb; ++k) set_tables(k, b, T, Ti);
-            tile = tune_batch(c, gauge_of(c, gauge_id).dev, clov, sprec, tos.s, ps.s, tes.s, d_b, d_T, d_Ti);
+            tile = tune_batch(c, gauge_of(c, gauge_id).dev, clov, sprec, tos.s, ps.s, tes.s, d_b, d_T, d_Ti, d_uniform);
         }
         Slot &s = slot[j];
         delete s.bp;
@@ -1341,9 +1349,12 @@ private:
     Vec te, t1, rS, rN;
     BVec xs, rs, ps, aps, tes, tos;       // CG: p, S^+S p (aps), tmp, S p (tos); BiCGStab: p, v, tmp, t
     std::unique_ptr<BVec> svec, rhat;     // BiCGStab only: s and the shadow residual
+    static constexpr size_t kTableBytes = 3 * kMaxBatch * sizeof(double) + 16;
     char *tables = nullptr;
     double *d_b = nullptr;
     const void **d_T = nullptr, **d_Ti = nullptr;
+    int *d_uniform = nullptr;
+    const void *h_T[kMaxBatch] = {};
     int gauge_id = -1;
     bool has_clover = false;
     BatchTile tile;
@@ -1357,12 +1368,17 @@ private:
     static constexpr int kMaxStalls = 3, kMaxRestarts = 3;
     Slot slot[kMaxBatch];
 
-    // the operator of slot j in the device tables: b = -kappa^2 and the FP32 T / Tinv bases
+    // the operator of slot j in the device tables: b = -kappa^2 and the FP32 T / Tinv bases,
+    // and the flag telling the stencil whether all slots now share one operator
     void set_tables(int j, double b, const void *T, const void *Ti)
     {
+        h_T[j] = T;
+        int uni = 1;
+        for (int k = 1; k < nb; ++k) uni &= h_T[k] == h_T[0];
         CK(cudaMemcpyAsync(d_b + j, &b, sizeof(double), cudaMemcpyHostToDevice, c->st));
         CK(cudaMemcpyAsync(d_T + j, &T, sizeof(void *), cudaMemcpyHostToDevice, c->st));
         CK(cudaMemcpyAsync(d_Ti + j, &Ti, sizeof(void *), cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(d_uniform, &uni, sizeof(int), cudaMemcpyHostToDevice, c->st));
         CK(cudaStreamSynchronize(c->st));
     }
     BatchCGState hs;
@@ -1554,11 +1570,11 @@ private:
         const GaugeDev &U = gauge_of(c, gauge_id).dev;
         Gate gate{&S->pause, nullptr};
         const int lognb = xs.s.lognb;
-        apply_schur_batch(c, U, has_clover, sprec, aps.s, ps.s, tes.s, 0, &S->pause, S->active, d_b, d_T, d_Ti, tile);
+        apply_schur_batch(c, U, has_clover, sprec, aps.s, ps.s, tes.s, 0, &S->pause, S->active, d_b, d_T, d_Ti, tile, d_uniform);
         run_batch(c, OpBBAlpha<BatchF, SP>{rhat->f(), v, S}, lognb, gate);
         run_batch(c, OpBBResidualS<BatchF, SP, SP>{rs.f(), v, sv, S}, lognb, gate);
         apply_schur_batch(c, U, has_clover, sprec, tos.s, svec->s, tes.s, 0, &S->pause, S->active, d_b, d_T, d_Ti,
-                          tile);
+                          tile, d_uniform);
         run_batch(c, OpBBOmega<SP, SP>{t, sv, S}, lognb, gate);
         run_batch(c, OpBBUpdate<BatchF, SP, SP, SP, BatchF, BatchF>{xs.f(), p, sv, t, rs.f(), rhat->f(), S}, lognb,
                   gate);
@@ -1574,8 +1590,8 @@ private:
         const GaugeDev &U = gauge_of(c, gauge_id).dev;
         Gate gate{&S->pause, nullptr};
         const int lognb = xs.s.lognb;
-        apply_schur_batch(c, U, has_clover, sprec, tos.s, ps.s, tes.s, 1, &S->pause, S->active, d_b, d_T, d_Ti, tile);
-        apply_schur_batch(c, U, has_clover, sprec, aps.s, tos.s, tes.s, 1, &S->pause, S->active, d_b, d_T, d_Ti, tile);
+        apply_schur_batch(c, U, has_clover, sprec, tos.s, ps.s, tes.s, 1, &S->pause, S->active, d_b, d_T, d_Ti, tile, d_uniform);
+        apply_schur_batch(c, U, has_clover, sprec, aps.s, tos.s, tes.s, 1, &S->pause, S->active, d_b, d_T, d_Ti, tile, d_uniform);
         if (sprec == PREC_F) {
             run_batch(c, OpBAlpha<BatchF, BatchF>{ps.f(), aps.f(), S}, lognb, gate);
             run_batch(c, OpBUpdate<BatchF, BatchF, BatchF, BatchF>{xs.f(), ps.f(), rs.f(), aps.f(), S}, lognb,
@@ -2356,7 +2372,7 @@ int lym_time_stencil_batch(lym_context *c, int op_id, int prec, int which, int b
         BVec a(c, prec, batch), b(c, prec, batch), y(c, prec, batch);
         for (BVec *v : {&a, &b, &y}) CK(cudaMemsetAsync(v->s.v, 0, v->bytes, c->st));
         SlotTables tab(c, std::vector<const OpEntry *>(batch, &op));  // every slot on this operator
-        const BatchTile tile = tune_batch(c, ge.dev, clov, prec, b.s, a.s, y.s, tab.b, tab.T, tab.Ti);
+        const BatchTile tile = tune_batch(c, ge.dev, clov, prec, b.s, a.s, y.s, tab.b, tab.T, tab.Ti, tab.uniform);
         DslashBatchParams P;
         P.g = c->g;
         P.prec = prec;
@@ -2366,6 +2382,7 @@ int lym_time_stencil_batch(lym_context *c, int op_id, int prec, int which, int b
         P.order = order_table(c, tile.by, tile.bz);
         P.minb = tile.minb;
         P.has_clover = clov;
+        P.uniform = tab.uniform;
         if (which == 0) {
             P.epi = EPI_XPAY_;
             P.parity = 1;
@@ -2425,9 +2442,9 @@ int lym_multiply_batch(lym_context *c, int prec, int nrhs, const int *op_ids, co
             else axpby_views(c, (*full).parity(1).d(), bin.h().slot(j), C2(1.0), C2(0.0));
         }
         const GaugeDev &U = gauge_of(c, ops[0]->gauge_id).dev;
-        const BatchTile tile = tune_batch(c, U, true, prec, btmp.s, bin.s, bout.s, tab.b, tab.T, tab.Ti);
+        const BatchTile tile = tune_batch(c, U, true, prec, btmp.s, bin.s, bout.s, tab.b, tab.T, tab.Ti, tab.uniform);
         apply_schur_batch(c, U, true, prec, bout.s, bin.s, btmp.s, ops[0]->gamma5, nullptr, nullptr, tab.b, tab.T,
-                          tab.Ti, tile);
+                          tab.Ti, tile, tab.uniform);
         for (int j = 0; j < nrhs; ++j) {
             upload_vec(c, *full, in[j], false, 0);  // the even parity passes through
             if (prec == PREC_F) axpby_views(c, bout.f().slot(j), (*full).parity(1).d(), C2(1.0), C2(0.0));

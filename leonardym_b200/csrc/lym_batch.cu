@@ -48,7 +48,7 @@ static void run(const DslashBatchParams &P, const SB &in, const SB &out, const S
     DslashBatchArg<SB, G> a{P.g,       in,          out,       y,         U,
                             P.parity,  P.gamma5,    P.has_clover, in.lognp, (float)P.a,
                             (float)P.b, NbrTable{P.nbr, P.g.stride}, P.order, P.skip_if, P.active,
-                            P.b_slot,  P.clover_slot};
+                            P.b_slot,  P.clover_slot, P.uniform};
     switch (P.epi) {
     case EPI_SCALE_: launch_minb<EPI_SCALE>(P, a, st); break;
     case EPI_CLOVINV_: launch_minb<EPI_CLOVINV>(P, a, st); break;

@@ -168,6 +168,15 @@ struct BatchF {
             x[c] = c2{make_float2(w.x, w.y), make_float2(w.z, w.w)};
         }
     }
+    // the 6 components of spin block blk (spins 0, 1 or 2, 3)
+    LYM_D void unstage_block(const float4 *p0, int step, int blk, c2 x[6]) const
+    {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            const float4 w = p0[(6 * blk + c) * step];
+            x[c] = c2{make_float2(w.x, w.y), make_float2(w.z, w.w)};
+        }
+    }
     LYM_HD SlotF slot(int r) const { return SlotF{(float *)v, stride, lognp, r}; }
 };
 
@@ -287,6 +296,18 @@ struct BatchH {
             x[2 * w + 1] = c2{mul2(__half22float2(hp[2]), n), mul2(__half22float2(hp[3]), n)};
         }
     }
+    LYM_D void unstage_block(const float4 *p0, int step, int blk, c2 x[6]) const
+    {
+        const float4 nw = p0[6 * step];
+        const float2 n = make_float2(nw.x, nw.y);
+#pragma unroll
+        for (int w = 0; w < 3; ++w) {
+            const int4 u = *reinterpret_cast<const int4 *>(p0 + (3 * blk + w) * step);
+            const __half2 *hp = reinterpret_cast<const __half2 *>(&u);
+            x[2 * w] = c2{mul2(__half22float2(hp[0]), n), mul2(__half22float2(hp[1]), n)};
+            x[2 * w + 1] = c2{mul2(__half22float2(hp[2]), n), mul2(__half22float2(hp[3]), n)};
+        }
+    }
     LYM_HD SlotH slot(int r) const { return SlotH{(__half *)v, (float *)norm, stride, lognp, r}; }
 };
 
@@ -399,67 +420,95 @@ template <bool REAL> LYM_D void mul_ud2(const LinkP &L, const c2 h[3], c2 w[3])
     }
 }
 
-// The 36 words of one clover block for the pair: SAME (both lanes on one operator) reads
-// them once and duplicates each into both lanes, otherwise each lane reads its own.
-template <bool SAME>
-LYM_D void clover_words(const float4 *ta, const float4 *tb, unsigned off, int stride, float2 v[36])
+// Clover words of one half-site for a pair: word k (0..8) of block blk as four lane
+// pairs.  From shared memory when the whole batch shares one operator (each value is
+// duplicated into both lanes), else from each lane's own clover term in HBM.
+struct CloverWordsSmem {
+    const float4 *w0, *w1;  // the 9 words of block 0 and of block 1
+    LYM_D void get(int blk, int k, float2 v[4]) const
+    {
+        const float4 x = (blk ? w1 : w0)[k];
+        v[0] = make_float2(x.x, x.x);
+        v[1] = make_float2(x.y, x.y);
+        v[2] = make_float2(x.z, x.z);
+        v[3] = make_float2(x.w, x.w);
+    }
+};
+struct CloverWordsGlobal {
+    const float4 *ta, *tb;
+    unsigned base;  // (p * 2 * 9) * stride + h
+    int stride;
+    bool same;
+    LYM_D void get(int blk, int k, float2 v[4]) const
+    {
+        const unsigned o = base + (unsigned)(blk * 9 + k) * stride;
+        const float4 wa = __ldcs(ta + o);
+        const float4 wb = same ? wa : __ldcs(tb + o);
+        v[0] = make_float2(wa.x, wb.x);
+        v[1] = make_float2(wa.y, wb.y);
+        v[2] = make_float2(wa.z, wb.z);
+        v[3] = make_float2(wa.w, wb.w);
+    }
+};
+
+LYM_HD constexpr int tri_row(int t) { return t < 1 ? 1 : t < 3 ? 2 : t < 6 ? 3 : t < 10 ? 4 : 5; }
+
+// out = SIGN (add + A x) for one Hermitian 6x6 block A of the FP32 clover term (packed as
+// in CloverF: 6 real diagonal entries, then the 15 entries below the diagonal, row-major),
+// for the two RHS of a pair.  With HAS_ADD, out holds SIGN * add on entry (the block is
+// accumulated in place); without it out is written.  The words are read one at a time in
+// storage order; products entering with the other sign are summed apart (nre, nim) and
+// subtracted once per row, so no negated operand is formed.
+template <int SIGN, bool HAS_ADD, class CW> LYM_D void clover_block_apply(const CW &cw, int blk, const c2 x[6], c2 out[6])
 {
+    float2 nre[6], nim[6];
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-        const float4 wa = __ldcs(ta + off + k * stride);
-        const float4 wb = SAME ? wa : __ldcs(tb + off + k * stride);
-        v[4 * k] = make_float2(wa.x, wb.x);
-        v[4 * k + 1] = make_float2(wa.y, wb.y);
-        v[4 * k + 2] = make_float2(wa.z, wb.z);
-        v[4 * k + 3] = make_float2(wa.w, wb.w);
-    }
-}
-
-// y = A x for one Hermitian 6x6 block of the FP32 clover term (packed as in CloverF: 6
-// real diagonal entries, then the 15 entries below the diagonal, row-major), for the two
-// RHS of a pair.  A_ij = a (i > j), A_ji = conj(a); the products entering with a minus
-// sign are summed apart (nre, nim) and subtracted once per row.
-template <bool SAME>
-LYM_D void clover_pair_block(const float4 *ta, const float4 *tb, int stride, int p, int blk, int h, const c2 x[6],
-                             c2 y[6])
-{
-    float2 v[36];
-    clover_words<SAME>(ta, tb, (unsigned)(p * 2 + blk) * 9 * stride + h, stride, v);
-    float2 pre[6], pim[6], nre[6], nim[6];
+        float2 w[4];
+        cw.get(blk, k, w);
 #pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        pre[i] = mul2(v[i], x[i].re);
-        pim[i] = mul2(v[i], x[i].im);
-    }
-#pragma unroll
-    for (int i = 1; i < 6; ++i)
-#pragma unroll
-        for (int j = 0; j < i; ++j) {
-            const int t = tri_index(i, j);
-            const float2 are = v[6 + 2 * t], aim = v[7 + 2 * t];
-            // y_i += a x_j
-            pre[i] = fma2(are, x[j].re, pre[i]);
-            nre[i] = j == 0 ? mul2(aim, x[j].im) : fma2(aim, x[j].im, nre[i]);
-            pim[i] = fma2(are, x[j].im, pim[i]);
-            pim[i] = fma2(aim, x[j].re, pim[i]);
-            // y_j += conj(a) x_i
-            pre[j] = fma2(are, x[i].re, pre[j]);
-            pre[j] = fma2(aim, x[i].im, pre[j]);
-            pim[j] = fma2(are, x[i].im, pim[j]);
-            nim[j] = i == j + 1 ? mul2(aim, x[i].re) : fma2(aim, x[i].re, nim[j]);
+        for (int l = 0; l < 4; ++l) {
+            const int e = 4 * k + l;
+            if (e < 6) {  // diagonal entry d_e (the first words: every row starts here)
+                if (SIGN > 0) {
+                    out[e].re = HAS_ADD ? fma2(w[l], x[e].re, out[e].re) : mul2(w[l], x[e].re);
+                    out[e].im = HAS_ADD ? fma2(w[l], x[e].im, out[e].im) : mul2(w[l], x[e].im);
+                } else {
+                    nre[e] = mul2(w[l], x[e].re);
+                    nim[e] = mul2(w[l], x[e].im);
+                }
+            } else if (((e - 6) & 1) == 0) {  // entry t = (i, j), i > j: (re, im) = w[l], w[l + 1]
+                const int t = (e - 6) / 2, i = tri_row(t), j = t - i * (i - 1) / 2;
+                const float2 are = w[l], aim = w[l + 1];
+                if (SIGN > 0) {
+                    // y_i += a x_j
+                    out[i].re = fma2(are, x[j].re, out[i].re);
+                    nre[i] = j == 0 ? mul2(aim, x[j].im) : fma2(aim, x[j].im, nre[i]);
+                    out[i].im = fma2(are, x[j].im, out[i].im);
+                    out[i].im = fma2(aim, x[j].re, out[i].im);
+                    // y_j += conj(a) x_i
+                    out[j].re = fma2(are, x[i].re, out[j].re);
+                    out[j].re = fma2(aim, x[i].im, out[j].re);
+                    out[j].im = fma2(are, x[i].im, out[j].im);
+                    nim[j] = i == j + 1 ? mul2(aim, x[i].re) : fma2(aim, x[i].re, nim[j]);
+                } else {
+                    nre[i] = fma2(are, x[j].re, nre[i]);
+                    out[i].re = fma2(aim, x[j].im, out[i].re);
+                    nim[i] = fma2(are, x[j].im, nim[i]);
+                    nim[i] = fma2(aim, x[j].re, nim[i]);
+                    nre[j] = fma2(are, x[i].re, nre[j]);
+                    nre[j] = fma2(aim, x[i].im, nre[j]);
+                    nim[j] = fma2(are, x[i].im, nim[j]);
+                    out[j].im = fma2(aim, x[i].re, out[j].im);
+                }
+            }
         }
+    }
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
-        y[i].re = i == 0 ? pre[0] : sub2(pre[i], nre[i]);
-        y[i].im = i == 5 ? pim[5] : sub2(pim[i], nim[i]);
+        if (SIGN < 0 || i > 0) out[i].re = sub2(out[i].re, nre[i]);
+        if (SIGN < 0 || i < 5) out[i].im = sub2(out[i].im, nim[i]);
     }
-}
-
-template <bool SAME>
-LYM_D void clover_pair(const float4 *ta, const float4 *tb, int stride, int p, int h, const c2 x[12], c2 y[12])
-{
-    clover_pair_block<SAME>(ta, tb, stride, p, 0, h, x, y);
-    clover_pair_block<SAME>(ta, tb, stride, p, 1, h, x + 6, y + 6);
 }
 
 // ---------------------------------------------------------- batch stencil --
@@ -535,65 +584,75 @@ template <class SB, class GaugeT> struct DslashBatchArg {
     // kappa, hence different b (nullptr: the shared b) and clover terms (FP32 bases)
     const double *b_slot;
     const void *const *clover_slot;
+    const int *uniform;  // device flag: every slot on one operator (nullptr: not known)
 };
 
-// The epilogue on H x (acc) for the pair q at half-site h; yv: the same-parity input
-// (EPI_XPAY only).
-template <int EPI, class SB, class GaugeT>
+// The epilogue on H x (acc) for the pair q at half-site h, written to out.  ysrc(blk, y6)
+// gives the 6 same-parity input components of block blk (EPI_XPAY); cw the clover words.
+template <int EPI, class SB, class GaugeT, class YSrc, class CW>
 LYM_D void batch_epilogue(const DslashBatchArg<SB, GaugeT> &arg, int h, int q, bool act_a, bool act_b, c2 acc[12],
-                          const c2 yv[12])
+                          const YSrc &ysrc, const CW &cw)
 {
     const int ra = 2 * q, rb = 2 * q + 1;
-    c2 res[12];
-    const float4 *ta = nullptr, *tb = nullptr;
-    if (EPI != EPI_SCALE && arg.has_clover) {  // an inactive lane borrows its partner's operator
-        ta = (const float4 *)arg.clover_slot[act_a ? ra : rb];
-        tb = (const float4 *)arg.clover_slot[act_b ? rb : ra];
-    }
-    if (EPI == EPI_SCALE) {
-        const float2 a = make_float2(arg.a, arg.a);
-#pragma unroll
-        for (int k = 0; k < 12; ++k) res[k] = c2{mul2(a, acc[k].re), mul2(a, acc[k].im)};
-    } else if (EPI == EPI_CLOVINV) {
+    if (EPI == EPI_SCALE || EPI == EPI_CLOVINV) {
         const float2 a = make_float2(arg.a, arg.a);
 #pragma unroll
         for (int k = 0; k < 12; ++k) acc[k] = c2{mul2(a, acc[k].re), mul2(a, acc[k].im)};
-        if (!arg.has_clover) {
+        if (EPI == EPI_CLOVINV && arg.has_clover) {
 #pragma unroll
-            for (int k = 0; k < 12; ++k) res[k] = acc[k];
-        } else if (ta == tb) {
-            clover_pair<true>(ta, tb, arg.g.stride, arg.parity, h, acc, res);
-        } else {
-            clover_pair<false>(ta, tb, arg.g.stride, arg.parity, h, acc, res);
+            for (int blk = 0; blk < 2; ++blk) {
+                c2 res[6];
+                clover_block_apply<+1, false>(cw, blk, acc + 6 * blk, res);
+#pragma unroll
+                for (int k = 0; k < 6; ++k) acc[6 * blk + k] = res[k];
+            }
         }
     } else {
-        if (!arg.has_clover) {
-#pragma unroll
-            for (int k = 0; k < 12; ++k) res[k] = yv[k];
-        } else if (ta == tb) {
-            clover_pair<true>(ta, tb, arg.g.stride, arg.parity, h, yv, res);
-        } else {
-            clover_pair<false>(ta, tb, arg.g.stride, arg.parity, h, yv, res);
-        }
         float ba = arg.b, bb = arg.b;
         if (arg.b_slot) {
             ba = (float)arg.b_slot[act_a ? ra : rb];
             bb = (float)arg.b_slot[act_b ? rb : ra];
         }
-        const float2 b = make_float2(ba, bb);
+        const float2 b = make_float2(ba, bb), nb = make_float2(-ba, -bb);
 #pragma unroll
-        for (int k = 0; k < 6; ++k) res[k] = c2{fma2(b, acc[k].re, res[k].re), fma2(b, acc[k].im, res[k].im)};
-        if (arg.gamma5) {  // lower spins: -(T y + b H x) = (-b) H x - T y
-            const float2 nb = make_float2(-ba, -bb);
+        for (int blk = 0; blk < 2; ++blk) {
+            c2 y6[6];
+            ysrc(blk, y6);
+            c2 *o = acc + 6 * blk;
+            if (blk == 1 && arg.gamma5) {  // lower spins: -(T y + b H x)
 #pragma unroll
-            for (int k = 6; k < 12; ++k)
-                res[k] = c2{sub2(mul2(nb, acc[k].re), res[k].re), sub2(mul2(nb, acc[k].im), res[k].im)};
-        } else {
+                for (int k = 0; k < 6; ++k) o[k] = c2{mul2(nb, o[k].re), mul2(nb, o[k].im)};
+                if (arg.has_clover) {
+                    clover_block_apply<-1, true>(cw, blk, y6, o);
+                } else {
 #pragma unroll
-            for (int k = 6; k < 12; ++k) res[k] = c2{fma2(b, acc[k].re, res[k].re), fma2(b, acc[k].im, res[k].im)};
+                    for (int k = 0; k < 6; ++k) o[k] = c2{sub2(o[k].re, y6[k].re), sub2(o[k].im, y6[k].im)};
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < 6; ++k) o[k] = c2{mul2(b, o[k].re), mul2(b, o[k].im)};
+                if (arg.has_clover) {
+                    clover_block_apply<+1, true>(cw, blk, y6, o);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 6; ++k) o[k] = c2{add2(o[k].re, y6[k].re), add2(o[k].im, y6[k].im)};
+                }
+            }
         }
     }
-    arg.out.store(h, q, res);
+    arg.out.store(h, q, acc);
+}
+
+template <int EPI, class SB, class GaugeT>
+LYM_D CloverWordsGlobal clover_global(const DslashBatchArg<SB, GaugeT> &arg, int h, int q, bool act_a, bool act_b)
+{
+    CloverWordsGlobal cw{nullptr, nullptr, (unsigned)arg.parity * 18 * arg.g.stride + h, arg.g.stride, true};
+    if (EPI != EPI_SCALE && arg.has_clover) {  // an inactive lane borrows its partner's operator
+        cw.ta = (const float4 *)arg.clover_slot[act_a ? 2 * q : 2 * q + 1];
+        cw.tb = (const float4 *)arg.clover_slot[act_b ? 2 * q + 1 : 2 * q];
+        cw.same = cw.ta == cw.tb;
+    }
+    return cw;
 }
 
 // out_r = a H in_r (EPI_SCALE), Tinv_r (a H in_r) (EPI_CLOVINV) or
@@ -620,12 +679,16 @@ __global__ void __launch_bounds__(128, MINB) dslash_batch_kernel(const DslashBat
     }
     c2 acc[12];
     hopping_pair<GaugeT::kReal>(nf, nbk, arg.in, arg.U, arg.parity, h, q, acc);
+    const CloverWordsGlobal cw = clover_global<EPI>(arg, h, q, act_a, act_b);
     if (EPI == EPI_XPAY) {
         c2 yv[12];
         arg.y.load_cs(h, q, yv);
-        batch_epilogue<EPI>(arg, h, q, act_a, act_b, acc, yv);
+        batch_epilogue<EPI>(arg, h, q, act_a, act_b, acc, [&](int blk, c2 y6[6]) {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) y6[k] = yv[6 * blk + k];
+        }, cw);
     } else {
-        batch_epilogue<EPI>(arg, h, q, act_a, act_b, acc, acc);
+        batch_epilogue<EPI>(arg, h, q, act_a, act_b, acc, [](int, c2 *) {}, cw);
     }
 }
 
@@ -649,6 +712,16 @@ template <bool STAGE_Y, class SB, class GaugeT> struct StagedHop {
     int nf[4], nbk[4];
     bool live;
     unsigned vmask;
+    bool clov_smem;       // the batch shares one operator: its clover words go through shared memory
+    const float4 *clov;   // that operator's clover term
+
+    // the 9 words of clover block blk of this half-site into link buffer blk
+    LYM_D void stage_clover(int blk) const
+    {
+        const unsigned base = ((unsigned)(arg.parity * 2 + blk) * 9) * arg.g.stride + h;
+        float4 *L = sl(blk);
+        for (int k = lane_in; k < 9; k += np) cp_async16(smem_u32(L + k), clov + base + k * arg.g.stride);
+    }
 
     LYM_D float4 *sx(int buf) const { return smem + buf * 12 * kStagedThreads + threadIdx.x; }
     LYM_D float4 *sl(int buf) const
@@ -668,8 +741,9 @@ template <bool STAGE_Y, class SB, class GaugeT> struct StagedHop {
     {
         if constexpr (D < 7) {
             issue<D + 1>();
-        } else if constexpr (STAGE_Y) {
-            if (live) arg.y.stage(smem_u32(sx(0)), kStagedThreads * 16, h, q);
+        } else {
+            if (STAGE_Y && live) arg.y.stage(smem_u32(sx(0)), kStagedThreads * 16, h, q);
+            if (clov_smem) stage_clover(0);
         }
         cp_async_commit();
         cp_async_wait<1>();  // the copies of direction D (this thread's)
@@ -712,6 +786,8 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
     }
     s.live = act_a || act_b;  // idle pairs still copy their share of the link words
     s.vmask = vmask;
+    s.clov_smem = EPI != EPI_SCALE && arg.has_clover && arg.uniform && *arg.uniform;
+    s.clov = s.clov_smem ? (const float4 *)arg.clover_slot[0] : nullptr;
     c2 acc[12];
 #pragma unroll
     for (int k = 0; k < 12; ++k) acc[k] = c2{make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
@@ -725,17 +801,16 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
     s.template step<5>(acc);
     s.template step<6>(acc);
     s.template step<7>(acc);
-    if (!s.live) {
-        cp_async_wait<0>();
-        return;
-    }
-    if (EPI == EPI_XPAY) {
-        cp_async_wait<0>();
-        c2 yv[12];
-        arg.y.unstage(s.sx(0), kStagedThreads, yv);
-        batch_epilogue<EPI>(arg, s.h, q, act_a, act_b, acc, yv);
+    if (s.clov_smem) s.stage_clover(1);  // link buffer 1 is free after the last direction
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncwarp(vmask);
+    if (!s.live) return;
+    auto ysrc = [&](int blk, c2 y6[6]) { arg.y.unstage_block(s.sx(0), kStagedThreads, blk, y6); };
+    if (s.clov_smem) {
+        batch_epilogue<EPI>(arg, s.h, q, act_a, act_b, acc, ysrc, CloverWordsSmem{s.sl(0), s.sl(1)});
     } else {
-        batch_epilogue<EPI>(arg, s.h, q, act_a, act_b, acc, acc);
+        batch_epilogue<EPI>(arg, s.h, q, act_a, act_b, acc, ysrc, clover_global<EPI>(arg, s.h, q, act_a, act_b));
     }
 }
 

@@ -109,6 +109,7 @@ struct DslashBatchParams {
     int minb = 1;                              // kernel variant: minimum resident blocks per SM
     const double *b_slot = nullptr;            // device array [nb] or nullptr
     const void *const *clover_slot = nullptr;  // device array [nb] of FP32 clover bases (T or Tinv)
+    const int *uniform = nullptr;              // device flag: every slot on one operator
 };
 
 void launch_dslash_batch(const DslashBatchParams &P, cudaStream_t st);
