@@ -75,6 +75,70 @@ def workload_sources(nc=3):
     return srcs
 
 
+# Serving workload (the configs' serving loop): 8 resident seeded fields, one per
+# (volume, representation), requests in a seeded Poisson stream of mean rate
+# SERVE_RATE with kappa uniform in the representation's range and 1-16 sources each.
+SERVE_VOLUMES = [(8, 8, 8, 8), (12, 12, 12, 12), (16, 16, 16, 32), (24, 24, 24, 48)]
+SERVE_RATE = 200.0
+SERVE_KAPPA = {"su3": (0.12, 0.135), "su2adj": (0.17, 0.185)}
+SERVE_CSW = {"su3": 1.7, "su2adj": 1.5}
+SERVE_EPS = {"su3": 0.25, "su2adj": 0.3}
+SERVE_POOL = 4  # distinct sources per field (reused across requests; every request gets its own solutions)
+
+
+def run_serving(window_s, batch=16, precision="single"):
+    """Open-loop serving measurement: requests arrive for window_s seconds at Poisson times
+    (seeded) and are submitted to the solve server as they arrive; the result is the
+    completed sources per second over the whole run, per-request latency p50 / p99 (submit
+    to completion, the server's own clock) and the largest FP64 true residual."""
+    from leonardym_b200 import synth
+    from leonardym_b200.server import SolveServer
+    rng = np.random.default_rng(SEED + 7)
+    fields = [(dims, rep) for dims in SERVE_VOLUMES for rep in ("su3", "su2adj")]
+    srv = SolveServer(batch=batch, precision=precision)
+    pools = {}
+    try:
+        for key, (dims, rep) in enumerate(fields):
+            srv.add_gauge(key, dims, rep, synth.fermion_links(dims, rep, SERVE_EPS[rep], SEED + 4 * key))
+            pools[key] = [synth.gaussian_spinor(dims, 3, SEED + 100 * key + j) for j in range(SERVE_POOL)]
+        t, arrivals = 0.0, []
+        while True:
+            t += rng.exponential(1.0 / SERVE_RATE)
+            if t > window_s:
+                break
+            key = int(rng.integers(len(fields)))
+            rep = fields[key][1]
+            kappa = float(rng.uniform(*SERVE_KAPPA[rep]))
+            nsrc = int(rng.integers(1, 17))
+            arrivals.append((t, key, kappa, nsrc))
+        tickets = []
+        t0 = time.perf_counter()
+        for (ta, key, kappa, nsrc) in arrivals:
+            delay = t0 + ta - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            srcs = [pools[key][j % SERVE_POOL] for j in range(nsrc)]
+            tickets.append(srv.submit(key, kappa, SERVE_CSW[fields[key][1]], srcs)[0])
+        lat, worst, nsolved, failed = [], 0.0, 0, 0
+        for tk in tickets:
+            ok, st = srv.wait(tk, timeout=1800.0)
+            lat.append(st.latency_s * 1e3)
+            worst = max(worst, st.max_true_residual)
+            nsolved += st.nsrc
+            failed += 0 if ok else 1
+        elapsed = time.perf_counter() - t0
+    finally:
+        srv.close()
+    lat.sort()
+    return {"requests": len(tickets), "sources": nsolved, "arrival_window_s": window_s,
+            "offered_requests_per_s": SERVE_RATE, "elapsed_s": elapsed,
+            "throughput_solves_per_s": nsolved / elapsed, "throughput_requests_per_s": len(tickets) / elapsed,
+            "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+            "max_true_residual": worst, "failed_requests": failed,
+            "fields": [f"{'x'.join(map(str, d))} {r}" for d, r in fields],
+            "solver": f"block even-odd CG, {batch} slots per field, {precision} storage, continuous batching"}
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled during the timed region."""
 
@@ -409,6 +473,9 @@ def run_ours(args, world, rank, local):
                           f"{info['sample_seconds']:.1f} s of CPU work), extrapolated to the {n_iter} iterations "
                           f"its GPU mirror needs on the same system")}
     lat.close()
+    serving = None
+    if rank == 0 and args.serve_window > 0:  # after the timed region: its own clock
+        serving = run_serving(args.serve_window, batch=args.batch, precision=args.precision)
     if rank != 0:
         return
     line = {
@@ -436,6 +503,7 @@ def run_ours(args, world, rank, local):
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": nrhs * nbytes,
                 "d2h_bytes_per_step": nrhs * nbytes},
         "cpu_baseline": cpu,
+        "serving": serving,
     }
     print(json.dumps(line), flush=True)
 
@@ -487,6 +555,8 @@ def main():
     ap.add_argument("--batch", type=int, default=16, help="right-hand sides per batched stencil (power of 2 <= 32)")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--profile", action="store_true", help="small fixed case for ncu captures")
+    ap.add_argument("--serve-window", type=float, default=0.25,
+                    help="seconds of Poisson arrivals for the serving measurement (0: skip it)")
     ap.add_argument("--tile", default="", help="with --profile: batched stencil column and variant 'by,bz,minb'")
     args = ap.parse_args()
     if args.profile:
