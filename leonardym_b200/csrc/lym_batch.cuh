@@ -1154,7 +1154,7 @@ template <class SX, class SP, class SS, class ST, class SR, class SRh> struct Op
         p.load_d(h, q, pv[0], pv[1]);
         sv.load_d(h, q, sw[0], sw[1]);
         tv.load_d(h, q, tw[0], tw[1]);
-        rv.load_d(h, q, rr[0], rr[1]);
+        if (!act[0] || !act[1]) rv.load_d(h, q, rr[0], rr[1]);  // an idle lane keeps its residual
         rh.load_d(h, q, hv[0], hv[1]);
 #pragma unroll
         for (int l = 0; l < 2; ++l) {
