@@ -85,7 +85,7 @@ struct lym_context {
 
 namespace {
 
-constexpr size_t kStateBytes = 4096;
+constexpr size_t kStateBytes = 8192;
 
 int fail(lym_context *c, int code, const char *fmt, ...)
 {
@@ -1009,6 +1009,7 @@ template <class Op> void run_batch(lym_context *c, const Op &op, int lognb, Gate
     const int lognp = lognb - 1;
     const long threads = (long)c->g.Vh << lognp;
     const int grid = (int)std::min<long>((threads + kBlasThreads - 1) / kBlasThreads, kBlasGridMax);
+    static_assert(Op::NRED <= kBatchMaxRed, "the per-RHS partial sums are sized for kBatchMaxRed reductions");
     site_batch_kernel<Op><<<grid, kBlasThreads, 0, c->st>>>(op, c->g.Vh, lognp, c->bpartials, c->counter, gate);
 }
 
@@ -1203,8 +1204,8 @@ public:
         if (algo == ALGO_BICGSTAB) {
             svec.reset(new BVec(c, sprec, nb));
             rhat.reset(new BVec(c, PREC_F, nb));
-            CK(cudaMemsetAsync(svec->s.v, 0, svec->bytes, c->st));
-            CK(cudaMemsetAsync(rhat->s.v, 0, rhat->bytes, c->st));
+            what.reset(new BVec(c, PREC_F, nb));
+            for (BVec *v : {svec.get(), rhat.get(), what.get()}) CK(cudaMemsetAsync(v->s.v, 0, v->bytes, c->st));
         }
         tables = (char *)dev_alloc(c, kTableBytes);
         d_b = (double *)tables;
@@ -1350,7 +1351,7 @@ private:
     int sprec, nb, algo;
     Vec te, t1, rS, rN;
     BVec xs, rs, ps, aps, tes, tos;       // CG: p, S^+S p (aps), tmp, S p (tos); BiCGStab: p, v, tmp, t
-    std::unique_ptr<BVec> svec, rhat;     // BiCGStab only: s and the shadow residual
+    std::unique_ptr<BVec> svec, rhat, what;  // BiCGStab only: s, the shadow residual rhat, S^+ rhat
     static constexpr size_t kTableBytes = 3 * kMaxBatch * sizeof(double) + 16;
     char *tables = nullptr;
     double *d_b = nullptr;
@@ -1418,12 +1419,36 @@ private:
         rrS = c->h_scal[0];
     }
     // BiCGStab (re)start of slot j from the true residual in rS: r = rhat = p = rS
+    // what = S^+ rhat = g5 S g5 rhat (S is gamma5-hermitian), in FP64 into rN and the slot;
+    // returns <what, p> for p = rhat = rS
+    double2 shadow_image(int j)
+    {
+        copy(c, *t1, *rS);
+        gamma5_inplace(c, *t1);
+        apply_schur(c, *slot[j].op, PREC_D, *rN, *t1, *te, 1);
+        axpby_views(c, (*rN).d(), what->f().slot(j), C2(1.0), C2(0.0));
+        run_site(c, OpDot<SpinorD, SpinorD>{(*rN).d(), (*rS).d(), c->d_scal}, 1);
+        CK(cudaMemcpyAsync(c->h_scal, c->d_scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        return make_double2(c->h_scal[0], c->h_scal[1]);
+    }
+    // <a, b> of two views of slot j
+    template <class SA, class SB> double2 slot_dot(const SA &a, const SB &b)
+    {
+        run_site(c, OpDot<SA, SB>{a, b, c->d_scal}, 1);
+        CK(cudaMemcpyAsync(c->h_scal, c->d_scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        return make_double2(c->h_scal[0], c->h_scal[1]);
+    }
+    // BiCGStab (re)start of slot j from the true residual in rS: r = rhat = p = rS,
+    // rho = |rS|^2, what = S^+ rhat, alpha = rho / <what, p>
     void restart_bicg(int j, double rrS)
     {
         axpby_views(c, (*rS).d(), rs.f().slot(j), C2(1.0), C2(0.0));
         axpby_views(c, (*rS).d(), rhat->f().slot(j), C2(1.0), C2(0.0));
         set_direction(j, 0.0);
         hs.rho[j] = make_double2(rrS, 0.0);
+        hs.alpha[j] = cdiv(hs.rho[j], shadow_image(j));
         hs.rr[j] = hs.rr_max[j] = rrS;
         hs.restart[j] = 0;
         hs.active[j] = 1;
@@ -1456,20 +1481,21 @@ private:
                 restart_bicg(j, rrS);
             } else {
                 // the recursion goes on with the true residual in place of the recursive
-                // one: rho = <rhat, r>, then the direction update the pause held back
-                axpby_views(c, (*rS).d(), rs.f().slot(j), C2(1.0), C2(0.0));
-                run_site(c, OpDot<SlotF, SpinorD>{rhat->f().slot(j), (*rS).d(), c->d_scal}, 1);
-                CK(cudaMemcpyAsync(c->h_scal, c->d_scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
-                CK(cudaStreamSynchronize(c->st));
-                hs.rho[j] = make_double2(c->h_scal[0], c->h_scal[1]);
-                const double2 be = hs.alpha[j], bo = cmul(be, hs.omega[j]);
+                // one: p += r_true - r_rec (p was formed from r_rec), r = r_true,
+                // rho = <rhat, r>, alpha = rho / <what, p>
+                double2 wp;
                 if (sprec == PREC_F) {
-                    axpby_views(c, aps.f().slot(j), ps.f().slot(j), make_double2(-bo.x, -bo.y), be);
-                    axpby_views(c, rs.f().slot(j), ps.f().slot(j), C2(1.0), C2(1.0));
+                    axpby_views(c, rs.f().slot(j), ps.f().slot(j), C2(-1.0), C2(1.0));
+                    axpby_views(c, (*rS).d(), ps.f().slot(j), C2(1.0), C2(1.0));
                 } else {
-                    axpby_views(c, aps.h().slot(j), ps.h().slot(j), make_double2(-bo.x, -bo.y), be);
-                    axpby_views(c, rs.f().slot(j), ps.h().slot(j), C2(1.0), C2(1.0));
+                    axpby_views(c, rs.f().slot(j), ps.h().slot(j), C2(-1.0), C2(1.0));
+                    axpby_views(c, (*rS).d(), ps.h().slot(j), C2(1.0), C2(1.0));
                 }
+                axpby_views(c, (*rS).d(), rs.f().slot(j), C2(1.0), C2(0.0));
+                hs.rho[j] = slot_dot(rhat->f().slot(j), (*rS).d());
+                if (sprec == PREC_F) wp = slot_dot(what->f().slot(j), ps.f().slot(j));
+                else wp = slot_dot(what->f().slot(j), ps.h().slot(j));
+                hs.alpha[j] = cdiv(hs.rho[j], wp);
                 hs.rr[j] = hs.rr_max[j] = rrS;
                 hs.active[j] = 1;
             }
@@ -1572,15 +1598,15 @@ private:
         const GaugeDev &U = gauge_of(c, gauge_id).dev;
         Gate gate{&S->pause, nullptr};
         const int lognb = xs.s.lognb;
-        apply_schur_batch(c, U, has_clover, sprec, aps.s, ps.s, tes.s, 0, &S->pause, S->active, d_b, d_T, d_Ti, tile, d_uniform);
-        run_batch(c, OpBBAlpha<BatchF, SP>{rhat->f(), v, S}, lognb, gate);
+        // alpha is known when the iteration starts (<rhat, S p> = <S^+ rhat, p>, reduced with p)
+        apply_schur_batch(c, U, has_clover, sprec, aps.s, ps.s, tes.s, 0, &S->pause, S->active, d_b, d_T, d_Ti, tile,
+                          d_uniform);
         run_batch(c, OpBBResidualS<BatchF, SP, SP>{rs.f(), v, sv, S}, lognb, gate);
         apply_schur_batch(c, U, has_clover, sprec, tos.s, svec->s, tes.s, 0, &S->pause, S->active, d_b, d_T, d_Ti,
                           tile, d_uniform);
-        run_batch(c, OpBBOmega<SP, SP>{t, sv, S}, lognb, gate);
-        run_batch(c, OpBBUpdate<BatchF, SP, SP, SP, BatchF, BatchF>{xs.f(), p, sv, t, rs.f(), rhat->f(), S}, lognb,
-                  gate);
-        run_batch(c, OpBBDirection<SP, BatchF, SP>{p, rs.f(), v, S}, lognb, gate);
+        run_batch(c, OpBBOmega<SP, SP, BatchF>{t, sv, rhat->f(), S}, lognb, gate);
+        run_batch(c, OpBBUpdate<BatchF, SP, SP, SP, SP, BatchF, BatchF>{xs.f(), p, sv, t, v, rs.f(), what->f(), S},
+                  lognb, gate);
     }
     void step(BatchCGState *S)
     {
@@ -1608,12 +1634,7 @@ private:
     }
     void direction_rest(BatchCGState *S)  // the direction update the pause skipped, for slots without an update
     {
-        if (algo == ALGO_BICGSTAB) {
-            if (sprec == PREC_F)
-                run_batch(c, OpBBDirection<BatchF, BatchF, BatchF>{ps.f(), rs.f(), aps.f(), S}, xs.s.lognb);
-            else run_batch(c, OpBBDirection<BatchH, BatchF, BatchH>{ps.h(), rs.f(), aps.h(), S}, xs.s.lognb);
-            return;
-        }
+        if (algo == ALGO_BICGSTAB) return;  // the direction is updated in the same pass as x and r
         if (sprec == PREC_F) run_batch(c, OpBDirection<BatchF, BatchF>{ps.f(), rs.f(), S}, xs.s.lognb);
         else run_batch(c, OpBDirection<BatchH, BatchF>{ps.h(), rs.f(), S}, xs.s.lognb);
     }
@@ -1645,7 +1666,7 @@ int lym_context_create(const int dims[4], int rep, int device, lym_context **out
         CK(cudaSetDevice(device));
         CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
         c->partials = (double *)dev_alloc(c, (size_t)kBlasGridMax * kMaxRed * sizeof(double));
-        c->bpartials = (double *)dev_alloc(c, (size_t)kBlasGridMax * kMaxBatch * 4 * sizeof(double));
+        c->bpartials = (double *)dev_alloc(c, (size_t)kBlasGridMax * kMaxBatch * kBatchMaxRed * sizeof(double));
         c->nbr = (int *)dev_alloc(c, (size_t)16 * c->g.stride * sizeof(int));
         launch_nbr_table(c->g, c->nbr, c->st);
         c->counter = (unsigned int *)dev_alloc(c, 64);

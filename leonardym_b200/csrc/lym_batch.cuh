@@ -27,6 +27,7 @@
 namespace lym {
 
 constexpr int kMaxBatch = 32;
+constexpr int kBatchMaxRed = 8;  // FP64 reductions per RHS a batched vector kernel may carry
 
 // ------------------------------------------------------- pair arithmetic ---
 struct c2 {  // one complex component of the two RHS of a pair
@@ -135,6 +136,17 @@ struct BatchF {
         const unsigned b = at(0, h, q), s = (unsigned)stride << lognp;
 #pragma unroll
         for (int c = 0; c < 12; ++c) __stcs(v + b + c * s, make_float4(x[c].re.x, x[c].re.y, x[c].im.x, x[c].im.y));
+    }
+    // component c of both RHS of the pair in FP64 (vector algebra, one word at a time)
+    LYM_D void get(int h, int q, int c, cx<double> &a, cx<double> &b) const
+    {
+        const float4 w = __ldg(v + at(c, h, q));
+        a = cx<double>{(double)w.x, (double)w.z};
+        b = cx<double>{(double)w.y, (double)w.w};
+    }
+    LYM_D void put(int h, int q, int c, cx<double> a, cx<double> b) const
+    {
+        v[at(c, h, q)] = make_float4((float)a.re, (float)b.re, (float)a.im, (float)b.im);
     }
     // FP64 values of both RHS of the pair (vector algebra)
     LYM_D void load_d(int h, int q, cx<double> a[12], cx<double> b[12]) const
@@ -257,6 +269,15 @@ struct BatchH {
             hp[3] = __float22half2_rn(mul2(x[2 * w + 1].im, inv));
             v[b + w * s] = u;
         }
+    }
+    LYM_D void get(int h, int q, int c, cx<double> &a, cx<double> &b) const
+    {
+        const float2 n = __ldg(norm + ((unsigned)h << lognp) + q);
+        int4 u = __ldg(v + at(c >> 1, h, q));
+        const __half2 *hp = reinterpret_cast<const __half2 *>(&u);
+        const float2 re = mul2(__half22float2(hp[2 * (c & 1)]), n), im = mul2(__half22float2(hp[2 * (c & 1) + 1]), n);
+        a = cx<double>{(double)re.x, (double)im.x};
+        b = cx<double>{(double)re.y, (double)im.y};
     }
     LYM_D void load_d(int h, int q, cx<double> a[12], cx<double> b[12]) const
     {
@@ -823,6 +844,7 @@ template <class Op>
 __global__ void __launch_bounds__(kBlasThreads) site_batch_kernel(Op op, int vh, int lognp, double *partials,
                                                                   unsigned int *counter, Gate gate)
 {
+    static_assert(Op::NRED <= kBatchMaxRed, "partials hold kBatchMaxRed sums per (block, RHS)");
     if (gate.closed()) return;
     constexpr int NR = Op::NRED > 0 ? Op::NRED : 1;
     const int np = 1 << lognp, nb = 2 * np;
@@ -902,10 +924,12 @@ struct BatchCGState {
     int need_update[kMaxBatch];
     int its[kMaxBatch];        // iterations each slot took part in
     int failed;
-    double2 rho[kMaxBatch], omega[kMaxBatch];  // BiCGStab only
+    double2 rho[kMaxBatch], omega[kMaxBatch], bbeta[kMaxBatch];  // BiCGStab only
     int restart[kMaxBatch];                    // BiCGStab broke down: restart at the update
     int last_update_its[kMaxBatch];            // its at the last reliable update
 };
+
+LYM_D cx<double> as_cx2(double2 z) { return cx<double>{z.x, z.y}; }
 
 // a slot gets a reliable update at least every kForcedUpdateIts of its iterations, so a
 // stagnating recursion still reaches the host's progress check
@@ -925,6 +949,35 @@ LYM_D void batch_iteration_done(BatchCGState *s)
     if (s->iter >= s->max_iter || running == 0 || parked >= s->park_limit) s->pause = 1;
 }
 
+// Output of one pair, written one component at a time: FP32 words go out at once, FP16
+// words wait for the whole site (the per-site norm needs every component).
+template <class B> struct PairOut;
+template <> struct PairOut<BatchF> {
+    BatchF b;
+    int h, q;
+    LYM_D void put(int c, cx<double> x, cx<double> y) { b.put(h, q, c, x, y); }
+    LYM_D void finish() {}
+};
+template <> struct PairOut<BatchH> {
+    BatchH b;
+    int h, q;
+    c2 buf[12];
+    LYM_D void put(int c, cx<double> x, cx<double> y)
+    {
+        buf[c] = c2{make_float2((float)x.re, (float)y.re), make_float2((float)x.im, (float)y.im)};
+    }
+    LYM_D void finish() { b.store(h, q, buf); }
+};
+template <class B> LYM_D PairOut<B> pair_out(const B &b, int h, int q) { return PairOut<B>{b, h, q}; }
+
+// acc += conj(a) b (re, im) and |a|^2 helpers for single components
+LYM_D void dot1(cx<double> a, cx<double> b, double &re, double &im)
+{
+    re += a.re * b.re + a.im * b.im;
+    im += a.re * b.im - a.im * b.re;
+}
+LYM_D double nrm1(cx<double> a) { return a.re * a.re + a.im * a.im; }
+
 // alpha_r = rr_r / <p_r, A p_r>
 template <class SP, class SAp> struct OpBAlpha {
     static constexpr int NRED = 2;
@@ -935,11 +988,14 @@ template <class SP, class SAp> struct OpBAlpha {
     {
         const bool a0 = s->active[2 * q] != 0, a1 = s->active[2 * q + 1] != 0;
         if (!a0 && !a1) return;
-        cx<double> x0[12], x1[12], y0[12], y1[12];
-        p.load_d(h, q, x0, x1);
-        ap.load_d(h, q, y0, y1);
-        if (a0) dotc(x0, y0, acc[0], acc[1]);
-        if (a1) dotc(x1, y1, acc[2], acc[3]);
+#pragma unroll 2
+        for (int c = 0; c < 12; ++c) {
+            cx<double> x0, x1, y0, y1;
+            p.get(h, q, c, x0, x1);
+            ap.get(h, q, c, y0, y1);
+            if (a0) dot1(x0, y0, acc[0], acc[1]);
+            if (a1) dot1(x1, y1, acc[2], acc[3]);
+        }
     }
     LYM_D void finalize(int r, const double *t) const
     {
@@ -961,24 +1017,28 @@ template <class SX, class SP, class SR, class SAp> struct OpBUpdate {
     {
         const bool act[2] = {s->active[2 * q] != 0, s->active[2 * q + 1] != 0};
         if (!act[0] && !act[1]) return;
-        cx<double> xv[2][12], pv[2][12], res[2][12], av[2][12];
-        x.load_d(h, q, xv[0], xv[1]);
-        p.load_d(h, q, pv[0], pv[1]);
-        rv.load_d(h, q, res[0], res[1]);
-        ap.load_d(h, q, av[0], av[1]);
+        const cx<double> al[2] = {as_cx2(s->alpha[2 * q]), as_cx2(s->alpha[2 * q + 1])};
+        auto xo = pair_out(x, h, q);
+        auto ro = pair_out(rv, h, q);
+#pragma unroll 2
+        for (int c = 0; c < 12; ++c) {
+            cx<double> xv[2], pv[2], res[2], av[2];
+            x.get(h, q, c, xv[0], xv[1]);
+            p.get(h, q, c, pv[0], pv[1]);
+            rv.get(h, q, c, res[0], res[1]);
+            ap.get(h, q, c, av[0], av[1]);
 #pragma unroll
-        for (int l = 0; l < 2; ++l) {
-            if (!act[l]) continue;
-            const cx<double> al = {s->alpha[2 * q + l].x, s->alpha[2 * q + l].y};
-#pragma unroll
-            for (int k = 0; k < 12; ++k) {
-                fma_c(xv[l][k], al, pv[l][k]);
-                res[l][k] = res[l][k] - al * av[l][k];
+            for (int l = 0; l < 2; ++l) {
+                if (!act[l]) continue;
+                fma_c(xv[l], al[l], pv[l]);
+                res[l] = res[l] - al[l] * av[l];
+                acc[l] += nrm1(res[l]);
             }
-            acc[l] += norm2(res[l]);
+            xo.put(c, xv[0], xv[1]);
+            ro.put(c, res[0], res[1]);
         }
-        x.store_d(h, q, xv[0], xv[1]);
-        rv.store_d(h, q, res[0], res[1]);
+        xo.finish();
+        ro.finish();
     }
     LYM_D void finalize(int r, const double *t) const
     {
@@ -1016,17 +1076,19 @@ template <class SP, class SR> struct OpBDirection {
 #pragma unroll
         for (int l = 0; l < 2; ++l) go[l] = s->active[2 * q + l] && !s->need_update[2 * q + l];
         if (!go[0] && !go[1]) return;
-        cx<double> pv[2][12], res[2][12];
-        p.load_d(h, q, pv[0], pv[1]);
-        rv.load_d(h, q, res[0], res[1]);
+        const double b[2] = {s->beta[2 * q], s->beta[2 * q + 1]};
+        auto po = pair_out(p, h, q);
+#pragma unroll 2
+        for (int c = 0; c < 12; ++c) {
+            cx<double> pv[2], res[2];
+            p.get(h, q, c, pv[0], pv[1]);
+            rv.get(h, q, c, res[0], res[1]);
 #pragma unroll
-        for (int l = 0; l < 2; ++l) {
-            if (!go[l]) continue;
-            const double b = s->beta[2 * q + l];
-#pragma unroll
-            for (int k = 0; k < 12; ++k) pv[l][k] = res[l][k] + b * pv[l][k];
+            for (int l = 0; l < 2; ++l)
+                if (go[l]) pv[l] = res[l] + b[l] * pv[l];
+            po.put(c, pv[0], pv[1]);
         }
-        p.store_d(h, q, pv[0], pv[1]);
+        po.finish();
     }
     LYM_D void finalize(int, const double *) const {}
     LYM_D void finalize_all() const {}
@@ -1043,36 +1105,6 @@ template <class SP, class SR> struct OpBDirection {
 LYM_D double2 as_d2(cx<double> z) { return make_double2(z.re, z.im); }
 LYM_D cx<double> as_cx(double2 z) { return cx<double>{z.x, z.y}; }
 
-// alpha_r = rho_r / <rhat_r, v_r>
-template <class SRh, class SV> struct OpBBAlpha {
-    static constexpr int NRED = 2;
-    SRh rh;
-    SV v;
-    BatchCGState *s;
-    LYM_D void site(int h, int q, double *acc) const
-    {
-        const bool a0 = s->active[2 * q] != 0, a1 = s->active[2 * q + 1] != 0;
-        if (!a0 && !a1) return;
-        cx<double> x0[12], x1[12], y0[12], y1[12];
-        rh.load_d(h, q, x0, x1);
-        v.load_d(h, q, y0, y1);
-        if (a0) dotc(x0, y0, acc[0], acc[1]);
-        if (a1) dotc(x1, y1, acc[2], acc[3]);
-    }
-    LYM_D void finalize(int r, const double *t) const
-    {
-        if (!s->active[r]) return;
-        if (t[0] == 0.0 && t[1] == 0.0) {  // breakdown: restart from the true residual
-            s->need_update[r] = 1;
-            s->restart[r] = 1;
-            s->active[r] = 0;
-            return;
-        }
-        s->alpha[r] = cdiv(s->rho[r], make_double2(t[0], t[1]));
-    }
-    LYM_D void finalize_all() const {}
-};
-
 // s_r = r_r - alpha_r v_r
 template <class SR, class SV, class SS> struct OpBBResidualS {
     static constexpr int NRED = 0;
@@ -1084,107 +1116,133 @@ template <class SR, class SV, class SS> struct OpBBResidualS {
     {
         const bool act[2] = {s->active[2 * q] != 0, s->active[2 * q + 1] != 0};
         if (!act[0] && !act[1]) return;
-        cx<double> r[2][12], w[2][12];
-        rv.load_d(h, q, r[0], r[1]);
-        v.load_d(h, q, w[0], w[1]);
+        const cx<double> al[2] = {as_cx(s->alpha[2 * q]), as_cx(s->alpha[2 * q + 1])};
+        auto so = pair_out(sv, h, q);
+#pragma unroll 2
+        for (int c = 0; c < 12; ++c) {
+            cx<double> r[2], w[2];
+            rv.get(h, q, c, r[0], r[1]);
+            v.get(h, q, c, w[0], w[1]);
 #pragma unroll
-        for (int l = 0; l < 2; ++l) {
-            if (!act[l]) continue;
-            const cx<double> al = as_cx(s->alpha[2 * q + l]);
-#pragma unroll
-            for (int k = 0; k < 12; ++k) r[l][k] = r[l][k] - al * w[l][k];
+            for (int l = 0; l < 2; ++l)
+                if (act[l]) r[l] = r[l] - al[l] * w[l];
+            so.put(c, r[0], r[1]);
         }
-        sv.store_d(h, q, r[0], r[1]);
+        so.finish();
     }
     LYM_D void finalize(int, const double *) const {}
     LYM_D void finalize_all() const {}
 };
 
-// omega_r = <t_r, s_r> / |t_r|^2
-template <class ST, class SS> struct OpBBOmega {
-    static constexpr int NRED = 3;
+// omega_r = <t_r, s_r> / |t_r|^2;  rho'_r = <rhat_r, r'_r> = <rhat_r, s_r> - omega_r <rhat_r, t_r>;
+// beta_r = (rho'_r / rho_r) (alpha_r / omega_r).  A zero |t|^2 or rho' marks the slot for a
+// restart (the update parks it).
+template <class ST, class SS, class SRh> struct OpBBOmega {
+    static constexpr int NRED = 7;
     ST tv;
     SS sv;
-    BatchCGState *s;
-    LYM_D void site(int h, int q, double *acc) const
-    {
-        const bool a0 = s->active[2 * q] != 0, a1 = s->active[2 * q + 1] != 0;
-        if (!a0 && !a1) return;
-        cx<double> t0[12], t1[12], s0[12], s1[12];
-        tv.load_d(h, q, t0, t1);
-        sv.load_d(h, q, s0, s1);
-        if (a0) {
-            dotc(t0, s0, acc[0], acc[1]);
-            acc[2] += norm2(t0);
-        }
-        if (a1) {
-            dotc(t1, s1, acc[3], acc[4]);
-            acc[5] += norm2(t1);
-        }
-    }
-    LYM_D void finalize(int r, const double *t) const
-    {
-        if (!s->active[r]) return;
-        if (t[2] == 0.0) {  // s = 0: alpha p already solved this RHS; the update decides
-            s->omega[r] = make_double2(0.0, 0.0);
-            return;
-        }
-        s->omega[r] = make_double2(t[0] / t[2], t[1] / t[2]);
-    }
-    LYM_D void finalize_all() const {}
-};
-
-// x_r += alpha_r p_r + omega_r s_r, r_r = s_r - omega_r t_r, rho' = <rhat_r, r_r>,
-// |r_r|^2, and the convergence / reliable-update decisions
-template <class SX, class SP, class SS, class ST, class SR, class SRh> struct OpBBUpdate {
-    static constexpr int NRED = 3;
-    SX x;
-    SP p;
-    SS sv;
-    ST tv;
-    SR rv;
     SRh rh;
     BatchCGState *s;
     LYM_D void site(int h, int q, double *acc) const
     {
         const bool act[2] = {s->active[2 * q] != 0, s->active[2 * q + 1] != 0};
         if (!act[0] && !act[1]) return;
-        cx<double> xv[2][12], pv[2][12], sw[2][12], tw[2][12], rr[2][12], hv[2][12];
-        x.load_d(h, q, xv[0], xv[1]);
-        p.load_d(h, q, pv[0], pv[1]);
-        sv.load_d(h, q, sw[0], sw[1]);
-        tv.load_d(h, q, tw[0], tw[1]);
-        if (!act[0] || !act[1]) rv.load_d(h, q, rr[0], rr[1]);  // an idle lane keeps its residual
-        rh.load_d(h, q, hv[0], hv[1]);
+#pragma unroll 2
+        for (int c = 0; c < 12; ++c) {
+            cx<double> t[2], sw[2], hv[2];
+            tv.get(h, q, c, t[0], t[1]);
+            sv.get(h, q, c, sw[0], sw[1]);
+            rh.get(h, q, c, hv[0], hv[1]);
+#pragma unroll
+            for (int l = 0; l < 2; ++l) {
+                if (!act[l]) continue;
+                double *a = acc + 7 * l;
+                dot1(t[l], sw[l], a[0], a[1]);
+                a[2] += nrm1(t[l]);
+                dot1(hv[l], sw[l], a[3], a[4]);
+                dot1(hv[l], t[l], a[5], a[6]);
+            }
+        }
+    }
+    LYM_D void finalize(int r, const double *t) const
+    {
+        if (!s->active[r]) return;
+        const double2 om = t[2] > 0.0 ? make_double2(t[0] / t[2], t[1] / t[2]) : make_double2(0.0, 0.0);
+        const double2 rho_new = csub(make_double2(t[3], t[4]), cmul(om, make_double2(t[5], t[6])));
+        const bool stalled = (om.x == 0.0 && om.y == 0.0) || (rho_new.x == 0.0 && rho_new.y == 0.0);
+        s->omega[r] = om;
+        s->bbeta[r] = stalled ? make_double2(0.0, 0.0) : cmul(cdiv(rho_new, s->rho[r]), cdiv(s->alpha[r], om));
+        s->rho[r] = rho_new;
+        if (stalled) s->restart[r] = 1;
+    }
+    LYM_D void finalize_all() const {}
+};
+
+// x_r += alpha_r p_r + omega_r s_r;  r_r = s_r - omega_r t_r;  p_r = r_r + beta_r (p_r - omega_r v_r);
+// |r_r|^2 and <what_r, p_r> (what = S^+ rhat, so that <rhat, S p> of the next iteration is
+// known now: alpha_r = rho_r / <what_r, p_r>), and the convergence / reliable-update decisions
+template <class SX, class SP, class SS, class ST, class SV, class SR, class SW> struct OpBBUpdate {
+    static constexpr int NRED = 3;
+    SX x;
+    SP p;
+    SS sv;
+    ST tv;
+    SV v;
+    SR rv;
+    SW wh;
+    BatchCGState *s;
+    LYM_D void site(int h, int q, double *acc) const
+    {
+        const bool act[2] = {s->active[2 * q] != 0, s->active[2 * q + 1] != 0};
+        if (!act[0] && !act[1]) return;
+        const bool idle = !act[0] || !act[1];
+        cx<double> al[2], om[2], be[2];
 #pragma unroll
         for (int l = 0; l < 2; ++l) {
-            if (!act[l]) continue;
-            const cx<double> al = as_cx(s->alpha[2 * q + l]), om = as_cx(s->omega[2 * q + l]);
-#pragma unroll
-            for (int k = 0; k < 12; ++k) {
-                fma_c(xv[l][k], al, pv[l][k]);
-                fma_c(xv[l][k], om, sw[l][k]);
-                rr[l][k] = sw[l][k] - om * tw[l][k];
-            }
-            dotc(hv[l], rr[l], acc[3 * l], acc[3 * l + 1]);
-            acc[3 * l + 2] += norm2(rr[l]);
+            al[l] = as_cx(s->alpha[2 * q + l]);
+            om[l] = as_cx(s->omega[2 * q + l]);
+            be[l] = as_cx(s->bbeta[2 * q + l]);
         }
-        x.store_d(h, q, xv[0], xv[1]);
-        rv.store_d(h, q, rr[0], rr[1]);
+        auto xo = pair_out(x, h, q);
+        auto ro = pair_out(rv, h, q);
+        auto po = pair_out(p, h, q);
+#pragma unroll 2
+        for (int c = 0; c < 12; ++c) {
+            cx<double> xv[2], pv[2], sw[2], tw[2], vv[2], rr[2], ww[2];
+            x.get(h, q, c, xv[0], xv[1]);
+            p.get(h, q, c, pv[0], pv[1]);
+            sv.get(h, q, c, sw[0], sw[1]);
+            tv.get(h, q, c, tw[0], tw[1]);
+            v.get(h, q, c, vv[0], vv[1]);
+            wh.get(h, q, c, ww[0], ww[1]);
+            if (idle) rv.get(h, q, c, rr[0], rr[1]);  // an idle lane keeps its residual
+#pragma unroll
+            for (int l = 0; l < 2; ++l) {
+                if (!act[l]) continue;
+                fma_c(xv[l], al[l], pv[l]);
+                fma_c(xv[l], om[l], sw[l]);
+                rr[l] = sw[l] - om[l] * tw[l];
+                pv[l] = rr[l] + be[l] * (pv[l] - om[l] * vv[l]);
+                acc[3 * l] += nrm1(rr[l]);
+                dot1(ww[l], pv[l], acc[3 * l + 1], acc[3 * l + 2]);
+            }
+            xo.put(c, xv[0], xv[1]);
+            ro.put(c, rr[0], rr[1]);
+            po.put(c, pv[0], pv[1]);
+        }
+        xo.finish();
+        ro.finish();
+        po.finish();
     }
     LYM_D void finalize(int r, const double *t) const
     {
         if (!s->active[r]) return;
         s->its[r] += 1;
-        const double rr_new = t[2];
-        const double2 rho_new = make_double2(t[0], t[1]);
-        const double2 om = s->omega[r];
+        const double rr_new = t[0];
         s->rr_prev[r] = s->rr[r];
         s->rr[r] = rr_new;
         if (rr_new > s->rr_max[r]) s->rr_max[r] = rr_new;
-        const bool stalled = (om.x == 0.0 && om.y == 0.0) || (rho_new.x == 0.0 && rho_new.y == 0.0);
-        if (!stalled) s->alpha[r] = cmul(cdiv(rho_new, s->rho[r]), cdiv(s->alpha[r], om));  // beta, kept in alpha
-        s->rho[r] = rho_new;
+        const bool breakdown = t[1] == 0.0 && t[2] == 0.0;
         if (!(rr_new == rr_new)) {
             s->failed = 1;
             s->pause = 1;
@@ -1192,44 +1250,16 @@ template <class SX, class SP, class SS, class ST, class SR, class SRh> struct Op
             s->converged[r] = 1;
             s->need_update[r] = 1;
             s->active[r] = 0;
-        } else if (stalled || rr_new < s->delta2 * s->rr_max[r] ||
+        } else if (s->restart[r] || breakdown || rr_new < s->delta2 * s->rr_max[r] ||
                    s->its[r] - s->last_update_its[r] >= kForcedUpdateIts) {
+            if (breakdown) s->restart[r] = 1;
             s->need_update[r] = 1;
-            s->restart[r] = stalled;
             s->active[r] = 0;
+        } else {
+            s->alpha[r] = cdiv(s->rho[r], make_double2(t[1], t[2]));
         }
     }
     LYM_D void finalize_all() const { batch_iteration_done(s); }
-};
-
-// p_r = r_r + beta_r (p_r - omega_r v_r) for the running RHS (beta is in alpha)
-template <class SP, class SR, class SV> struct OpBBDirection {
-    static constexpr int NRED = 0;
-    SP p;
-    SR rv;
-    SV v;
-    BatchCGState *s;
-    LYM_D void site(int h, int q, double *) const
-    {
-        bool go[2];
-#pragma unroll
-        for (int l = 0; l < 2; ++l) go[l] = s->active[2 * q + l] && !s->need_update[2 * q + l];
-        if (!go[0] && !go[1]) return;
-        cx<double> pv[2][12], rr[2][12], w[2][12];
-        p.load_d(h, q, pv[0], pv[1]);
-        rv.load_d(h, q, rr[0], rr[1]);
-        v.load_d(h, q, w[0], w[1]);
-#pragma unroll
-        for (int l = 0; l < 2; ++l) {
-            if (!go[l]) continue;
-            const cx<double> be = as_cx(s->alpha[2 * q + l]), om = as_cx(s->omega[2 * q + l]);
-#pragma unroll
-            for (int k = 0; k < 12; ++k) pv[l][k] = rr[l][k] + be * (pv[l][k] - om * w[l][k]);
-        }
-        p.store_d(h, q, pv[0], pv[1]);
-    }
-    LYM_D void finalize(int, const double *) const {}
-    LYM_D void finalize_all() const {}
 };
 
 }  // namespace lym
