@@ -86,7 +86,7 @@ SERVE_EPS = {"su3": 0.25, "su2adj": 0.3}
 SERVE_POOL = 4  # distinct sources per field (reused across requests; every request gets its own solutions)
 
 
-def run_serving(window_s, batch=16, precision="single"):
+def run_serving(window_s, batch=16, precision="single", solver="bicgstab"):
     """Open-loop serving measurement: requests arrive for window_s seconds at Poisson times
     (seeded) and are submitted to the solve server as they arrive; the result is the
     completed sources per second over the whole run, per-request latency p50 / p99 (submit
@@ -95,7 +95,7 @@ def run_serving(window_s, batch=16, precision="single"):
     from leonardym_b200.server import SolveServer
     rng = np.random.default_rng(SEED + 7)
     fields = [(dims, rep) for dims in SERVE_VOLUMES for rep in ("su3", "su2adj")]
-    srv = SolveServer(batch=batch, precision=precision)
+    srv = SolveServer(batch=batch, precision=precision, solver=solver)
     pools = {}
     try:
         for key, (dims, rep) in enumerate(fields):
@@ -136,7 +136,7 @@ def run_serving(window_s, batch=16, precision="single"):
             "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
             "max_true_residual": worst, "failed_requests": failed,
             "fields": [f"{'x'.join(map(str, d))} {r}" for d, r in fields],
-            "solver": f"block even-odd CG, {batch} slots per field, {precision} storage, continuous batching"}
+            "solver": f"{SOLVER_NAMES[solver]}, {batch} slots per field, {precision} storage, continuous batching"}
 
 
 class ClockSampler:
@@ -475,7 +475,7 @@ def run_ours(args, world, rank, local):
     lat.close()
     serving = None
     if rank == 0 and args.serve_window > 0:  # after the timed region: its own clock
-        serving = run_serving(args.serve_window, batch=args.batch, precision=args.precision)
+        serving = run_serving(args.serve_window, batch=args.batch, precision=args.precision, solver=args.solver)
     if rank != 0:
         return
     line = {

@@ -208,7 +208,10 @@ int lym_multishift_device(lym_context *ctx, int op_id, int algorithm, int nshift
  * Keeps gauge fields resident by key (one context, CUDA stream and worker thread per
  * field, so work on different fields overlaps on the device) and serves solve requests
  * D x_k = b_k (an Improved operator: kappa, c_sw; 1..n sources; relative tolerance on the
- * true residual) with the block mixed-precision even-odd CG.  Sources of all requests on a
+ * true residual) with the block mixed-precision even-odd solvers: `solver` is
+ * LYM_SOLVER_EO_CG_MIXED_SINGLE / _HALF or LYM_SOLVER_EO_BICGSTAB_MIXED_SINGLE / _HALF (1 and 2
+ * are accepted for the two CG solvers; with BiCGStab, a source on which it breaks down is
+ * solved again with CG on the same lane).  Sources of all requests on a
  * field are continuously batched: they enter free slots of the running batch as earlier
  * ones finish, whatever their kappa.  A request's clover term is built when its first
  * source is admitted and freed with its last; a new clover term is admitted only while
@@ -224,7 +227,7 @@ typedef struct {
     int converged;
     int status;                /* lym_status of the request                         */
 } lym_request_stats;
-int lym_server_create(int device, size_t hbm_budget_bytes, int batch, int precision, lym_server **server);
+int lym_server_create(int device, size_t hbm_budget_bytes, int batch, int solver, lym_server **server);
 void lym_server_destroy(lym_server *server);
 const char *lym_server_last_error(lym_server *server);
 size_t lym_server_device_bytes(lym_server *server);

@@ -1456,7 +1456,7 @@ private:
     void reliable_update_bicg(int j)
     {
         Slot &s = slot[j];
-        axpby_views(c, xs.f().slot(j), s.X.parity(1).d(), C2(1.0), C2(1.0));
+        if (hs.restart[j] != 2) axpby_views(c, xs.f().slot(j), s.X.parity(1).d(), C2(1.0), C2(1.0));
         axpby_views(c, xs.f().slot(j), xs.f().slot(j), C2(0.0), C2(0.0));
         double rrS;
         true_res_S(j, rrS);

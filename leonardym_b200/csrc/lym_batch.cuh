@@ -926,6 +926,7 @@ struct BatchCGState {
     int failed;
     double2 rho[kMaxBatch], omega[kMaxBatch], bbeta[kMaxBatch];  // BiCGStab only
     int restart[kMaxBatch];                    // BiCGStab broke down: restart at the update
+                                               // (2: non-finite, drop the FP32 accumulator)
     int last_update_its[kMaxBatch];            // its at the last reliable update
 };
 
@@ -1243,9 +1244,10 @@ template <class SX, class SP, class SS, class ST, class SV, class SR, class SW> 
         s->rr[r] = rr_new;
         if (rr_new > s->rr_max[r]) s->rr_max[r] = rr_new;
         const bool breakdown = t[1] == 0.0 && t[2] == 0.0;
-        if (!(rr_new == rr_new)) {
-            s->failed = 1;
-            s->pause = 1;
+        if (!(rr_new <= 1e300)) {  // non-finite: the recursion broke down on this RHS; its FP32
+            s->restart[r] = 2;     // accumulator is discarded and it restarts from its FP64 x
+            s->need_update[r] = 1;
+            s->active[r] = 0;
         } else if (rr_new < s->eps[r]) {
             s->converged[r] = 1;
             s->need_update[r] = 1;

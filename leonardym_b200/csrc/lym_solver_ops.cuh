@@ -82,12 +82,16 @@ template <class SX, class SY> struct OpAxpby {
     double2 a, b;
     LYM_D void site(int p, int h, double *) const
     {
+        // a term with a zero coefficient is not read: y = a x overwrites y whatever it held
+        const bool use_x = a.x != 0.0 || a.y != 0.0, use_y = b.x != 0.0 || b.y != 0.0;
         cx<double> u[12], v[12];
-        x.par(p).template load<double>(h, u);
-        y.par(p).template load<double>(h, v);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) u[k] = v[k] = cx<double>{0.0, 0.0};
+        if (use_x) x.par(p).template load<double>(h, u);
+        if (use_y) y.par(p).template load<double>(h, v);
         const cx<double> A = {a.x, a.y}, B = {b.x, b.y};
 #pragma unroll
-        for (int k = 0; k < 12; ++k) v[k] = A * u[k] + B * v[k];
+        for (int k = 0; k < 12; ++k) v[k] = (use_x ? A * u[k] : cx<double>{0.0, 0.0}) + (use_y ? B * v[k] : cx<double>{0.0, 0.0});
         y.par(p).template store<double>(h, v);
     }
     LYM_D void finalize(const double *) const {}

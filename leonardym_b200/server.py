@@ -41,14 +41,18 @@ def _bind():
 class SolveServer:
     """Serves D x = b requests for Wilson-clover operators on resident gauge fields.
 
-    ``precision`` is the inner storage ("single" or "half"); ``batch`` the number of
-    slots of each field's batched CG; ``hbm_budget`` caps the server's device bytes."""
+    ``precision`` is the inner storage ("single" or "half"); ``solver`` "cg" (CG on
+    (gamma5 S)^2) or "bicgstab" (BiCGStab on S, falling back to CG for a source it breaks
+    down on); ``batch`` the number of slots of each field's batched solver; ``hbm_budget``
+    caps the server's device bytes."""
 
-    def __init__(self, device=0, hbm_budget=0, batch=16, precision="single"):
+    SOLVERS = {("cg", "single"): 4, ("cg", "half"): 5, ("bicgstab", "single"): 6, ("bicgstab", "half"): 7}
+
+    def __init__(self, device=0, hbm_budget=0, batch=16, precision="single", solver="cg"):
         self._L = _bind()
         self._ptr = C.c_void_p()
-        prec = {"single": 1, "half": 2}[precision]
-        rc = self._L.lym_server_create(int(device), int(hbm_budget), int(batch), prec, C.byref(self._ptr))
+        code = self.SOLVERS[(solver, precision)]
+        rc = self._L.lym_server_create(int(device), int(hbm_budget), int(batch), code, C.byref(self._ptr))
         if rc != 0:
             raise LymError(rc, "lym_server_create failed")
         self._keep = {}

@@ -37,9 +37,10 @@ def links():
     return {key: synth.fermion_links(d, rep, eps, seed) for key, (d, rep, eps, seed) in FIELDS.items()}
 
 
-@pytest.mark.parametrize("precision,batch", [("single", 4), ("half", 8)])
-def test_server_mix_equals_alone(links, precision, batch, oracle):
-    srv = SolveServer(batch=batch, precision=precision)
+@pytest.mark.parametrize("precision,batch,solver", [("single", 4, "cg"), ("half", 8, "cg"),
+                                                   ("single", 4, "bicgstab"), ("half", 8, "bicgstab")])
+def test_server_mix_equals_alone(links, precision, batch, solver, oracle):
+    srv = SolveServer(batch=batch, precision=precision, solver=solver)
     try:
         for key, (dims, rep, _, _) in FIELDS.items():
             srv.add_gauge(key, dims, rep, links[key])
