@@ -80,7 +80,11 @@ enum lym_solver {
 enum lym_multishift_solver {
     LYM_MULTISHIFT_ME = 0,    /* "mass_estrapolation": MEMultishiftSolver (inverters/MEMultishiftSolver.cpp:10-143) */
     LYM_MULTISHIFT_MMMR = 1,  /* "minimal_residual": MMMRMultishiftSolver (inverters/MMMRMultishiftSolver.cpp:42-198) */
-    LYM_MULTISHIFT_CG = 2     /* multishift CG (no reference counterpart; a new MultishiftSolver subclass) */
+    LYM_MULTISHIFT_CG = 2,    /* multishift CG (no reference counterpart; a new MultishiftSolver subclass) */
+    /* "chronological_mass_estrapolation": ChronologicalMultishiftSolver
+     * (inverters/ChronologicalMultishiftSolver.cpp:11-194); solutions[i], i >= 1, hold the
+     * chronological guess of shift i on entry (zeros for none) */
+    LYM_MULTISHIFT_CHRONOLOGICAL = 3
 };
 
 typedef struct {
@@ -177,6 +181,17 @@ int lym_solve_device(lym_context *ctx, int op_id, int solver, double precision, 
  * (BiConjugateGradient.cpp:510-690) */
 int lym_solve_shifted(lym_context *ctx, int op_id, double shift_re, double shift_im, double precision, int max_steps,
                       const double *source, double *solution, const double *guess, lym_solve_stats *stats);
+/* BiCGStab(l): BiConjugateGradient::solve(dirac, source, solution, int l, guess)
+ * (inverters/BiConjugateGradient.cpp:130-317), FP64, 1 <= l <= 16 */
+int lym_solve_bicgstab_l(lym_context *ctx, int op_id, int l, double precision, int max_steps, const double *source,
+                         double *solution, const double *guess, lym_solve_stats *stats);
+/* BiCGStab with a preconditioner operator: BiConjugateGradient::solve(dirac, source,
+ * solution, preconditioner, guess) (inverters/BiConjugateGradient.cpp:11-128), FP64, with the
+ * reference's steps as they are (t = A s, convergence only after step 5: its result solves
+ * A x = b only where the preconditioner commutes with that choice, e.g. P = 1) */
+int lym_solve_preconditioned(lym_context *ctx, int op_id, int preconditioner_op_id, double precision,
+                             int max_steps, const double *source, double *solution, const double *guess,
+                             lym_solve_stats *stats);
 
 /* ---- many right-hand sides (no reference counterpart: the reference solves point and
  * noise sources one by one, correlators/MesonCorrelator.cpp:92-98,

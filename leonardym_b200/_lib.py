@@ -88,6 +88,8 @@ def lib():
         "lym_solve": (i, [vp, i, i, dp, i, vp, vp, vp, sp]),
         "lym_solve_device": (i, [vp, i, i, dp, i, vp, vp, vp, sp]),
         "lym_solve_shifted": (i, [vp, i, dp, dp, dp, i, vp, vp, vp, sp]),
+        "lym_solve_bicgstab_l": (i, [vp, i, i, dp, i, vp, vp, vp, sp]),
+        "lym_solve_preconditioned": (i, [vp, i, i, dp, i, vp, vp, vp, sp]),
         "lym_solve_block": (i, [vp, i, i, dp, i, i, C.POINTER(vp), C.POINTER(vp), i, sp]),
         "lym_solve_block_device": (i, [vp, i, i, dp, i, i, C.POINTER(vp), C.POINTER(vp), i, sp]),
         "lym_multishift": (i, [vp, i, i, i, vp, dp, i, vp, C.POINTER(vp), sp]),

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <complex>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -554,6 +555,38 @@ int cg_solve(lym_context *c, MatVec matvec, int nparity, const Spinor &b, const 
     return R.converged ? LYM_OK : LYM_NOT_CONVERGED;
 }
 
+// Start vector of the reference's BiCGStab variants: the guess, else the source when its
+// squared norm exceeds the precision, else a uniform random vector (BiConjugateGradient.cpp
+// :333-340).  The reference seeds that vector from the clock (AlgebraUtils.h:123-167); a
+// fixed deterministic stream is used instead.
+void reference_start(lym_context *c, const Spinor &b, const Spinor &x, const Spinor *guess, double precision,
+                     double norm_offset, int nparity)
+{
+    if (guess) {
+        copy(c, x, *guess);
+        return;
+    }
+    const double ns = norm2_now(c, b) + norm_offset;
+    if (ns > precision) {
+        copy(c, x, b);
+        return;
+    }
+    std::vector<double> host((size_t)c->g.V * 24);
+    unsigned long long z = 0x9E3779B97F4A7C15ull;
+    for (auto &v : host) {
+        z += 0x9E3779B97F4A7C15ull;
+        unsigned long long q = z;
+        q = (q ^ (q >> 30)) * 0xBF58476D1CE4E5B9ull;
+        q = (q ^ (q >> 27)) * 0x94D049BB133111EBull;
+        q ^= q >> 31;
+        v = (double)(q >> 11) * (1.0 / 9007199254740992.0);
+    }
+    Vec full(c, PREC_D, 2);
+    upload_vec(c, *full, host.data(), false, 2);
+    CK(cudaStreamSynchronize(c->st));
+    copy(c, x, nparity == 2 ? *full : full.par(1));
+}
+
 // --- BiCGStab (BiConjugateGradient::solve, BiConjugateGradient.cpp:321-507) ---
 template <class MatVec>
 int bicgstab_solve(lym_context *c, MatVec matvec, int nparity, const Spinor &b, const Spinor &x,
@@ -561,31 +594,7 @@ int bicgstab_solve(lym_context *c, MatVec matvec, int nparity, const Spinor &b, 
 {
     Vec r(c, PREC_D, nparity), rhat(c, PREC_D, nparity), p(c, PREC_D, nparity), nu(c, PREC_D, nparity),
         s(c, PREC_D, nparity), t(c, PREC_D, nparity);
-    if (guess) {
-        copy(c, x, *guess);
-    } else {
-        const double ns = norm2_now(c, b) + norm_offset;
-        if (ns > precision) {
-            copy(c, x, b);
-        } else {
-            // the reference draws a time-seeded uniform random start here (AlgebraUtils.h:123-167);
-            // a fixed deterministic start is used instead
-            std::vector<double> host((size_t)c->g.V * 24);
-            unsigned long long z = 0x9E3779B97F4A7C15ull;
-            for (auto &v : host) {
-                z += 0x9E3779B97F4A7C15ull;
-                unsigned long long q = z;
-                q = (q ^ (q >> 30)) * 0xBF58476D1CE4E5B9ull;
-                q = (q ^ (q >> 27)) * 0x94D049BB133111EBull;
-                q ^= q >> 31;
-                v = (double)(q >> 11) * (1.0 / 9007199254740992.0);
-            }
-            Vec full(c, PREC_D, 2);
-            upload_vec(c, *full, host.data(), false, 2);
-            CK(cudaStreamSynchronize(c->st));
-            copy(c, x, nparity == 2 ? *full : full.par(1));
-        }
-    }
+    reference_start(c, b, x, guess, precision, norm_offset, nparity);
     matvec(*p, x, nullptr);
     // r = b - A x ; rhat = b + A x
     copy(c, *r, b);
@@ -1169,6 +1178,225 @@ struct SlotTables {
     SlotTables &operator=(const SlotTables &) = delete;
 };
 
+// ----------------------------------------- reference solver variants (FP64) --
+double2 dot_now(lym_context *c, const Spinor &a, const Spinor &b)
+{
+    run_site(c, OpDot<SpinorD, SpinorD>{a.d(), b.d(), c->d_scal}, a.nparity);
+    CK(cudaMemcpyAsync(c->h_scal, c->d_scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return make_double2(c->h_scal[0], c->h_scal[1]);
+}
+typedef std::complex<double> zc;
+inline zc zc_of(double2 v) { return zc(v.x, v.y); }
+inline double2 d2_of(zc v) { return make_double2(v.real(), v.imag()); }
+
+// BiCGStab(l): BiConjugateGradient::solve(dirac, source, solution, int l, guess)
+// (inverters/BiConjugateGradient.cpp:130-317), step for step: the l BiCG steps, then the
+// minimal-residual polynomial update (tau, sigma, gamma, gamma', gamma'').
+int bicgstab_l_solve(lym_context *c, OpEntry &op, int l, const Spinor &b, const Spinor &x, const Spinor *guess,
+                     double precision, int max_steps, lym_solve_stats *st)
+{
+    auto A = [&](const Spinor &out, const Spinor &in) { op_apply(c, op, PREC_D, out, in, nullptr, C2(0.0)); };
+    std::vector<std::unique_ptr<Vec>> u, r;
+    for (int j = 0; j <= l; ++j) {
+        u.emplace_back(new Vec(c, PREC_D, 2));
+        r.emplace_back(new Vec(c, PREC_D, 2));
+    }
+    Vec rh(c, PREC_D, 2), tmp(c, PREC_D, 2);
+    reference_start(c, b, x, guess, precision, 0.0, 2);
+    A(*tmp, x);
+    copy(c, **r[0], b);
+    axpby(c, *tmp, **r[0], C2(-1.0), C2(1.0));
+    copy(c, *rh, b);
+    axpby(c, *tmp, *rh, C2(1.0), C2(1.0));
+    zero(c, **u[0]);
+    zc rho0 = 1.0, alpha = 0.0, omega = 1.0;
+    std::vector<zc> tau((l + 1) * (l + 1)), sigma(l + 1), gam(l + 1), gp(l + 1), gpp(l + 1);
+    auto T = [&](int i, int j) -> zc & { return tau[i * (l + 1) + j]; };
+    int step = 0;
+    bool ok = false;
+    double last = 0.0;
+    while (step < max_steps) {
+        rho0 = -omega * rho0;
+        for (int j = 0; j < l; ++j) {
+            const zc rho1 = zc_of(dot_now(c, **r[j], *rh));
+            const zc beta = (rho1 / rho0) * alpha;
+            rho0 = rho1;
+            for (int i = 0; i <= j; ++i) axpby(c, **r[i], **u[i], C2(1.0), d2_of(-beta));
+            A(**u[j + 1], **u[j]);
+            alpha = rho0 / zc_of(dot_now(c, **u[j + 1], *rh));
+            for (int i = 0; i <= j; ++i) axpby(c, **u[i + 1], **r[i], d2_of(-alpha), C2(1.0));
+            A(**r[j + 1], **r[j]);
+            axpby(c, **u[0], x, d2_of(alpha), C2(1.0));
+        }
+        for (int j = 1; j <= l; ++j) {
+            for (int i = 1; i < j; ++i) {
+                T(i, j) = zc_of(dot_now(c, **r[j], **r[i])) / sigma[i];
+                axpby(c, **r[i], **r[j], d2_of(-T(i, j)), C2(1.0));
+            }
+            sigma[j] = zc_of(dot_now(c, **r[j], **r[j]));
+            gp[j] = zc_of(dot_now(c, **r[0], **r[j])) / sigma[j];
+        }
+        gam[l] = gp[l];
+        omega = gam[l];
+        for (int j = l - 1; j > 0; --j) {
+            zc t = 0.0;
+            for (int i = j + 1; i <= l; ++i) t += T(j, i) * gam[i];
+            gam[j] = gp[j] - t;
+        }
+        for (int j = 1; j < l; ++j) {
+            zc t = 0.0;
+            for (int i = j + 1; i < l; ++i) t += T(j, i) * gam[i + 1];
+            gpp[j] = gam[j + 1] + t;
+        }
+        axpby(c, **r[0], x, d2_of(gam[1]), C2(1.0));
+        axpby(c, **r[l], **r[0], d2_of(-gp[l]), C2(1.0));
+        axpby(c, **u[l], **u[0], d2_of(-gam[l]), C2(1.0));
+        for (int j = 1; j < l; ++j) {
+            axpby(c, **u[j], **u[0], d2_of(-gam[j]), C2(1.0));
+            axpby(c, **r[j], x, d2_of(gpp[j]), C2(1.0));
+            axpby(c, **r[j], **r[0], d2_of(-gp[j]), C2(1.0));
+        }
+        last = norm2_now(c, **r[0]);
+        if (last < precision) {
+            ok = true;
+            break;
+        }
+        if (!(last == last)) break;  // diverged to non-finite values
+        ++step;
+    }
+    if (st) {
+        st->iterations = ok ? step + 1 : step;
+        st->steps = ok ? step : max_steps;
+        st->converged = ok;
+        st->last_error = last;
+    }
+    return ok ? LYM_OK : LYM_NOT_CONVERGED;
+}
+
+// BiCGStab with a preconditioner operator P: BiConjugateGradient::solve(dirac, source,
+// solution, preconditioner, guess) (inverters/BiConjugateGradient.cpp:11-128), step for
+// step, including its t = A s (not A P s) and its convergence test only after step 5.
+int bicgstab_precond_solve(lym_context *c, OpEntry &op, OpEntry &pre, const Spinor &b, const Spinor &x,
+                           const Spinor *guess, double precision, int max_steps, lym_solve_stats *st)
+{
+    auto A = [&](const Spinor &out, const Spinor &in) { op_apply(c, op, PREC_D, out, in, nullptr, C2(0.0)); };
+    auto P = [&](const Spinor &out, const Spinor &in) { op_apply(c, pre, PREC_D, out, in, nullptr, C2(0.0)); };
+    Vec r(c, PREC_D, 2), rh(c, PREC_D, 2), p(c, PREC_D, 2), nu(c, PREC_D, 2), s(c, PREC_D, 2), t(c, PREC_D, 2),
+        pt(c, PREC_D, 2), sts(c, PREC_D, 2);
+    reference_start(c, b, x, guess, precision, 0.0, 2);
+    A(*p, x);
+    copy(c, *r, b);
+    axpby(c, *p, *r, C2(-1.0), C2(1.0));
+    copy(c, *rh, b);
+    axpby(c, *p, *rh, C2(1.0), C2(1.0));
+    zc rho_prev = 0.0, alpha = 0.0, omega = 0.0;
+    int step = 0, rc = LYM_NOT_CONVERGED;
+    double last = 0.0;
+    while (step < max_steps) {
+        const zc rho = zc_of(dot_now(c, *rh, *r));
+        if (std::norm(rho) == 0.0) {
+            rc = LYM_ERR_BREAKDOWN;
+            break;
+        }
+        if (step == 0) {
+            copy(c, *p, *r);
+        } else {
+            const zc beta = (rho / rho_prev) * (alpha / omega);
+            axpby(c, *nu, *p, d2_of(-omega), C2(1.0));
+            axpby(c, *r, *p, C2(1.0), d2_of(beta));
+        }
+        P(*pt, *p);
+        A(*nu, *pt);
+        alpha = rho / zc_of(dot_now(c, *rh, *nu));
+        copy(c, *s, *r);
+        axpby(c, *nu, *s, d2_of(-alpha), C2(1.0));
+        P(*sts, *s);
+        A(*t, *s);
+        omega = zc_of(dot_now(c, *t, *s)) / norm2_now(c, *t);
+        axpby(c, *pt, x, d2_of(alpha), C2(1.0));
+        axpby(c, *sts, x, d2_of(omega), C2(1.0));
+        copy(c, *r, *s);
+        axpby(c, *t, *r, d2_of(-omega), C2(1.0));
+        const double norm = norm2_now(c, *r);
+        if (norm < precision && step > 5) {
+            rc = LYM_OK;
+            last = norm;
+            break;
+        }
+        rho_prev = rho;
+        last = norm;
+        ++step;
+    }
+    if (st) {
+        st->iterations = rc == LYM_OK ? step + 1 : step;
+        st->steps = rc == LYM_OK ? step : max_steps;
+        st->converged = rc == LYM_OK;
+        st->last_error = last;
+    }
+    return rc;
+}
+
+// Chronological multishift: ChronologicalMultishiftSolver::solve
+// (inverters/ChronologicalMultishiftSolver.cpp:11-194).  Shift 0 by CG from zero; shift k
+// by CG from c1 x_{k-1} + c2 h_k, the combination minimising |(A + s_k)(.) - b| in the
+// reference's closed form, where h_k (the chronological guess) is what xs[k] holds on
+// entry.  A singular 2x2 system (h_k = 0 or parallel) takes c2 = 0 and the one-vector
+// minimiser for c1.
+int multishift_chrono(lym_context *c, OpEntry &op, int nshift, const double *shifts, double eps, int max_steps,
+                      const Spinor &b, const std::vector<Spinor> &xs, lym_solve_stats *st)
+{
+    Vec pA(c, PREC_D, 2), hA(c, PREC_D, 2), g(c, PREC_D, 2);
+    int total = 0;
+    bool ok = true;
+    for (int i = 0; i < nshift; ++i) {
+        const double sh = shifts[i];
+        auto mv = [&](const Spinor &out, const Spinor &in, const int *skip) {
+            op_apply(c, op, PREC_D, out, in, &in, C2(sh), skip);
+        };
+        if (i == 0) {
+            zero(c, *g);
+        } else {
+            mv(*pA, xs[i - 1], nullptr);
+            mv(*hA, xs[i], nullptr);
+            typedef std::complex<long double> lz;
+            const long double pApA = norm2_now(c, *pA), hAhA = norm2_now(c, *hA);
+            const double2 d1 = dot_now(c, *pA, b), d2 = dot_now(c, *hA, b), d3 = dot_now(c, *hA, *pA);
+            const lz pAb(d1.x, d1.y), hAb(d2.x, d2.y), hApA(d3.x, d3.y);
+            const lz den = -(hAhA * pApA) + hApA * std::conj(hApA);
+            zc c1, c2;
+            if (std::abs(den) > 1e-12L * hAhA * pApA && hAhA > 0) {
+                const lz mi(0.0L, -0.5L);
+                const long double c1R = std::real((-(hAhA * pAb) + hApA * std::conj(hAb) + hAb * std::conj(hApA) -
+                                                   hAhA * std::conj(pAb)) / (lz(2.0L) * den));
+                const long double c1I = std::real(mi * (-(hAhA * pAb) - hApA * std::conj(hAb) +
+                                                        hAb * std::conj(hApA) + hAhA * std::conj(pAb)) / den);
+                const long double c2R = std::real((hApA * pAb - hAb * pApA - pApA * std::conj(hAb) +
+                                                   std::conj(hApA) * std::conj(pAb)) / (lz(2.0L) * den));
+                const long double c2I = std::real(mi * (hApA * pAb - hAb * pApA + pApA * std::conj(hAb) -
+                                                        std::conj(hApA) * std::conj(pAb)) / den);
+                c1 = zc((double)c1R, (double)c1I);
+                c2 = zc((double)c2R, (double)c2I);
+            } else {
+                c1 = pApA > 0 ? zc((double)(pAb.real() / pApA), (double)(pAb.imag() / pApA)) : zc(0.0);
+                c2 = 0.0;
+            }
+            copy(c, *g, xs[i]);
+            axpby(c, xs[i - 1], *g, d2_of(c1), d2_of(c2));
+        }
+        lym_solve_stats s1;
+        memset(&s1, 0, sizeof(s1));
+        const int rc = cg_solve(c, mv, 2, b, xs[i], &*g, eps, max_steps, &s1);
+        ok = ok && rc == LYM_OK;
+        total += s1.iterations;
+    }
+    if (st) {
+        st->iterations = st->steps = total;
+        st->converged = ok;
+    }
+    return ok ? LYM_OK : LYM_NOT_CONVERGED;
+}
+
 enum BlockAlgo : int { ALGO_CG = 0, ALGO_BICGSTAB = 1 };
 
 // Block even-odd CG engine: nb slots on one resident gauge field.  Every slot solves its
@@ -1639,6 +1867,33 @@ private:
         else run_batch(c, OpBDirection<BatchH, BatchF>{ps.h(), rs.f(), S}, xs.s.lognb);
     }
 };
+
+// upload of source and guess, device timing and download around one FP64 solve
+template <class F>
+int solve_framed(lym_context *c, const double *source, double *solution, const double *guess,
+                        lym_solve_stats *stats, F solve)
+{
+    lym_solve_stats local;
+    memset(&local, 0, sizeof(local));
+    Vec b(c, PREC_D, 2), x(c, PREC_D, 2);
+    std::unique_ptr<Vec> gs;
+    upload_vec(c, *b, source, false, 0);
+    if (guess) {
+        gs.reset(new Vec(c, PREC_D, 2));
+        upload_vec(c, **gs, guess, false, 1);
+    }
+    CK(cudaEventRecord(c->ev0, c->st));
+    const int rc = solve(*b, *x, gs ? &**gs : nullptr, &local);
+    CK(cudaEventRecord(c->ev1, c->st));
+    download_vec(c, solution, *x, false, 2);
+    CK(cudaStreamSynchronize(c->st));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    local.seconds = ms * 1e-3;
+    if (stats) *stats = local;
+    CK(cudaGetLastError());
+    return rc;
+}
 
 }  // namespace
 
@@ -2224,6 +2479,35 @@ int lym_solve_shifted(lym_context *c, int op_id, double sre, double sim, double 
                     C2(sre, sim));
 }
 
+int lym_solve_bicgstab_l(lym_context *c, int op_id, int l, double precision, int max_steps, const double *source,
+                         double *solution, const double *guess, lym_solve_stats *stats)
+{
+    if (!source || !solution || max_steps < 0 || l < 1 || l > 16) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        OpEntry &op = op_of(c, op_id);
+        return solve_framed(c, source, solution, guess, stats,
+                            [&](const Spinor &b, const Spinor &x, const Spinor *g, lym_solve_stats *st) {
+                                return bicgstab_l_solve(c, op, l, b, x, g, precision, max_steps, st);
+                            });
+    });
+}
+
+int lym_solve_preconditioned(lym_context *c, int op_id, int preconditioner_op_id, double precision, int max_steps,
+                             const double *source, double *solution, const double *guess, lym_solve_stats *stats)
+{
+    if (!source || !solution || max_steps < 0) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        OpEntry &op = op_of(c, op_id);
+        OpEntry &pre = op_of(c, preconditioner_op_id);
+        if (pre.gauge_id != op.gauge_id)
+            fail(c, LYM_ERR_ARGUMENT, "the preconditioner must act on the operator's gauge field");
+        return solve_framed(c, source, solution, guess, stats,
+                            [&](const Spinor &b, const Spinor &x, const Spinor *g, lym_solve_stats *st) {
+                                return bicgstab_precond_solve(c, op, pre, b, x, g, precision, max_steps, st);
+                            });
+    });
+}
+
 static int do_multishift(lym_context *c, int op_id, int algorithm, int nshift, const double *shifts, double precision,
                          int max_steps, const double *source, double **solutions, lym_solve_stats *stats,
                          bool device_ptr)
@@ -2275,6 +2559,10 @@ static int do_multishift(lym_context *c, int op_id, int algorithm, int nshift, c
                 rc = ok ? LYM_OK : LYM_NOT_CONVERGED;
             } else if (algorithm == LYM_MULTISHIFT_MMMR) {
                 rc = multishift_mmmr(c, op, nshift, shifts, precision, max_steps, *b, xv, &local);
+            } else if (algorithm == LYM_MULTISHIFT_CHRONOLOGICAL) {
+                // solutions[i] (i >= 1) hold the chronological guesses on entry
+                for (int i = 1; i < nshift; ++i) upload_vec(c, xv[i], solutions[i], device_ptr, 1);
+                rc = multishift_chrono(c, op, nshift, shifts, precision, max_steps, *b, xv, &local);
             } else {
                 fail(c, LYM_ERR_UNSUPPORTED, "multishift algorithm %d", algorithm);
             }

@@ -20,7 +20,8 @@ from ._lib import LymError, SolveStats, lib
 SOLVER_CG, SOLVER_BICGSTAB, SOLVER_EO_BICGSTAB = 0, 1, 2
 SOLVER_EO_CG, SOLVER_EO_CG_MIXED_SINGLE, SOLVER_EO_CG_MIXED_HALF = 3, 4, 5
 SOLVER_EO_BICGSTAB_MIXED_SINGLE, SOLVER_EO_BICGSTAB_MIXED_HALF = 6, 7
-MULTISHIFT = {"mass_estrapolation": 0, "minimal_residual": 1, "multishift_cg": 2}
+MULTISHIFT = {"mass_estrapolation": 0, "minimal_residual": 1, "multishift_cg": 2,
+              "chronological_mass_estrapolation": 3}
 
 
 def _p(a):
@@ -92,23 +93,31 @@ class ConjugateGradient(Solver):
 
 
 class BiConjugateGradient(Solver):
-    """inverters/BiConjugateGradient.cpp:321-507; the shifted overload solve(..., shift)
-    solves (A + shift) x = b (:510-690)."""
+    """inverters/BiConjugateGradient.cpp:321-507.  The reference's other overloads are the
+    keyword arguments: shift solves (A + shift) x = b (:510-690), l runs BiCGStab(l)
+    (:130-317), preconditioner runs BiCGStab with that operator as preconditioner (:11-128)."""
     ALGORITHM = SOLVER_BICGSTAB
 
     def __init__(self):
         super().__init__("BiConjugateGradient")
 
-    def solve(self, dirac, source, solution, initial_guess=None, shift=None):
-        if shift is None:
+    def solve(self, dirac, source, solution, initial_guess=None, shift=None, l=None, preconditioner=None):
+        if shift is None and l is None and preconditioner is None:
             return super().solve(dirac, source, solution, initial_guess)
         lat = dirac.lattice
         src = dirac._vec(source)
         g = _p(dirac._vec(initial_guess)) if initial_guess is not None else None
         st = SolveStats()
-        s = complex(shift)
-        rc = lib().lym_solve_shifted(lat.handle, dirac.op_id, s.real, s.imag, float(self.precision),
-                                     int(self.maxSteps), _p(src), _p(solution), g, C.byref(st))
+        if l is not None:
+            rc = lib().lym_solve_bicgstab_l(lat.handle, dirac.op_id, int(l), float(self.precision),
+                                            int(self.maxSteps), _p(src), _p(solution), g, C.byref(st))
+        elif preconditioner is not None:
+            rc = lib().lym_solve_preconditioned(lat.handle, dirac.op_id, preconditioner.op_id, float(self.precision),
+                                                int(self.maxSteps), _p(src), _p(solution), g, C.byref(st))
+        else:
+            s = complex(shift)
+            rc = lib().lym_solve_shifted(lat.handle, dirac.op_id, s.real, s.imag, float(self.precision),
+                                         int(self.maxSteps), _p(src), _p(solution), g, C.byref(st))
         if rc < 0 and rc != -5:
             raise LymError(rc, lib().lym_last_error(lat.handle).decode())
         self.stats = st
@@ -213,6 +222,11 @@ class MultishiftSolver:
         for s in solutions:
             if s.shape != src.shape or s.dtype != np.complex128 or not s.flags.c_contiguous:
                 raise LymError(-1, "solutions must be contiguous complex128 arrays shaped like the source")
+        if self.algorithm == MULTISHIFT["chronological_mass_estrapolation"]:
+            # the chronological guesses are this solver's previous solutions (zeros at first)
+            prev = getattr(self, "_chrono", None)
+            for k in range(1, len(shifts)):
+                solutions[k][...] = prev[k] if prev is not None and k < len(prev) else 0.0
         ptrs = (C.c_void_p * len(shifts))(*[s.ctypes.data for s in solutions[: len(shifts)]])
         sh = np.ascontiguousarray(shifts, dtype=np.float64)
         st = SolveStats()
@@ -220,5 +234,7 @@ class MultishiftSolver:
                                   self.maxSteps, _p(src), ptrs, C.byref(st))
         if rc < 0:
             raise LymError(rc, lib().lym_last_error(lat.handle).decode())
+        if self.algorithm == MULTISHIFT["chronological_mass_estrapolation"]:
+            self._chrono = [s.copy() for s in solutions[: len(shifts)]]
         self.stats = st
         return rc == 0

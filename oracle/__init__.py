@@ -40,6 +40,10 @@ def lib():
         L.orc_preconditioned_bicgstab.argtypes = [vp, vp, vp, vp, dp, C.c_int, ip]
         L.orc_me_multishift.argtypes = [vp, vp, C.POINTER(C.c_void_p), C.POINTER(C.c_double), C.c_int, dp, C.c_int]
         L.orc_mmmr_multishift.argtypes = [vp, vp, C.POINTER(C.c_void_p), C.POINTER(C.c_double), C.c_int, dp, C.c_int, ip]
+        L.orc_bicgstab_l.argtypes = [vp, C.c_int, vp, vp, vp, dp, C.c_int, ip, C.POINTER(C.c_double)]
+        L.orc_bicgstab_precond.argtypes = [vp, vp, vp, vp, vp, dp, C.c_int, ip, C.POINTER(C.c_double)]
+        L.orc_chrono_multishift.argtypes = [vp, vp, C.POINTER(C.c_void_p), C.POINTER(C.c_double), C.c_int, dp,
+                                            C.c_int]
         L.orc_op_field_strength.argtypes = [vp]
         L.orc_op_field_strength.restype = vp
         L.orc_eo_multiply_even_odd.argtypes = [vp, vp, vp, C.c_int]
@@ -213,6 +217,40 @@ def _multishift(fn, op, src, shifts, eps, max_steps, with_steps):
         return rc, sols, steps.value
     rc = fn(C.byref(op._op), _ptr(src), ptrs, sh, len(shifts), float(eps), int(max_steps))
     return rc, sols, None
+
+
+def bicgstab_l(op, l, src, precision, max_steps=1000, guess=None):
+    """BiCGStab(l) (inverters/BiConjugateGradient.cpp:130-317)."""
+    src = np.ascontiguousarray(src, dtype=np.complex128)
+    sol = op._vec()
+    steps, last = C.c_int(0), C.c_double(0)
+    g = _ptr(np.ascontiguousarray(guess, dtype=np.complex128)) if guess is not None else None
+    rc = lib().orc_bicgstab_l(C.byref(op._op), int(l), _ptr(src), _ptr(sol), g, float(precision), int(max_steps),
+                              C.byref(steps), C.byref(last))
+    return rc, sol, steps.value
+
+
+def bicgstab_precond(op, pre, src, precision, max_steps=1000, guess=None):
+    """BiCGStab with a preconditioner operator (inverters/BiConjugateGradient.cpp:11-128)."""
+    src = np.ascontiguousarray(src, dtype=np.complex128)
+    sol = op._vec()
+    steps, last = C.c_int(0), C.c_double(0)
+    g = _ptr(np.ascontiguousarray(guess, dtype=np.complex128)) if guess is not None else None
+    rc = lib().orc_bicgstab_precond(C.byref(op._op), C.byref(pre._op), _ptr(src), _ptr(sol), g, float(precision),
+                                    int(max_steps), C.byref(steps), C.byref(last))
+    return rc, sol, steps.value
+
+
+def chrono_multishift(op, src, shifts, eps, max_steps=3000, previous=None):
+    """ChronologicalMultishiftSolver (inverters/ChronologicalMultishiftSolver.cpp:11-194);
+    previous[k]: the chronological guess of shift k (zeros when None)."""
+    src = np.ascontiguousarray(src, dtype=np.complex128)
+    sols = [np.ascontiguousarray(previous[k], dtype=np.complex128).copy() if previous is not None else op._vec()
+            for k in range(len(shifts))]
+    ptrs = (C.c_void_p * len(sols))(*[s.ctypes.data for s in sols])
+    sh = (C.c_double * len(shifts))(*[float(s) for s in shifts])
+    rc = lib().orc_chrono_multishift(C.byref(op._op), _ptr(src), ptrs, sh, len(shifts), float(eps), int(max_steps))
+    return rc, sols
 
 
 def me_multishift(op, src, shifts, eps, max_steps=3000):

@@ -1024,3 +1024,237 @@ int orc_mmmr_multishift(const orc_op *op, const orc_cplx *src, orc_cplx **sols, 
     free(r); free(p); free(t);
     return 0;
 }
+
+/* ---------------------------------------------------------------------------------
+ * BiCGStab(l): BiConjugateGradient::solve(dirac, source, solution, int l, guess)
+ * (inverters/BiConjugateGradient.cpp:130-317).  Inner products as the reference takes
+ * them: dot(a, b) = sum conj(a) b in long double, cast to a double complex scalar. */
+static orc_cplx cdot_c(const orc_op *op, const orc_cplx *a, const orc_cplx *b)
+{
+    long double re, im;
+    orc_dot(op->g, op->nc, a, b, &re, &im);
+    return (double)re + (double)im * I;
+}
+
+int orc_bicgstab_l(const orc_op *op, int l, const orc_cplx *src, orc_cplx *sol, const orc_cplx *guess,
+                   double precision, int max_steps, int *steps, double *last_error)
+{
+    if (l < 1) return -1;
+    const size_t L = vec_len(op);
+    orc_cplx *tmp = (orc_cplx *)malloc(sizeof(orc_cplx) * L), *rh = (orc_cplx *)malloc(sizeof(orc_cplx) * L);
+    orc_cplx **u = (orc_cplx **)malloc(sizeof(orc_cplx *) * (l + 1)), **r = (orc_cplx **)malloc(sizeof(orc_cplx *) * (l + 1));
+    for (int j = 0; j <= l; ++j) {
+        u[j] = (orc_cplx *)calloc(L, sizeof(orc_cplx));
+        r[j] = (orc_cplx *)calloc(L, sizeof(orc_cplx));
+    }
+    orc_cplx *tau = (orc_cplx *)calloc((size_t)(l + 1) * (l + 1), sizeof(orc_cplx));
+    orc_cplx *sigma = (orc_cplx *)calloc(l + 1, sizeof(orc_cplx)), *gam = (orc_cplx *)calloc(l + 1, sizeof(orc_cplx));
+    orc_cplx *gp = (orc_cplx *)calloc(l + 1, sizeof(orc_cplx)), *gpp = (orc_cplx *)calloc(l + 1, sizeof(orc_cplx));
+#define TAU(i, j) tau[(size_t)(i) * (l + 1) + (j)]
+    if (!guess) {
+        long double ns = orc_squared_norm(op->g, op->nc, src);
+        if (ns > precision) memcpy(sol, src, sizeof(orc_cplx) * L);
+        else seeded_uniform_vector(sol, L);
+    } else {
+        memcpy(sol, guess, sizeof(orc_cplx) * L);
+    }
+    orc_multiply(op, tmp, sol);
+    for (size_t k = 0; k < L; ++k) {
+        r[0][k] = src[k] - tmp[k];
+        rh[k] = src[k] + tmp[k];
+        u[0][k] = 0;
+    }
+    orc_cplx rho0 = 1, alpha = 0, omega = 1;
+    int step = 0, ok = 0;
+    double last = 0;
+    while (step < max_steps) {
+        rho0 = -omega * rho0;
+        for (int j = 0; j < l; ++j) {
+            const orc_cplx rho1 = cdot_c(op, r[j], rh);
+            const orc_cplx beta = (rho1 / rho0) * alpha;
+            rho0 = rho1;
+            for (int i = 0; i <= j; ++i)
+                for (size_t k = 0; k < L; ++k) u[i][k] = r[i][k] - beta * u[i][k];
+            orc_multiply(op, u[j + 1], u[j]);
+            const orc_cplx gamma = cdot_c(op, u[j + 1], rh);
+            alpha = rho0 / gamma;
+            for (int i = 0; i <= j; ++i)
+                for (size_t k = 0; k < L; ++k) r[i][k] = r[i][k] - alpha * u[i + 1][k];
+            orc_multiply(op, r[j + 1], r[j]);
+            for (size_t k = 0; k < L; ++k) sol[k] = sol[k] + alpha * u[0][k];
+        }
+        for (int j = 1; j <= l; ++j) {
+            for (int i = 1; i < j; ++i) {
+                TAU(i, j) = cdot_c(op, r[j], r[i]) / sigma[i];
+                for (size_t k = 0; k < L; ++k) r[j][k] = r[j][k] - TAU(i, j) * r[i][k];
+            }
+            sigma[j] = cdot_c(op, r[j], r[j]);
+            gp[j] = cdot_c(op, r[0], r[j]) / sigma[j];
+        }
+        gam[l] = gp[l];
+        omega = gam[l];
+        for (int j = l - 1; j > 0; --j) {
+            orc_cplx t = 0;
+            for (int i = j + 1; i <= l; ++i) t += TAU(j, i) * gam[i];
+            gam[j] = gp[j] - t;
+        }
+        for (int j = 1; j < l; ++j) {
+            orc_cplx t = 0;
+            for (int i = j + 1; i < l; ++i) t += TAU(j, i) * gam[i + 1];
+            gpp[j] = gam[j + 1] + t;
+        }
+        for (size_t k = 0; k < L; ++k) sol[k] = sol[k] + gam[1] * r[0][k];
+        for (size_t k = 0; k < L; ++k) r[0][k] = r[0][k] - gp[l] * r[l][k];
+        for (size_t k = 0; k < L; ++k) u[0][k] = u[0][k] - gam[l] * u[l][k];
+        for (int j = 1; j < l; ++j) {
+            for (size_t k = 0; k < L; ++k) u[0][k] = u[0][k] - gam[j] * u[j][k];
+            for (size_t k = 0; k < L; ++k) sol[k] = sol[k] + gpp[j] * r[j][k];
+            for (size_t k = 0; k < L; ++k) r[0][k] = r[0][k] - gp[j] * r[j][k];
+        }
+        const long double norm = orc_squared_norm(op->g, op->nc, r[0]);
+        last = (double)norm;
+        if (norm < precision) {
+            ok = 1;
+            break;
+        }
+        ++step;
+    }
+#undef TAU
+    if (steps) *steps = ok ? step : max_steps;
+    if (last_error) *last_error = last;
+    for (int j = 0; j <= l; ++j) {
+        free(u[j]);
+        free(r[j]);
+    }
+    free(u); free(r); free(tmp); free(rh); free(tau); free(sigma); free(gam); free(gp); free(gpp);
+    return ok;
+}
+
+/* ---------------------------------------------------------------------------------
+ * BiCGStab with a preconditioner operator P: BiConjugateGradient::solve(dirac, source,
+ * solution, preconditioner, guess) (inverters/BiConjugateGradient.cpp:11-128), with the
+ * reference's steps as they are: t = A s (not A P s), convergence only after step 5. */
+int orc_bicgstab_precond(const orc_op *op, const orc_op *pre, const orc_cplx *src, orc_cplx *sol,
+                         const orc_cplx *guess, double precision, int max_steps, int *steps, double *last_error)
+{
+    const size_t L = vec_len(op);
+    orc_cplx *res = (orc_cplx *)malloc(sizeof(orc_cplx) * L), *rhat = (orc_cplx *)malloc(sizeof(orc_cplx) * L);
+    orc_cplx *p = (orc_cplx *)malloc(sizeof(orc_cplx) * L), *nu = (orc_cplx *)malloc(sizeof(orc_cplx) * L);
+    orc_cplx *s = (orc_cplx *)malloc(sizeof(orc_cplx) * L), *t = (orc_cplx *)malloc(sizeof(orc_cplx) * L);
+    orc_cplx *pt = (orc_cplx *)malloc(sizeof(orc_cplx) * L), *st = (orc_cplx *)malloc(sizeof(orc_cplx) * L);
+    if (!guess) {
+        long double ns = orc_squared_norm(op->g, op->nc, src);
+        if (ns > precision) memcpy(sol, src, sizeof(orc_cplx) * L);
+        else seeded_uniform_vector(sol, L);
+    } else {
+        memcpy(sol, guess, sizeof(orc_cplx) * L);
+    }
+    orc_multiply(op, p, sol);
+    for (size_t k = 0; k < L; ++k) {
+        res[k] = src[k] - p[k];
+        rhat[k] = src[k] + p[k];
+    }
+    orc_cplx rho_prev = 0, alpha = 0, omega = 0;
+    int step = 0, ok = 0, done = 0;
+    double last = 0;
+    while (step < max_steps) {
+        const orc_cplx rho = cdot_c(op, rhat, res);
+        if (creal(rho) * creal(rho) + cimag(rho) * cimag(rho) == 0.) {
+            done = 1; /* breakdown: false, steps unchanged (BiConjugateGradient.cpp:40) */
+            break;
+        }
+        if (step == 0) {
+            memcpy(p, res, sizeof(orc_cplx) * L);
+        } else {
+            const orc_cplx beta = (rho / rho_prev) * (alpha / omega);
+            for (size_t k = 0; k < L; ++k) p[k] = res[k] + beta * (p[k] - omega * nu[k]);
+        }
+        orc_multiply(pre, pt, p);
+        orc_multiply(op, nu, pt);
+        alpha = rho / cdot_c(op, rhat, nu);
+        for (size_t k = 0; k < L; ++k) s[k] = res[k] - alpha * nu[k];
+        orc_multiply(pre, st, s);
+        orc_multiply(op, t, s);
+        long double dre, dim;
+        orc_dot(op->g, op->nc, t, s, &dre, &dim);
+        const long double tt = orc_squared_norm(op->g, op->nc, t);
+        omega = (double)(dre / tt) + (double)(dim / tt) * I;
+        for (size_t k = 0; k < L; ++k) sol[k] = sol[k] + alpha * pt[k] + omega * st[k];
+        for (size_t k = 0; k < L; ++k) res[k] = s[k] - omega * t[k];
+        const long double norm = orc_squared_norm(op->g, op->nc, res);
+        if (norm < precision && step > 5) {
+            ok = 1;
+            break;
+        }
+        rho_prev = rho;
+        last = (double)norm;
+        ++step;
+    }
+    if (steps) *steps = ok ? step : (done ? step : max_steps);
+    if (last_error) *last_error = last;
+    free(res); free(rhat); free(p); free(nu); free(s); free(t); free(pt); free(st);
+    return ok;
+}
+
+/* ---------------------------------------------------------------------------------
+ * Chronological multishift: ChronologicalMultishiftSolver::solve
+ * (inverters/ChronologicalMultishiftSolver.cpp:11-194).  Shift 0 by CG from zero; every
+ * further shift k starts CG from c1 x_{k-1} + c2 h_k, the combination minimising
+ * |(A + s_k)(c1 x_{k-1} + c2 h_k) - b| (the reference's closed form).  h_k, the
+ * chronological guess, is sols[k] on entry (the reference reads it from uninitialised
+ * storage); when the 2x2 system is singular (h_k = 0 or parallel) c2 = 0 and c1
+ * minimises the one-vector residual. */
+int orc_chrono_multishift(const orc_op *op, const orc_cplx *src, orc_cplx **sols, const double *shifts, int nshift,
+                          double epsilon, int max_steps)
+{
+    const size_t L = vec_len(op);
+    orc_cplx *r = (orc_cplx *)malloc(sizeof(orc_cplx) * L), *p = (orc_cplx *)malloc(sizeof(orc_cplx) * L);
+    orc_cplx *t = (orc_cplx *)malloc(sizeof(orc_cplx) * L), *gs = (orc_cplx *)malloc(sizeof(orc_cplx) * L);
+    if (!r || !p || !t || !gs) return -2;
+    int ok = 1;
+    for (size_t k = 0; k < L; ++k) {
+        sols[0][k] = 0;
+        p[k] = src[k];
+        r[k] = src[k];
+    }
+    ok &= cg_shift_block(op, src, sols[0], r, p, t, shifts[0], epsilon, max_steps);
+    for (int i = 1; i < nshift; ++i) {
+        multiply_add_c(op, p, sols[i - 1], sols[i - 1], shifts[i]);
+        multiply_add_c(op, t, sols[i], sols[i], shifts[i]);
+        long double re, im;
+        const long double pApA = orc_squared_norm(op->g, op->nc, p), hAhA = orc_squared_norm(op->g, op->nc, t);
+        orc_dot(op->g, op->nc, p, src, &re, &im);
+        const long double complex pAb = re + im * I;
+        orc_dot(op->g, op->nc, t, src, &re, &im);
+        const long double complex hAb = re + im * I;
+        orc_dot(op->g, op->nc, t, p, &re, &im);
+        const long double complex hApA = re + im * I;
+        const long double complex den = -(hAhA * pApA) + hApA * conjl(hApA);
+        orc_cplx c1, c2;
+        if (cabsl(den) > 1e-12L * hAhA * pApA && hAhA > 0) {
+            const long double c1R = creall((-(hAhA * pAb) + hApA * conjl(hAb) + hAb * conjl(hApA) - hAhA * conjl(pAb)) /
+                                           (2.0L * den));
+            const long double c1I = creall((-0.5L * I) * (-(hAhA * pAb) - hApA * conjl(hAb) + hAb * conjl(hApA) +
+                                                          hAhA * conjl(pAb)) / den);
+            const long double c2R = creall((hApA * pAb - hAb * pApA - pApA * conjl(hAb) + conjl(hApA) * conjl(pAb)) /
+                                           (2.0L * den));
+            const long double c2I = creall((-0.5L * I) * (hApA * pAb - hAb * pApA + pApA * conjl(hAb) -
+                                                          conjl(hApA) * conjl(pAb)) / den);
+            c1 = (double)c1R + (double)c1I * I;
+            c2 = (double)c2R + (double)c2I * I;
+        } else {
+            c1 = pApA > 0 ? (orc_cplx)(pAb / pApA) : 0;
+            c2 = 0;
+        }
+        for (size_t k = 0; k < L; ++k) gs[k] = c1 * sols[i - 1][k] + c2 * sols[i][k];
+        multiply_add_c(op, t, gs, gs, shifts[i]);
+        for (size_t k = 0; k < L; ++k) {
+            sols[i][k] = gs[k];
+            r[k] = src[k] - t[k];
+            p[k] = src[k] - t[k];
+        }
+        ok &= cg_shift_block(op, src, sols[i], r, p, t, shifts[i], epsilon, max_steps);
+    }
+    free(r); free(p); free(t); free(gs);
+    return ok;
+}

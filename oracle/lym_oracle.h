@@ -113,6 +113,12 @@ int orc_me_multishift(const orc_op *op, const orc_cplx *src, orc_cplx **sols,
 int orc_mmmr_multishift(const orc_op *op, const orc_cplx *src, orc_cplx **sols,
                         const double *shifts, int nshift, double epsilon, int max_steps,
                         int *steps);
+int orc_bicgstab_l(const orc_op *op, int l, const orc_cplx *src, orc_cplx *sol, const orc_cplx *guess,
+                   double precision, int max_steps, int *steps, double *last_error);
+int orc_bicgstab_precond(const orc_op *op, const orc_op *pre, const orc_cplx *src, orc_cplx *sol,
+                         const orc_cplx *guess, double precision, int max_steps, int *steps, double *last_error);
+int orc_chrono_multishift(const orc_op *op, const orc_cplx *src, orc_cplx **sols, const double *shifts, int nshift,
+                          double epsilon, int max_steps);
 
 #ifdef __cplusplus
 }

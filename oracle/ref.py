@@ -34,6 +34,7 @@ def lib(rep):
         L.ref_multiply_add.argtypes = [ip, i, dp, dp, i, vp, vp, vp, dp, dp, vp]
         L.ref_field_strength.argtypes = [ip, dp, dp, vp, vp]
         L.ref_solve.argtypes = [ip, i, dp, dp, i, vp, i, dp, i, dp, dp, vp, vp, ip]
+        L.ref_solve2.argtypes = [ip, i, dp, dp, i, vp, i, dp, i, i, i, dp, dp, vp, vp, ip]
         L.ref_multishift.argtypes = [ip, i, dp, dp, i, vp, i, i, vp, dp, i, vp, C.POINTER(C.c_void_p)]
         L.ref_neighbours.argtypes = [ip, ip, ip]
         L.ref_antiperiodic.argtypes = [ip, vp]
@@ -96,12 +97,24 @@ class Reference:
                               float(precision), int(max_steps), s.real, s.imag, _p(b), _p(x), C.byref(steps))
         return rc, x, steps.value
 
+    def solve2(self, kind, solver, b, precision, max_steps, kappa, csw=0.0, gamma5=True, l=2, pre_kind="DiracWilson",
+               pre_kappa=0.1, pre_csw=0.0):
+        """BiCGStab(l) (solver "bicgstab_l") or BiCGStab with a preconditioner operator
+        (solver "bicgstab_precond") of the compiled reference."""
+        b = np.ascontiguousarray(b, np.complex128)
+        x = self._vec()
+        steps = C.c_int(0)
+        rc = self.L.ref_solve2(_d(self.dims), KIND[kind], kappa, csw, int(gamma5), _p(self.links),
+                               {"bicgstab_l": 0, "bicgstab_precond": 1}[solver], float(precision), int(max_steps),
+                               int(l), KIND[pre_kind], float(pre_kappa), float(pre_csw), _p(b), _p(x), C.byref(steps))
+        return rc, x, steps.value
+
     def multishift(self, kind, algorithm, b, shifts, epsilon, max_steps, kappa, csw=0.0, gamma5=True):
         b = np.ascontiguousarray(b, np.complex128)
         sols = [self._vec() for _ in shifts]
         ptrs = (C.c_void_p * len(sols))(*[s.ctypes.data for s in sols])
         sh = np.ascontiguousarray(shifts, np.float64)
-        alg = {"mass_estrapolation": 0, "minimal_residual": 1}[algorithm]
+        alg = {"mass_estrapolation": 0, "minimal_residual": 1, "chronological_mass_estrapolation": 2}[algorithm]
         rc = self.L.ref_multishift(_d(self.dims), KIND[kind], kappa, csw, int(gamma5), _p(self.links), alg,
                                    len(shifts), _p(sh), float(epsilon), int(max_steps), _p(b), ptrs)
         return rc, sols

@@ -21,6 +21,7 @@
 #include "inverters/ConjugateGradient.h"
 #include "inverters/MEMultishiftSolver.h"
 #include "inverters/MMMRMultishiftSolver.h"
+#include "inverters/ChronologicalMultishiftSolver.h"
 #include "inverters/PreconditionedBiCGStab.h"
 #include "utils/ConvertLattice.h"
 
@@ -208,7 +209,45 @@ int ref_solve(const int dims[4], int kind, double kappa, double csw, int gamma5,
     return ok ? 1 : 0;
 }
 
-// algorithm 0 MEMultishiftSolver, 1 MMMRMultishiftSolver
+// solver 0: BiConjugateGradient::solve(op, b, x, int l) (BiCGStab(l), l = ival);
+// solver 1: BiConjugateGradient::solve(op, b, x, preconditioner) with the preconditioner an
+// operator of kind pkind (pkappa, pcsw, gamma5 as the solved operator)
+int ref_solve2(const int dims[4], int kind, double kappa, double csw, int gamma5, const double *links, int solver,
+               double precision, int max_steps, int ival, int pkind, double pkappa, double pcsw, const double *src,
+               double *sol, int *steps)
+{
+    init_layout(dims);
+    extended_fermion_lattice_t L;
+    load(L, links);
+    DiracOperator *op = make_operator(kind, kappa, csw, gamma5, L);
+    if (!op) return -1;
+    reduced_dirac_vector_t b, x;
+    load(b, src);
+    BiConjugateGradient bi;
+    bi.setPrecision(precision);
+    bi.setMaximumSteps(max_steps);
+    bool ok = false;
+    if (solver == 0) {
+        ok = bi.solve(op, b, x, ival);
+    } else if (solver == 1) {
+        DiracOperator *pre = make_operator(pkind, pkappa, pcsw, gamma5, L);
+        if (!pre) {
+            delete op;
+            return -1;
+        }
+        ok = bi.solve(op, b, x, pre);
+        delete pre;
+    } else {
+        delete op;
+        return -1;
+    }
+    *steps = bi.getLastSteps();
+    store(x, sol);
+    delete op;
+    return ok ? 1 : 0;
+}
+
+// algorithm 0 MEMultishiftSolver, 1 MMMRMultishiftSolver, 2 ChronologicalMultishiftSolver
 int ref_multishift(const int dims[4], int kind, double kappa, double csw, int gamma5, const double *links,
                    int algorithm, int nshift, const double *shifts, double epsilon, int max_steps, const double *src,
                    double **sols)
@@ -222,8 +261,9 @@ int ref_multishift(const int dims[4], int kind, double kappa, double csw, int ga
     load(b, src);
     std::vector<extended_dirac_vector_t> xs(nshift);
     std::vector<real_t> sh(shifts, shifts + nshift);
-    MultishiftSolver *ms = algorithm == 0 ? (MultishiftSolver *)new MEMultishiftSolver(epsilon, max_steps)
-                                          : (MultishiftSolver *)new MMMRMultishiftSolver(epsilon, max_steps);
+    MultishiftSolver *ms = algorithm == 0   ? (MultishiftSolver *)new MEMultishiftSolver(epsilon, max_steps)
+                           : algorithm == 1 ? (MultishiftSolver *)new MMMRMultishiftSolver(epsilon, max_steps)
+                                            : (MultishiftSolver *)new ChronologicalMultishiftSolver(epsilon, max_steps);
     const bool ok = ms->solve(op, b, xs, sh);
     for (int i = 0; i < nshift; ++i) store(xs[i], sols[i]);
     delete ms;

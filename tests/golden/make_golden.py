@@ -53,6 +53,20 @@ def make(rep):
         rc, sols = ref.multishift("SquareImproved", alg, x, shifts, prec, 5000, kappa, csw, True)
         assert rc == 1, alg
         out[f"multishift/{alg}"] = np.stack(sols)
+    # BiCGStab(l) and BiCGStab with a preconditioner operator (BiConjugateGradient.cpp:11-317)
+    for l in (2, 4):
+        rc, sol, steps = ref.solve2("SquareImproved", "bicgstab_l", x, prec, 5000, kappa, csw, True, l=l)
+        out[f"rc/bicgstab_l{l}"], out[f"solve/bicgstab_l{l}"], out[f"steps/bicgstab_l{l}"] = rc, sol, steps
+    rc, sol, steps = ref.solve2("Improved", "bicgstab_precond", x, prec, 5000, kappa, csw, False,
+                                pre_kind="DiracWilson", pre_kappa=0.05, pre_csw=0.0)
+    out["rc/bicgstab_precond"], out["solve/bicgstab_precond"], out["steps/bicgstab_precond"] = rc, sol, steps
+    # ChronologicalMultishiftSolver: its first shift is plain CG from zero; the later shifts
+    # start from a guess built from vectors the reference never initialises, so only the
+    # first shift is a fixture (and whether the others came out finite)
+    rc, sols = ref.multishift("SquareImproved", "chronological_mass_estrapolation", x, shifts, prec, 5000, kappa,
+                              csw, True)
+    out["multishift/chronological/0"] = sols[0]
+    out["multishift/chronological/finite"] = np.array([bool(np.isfinite(s).all()) for s in sols])
     sup, sdn = R.neighbours(DIMS, rep)
     out["sup"], out["sdn"] = sup, sdn
     if rep == "su2adj":

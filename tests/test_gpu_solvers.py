@@ -205,3 +205,73 @@ def test_multishift_minimal_residual(setup, oracle):
     for x, xo, s in zip(sols, osols, shifts):
         assert true_res(orc, b, x, s) < 2e-10
         assert rel(x, xo) < 1e-7
+
+
+@pytest.mark.parametrize("l", [2, 4])
+def test_bicgstab_l_matches_oracle(setup, l, oracle):
+    # BiConjugateGradient::solve(dirac, source, solution, int l) (BiConjugateGradient.cpp:130-317)
+    b = setup["b"]
+    eps = (1e-10) ** 2 * float(np.vdot(b, b).real)
+    orc = oracle.Operator(setup["geom"], setup["links"], "SquareImproved", setup["kappa"], setup["csw"], True)
+    rc, xo, steps = oracle.bicgstab_l(orc, l, b, eps, 3000)
+    s = L.BiConjugateGradient()
+    s.setPrecision(eps)
+    s.setMaximumSteps(3000)
+    x = setup["lat"].new_vector()
+    ok = s.solve(gpu_op(setup, L.SquareImprovedDiracWilsonOperator), b, x, l=l)
+    if rc != 1:  # the algorithm does not converge on this system in the oracle either
+        assert not ok or true_res(orc, b, x) < 1.5e-10
+        return
+    assert ok
+    assert abs(s.getLastSteps() - steps) <= max(3, steps // 4)
+    assert true_res(orc, b, x) < 1.5e-10
+    assert rel(x, xo) < 1e-7
+
+
+def test_bicgstab_preconditioned_matches_oracle(setup, oracle):
+    # BiConjugateGradient::solve(dirac, source, solution, preconditioner) (BiConjugateGradient.cpp:11-128)
+    b = setup["b"]
+    eps = (1e-10) ** 2 * float(np.vdot(b, b).real)
+    orc = oracle.Operator(setup["geom"], setup["links"], "Improved", setup["kappa"], setup["csw"], False)
+    pre_o = oracle.Operator(setup["geom"], setup["links"], "DiracWilson", 0.05, 0.0, False)
+    rc, xo, steps = oracle.bicgstab_precond(orc, pre_o, b, eps, 3000)
+    pre = L.DiracWilsonOperator(setup["lat"], 0.05)
+    pre.setGamma5(False)
+    pre.setLattice(setup["gid"])
+    s = L.BiConjugateGradient()
+    s.setPrecision(eps)
+    s.setMaximumSteps(3000)
+    x = setup["lat"].new_vector()
+    ok = s.solve(gpu_op(setup, L.ImprovedDiracWilsonOperator, False), b, x, preconditioner=pre)
+    assert ok == (rc == 1)
+    if rc == 1:
+        assert abs(s.getLastSteps() - steps) <= max(3, steps // 4)
+        assert rel(x, xo) < 1e-7
+
+
+def test_multishift_chronological(setup, oracle):
+    # ChronologicalMultishiftSolver (ChronologicalMultishiftSolver.cpp:11-194): the second solve
+    # starts every shift from the first solve's solutions (the chronological guesses)
+    b = setup["b"]
+    shifts = [0.5, 0.1, 0.01]
+    eps = (1e-10) ** 2 * float(np.vdot(b, b).real)
+    op = gpu_op(setup, L.SquareImprovedDiracWilsonOperator)
+    orc = oracle.Operator(setup["geom"], setup["links"], "SquareImproved", setup["kappa"], setup["csw"], True)
+    ms = L.MultishiftSolver.getInstance("chronological_mass_estrapolation")
+    ms.setPrecision(eps)
+    sols = []
+    assert ms.solve(op, b, sols, shifts)
+    first_iters = ms.stats.iterations
+    rc, osols = oracle.chrono_multishift(orc, b, shifts, eps)
+    assert rc == 1
+    for x, xo, s in zip(sols, osols, shifts):
+        assert true_res(orc, b, x, s) < 1.5e-10
+        assert rel(x, xo) < 1e-7
+    b2 = b + 1e-3 * synth.gaussian_spinor(setup["dims"], 3, 22)
+    sols2 = []
+    assert ms.solve(op, b2, sols2, shifts)
+    rc, osols2 = oracle.chrono_multishift(orc, b2, shifts, eps, previous=osols)
+    for x, xo, s in zip(sols2, osols2, shifts):
+        assert true_res(orc, b2, x, s) < 1.5e-10
+        assert rel(x, xo) < 1e-7
+    assert ms.stats.iterations < first_iters

@@ -99,3 +99,39 @@ def test_live_against_compiled_reference(rep, oracle):
         assert rel(got, ref.multiply(kind, x, kappa, c, True)) <= 1e-15
     # BasicDiracWilsonOperator equals DiracWilsonOperator (TestLinearAlgebra.cpp:145-150)
     assert rel(ref.multiply("BasicDiracWilson", x, kappa), ref.multiply("DiracWilson", x, kappa)) < 1e-15
+
+
+def test_bicgstab_variants_pinned(gold, oracle):
+    """BiCGStab(l) and BiCGStab with a preconditioner operator (BiConjugateGradient.cpp:11-317)
+    where the reference converged; the same steps, the same solution."""
+    x = gold["x"]
+    prec = 1e-20 * float(np.vdot(x, x).real)
+    for l in (2, 4):
+        if int(gold[f"rc/bicgstab_l{l}"]) != 1:
+            continue
+        rc, sol, steps = oracle.bicgstab_l(op(oracle, gold, "SquareImproved"), l, x, prec, 5000)
+        ref_steps = int(gold[f"steps/bicgstab_l{l}"])
+        assert rc == 1 and abs(steps - ref_steps) <= max(3, ref_steps // 4), (l, steps, ref_steps)
+        assert rel(sol, gold[f"solve/bicgstab_l{l}"]) < 1e-8
+    if int(gold["rc/bicgstab_precond"]) == 1:
+        pre = oracle.Operator(gold["geom"], gold["links"], "DiracWilson", 0.05, 0.0, False)
+        rc, sol, steps = oracle.bicgstab_precond(op(oracle, gold, "Improved", False), pre, x, prec, 5000)
+        assert rc == 1 and steps == int(gold["steps/bicgstab_precond"])
+        assert rel(sol, gold["solve/bicgstab_precond"]) < 1e-10
+
+
+def test_chronological_multishift_pinned(gold, oracle):
+    """ChronologicalMultishiftSolver: its first shift (CG from zero) equals the reference's;
+    the later shifts, which the reference builds from uninitialised storage (non-finite in
+    its run), solve their systems."""
+    x = gold["x"]
+    prec = 1e-20 * float(np.vdot(x, x).real)
+    shifts = list(gold["shifts"])
+    A = op(oracle, gold, "SquareImproved")
+    rc, sols = oracle.chrono_multishift(A, x, shifts, prec)
+    assert rc == 1
+    assert rel(sols[0], gold["multishift/chronological/0"]) < 1e-12
+    assert not gold["multishift/chronological/finite"][1:].all()
+    for s, sh in zip(sols, shifts):
+        r = x - A.multiply(s) - sh * s
+        assert float(np.vdot(r, r).real) < 4 * prec
