@@ -84,7 +84,17 @@ enum lym_multishift_solver {
     /* "chronological_mass_estrapolation": ChronologicalMultishiftSolver
      * (inverters/ChronologicalMultishiftSolver.cpp:11-194); solutions[i], i >= 1, hold the
      * chronological guess of shift i on entry (zeros for none) */
-    LYM_MULTISHIFT_CHRONOLOGICAL = 3
+    LYM_MULTISHIFT_CHRONOLOGICAL = 3,
+    /* multishift CG for RHMC (no reference counterpart) on the squared even-odd operator with
+     * gamma5 (SquareEvenOddImprovedDiracWilsonOperator, the operator of
+     * actions/NFlavorFermionAction.cpp:76-96): FP32 / FP16-with-norms directions and operator,
+     * FP32 residual and solution accumulators, FP64 shift recurrences, inner products and
+     * reliable updates of the base system, then mixed-precision CG per shift until every
+     * |b - (A + shifts[i]) x_i|^2 < precision in FP64 (stats->true_residual: the largest,
+     * relative to |b|; stats->steps: iterations of the shared Krylov space, stats->iterations:
+     * those plus the per-shift refinement); other operator kinds: LYM_ERR_UNSUPPORTED */
+    LYM_MULTISHIFT_CG_MIXED_SINGLE = 4,
+    LYM_MULTISHIFT_CG_MIXED_HALF = 5
 };
 
 typedef struct {

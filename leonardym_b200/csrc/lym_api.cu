@@ -11,6 +11,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/lym_b200.h"
@@ -910,6 +911,297 @@ int multishift_cg(lym_context *c, OpEntry &op, int nshift, const double *shifts,
     }
     for (auto v : ps) delete v;
     dev_free(c, dviews, 2 * kMaxShifts * sizeof(SpinorD));
+    return rc;
+}
+
+// The odd-site system of the RHMC operator with a shift, M = (G5 S)^2 + sigma, applied in
+// `prec` through the Schur complement: out = G5 S (G5 S in) + sigma in.
+void schur_square_shift(lym_context *c, OpEntry &op, int prec, const Spinor &out, const Spinor &in,
+                        const Spinor &tmp_o, const Spinor &tmp_e, double sigma, const int *skip = nullptr)
+{
+    apply_schur(c, op, prec, tmp_o, in, tmp_e, 1, nullptr, C2(0.0), skip);
+    apply_schur(c, op, prec, out, tmp_o, tmp_e, 1, &in, C2(sigma), skip);
+}
+
+// Mixed-precision CG on ((G5 S)^2 + sigma) x_o = b_o from the FP64 x_o it is given: directions
+// and operator applications in `sprec`, residual and the solution accumulator in FP32 (FP64 for
+// sprec FP64), every inner product and the recurrences in FP64; reliable updates (x += x_sloppy,
+// FP64 true residual) whenever the recursive residual falls by delta, and a direction rebuilt
+// from the true residual after each.  Stops when |b_o - M x_o|^2 < eps (FP64).
+int shift_cg_mixed(lym_context *c, OpEntry &op, int sprec, double sigma, const Spinor &bo, const Spinor &xo,
+                   double eps, int max_steps, int &iters, int &updates, double &rr_true)
+{
+    const int aprec = sprec == PREC_H ? PREC_F : sprec;
+    Vec r64(c, PREC_D, 1), t64(c, PREC_D, 1), u64(c, PREC_D, 1), te64(c, PREC_D, 1);
+    Vec rs(c, aprec, 1), xs(c, aprec, 1), ps(c, sprec, 1), aps(c, sprec, 1), tos(c, sprec, 1), tes(c, sprec, 1);
+    auto true_res = [&]() {
+        schur_square_shift(c, op, PREC_D, *u64, xo, *t64, *te64, sigma);
+        run_site(c, OpSubNorm<SpinorD, SpinorD, SpinorD>{bo.d(), (*u64).d(), (*r64).d(), c->d_scal}, 1);
+        CK(cudaMemcpyAsync(c->h_scal, c->d_scal, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        return c->h_scal[0];
+    };
+    rr_true = true_res();
+    if (rr_true < eps) return LYM_OK;
+    if (max_steps <= 0) return LYM_NOT_CONVERGED;
+    copy(c, *rs, *r64);
+    copy(c, *ps, *rs);
+    zero(c, *xs);
+    CGState &H = cg_host(c);
+    memset(&H, 0, sizeof(H));
+    H.rr = rr_true;
+    H.rr_max = rr_true;
+    H.eps = eps;
+    H.delta2 = sprec == PREC_D ? 0.0 : 0.01;
+    H.max_iter = iters + max_steps;
+    H.iter = iters;
+    push_state(c, sizeof(CGState));
+    CGState *S = cg_state(c);
+    Gate gate{&S->pause, nullptr};
+    double eps_rec = eps;
+    auto step = [&]() {
+        schur_square_shift(c, op, sprec, *aps, *ps, *tos, *tes, sigma, &S->pause);
+        auto go = [&](auto P, auto AP, auto X, auto R) {
+            run_site(c, OpCGAlpha<decltype(P), decltype(AP)>{P, AP, S}, 1, gate);
+            run_site(c, OpCGUpdate<decltype(X), decltype(P), decltype(R), decltype(AP)>{X, P, R, AP, S}, 1, gate);
+            run_site(c, OpCGDirection<decltype(P), decltype(R)>{P, R, S}, 1, gate);
+        };
+        if (sprec == PREC_D) go((*ps).d(), (*aps).d(), (*xs).d(), (*rs).d());
+        else if (sprec == PREC_F) go((*ps).f(), (*aps).f(), (*xs).f(), (*rs).f());
+        else go((*ps).h(), (*aps).h(), (*xs).f(), (*rs).f());
+    };
+    int rc = LYM_NOT_CONVERGED;
+    for (int outer = 0; outer < 100000; ++outer) {
+        run_gated_state(c, S, step, 8, (long)(H.max_iter - cg_host(c).iter) + 8);
+        CGState R = cg_host(c);
+        iters = R.iter;
+        if (R.failed) fail(c, LYM_ERR_NUMERIC, "shifted CG produced a non-finite residual");
+        axpby(c, *xs, xo, C2(1.0), C2(1.0));
+        zero(c, *xs);
+        rr_true = true_res();
+        ++updates;
+        if (rr_true < eps) {
+            rc = LYM_OK;
+            break;
+        }
+        if (R.iter >= R.max_iter) break;
+        if (R.converged) eps_rec = std::max(eps_rec * 0.5 * eps / rr_true, 1e-300);
+        copy(c, *rs, *r64);
+        CGState &W = cg_host(c);
+        W = R;
+        W.beta = rr_true / R.rr_prev;
+        W.rr = rr_true;
+        W.rr_max = rr_true;
+        W.eps = eps_rec;
+        W.pause = 0;
+        W.converged = 0;
+        W.need_update = 0;
+        push_state(c, sizeof(CGState));
+        if (sprec == PREC_D) run_site(c, OpCGDirection<SpinorD, SpinorD>{(*ps).d(), (*rs).d(), S}, 1);
+        else if (sprec == PREC_F) run_site(c, OpCGDirection<SpinorF, SpinorF>{(*ps).f(), (*rs).f(), S}, 1);
+        else run_site(c, OpCGDirection<SpinorH, SpinorF>{(*ps).h(), (*rs).f(), S}, 1);
+    }
+    return rc;
+}
+
+// Mixed-precision multishift CG for the RHMC operator (SquareEvenOddImproved with gamma5:
+// odd <- (G5 S)^2 x_o, even <- x_e; NFlavorFermionAction's multishift on the squared
+// operator, actions/NFlavorFermionAction.cpp:76-96).  Even sites: x_e = b_e / (1 + sigma_i).
+// Odd sites: one Krylov space on the smallest shift with the directions p_i and the
+// operator applications in `sprec`, the residual and the per-shift solution accumulators in
+// FP32, the shift recurrences (Jegerlehner) and every inner product in FP64.  Whenever the
+// base residual falls by delta = 0.1, the accumulators are added to the FP64 solutions, the
+// base residual is recomputed in FP64 and the directions are rebuilt from it (shifted
+// residuals stay zeta_i r).  Then each shift whose FP64 true residual misses eps is refined
+// by shift_cg_mixed from its multishift solution.  eps: |b - (A + sigma_i) x_i|^2 (FP64).
+int multishift_cg_mixed(lym_context *c, OpEntry &op, int sprec, int nshift, const double *shifts, double eps,
+                        int max_steps, const Spinor &b, std::vector<Spinor> &xs, lym_solve_stats *st)
+{
+    if (op.kind != LYM_OP_SQUARE_EVEN_ODD_IMPROVED || !op.gamma5)
+        fail(c, LYM_ERR_UNSUPPORTED,
+             "mixed-precision multishift needs the squared even-odd operator with gamma5 (kind %d, gamma5 %d)",
+             op.kind, op.gamma5);
+    if (nshift < 1 || nshift > kMaxShifts) fail(c, LYM_ERR_ARGUMENT, "multishift: 1..%d shifts", kMaxShifts);
+    for (int i = 0; i < nshift; ++i)
+        if (!(1.0 + shifts[i] != 0.0) || !std::isfinite(shifts[i]))
+            fail(c, LYM_ERR_ARGUMENT, "multishift: shift %d = %g gives a singular even-site system", i, shifts[i]);
+    const int aprec = sprec == PREC_H ? PREC_F : sprec;
+    int base = 0;
+    for (int i = 1; i < nshift; ++i)
+        if (shifts[i] < shifts[base]) base = i;
+    const double s0 = shifts[base];
+    const Spinor bo = b.parity(1);
+    for (int i = 0; i < nshift; ++i) {
+        axpby(c, b.parity(0), xs[i].parity(0), C2(1.0 / (1.0 + shifts[i])), C2(0.0));
+        zero(c, xs[i].parity(1));
+    }
+    const double bbo = norm2_now(c, bo);
+    Vec r(c, aprec, 1), ap(c, sprec, 1), tos(c, sprec, 1), tes(c, sprec, 1);
+    Vec r64(c, PREC_D, 1), t64(c, PREC_D, 1), u64(c, PREC_D, 1), te64(c, PREC_D, 1);
+    std::vector<Vec *> ps, acc;
+    struct Views {
+        std::vector<Vec *> &ps, &acc;
+        ~Views()
+        {
+            for (auto v : ps) delete v;
+            for (auto v : acc) delete v;
+        }
+    } owner{ps, acc};
+    for (int i = 0; i < nshift; ++i) {
+        ps.push_back(new Vec(c, sprec, 1));
+        acc.push_back(new Vec(c, aprec, 1));
+        copy(c, **ps.back(), bo);
+        zero(c, **acc.back());
+    }
+    copy(c, *r, bo);
+    // device arrays of the per-shift views: accumulators at 0, directions at kMaxShifts
+    const size_t vbytes = std::max(sizeof(SpinorH), sizeof(SpinorD));
+    char *dviews = (char *)dev_alloc(c, 2 * kMaxShifts * vbytes);
+    struct ViewsMem {
+        lym_context *c;
+        void *p;
+        size_t n;
+        ~ViewsMem() { dev_free(c, p, n); }
+    } vmem{c, dviews, 2 * kMaxShifts * vbytes};
+    auto upload_views = [&](auto tag_x, auto tag_p) {
+        using VX = decltype(tag_x);
+        using VP = decltype(tag_p);
+        std::vector<VX> hx(nshift);
+        std::vector<VP> hp(nshift);
+        for (int i = 0; i < nshift; ++i) {
+            const Spinor &a = **acc[i], &p = **ps[i];
+            if constexpr (std::is_same<VX, SpinorD>::value) hx[i] = a.d(); else hx[i] = a.f();
+            if constexpr (std::is_same<VP, SpinorD>::value) hp[i] = p.d();
+            else if constexpr (std::is_same<VP, SpinorF>::value) hp[i] = p.f();
+            else hp[i] = p.h();
+        }
+        CK(cudaMemcpyAsync(dviews, hx.data(), nshift * sizeof(VX), cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(dviews + kMaxShifts * vbytes, hp.data(), nshift * sizeof(VP), cudaMemcpyHostToDevice,
+                           c->st));
+        CK(cudaStreamSynchronize(c->st));
+    };
+    if (sprec == PREC_D) upload_views(SpinorD{}, SpinorD{});
+    else if (sprec == PREC_F) upload_views(SpinorF{}, SpinorF{});
+    else upload_views(SpinorF{}, SpinorH{});
+
+    // build the clover terms and pool the temporaries before graph capture
+    schur_square_shift(c, op, sprec, *ap, **ps[base], *tos, *tes, s0);
+    schur_square_shift(c, op, PREC_D, *u64, bo, *t64, *te64, s0);
+
+    MultishiftState &H = *(MultishiftState *)c->h_state;
+    memset(&H, 0, sizeof(H));
+    H.nshift = nshift;
+    H.base = base;
+    for (int i = 0; i < nshift; ++i) {
+        H.sigma[i] = shifts[i] - s0;
+        H.zeta[i] = H.zeta_prev[i] = 1.0;
+        H.active[i] = 1;
+    }
+    H.rr = bbo;
+    H.rr_max = bbo;
+    H.alpha = 1.0;
+    H.beta = 0.0;
+    H.eps = eps;
+    H.max_iter = max_steps;
+    H.delta2 = sprec == PREC_D ? 0.0 : 0.01;
+    CK(cudaMemcpyAsync(c->d_state, c->h_state, sizeof(MultishiftState), cudaMemcpyHostToDevice, c->st));
+    MultishiftState *S = (MultishiftState *)c->d_state;
+    Gate gate{&S->pause, nullptr};
+    const Spinor pb = **ps[base];
+    const Spinor xb = xs[base].parity(1);
+    auto step = [&]() {
+        schur_square_shift(c, op, sprec, *ap, pb, *tos, *tes, s0, &S->pause);
+        auto go = [&](auto P, auto AP, auto R, auto X) {
+            using VP = decltype(P);
+            using VR = decltype(R);
+            using VX = decltype(X);
+            run_site(c, OpMsAlpha<VP, VP>{P, AP, S}, 1, gate);
+            run_site(c, OpMsResidual<VR, VP>{R, AP, S}, 1, gate);
+            run_site(c, OpMsUpdate<VX, VP, VR>{(VX *)dviews, (VP *)(dviews + kMaxShifts * vbytes), R, S, nshift}, 1,
+                     gate);
+        };
+        if (sprec == PREC_D) go(pb.d(), (*ap).d(), (*r).d(), SpinorD{});
+        else if (sprec == PREC_F) go(pb.f(), (*ap).f(), (*r).f(), SpinorF{});
+        else go(pb.h(), (*ap).h(), (*r).f(), SpinorF{});
+    };
+    auto base_true_res = [&]() {
+        schur_square_shift(c, op, PREC_D, *u64, xb, *t64, *te64, s0);
+        run_site(c, OpSubNorm<SpinorD, SpinorD, SpinorD>{bo.d(), (*u64).d(), (*r64).d(), c->d_scal}, 1);
+        CK(cudaMemcpyAsync(c->h_scal, c->d_scal, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        return c->h_scal[0];
+    };
+    int iters = 0, updates = 0;
+    bool base_done = bbo < eps || bbo == 0.0;
+    std::vector<int> was_active(nshift, 1);
+    if (!base_done && max_steps > 0) {
+        for (int outer = 0; outer < 100000; ++outer) {
+            run_gated_state(c, S, step, 8, (long)max_steps - ((MultishiftState *)c->h_state)->iter + 8);
+            MultishiftState R = *(MultishiftState *)c->h_state;
+            iters = R.iter;
+            if (R.failed) fail(c, LYM_ERR_NUMERIC, "multishift CG produced a non-finite residual");
+            // fold the accumulators of every shift that ran since the last fold
+            for (int i = 0; i < nshift; ++i) {
+                if (!was_active[i]) continue;
+                axpby(c, **acc[i], xs[i].parity(1), C2(1.0), C2(1.0));
+                zero(c, **acc[i]);
+                was_active[i] = R.active[i] != 0;
+            }
+            const double rr = base_true_res();
+            ++updates;
+            if (R.converged && rr < eps) {
+                base_done = true;
+                break;
+            }
+            if (R.iter >= max_steps) break;
+            MultishiftState &W = *(MultishiftState *)c->h_state;
+            W = R;
+            if (R.converged) W.eps = std::max(R.eps * 0.5 * eps / rr, 1e-300);
+            W.beta = rr / R.rr_prev;
+            for (int i = 0; i < nshift; ++i) {
+                if (W.active[i] == 2) W.active[i] = 0;
+                if (W.active[i] == 1) {
+                    const double zr = W.zeta[i] / W.zeta_prev[i];
+                    W.beta_s[i] = W.beta * zr * zr;
+                }
+            }
+            W.active[base] = 1;
+            W.rr = rr;
+            W.rr_max = rr;
+            W.pause = W.stop = W.converged = W.need_update = 0;
+            CK(cudaMemcpyAsync(c->d_state, c->h_state, sizeof(MultishiftState), cudaMemcpyHostToDevice, c->st));
+            copy(c, *r, *r64);
+            auto dir = [&](auto P, auto R2) {
+                using VP = decltype(P);
+                run_site(c, OpMsDirection<VP, decltype(R2)>{(VP *)(dviews + kMaxShifts * vbytes), R2, S, nshift}, 1);
+            };
+            if (sprec == PREC_D) dir(SpinorD{}, (*r).d());
+            else if (sprec == PREC_F) dir(SpinorF{}, (*r).f());
+            else dir(SpinorH{}, (*r).f());
+        }
+    }
+    // refinement: every shift to the FP64 target on its own
+    int rc = LYM_OK;
+    int refine_its = iters;
+    double worst = 0.0;
+    for (int i = 0; i < nshift; ++i) {
+        double rr_i = 0.0;
+        const int budget = std::max(0, max_steps - (refine_its - iters));
+        const int r_i = shift_cg_mixed(c, op, sprec, shifts[i], bo, xs[i].parity(1), eps, budget, refine_its,
+                                       updates, rr_i);
+        if (r_i != LYM_OK) rc = LYM_NOT_CONVERGED;
+        worst = std::max(worst, rr_i);
+    }
+    (void)base_done;
+    if (st) {
+        st->iterations = refine_its;
+        st->steps = iters;
+        st->reliable_updates = updates;
+        st->converged = rc == LYM_OK;
+        st->last_error = worst;
+        const double bb = norm2_now(c, b);
+        st->true_residual = bb > 0 ? std::sqrt(worst / bb) : 0.0;
+    }
     return rc;
 }
 
@@ -2559,6 +2851,9 @@ static int do_multishift(lym_context *c, int op_id, int algorithm, int nshift, c
                 rc = ok ? LYM_OK : LYM_NOT_CONVERGED;
             } else if (algorithm == LYM_MULTISHIFT_MMMR) {
                 rc = multishift_mmmr(c, op, nshift, shifts, precision, max_steps, *b, xv, &local);
+            } else if (algorithm == LYM_MULTISHIFT_CG_MIXED_SINGLE || algorithm == LYM_MULTISHIFT_CG_MIXED_HALF) {
+                const int sp = algorithm == LYM_MULTISHIFT_CG_MIXED_SINGLE ? PREC_F : PREC_H;
+                rc = multishift_cg_mixed(c, op, sp, nshift, shifts, precision, max_steps, *b, xv, &local);
             } else if (algorithm == LYM_MULTISHIFT_CHRONOLOGICAL) {
                 // solutions[i] (i >= 1) hold the chronological guesses on entry
                 for (int i = 1; i < nshift; ++i) upload_vec(c, xv[i], solutions[i], device_ptr, 1);

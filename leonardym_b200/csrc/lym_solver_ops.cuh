@@ -406,6 +406,10 @@ struct MultishiftState {
     double alpha, alpha_prev, beta;
     double eps;                   // per-shift stop: zeta_i^2 rr < eps
     int iter, max_iter, converged, stop;
+    // mixed precision: reliable update of the base system when rr < delta2 * rr_max
+    // (0: never); the step that sets need_update updates x but not the directions
+    double delta2, rr_max;
+    int need_update, failed;
 };
 
 // base alpha = rr / <p, Ap>, then the shifted coefficients (Jegerlehner recursions)
@@ -470,6 +474,13 @@ template <class SR, class SAp> struct OpMsResidual {
         s->beta = rr_new / s->rr;
         s->rr_prev = s->rr;
         s->rr = rr_new;
+        if (rr_new > s->rr_max) s->rr_max = rr_new;
+        if (!(rr_new == rr_new)) {  // NaN: stop before the update
+            s->failed = 1;
+            s->stop = 1;
+            s->pause = 1;
+            return;
+        }
         int any = 0;
         for (int i = 0; i < s->nshift; ++i) {
             if (!s->active[i]) continue;
@@ -486,24 +497,30 @@ template <class SR, class SAp> struct OpMsResidual {
         if (!any) {
             s->converged = 1;
             s->stop = 1;
+            s->need_update = s->delta2 > 0.0;
+        } else if (s->delta2 > 0.0 && rr_new < s->delta2 * s->rr_max) {
+            s->need_update = 1;
+            s->stop = 1;
         } else if (s->iter >= s->max_iter) {
             s->stop = 1;
         }
     }
 };
 
-// per shift: x_i += alpha_i p_i ; p_i = zeta_i r + beta_i p_i  (one launch over all shifts)
-template <class SV> struct OpMsUpdate {
+// per shift: x_i += alpha_i p_i ; p_i = zeta_i r + beta_i p_i  (one launch over all shifts;
+// a step that asks for a reliable update leaves the directions to OpMsDirection)
+template <class SX, class SP = SX, class SR = SX> struct OpMsUpdate {
     static constexpr int NRED = 1;  // no sum; finalize ends the step
-    SV *x;   // device array of nshift views
-    SV *ps;
-    SV r;
+    SX *x;   // device array of nshift views
+    SP *ps;
+    SR r;
     MultishiftState *s;
     int nshift;
     LYM_D void site(int q, int h, double *) const
     {
         cx<double> rv[12];
-        r.par(q).template load<double>(h, rv);
+        const bool dir = !s->need_update;
+        if (dir) r.par(q).template load<double>(h, rv);
         for (int i = 0; i < nshift; ++i) {
             const int act = s->active[i];
             if (!act) continue;
@@ -514,7 +531,7 @@ template <class SV> struct OpMsUpdate {
 #pragma unroll
             for (int k = 0; k < 12; ++k) fma_r(xv[k], ai, pv[k]);
             x[i].par(q).template store<double>(h, xv);
-            if (act == 1) {
+            if (act == 1 && dir) {
                 const double z = s->zeta[i], b = s->beta_s[i];
 #pragma unroll
                 for (int k = 0; k < 12; ++k) pv[k] = z * rv[k] + b * pv[k];
@@ -525,6 +542,29 @@ template <class SV> struct OpMsUpdate {
     LYM_D void finalize(const double *) const
     {
         if (s->stop) s->pause = 1;
+    }
+};
+
+// p_i = zeta_i r + beta_i p_i for the running shifts (after a reliable update of r)
+template <class SP, class SR> struct OpMsDirection {
+    static constexpr int NRED = 0;
+    SP *ps;
+    SR r;
+    MultishiftState *s;
+    int nshift;
+    LYM_D void site(int q, int h, double *) const
+    {
+        cx<double> rv[12];
+        r.par(q).template load<double>(h, rv);
+        for (int i = 0; i < nshift; ++i) {
+            if (s->active[i] != 1) continue;
+            cx<double> pv[12];
+            ps[i].par(q).template load<double>(h, pv);
+            const double z = s->zeta[i], b = s->beta_s[i];
+#pragma unroll
+            for (int k = 0; k < 12; ++k) pv[k] = z * rv[k] + b * pv[k];
+            ps[i].par(q).template store<double>(h, pv);
+        }
     }
 };
 

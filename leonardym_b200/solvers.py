@@ -20,8 +20,11 @@ from ._lib import LymError, SolveStats, lib
 SOLVER_CG, SOLVER_BICGSTAB, SOLVER_EO_BICGSTAB = 0, 1, 2
 SOLVER_EO_CG, SOLVER_EO_CG_MIXED_SINGLE, SOLVER_EO_CG_MIXED_HALF = 3, 4, 5
 SOLVER_EO_BICGSTAB_MIXED_SINGLE, SOLVER_EO_BICGSTAB_MIXED_HALF = 6, 7
+# multishift_cg_mixed_*: the RHMC multishift on SquareEvenOddImprovedDiracWilsonOperator
+# (gamma5) with FP32 / FP16 inner storage, FP64 recurrences and per-shift FP64 true residuals
 MULTISHIFT = {"mass_estrapolation": 0, "minimal_residual": 1, "multishift_cg": 2,
-              "chronological_mass_estrapolation": 3}
+              "chronological_mass_estrapolation": 3, "multishift_cg_mixed_single": 4,
+              "multishift_cg_mixed_half": 5}
 
 
 def _p(a):

@@ -18,7 +18,7 @@ import numpy as np
 __all__ = [
     "volume", "gell_mann", "su3_links", "su2_links", "su2_to_adjoint",
     "antiperiodic_bc", "fermion_links", "gaussian_spinor", "point_source", "z2_source",
-    "lex_coords",
+    "lex_coords", "su3_fermion_links_device", "gaussian_spinor_device",
 ]
 
 
@@ -173,3 +173,61 @@ def z2_source(dims, nc, seed, stream=1 << 21):
     rng = _rng(seed, stream)
     b = rng.integers(0, 2, size=(V, 4, nc, 2)) * 2 - 1
     return np.ascontiguousarray((b[..., 0] + 1j * b[..., 1]) / np.sqrt(2.0))
+
+
+def _reunit_torch(U):
+    """_reunit on a batch of torch matrices (rows Gram-Schmidt, then the det phase)."""
+    import torch
+
+    U = U.clone()
+    n = U.shape[-1]
+    for i in range(n):
+        for j in range(i):
+            proj = (U[:, j, :].conj() * U[:, i, :]).sum(-1)
+            U[:, i, :] -= proj[:, None] * U[:, j, :]
+        nv = (U[:, i, :].abs() ** 2).sum(-1).sqrt()
+        U[:, i, :] /= nv[:, None]
+    a = U
+    d = (a[:, 0, 0] * (a[:, 1, 1] * a[:, 2, 2] - a[:, 1, 2] * a[:, 2, 1])
+         - a[:, 0, 1] * (a[:, 1, 0] * a[:, 2, 2] - a[:, 1, 2] * a[:, 2, 0])
+         + a[:, 0, 2] * (a[:, 1, 0] * a[:, 2, 1] - a[:, 1, 1] * a[:, 2, 0]))
+    U[:, n - 1, :] *= torch.exp(-1j * torch.angle(d))[:, None]
+    return U
+
+
+def su3_fermion_links_device(dims, eps, seed, device, chunk=1 << 22):
+    """SU(3) fermion links on a CUDA device: U = exp(i eps H), H = sum_a h_a lambda_a with
+    h_a ~ N(0,1) from torch's seeded device generator, reunitarised, antiperiodic in time
+    (U_t negated at t = Lt-1).  The distribution of su3_links + antiperiodic_bc, for lattices
+    whose host generation would take minutes; not the same numbers.  Returns a torch
+    complex128 tensor [V, 4, 3, 3] in the column-major link layout."""
+    import torch
+
+    V = volume(dims)
+    n = 4 * V
+    out = torch.empty((V, 4, 3, 3), dtype=torch.complex128, device=device)
+    flat = out.view(n, 3, 3)
+    lam = torch.from_numpy(gell_mann()).to(device=device, dtype=torch.complex128)
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    for c0 in range(0, n, chunk):
+        c1 = min(n, c0 + chunk)
+        h = torch.randn((c1 - c0, 8), generator=g, device=device, dtype=torch.float64)
+        H = torch.einsum("na,aij->nij", h.to(torch.complex128), lam)
+        U = _reunit_torch(torch.linalg.matrix_exp(1j * float(eps) * H))
+        flat[c0:c1] = U.transpose(-1, -2)
+        del h, H, U
+    Lt = int(dims[3])
+    out.view(-1, Lt, 4, 3, 3)[:, Lt - 1, 3] *= -1
+    return out
+
+
+def gaussian_spinor_device(dims, nc, seed, device):
+    """Complex-normal spinor (E|z|^2 = 1 per component) from torch's seeded device generator,
+    as a torch complex128 tensor [V, 4, nc]."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    a = torch.randn((volume(dims), 4, nc, 2), generator=g, device=device, dtype=torch.float64) * np.sqrt(0.5)
+    return torch.view_as_complex(a).contiguous()

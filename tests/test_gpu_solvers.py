@@ -275,3 +275,38 @@ def test_multishift_chronological(setup, oracle):
         assert true_res(orc, b2, x, s) < 1.5e-10
         assert rel(x, xo) < 1e-7
     assert ms.stats.iterations < first_iters
+
+
+@pytest.mark.parametrize("mode", ["single", "half"])
+def test_multishift_cg_mixed(setup, oracle, mode):
+    # RHMC multishift on the squared even-odd operator: FP32 / FP16 inner storage, FP64
+    # recurrences; every shift's FP64 true residual <= 1e-10 and the solutions equal the
+    # oracle's FP64 mass-estrapolation solutions
+    b = setup["b"]
+    shifts = list(np.logspace(-4, 0, 12))
+    eps = (1e-10) ** 2 * float(np.vdot(b, b).real)
+    op = gpu_op(setup, L.SquareEvenOddImprovedDiracWilsonOperator)
+    ms = L.MultishiftSolver.getInstance(f"multishift_cg_mixed_{mode}")
+    ms.setPrecision(eps)
+    ms.setMaxSteps(10000)
+    sols = []
+    assert ms.solve(op, b, sols, shifts)
+    assert ms.stats.true_residual <= 1e-10
+    assert ms.stats.reliable_updates >= 1
+    orc = oracle.Operator(setup["geom"], setup["links"], "SquareEvenOddImproved", setup["kappa"], setup["csw"],
+                          True)
+    rc, osols, _ = oracle.me_multishift(orc, b, shifts, eps, 10000)
+    assert rc == 1
+    for x, xo, s in zip(sols, osols, shifts):
+        assert true_res(orc, b, x, s) <= 1.05e-10
+        assert rel(x, xo) < 1e-7
+
+
+def test_multishift_cg_mixed_needs_rhmc_operator(setup):
+    op = gpu_op(setup, L.SquareImprovedDiracWilsonOperator)
+    ms = L.MultishiftSolver.getInstance("multishift_cg_mixed_single")
+    with pytest.raises(L.LymError):
+        ms.solve(op, setup["b"], [], [0.1, 0.01])
+    op = gpu_op(setup, L.SquareEvenOddImprovedDiracWilsonOperator)
+    with pytest.raises(L.LymError):
+        ms.solve(op, setup["b"], [], [-1.0, 0.01])
