@@ -45,6 +45,10 @@ STENCIL_RHS_BYTES = {1: 3 * 96, 2: 3 * 52}
 STENCIL_FLOPS = 1320 + 504 + 48  # hopping + clover apply + xpay, per site
 
 
+def log(msg):
+    print(msg, file=sys.stderr, flush=True)
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -508,12 +512,162 @@ def run_ours(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+RHMC_DIMS = (48, 48, 48, 96)
+RHMC_KAPPA, RHMC_CSW, RHMC_EPS, RHMC_SEED = 0.1365, 1.7, 0.25, 1239
+RHMC_SHIFTS = list(np.logspace(-4, 0, 12))
+RHMC_METRIC = "RHMC multishift solves/s @48^3x96, 12 shifts to res 1e-10 (FP16 inner vs FP64)"
+
+
+def run_rhmc(args, world, rank, local, dims=RHMC_DIMS):
+    """The configs' RHMC case: SU(3) Wilson-clover 48^3x96, kappa 0.1365, c_sw 1.7, 12 shifts
+    log-spaced in [1e-4, 1] on the squared even-odd operator (the RHMC operator), every
+    shift to a FP64 true residual 1e-10; one step = one multishift solve of one
+    complex-normal source.  Links and source are seeded on the device (the host generator
+    would take minutes at 10.6M sites)."""
+    import torch
+
+    import leonardym_b200 as L
+    from leonardym_b200 import synth
+    from leonardym_b200.solvers import MULTISHIFT
+
+    lib = L.lib()
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    prec = args.precision or "half"
+    algo = MULTISHIFT[f"multishift_cg_mixed_{prec}"]
+    lat = L.Lattice(dims, "su3", device=local)
+    ctx = lat.handle
+    links = synth.su3_fermion_links_device(dims, RHMC_EPS, RHMC_SEED, dev)
+    if lib.lym_gauge_upload_device(ctx, 1, C.c_void_p(links.data_ptr())) != 0:
+        raise RuntimeError(lib.lym_last_error(ctx))
+    del links
+    torch.cuda.empty_cache()
+    opid = C.c_int(0)
+    if lib.lym_operator_create(ctx, 1, 5, RHMC_KAPPA, RHMC_CSW, 1, C.byref(opid)) != 0:
+        raise RuntimeError(lib.lym_last_error(ctx))
+    opid = opid.value
+    b = synth.gaussian_spinor_device(dims, 3, RHMC_SEED + 1, dev)
+    bb = float(torch.vdot(b.flatten(), b.flatten()).real)
+    eps = TOL * TOL * bb
+    nsh = len(RHMC_SHIFTS)
+    sh = np.ascontiguousarray(RHMC_SHIFTS, dtype=np.float64)
+    sols = [torch.zeros_like(b) for _ in range(nsh)]
+    ptrs = (C.c_void_p * nsh)(*[x.data_ptr() for x in sols])
+    st = L.SolveStats()
+
+    def solve(algorithm=algo, src=b, out=ptrs, device=True):
+        fn = lib.lym_multishift_device if device else lib.lym_multishift
+        rc = fn(ctx, opid, algorithm, nsh, sh.ctypes.data_as(C.c_void_p), eps, 20000,
+                C.c_void_p(src if isinstance(src, int) else src.data_ptr()), out, C.byref(st))
+        if rc != 0:
+            raise RuntimeError(f"multishift failed: {rc} {lib.lym_last_error(ctx)}")
+        if st.true_residual > TOL:
+            raise RuntimeError(f"multishift true residual {st.true_residual:.3e} > {TOL}")
+        return st.seconds, st.steps, st.iterations
+
+    for _ in range(args.warmup):
+        log(f"rhmc: warm-up solve {solve()}")
+    sampler = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    lib.lym_synchronize(ctx)
+    launches0 = lib.lym_context_kernel_launches(ctx)
+    sampler.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    rec = [solve() for _ in range(args.steps)]
+    lib.lym_synchronize(ctx)
+    ev1.record()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = int(lib.lym_context_kernel_launches(ctx) - launches0)
+    elapsed = max_over_ranks(world, ev0.elapsed_time(ev1) / 1e3)
+    value = world * args.steps / elapsed
+
+    # every shift's true residual, re-measured with the FP64 multiplyAdd of the operator
+    out = torch.empty_like(b)
+    worst = 0.0
+    for x, s in zip(sols, RHMC_SHIFTS):
+        lib.lym_multiply_add_device(ctx, opid, C.c_void_p(out.data_ptr()), C.c_void_p(x.data_ptr()),
+                                    C.c_void_p(x.data_ptr()), float(s), 0.0)
+        worst = max(worst, float(torch.linalg.vector_norm((b - out).flatten())) / np.sqrt(bb))
+    if worst > 1.02 * TOL:
+        raise RuntimeError(f"re-measured true residual {worst:.3e}")
+
+    # end to end: pinned host source and solutions, copies inside the timed region
+    nbytes = lat.V * 24 * 8
+    log(f"rhmc: timed {args.steps} solves in {elapsed:.2f} s; end to end with pinned host buffers")
+    hsrc = lib.lym_host_alloc(nbytes)
+    hsol = [lib.lym_host_alloc(nbytes) for _ in range(nsh)]
+    if not hsrc or not all(hsol):
+        for p in [hsrc] + hsol:
+            lib.lym_host_free(p)
+        raise RuntimeError(f"pinned host allocation of {(nsh + 1) * nbytes / 1e9:.1f} GB failed")
+    bh = b.cpu().numpy()
+    C.memmove(hsrc, bh.ctypes.data, nbytes)
+    del bh
+    hptrs = (C.c_void_p * nsh)(*hsol)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        solve(src=hsrc, out=hptrs, device=False)
+    lib.lym_synchronize(ctx)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_value = world * args.steps / max_over_ranks(world, e0.elapsed_time(e1) / 1e3)
+    for p in [hsrc] + hsol:
+        lib.lym_host_free(p)
+
+    # the plain FP64 multishift CG on the same system (one solve)
+    log("rhmc: FP64 multishift CG")
+    fp64 = solve(algorithm=MULTISHIFT["multishift_cg"])
+    # dominant kernel: the Schur stencil with the clover term in the inner precision
+    sp = 1 if prec == "single" else 2
+    ms = C.c_double(0)
+    lib.lym_time_stencil(ctx, opid, sp, 0, 30, C.byref(ms))
+    Vh = lat.V // 2
+    achieved = STENCIL_BYTES[sp] * Vh / (ms.value * 1e-3) / 1e9
+    pk = peaks()
+    lat.close()
+    if rank != 0:
+        return
+    line = {
+        "metric": RHMC_METRIC, "value": value, "unit": "multishift solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16" if sp == 2 else "f32",
+        "data": "synthetic (links and source seeded on the device)",
+        "config": {"workload": "su3-clover-48^3x96-kappa0.1365-csw1.7-12shifts-tol1e-10",
+                   "lattice": "x".join(str(d) for d in dims), "operator": "SquareEvenOddImproved (gamma5)",
+                   "shifts": "12, log-spaced in [1e-4, 1]", "solver": f"multishift_cg_mixed_{prec}",
+                   "l2": "inputs larger than L2: FP64 links 6.1 GB, spinors 2 GB each",
+                   "parallelism": "replicas (one independent solve stream per GPU)"},
+        "multishift_steps": [r[1] for r in rec], "total_iterations": [r[2] for r in rec],
+        "worst_true_residual": worst,
+        "fp64_multishift_cg_solves_per_s": 1.0 / fp64[0], "fp64_multishift_cg_iterations": fp64[2],
+        "mixed_over_fp64": value / world * fp64[0],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / pk["hbm_gbs"], "traffic": None,
+                     "kernel": f"Schur stencil with clover, {prec} storage, {ms.value * 1e3:.1f} us/launch",
+                     "algorithmic_bytes_per_launch": STENCIL_BYTES[sp] * Vh,
+                     "peak_source": f"{pk['which']} hbm_gbs"},
+        "clocks": clocks, "gpu_launches": launches,
+        "e2e": {"value": e2e_value, "unit": "multishift solves/s", "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": nsh * nbytes},
+        "cpu_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_profile(args):
     """Small fixed case for ncu captures: one block solve of the benchmark's first
     `batch` noise sources, then 10 launches each of the single-RHS and the batched
     stencil kernels (a few GB on the device)."""
     import leonardym_b200 as L
     lib = L.lib()
+    if args.workload.startswith("rhmc"):
+        return run_profile_rhmc(args)
     lat = L.Lattice(DIMS, "su3", device=0)
     op = L.ImprovedDiracWilsonOperator(lat, KAPPA, CSW, gamma5=False)
     op.setLattice(workload_links())
@@ -543,13 +697,50 @@ def run_profile(args):
         sys.exit(1)
 
 
+def run_profile_rhmc(args):
+    """Small case for ncu captures of the RHMC multishift: one solve of the 12-shift system
+    on 24^3x48 (links and source seeded on the device, about 10 GB on the device)."""
+    import torch
+
+    import leonardym_b200 as L
+    from leonardym_b200 import synth
+    from leonardym_b200.solvers import MULTISHIFT
+    lib = L.lib()
+    prec = args.precision or "half"
+    lat = L.Lattice(DIMS, "su3", device=0)
+    ctx = lat.handle
+    links = synth.su3_fermion_links_device(DIMS, RHMC_EPS, RHMC_SEED, "cuda:0")
+    lib.lym_gauge_upload_device(ctx, 1, C.c_void_p(links.data_ptr()))
+    del links
+    opid = C.c_int(0)
+    lib.lym_operator_create(ctx, 1, 5, RHMC_KAPPA, RHMC_CSW, 1, C.byref(opid))
+    b = synth.gaussian_spinor_device(DIMS, 3, RHMC_SEED + 1, "cuda:0")
+    bb = float(torch.vdot(b.flatten(), b.flatten()).real)
+    sols = [torch.zeros_like(b) for _ in RHMC_SHIFTS]
+    ptrs = (C.c_void_p * len(sols))(*[x.data_ptr() for x in sols])
+    sh = np.ascontiguousarray(RHMC_SHIFTS, dtype=np.float64)
+    st = L.SolveStats()
+    rc = lib.lym_multishift_device(ctx, opid.value, MULTISHIFT[f"multishift_cg_mixed_{prec}"], len(sols),
+                                   sh.ctypes.data_as(C.c_void_p), TOL * TOL * bb, 20000, C.c_void_p(b.data_ptr()),
+                                   ptrs, C.byref(st))
+    print(f"rhmc profile case: rc {rc}, {st.seconds:.3f} s, multishift steps {st.steps}, iterations "
+          f"{st.iterations}, reliable updates {st.reliable_updates}, true residual {st.true_residual:.2e}")
+    lat.close()
+    if rc != 0:
+        sys.exit(1)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="single", choices=["single", "half"])
+    ap.add_argument("--precision", default=None, choices=["single", "half"],
+                    help="inner storage (default: single for the propagator solves, half for rhmc)")
+    ap.add_argument("--workload", default="propagators", choices=["propagators", "rhmc", "rhmc-small"],
+                    help="propagators: the 24^3x48 block solves (the headline); rhmc: the 48^3x96 multishift; "
+                         "rhmc-small: the same at 24^3x48")
     ap.add_argument("--solver", default="bicgstab", choices=["cg", "bicgstab"],
                     help="the block solver of the timed solves")
     ap.add_argument("--batch", type=int, default=16, help="right-hand sides per batched stencil (power of 2 <= 32)")
@@ -559,6 +750,8 @@ def main():
                     help="seconds of Poisson arrivals for the serving measurement (0: skip it)")
     ap.add_argument("--tile", default="", help="with --profile: batched stencil column and variant 'by,bz,minb'")
     args = ap.parse_args()
+    if args.workload == "propagators" and args.precision is None:
+        args.precision = "single"
     if args.profile:
         run_profile(args)
         return
@@ -566,6 +759,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.workload.startswith("rhmc"):
+            run_rhmc(args, world, rank, local, RHMC_DIMS if args.workload == "rhmc" else DIMS)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -92,7 +92,8 @@ enum lym_multishift_solver {
      * reliable updates of the base system, then mixed-precision CG per shift until every
      * |b - (A + shifts[i]) x_i|^2 < precision in FP64 (stats->true_residual: the largest,
      * relative to |b|; stats->steps: iterations of the shared Krylov space, stats->iterations:
-     * those plus the per-shift refinement); other operator kinds: LYM_ERR_UNSUPPORTED */
+     * those plus the per-shift refinement; max_steps bounds the sum); other operator kinds:
+     * LYM_ERR_UNSUPPORTED */
     LYM_MULTISHIFT_CG_MIXED_SINGLE = 4,
     LYM_MULTISHIFT_CG_MIXED_HALF = 5
 };

@@ -88,6 +88,8 @@ struct lym_context {
 namespace {
 
 constexpr size_t kStateBytes = 8192;
+static_assert(sizeof(MultishiftState) <= kStateBytes, "state buffer too small");
+static_assert(sizeof(CGState) <= kStateBytes && sizeof(BiCGState) <= kStateBytes, "state buffer too small");
 
 int fail(lym_context *c, int code, const char *fmt, ...)
 {
@@ -1007,14 +1009,17 @@ int shift_cg_mixed(lym_context *c, OpEntry &op, int sprec, double sigma, const S
 // Mixed-precision multishift CG for the RHMC operator (SquareEvenOddImproved with gamma5:
 // odd <- (G5 S)^2 x_o, even <- x_e; NFlavorFermionAction's multishift on the squared
 // operator, actions/NFlavorFermionAction.cpp:76-96).  Even sites: x_e = b_e / (1 + sigma_i).
-// Odd sites: one Krylov space on the smallest shift with the directions p_i and the
-// operator applications in `sprec`, the residual and the per-shift solution accumulators in
-// FP32, the shift recurrences (Jegerlehner) and every inner product in FP64.  Whenever the
-// base residual falls by delta = 0.1, the accumulators are added to the FP64 solutions, the
-// base residual is recomputed in FP64 and the directions are rebuilt from it (shifted
-// residuals stay zeta_i r).  Then each shift whose FP64 true residual misses eps is refined
-// by shift_cg_mixed from its multishift solution.  eps: |b - (A + sigma_i) x_i|^2 (FP64).
-int multishift_cg_mixed(lym_context *c, OpEntry &op, int sprec, int nshift, const double *shifts, double eps,
+// Odd sites: one Krylov space on the smallest shift, FP32 storage and operator, the shift
+// recurrences (Jegerlehner) and every inner product in FP64.  The shifted x_i and p_i are not
+// touched every step: each step records its residual in a ring of kMsWin + 1 slots and
+// updates, per shift, the coefficients of x_i and p_i on the window's residuals; one pass per
+// window (ms_flush_kernel) applies them, so a step streams the base system's vectors only.
+// Whenever the base residual falls by delta = 0.1, the FP32 accumulators are added to the
+// FP64 solutions, the base residual is recomputed in FP64 and the directions are rebuilt from
+// it (shifted residuals stay zeta_i r).  Then every shift whose FP64 true residual misses eps
+// is refined by shift_cg_mixed in `rprec` from its multishift solution.
+// eps: |b - (A + sigma_i) x_i|^2 (FP64).
+int multishift_cg_mixed(lym_context *c, OpEntry &op, int rprec, int nshift, const double *shifts, double eps,
                         int max_steps, const Spinor &b, std::vector<Spinor> &xs, lym_solve_stats *st)
 {
     if (op.kind != LYM_OP_SQUARE_EVEN_ODD_IMPROVED || !op.gamma5)
@@ -1025,7 +1030,6 @@ int multishift_cg_mixed(lym_context *c, OpEntry &op, int sprec, int nshift, cons
     for (int i = 0; i < nshift; ++i)
         if (!(1.0 + shifts[i] != 0.0) || !std::isfinite(shifts[i]))
             fail(c, LYM_ERR_ARGUMENT, "multishift: shift %d = %g gives a singular even-site system", i, shifts[i]);
-    const int aprec = sprec == PREC_H ? PREC_F : sprec;
     int base = 0;
     for (int i = 1; i < nshift; ++i)
         if (shifts[i] < shifts[base]) base = i;
@@ -1036,56 +1040,75 @@ int multishift_cg_mixed(lym_context *c, OpEntry &op, int sprec, int nshift, cons
         zero(c, xs[i].parity(1));
     }
     const double bbo = norm2_now(c, bo);
-    Vec r(c, aprec, 1), ap(c, sprec, 1), tos(c, sprec, 1), tes(c, sprec, 1);
+    Vec ap(c, PREC_F, 1), tos(c, PREC_F, 1), tes(c, PREC_F, 1);
     Vec r64(c, PREC_D, 1), t64(c, PREC_D, 1), u64(c, PREC_D, 1), te64(c, PREC_D, 1);
-    std::vector<Vec *> ps, acc;
-    struct Views {
-        std::vector<Vec *> &ps, &acc;
-        ~Views()
+    std::vector<Vec *> owned;
+    struct Owner {
+        std::vector<Vec *> &v;
+        ~Owner()
         {
-            for (auto v : ps) delete v;
-            for (auto v : acc) delete v;
+            for (auto p : v) delete p;
         }
-    } owner{ps, acc};
+    } owner{owned};
+    auto fresh = [&]() {
+        owned.push_back(new Vec(c, PREC_F, 1));
+        return **owned.back();
+    };
+    std::vector<SpinorF> hring(kMsWin + 1), hacc(nshift), hp(nshift);
+    for (int j = 0; j <= kMsWin; ++j) hring[j] = fresh().f();
     for (int i = 0; i < nshift; ++i) {
-        ps.push_back(new Vec(c, sprec, 1));
-        acc.push_back(new Vec(c, aprec, 1));
-        copy(c, **ps.back(), bo);
-        zero(c, **acc.back());
+        const Spinor a = fresh(), p = fresh();
+        zero(c, a);
+        copy(c, p, bo);
+        hacc[i] = a.f();
+        hp[i] = p.f();
     }
-    copy(c, *r, bo);
-    // device arrays of the per-shift views: accumulators at 0, directions at kMaxShifts
-    const size_t vbytes = std::max(sizeof(SpinorH), sizeof(SpinorD));
-    char *dviews = (char *)dev_alloc(c, 2 * kMaxShifts * vbytes);
+    // ring slot 0 holds r_0 = b_o
+    {
+        Spinor r0 = **owned.front();
+        copy(c, r0, bo);
+    }
+    // device arrays of views: ring, accumulators, directions
+    const size_t vb = sizeof(SpinorF);
+    const size_t nview = (kMsWin + 1) + 2 * kMaxShifts;
+    char *dviews = (char *)dev_alloc(c, nview * vb);
     struct ViewsMem {
         lym_context *c;
         void *p;
         size_t n;
         ~ViewsMem() { dev_free(c, p, n); }
-    } vmem{c, dviews, 2 * kMaxShifts * vbytes};
-    auto upload_views = [&](auto tag_x, auto tag_p) {
-        using VX = decltype(tag_x);
-        using VP = decltype(tag_p);
-        std::vector<VX> hx(nshift);
-        std::vector<VP> hp(nshift);
-        for (int i = 0; i < nshift; ++i) {
-            const Spinor &a = **acc[i], &p = **ps[i];
-            if constexpr (std::is_same<VX, SpinorD>::value) hx[i] = a.d(); else hx[i] = a.f();
-            if constexpr (std::is_same<VP, SpinorD>::value) hp[i] = p.d();
-            else if constexpr (std::is_same<VP, SpinorF>::value) hp[i] = p.f();
-            else hp[i] = p.h();
-        }
-        CK(cudaMemcpyAsync(dviews, hx.data(), nshift * sizeof(VX), cudaMemcpyHostToDevice, c->st));
-        CK(cudaMemcpyAsync(dviews + kMaxShifts * vbytes, hp.data(), nshift * sizeof(VP), cudaMemcpyHostToDevice,
-                           c->st));
-        CK(cudaStreamSynchronize(c->st));
+    } vmem{c, dviews, nview * vb};
+    SpinorF *d_ring = (SpinorF *)dviews;
+    SpinorF *d_acc = d_ring + (kMsWin + 1);
+    SpinorF *d_p = d_acc + kMaxShifts;
+    CK(cudaMemcpyAsync(d_ring, hring.data(), (kMsWin + 1) * vb, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(d_acc, hacc.data(), nshift * vb, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(d_p, hp.data(), nshift * vb, cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    auto pview = [&](int i) {
+        Spinor v;
+        v.prec = PREC_F;
+        v.nparity = 1;
+        v.stride = c->g.stride;
+        v.v = hp[i].v;
+        return v;
     };
-    if (sprec == PREC_D) upload_views(SpinorD{}, SpinorD{});
-    else if (sprec == PREC_F) upload_views(SpinorF{}, SpinorF{});
-    else upload_views(SpinorF{}, SpinorH{});
+    auto ring_view = [&](int k) {
+        Spinor v;
+        v.prec = PREC_F;
+        v.nparity = 1;
+        v.stride = c->g.stride;
+        v.v = hring[k % (kMsWin + 1)].v;
+        return v;
+    };
+    // the base direction of the current step (the operator's input); P_base holds it as of
+    // the window start, like every other shift's P_i
+    Vec pcur(c, PREC_F, 1);
+    copy(c, *pcur, bo);
+    const Spinor pb = *pcur;
 
     // build the clover terms and pool the temporaries before graph capture
-    schur_square_shift(c, op, sprec, *ap, **ps[base], *tos, *tes, s0);
+    schur_square_shift(c, op, PREC_F, *ap, pb, *tos, *tes, s0);
     schur_square_shift(c, op, PREC_D, *u64, bo, *t64, *te64, s0);
 
     MultishiftState &H = *(MultishiftState *)c->h_state;
@@ -1096,6 +1119,7 @@ int multishift_cg_mixed(lym_context *c, OpEntry &op, int sprec, int nshift, cons
         H.sigma[i] = shifts[i] - s0;
         H.zeta[i] = H.zeta_prev[i] = 1.0;
         H.active[i] = 1;
+        H.cp[i][0] = 1.0;
     }
     H.rr = bbo;
     H.rr_max = bbo;
@@ -1103,26 +1127,25 @@ int multishift_cg_mixed(lym_context *c, OpEntry &op, int sprec, int nshift, cons
     H.beta = 0.0;
     H.eps = eps;
     H.max_iter = max_steps;
-    H.delta2 = sprec == PREC_D ? 0.0 : 0.01;
+    H.delta2 = 0.01;
     CK(cudaMemcpyAsync(c->d_state, c->h_state, sizeof(MultishiftState), cudaMemcpyHostToDevice, c->st));
     MultishiftState *S = (MultishiftState *)c->d_state;
     Gate gate{&S->pause, nullptr};
-    const Spinor pb = **ps[base];
     const Spinor xb = xs[base].parity(1);
+    int nstep = 0;
+    const int fgrid = std::min((c->g.Vh + kMsFlushThreads - 1) / kMsFlushThreads, 4 * 148);
+    auto flush = [&]() {
+        MsFlushArg fa{d_ring, d_acc, d_p, S, nshift, c->g.Vh};
+        ms_flush_kernel<<<fgrid, kMsFlushThreads, 0, c->st>>>(fa);
+        ms_window_reset_kernel<<<1, 32, 0, c->st>>>(S, nshift);
+        count(c, 2);
+    };
     auto step = [&]() {
-        schur_square_shift(c, op, sprec, *ap, pb, *tos, *tes, s0, &S->pause);
-        auto go = [&](auto P, auto AP, auto R, auto X) {
-            using VP = decltype(P);
-            using VR = decltype(R);
-            using VX = decltype(X);
-            run_site(c, OpMsAlpha<VP, VP>{P, AP, S}, 1, gate);
-            run_site(c, OpMsResidual<VR, VP>{R, AP, S}, 1, gate);
-            run_site(c, OpMsUpdate<VX, VP, VR>{(VX *)dviews, (VP *)(dviews + kMaxShifts * vbytes), R, S, nshift}, 1,
-                     gate);
-        };
-        if (sprec == PREC_D) go(pb.d(), (*ap).d(), (*r).d(), SpinorD{});
-        else if (sprec == PREC_F) go(pb.f(), (*ap).f(), (*r).f(), SpinorF{});
-        else go(pb.h(), (*ap).h(), (*r).f(), SpinorF{});
+        schur_square_shift(c, op, PREC_F, *ap, pb, *tos, *tes, s0, &S->pause);
+        run_site(c, OpMsAlpha<SpinorF, SpinorF>{pb.f(), (*ap).f(), S}, 1, gate);
+        run_site(c, OpMsResidualRing<SpinorF>{d_ring, (*ap).f(), S}, 1, gate);
+        run_site(c, OpMsBaseDirection<SpinorF>{d_ring, pb.f(), S}, 1, gate);
+        if (++nstep % kMsWin == 0) flush();
     };
     auto base_true_res = [&]() {
         schur_square_shift(c, op, PREC_D, *u64, xb, *t64, *te64, s0);
@@ -1132,27 +1155,25 @@ int multishift_cg_mixed(lym_context *c, OpEntry &op, int sprec, int nshift, cons
         return c->h_scal[0];
     };
     int iters = 0, updates = 0;
-    bool base_done = bbo < eps || bbo == 0.0;
     std::vector<int> was_active(nshift, 1);
-    if (!base_done && max_steps > 0) {
+    if (!(bbo < eps || bbo == 0.0) && max_steps > 0) {
         for (int outer = 0; outer < 100000; ++outer) {
-            run_gated_state(c, S, step, 8, (long)max_steps - ((MultishiftState *)c->h_state)->iter + 8);
+            nstep = 0;
+            run_gated_state(c, S, step, kMsWin, (long)max_steps - ((MultishiftState *)c->h_state)->iter + kMsWin);
             MultishiftState R = *(MultishiftState *)c->h_state;
             iters = R.iter;
             if (R.failed) fail(c, LYM_ERR_NUMERIC, "multishift CG produced a non-finite residual");
             // fold the accumulators of every shift that ran since the last fold
             for (int i = 0; i < nshift; ++i) {
                 if (!was_active[i]) continue;
-                axpby(c, **acc[i], xs[i].parity(1), C2(1.0), C2(1.0));
-                zero(c, **acc[i]);
+                const Spinor a = **owned[(kMsWin + 1) + 2 * i];
+                axpby(c, a, xs[i].parity(1), C2(1.0), C2(1.0));
+                zero(c, a);
                 was_active[i] = R.active[i] != 0;
             }
             const double rr = base_true_res();
             ++updates;
-            if (R.converged && rr < eps) {
-                base_done = true;
-                break;
-            }
+            if (R.converged && rr < eps) break;
             if (R.iter >= max_steps) break;
             MultishiftState &W = *(MultishiftState *)c->h_state;
             W = R;
@@ -1170,14 +1191,10 @@ int multishift_cg_mixed(lym_context *c, OpEntry &op, int sprec, int nshift, cons
             W.rr_max = rr;
             W.pause = W.stop = W.converged = W.need_update = 0;
             CK(cudaMemcpyAsync(c->d_state, c->h_state, sizeof(MultishiftState), cudaMemcpyHostToDevice, c->st));
-            copy(c, *r, *r64);
-            auto dir = [&](auto P, auto R2) {
-                using VP = decltype(P);
-                run_site(c, OpMsDirection<VP, decltype(R2)>{(VP *)(dviews + kMaxShifts * vbytes), R2, S, nshift}, 1);
-            };
-            if (sprec == PREC_D) dir(SpinorD{}, (*r).d());
-            else if (sprec == PREC_F) dir(SpinorF{}, (*r).f());
-            else dir(SpinorH{}, (*r).f());
+            const Spinor rcur = ring_view(R.iter);
+            copy(c, rcur, *r64);
+            run_site(c, OpMsDirection<SpinorF, SpinorF>{d_p, rcur.f(), S, nshift}, 1);
+            copy(c, *pcur, pview(base));
         }
     }
     // refinement: every shift to the FP64 target on its own
@@ -1186,13 +1203,12 @@ int multishift_cg_mixed(lym_context *c, OpEntry &op, int sprec, int nshift, cons
     double worst = 0.0;
     for (int i = 0; i < nshift; ++i) {
         double rr_i = 0.0;
-        const int budget = std::max(0, max_steps - (refine_its - iters));
-        const int r_i = shift_cg_mixed(c, op, sprec, shifts[i], bo, xs[i].parity(1), eps, budget, refine_its,
+        const int budget = std::max(0, max_steps - refine_its);
+        const int r_i = shift_cg_mixed(c, op, rprec, shifts[i], bo, xs[i].parity(1), eps, budget, refine_its,
                                        updates, rr_i);
         if (r_i != LYM_OK) rc = LYM_NOT_CONVERGED;
         worst = std::max(worst, rr_i);
     }
-    (void)base_done;
     if (st) {
         st->iterations = refine_its;
         st->steps = iters;
@@ -2852,8 +2868,11 @@ static int do_multishift(lym_context *c, int op_id, int algorithm, int nshift, c
             } else if (algorithm == LYM_MULTISHIFT_MMMR) {
                 rc = multishift_mmmr(c, op, nshift, shifts, precision, max_steps, *b, xv, &local);
             } else if (algorithm == LYM_MULTISHIFT_CG_MIXED_SINGLE || algorithm == LYM_MULTISHIFT_CG_MIXED_HALF) {
-                const int sp = algorithm == LYM_MULTISHIFT_CG_MIXED_SINGLE ? PREC_F : PREC_H;
-                rc = multishift_cg_mixed(c, op, sp, nshift, shifts, precision, max_steps, *b, xv, &local);
+                // the shared Krylov space runs in FP32 for both: the precision of its operator
+                // bounds the accuracy of every shifted solution (FP16 leaves them near 1e-3, FP32
+                // near 1e-7), and the refinement from there is what the storage choice saves on
+                const int rp = algorithm == LYM_MULTISHIFT_CG_MIXED_SINGLE ? PREC_F : PREC_H;
+                rc = multishift_cg_mixed(c, op, rp, nshift, shifts, precision, max_steps, *b, xv, &local);
             } else if (algorithm == LYM_MULTISHIFT_CHRONOLOGICAL) {
                 // solutions[i] (i >= 1) hold the chronological guesses on entry
                 for (int i = 1; i < nshift; ++i) upload_vec(c, xv[i], solutions[i], device_ptr, 1);

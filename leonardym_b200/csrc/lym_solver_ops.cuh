@@ -391,6 +391,7 @@ template <class SX, class SP, class SS, class ST, class SR, class SH> struct OpB
 
 // ------------------------------------------------------ multishift CG ------
 constexpr int kMaxShifts = 32;
+constexpr int kMsWin = 8;  // steps per windowed update of the shifted x_i and p_i
 
 struct MultishiftState {
     int pause;                    // first word: gates every captured kernel
@@ -410,6 +411,12 @@ struct MultishiftState {
     // (0: never); the step that sets need_update updates x but not the directions
     double delta2, rr_max;
     int need_update, failed;
+    // windowed updates: the step within the window and, per shift, the coefficients of
+    // x_i - x_i(window start) and of p_i on P_i (p_i at the window start, slot 0) and on
+    // the window's residuals R_0..R_{win-1} (slots 1..win)
+    int win;
+    int xupd[kMaxShifts], pupd[kMaxShifts];
+    double cx[kMaxShifts][kMsWin + 1], cp[kMaxShifts][kMsWin + 1];
 };
 
 // base alpha = rr / <p, Ap>, then the shifted coefficients (Jegerlehner recursions)
@@ -450,6 +457,47 @@ template <class SP, class SAp> struct OpMsAlpha {
     }
 };
 
+// After r_{k+1}: beta, the shifted betas, per-shift convergence, reliable-update and stop
+// flags.  False when the residual is not finite (the state is paused).
+LYM_D bool ms_residual_step(MultishiftState *s, double rr_new)
+{
+    s->iter += 1;
+    s->beta = rr_new / s->rr;
+    s->rr_prev = s->rr;
+    s->rr = rr_new;
+    if (rr_new > s->rr_max) s->rr_max = rr_new;
+    if (!(rr_new == rr_new)) {  // NaN: stop before the update
+        s->failed = 1;
+        s->stop = 1;
+        s->pause = 1;
+        return false;
+    }
+    int any = 0;
+    for (int i = 0; i < s->nshift; ++i) {
+        if (!s->active[i]) continue;
+        // residual of shift i after this step: zeta_{k+1} r_{k+1}
+        const double zr = s->zeta[i] * s->zeta[i] * rr_new;
+        s->beta_s[i] = s->beta * (s->zeta[i] / s->zeta_prev[i]) * (s->zeta[i] / s->zeta_prev[i]);
+        // converged: this step's x update still runs, then the shift is frozen.
+        // The base system (sigma 0, index base) keeps its direction p, which
+        // drives the recursion of all the others.
+        if (zr < s->eps && i != s->base) s->active[i] = 2;
+        else if (zr >= s->eps) any = 1;
+    }
+    // the x / p update of this step (OpMsUpdate) still runs; it turns stop into pause
+    if (!any) {
+        s->converged = 1;
+        s->stop = 1;
+        s->need_update = s->delta2 > 0.0;
+    } else if (s->delta2 > 0.0 && rr_new < s->delta2 * s->rr_max) {
+        s->need_update = 1;
+        s->stop = 1;
+    } else if (s->iter >= s->max_iter) {
+        s->stop = 1;
+    }
+    return true;
+}
+
 // x_i += alpha_i p_i ; r -= alpha Ap ; rr_new
 template <class SR, class SAp> struct OpMsResidual {
     static constexpr int NRED = 1;
@@ -467,45 +515,159 @@ template <class SR, class SAp> struct OpMsResidual {
         acc[0] += norm2(rv);
         r.par(q).template store<double>(h, rv);
     }
-    LYM_D void finalize(const double *t) const
-    {
-        const double rr_new = t[0];
-        s->iter += 1;
-        s->beta = rr_new / s->rr;
-        s->rr_prev = s->rr;
-        s->rr = rr_new;
-        if (rr_new > s->rr_max) s->rr_max = rr_new;
-        if (!(rr_new == rr_new)) {  // NaN: stop before the update
-            s->failed = 1;
-            s->stop = 1;
-            s->pause = 1;
-            return;
-        }
-        int any = 0;
-        for (int i = 0; i < s->nshift; ++i) {
-            if (!s->active[i]) continue;
-            // residual of shift i after this step: zeta_{k+1} r_{k+1}
-            const double zr = s->zeta[i] * s->zeta[i] * rr_new;
-            s->beta_s[i] = s->beta * (s->zeta[i] / s->zeta_prev[i]) * (s->zeta[i] / s->zeta_prev[i]);
-            // converged: this step's x update still runs, then the shift is frozen.
-            // The base system (sigma 0, index base) keeps its direction p, which
-            // drives the recursion of all the others.
-            if (zr < s->eps && i != s->base) s->active[i] = 2;
-            else if (zr >= s->eps) any = 1;
-        }
-        // the x / p update of this step (OpMsUpdate) still runs; it turns stop into pause
-        if (!any) {
-            s->converged = 1;
-            s->stop = 1;
-            s->need_update = s->delta2 > 0.0;
-        } else if (s->delta2 > 0.0 && rr_new < s->delta2 * s->rr_max) {
-            s->need_update = 1;
-            s->stop = 1;
-        } else if (s->iter >= s->max_iter) {
-            s->stop = 1;
+    LYM_D void finalize(const double *t) const { ms_residual_step(s, t[0]); }
+};
+
+// Windowed form of OpMsUpdate's step: x_i += alpha_i p_i and p_i = zeta_i R_m + beta_i p_i
+// applied to the coefficients of x_i and p_i (same conditions as OpMsUpdate), R_m = r_{k+1}.
+LYM_D void ms_window_step(MultishiftState *s)
+{
+    const int m = s->win;
+    const bool dir = !s->need_update;
+    for (int i = 0; i < s->nshift; ++i) {
+        const int act = s->active[i];
+        if (!act) continue;
+        const double a = s->alpha_s[i];
+        for (int j = 0; j <= m; ++j) s->cx[i][j] += a * s->cp[i][j];
+        s->xupd[i] = 1;
+        if (act == 1 && dir) {
+            const double b = s->beta_s[i];
+            for (int j = 0; j <= m; ++j) s->cp[i][j] *= b;
+            s->cp[i][m + 1] = s->zeta[i];
+            s->pupd[i] = 1;
         }
     }
+    s->win = m + 1;
+}
+
+// r_{k+1} = r_k - alpha Ap with the residuals in a ring of kMsWin + 1 FP32 slots (r_k in
+// slot k mod (kMsWin + 1)), |r_{k+1}|^2, then the step's scalars and window coefficients.
+template <class SAp> struct OpMsResidualRing {
+    static constexpr int NRED = 1;
+    const SpinorF *ring;
+    SAp ap;
+    MultishiftState *s;
+    LYM_D void site(int q, int h, double *acc) const
+    {
+        const int k = s->iter;
+        const SpinorF rin = ring[k % (kMsWin + 1)], rout = ring[(k + 1) % (kMsWin + 1)];
+        const double a = s->alpha;
+        cx<double> rv[12], av[12];
+        rin.par(q).template load<double>(h, rv);
+        ap.par(q).template load<double>(h, av);
+#pragma unroll
+        for (int c = 0; c < 12; ++c) rv[c] = rv[c] - a * av[c];
+        acc[0] += norm2(rv);
+        rout.par(q).template store<double>(h, rv);
+    }
+    LYM_D void finalize(const double *t) const
+    {
+        if (ms_residual_step(s, t[0])) ms_window_step(s);
+    }
 };
+
+// the base system's direction, materialised every step for the operator: p = r_{k+1} + beta p
+// (not after a step that asks for a reliable update: the host rebuilds it from the true residual)
+template <class SP> struct OpMsBaseDirection {
+    static constexpr int NRED = 1;  // no sum; finalize ends the step
+    const SpinorF *ring;
+    SP p;
+    MultishiftState *s;
+    LYM_D void site(int q, int h, double *) const
+    {
+        if (s->need_update || s->active[s->base] != 1) return;
+        const double b = s->beta;
+        cx<double> rv[12], pv[12];
+        ring[s->iter % (kMsWin + 1)].par(q).template load<double>(h, rv);
+        p.par(q).template load<double>(h, pv);
+#pragma unroll
+        for (int c = 0; c < 12; ++c) pv[c] = rv[c] + b * pv[c];
+        p.par(q).template store<double>(h, pv);
+    }
+    LYM_D void finalize(const double *) const
+    {
+        if (s->stop) s->pause = 1;
+    }
+};
+
+// Window flush: per shift x_i += cx_i0 P_i + sum_j cx_i(j+1) R_j and (running shifts)
+// P_i = cp_i0 P_i + sum_j cp_i(j+1) R_j, R_j = r_{k0+1+j}: one pass over x_i and P_i
+// per window instead of one per step.  FP32 words streamed one at a time; coefficients in
+// shared memory.  Runs whether or not the state is paused (a pause ends the window early).
+struct MsFlushArg {
+    const SpinorF *ring;  // kMsWin + 1 residual slots
+    const SpinorF *x;     // per-shift FP32 solution accumulators
+    const SpinorF *p;     // per-shift directions
+    MultishiftState *s;
+    int nshift;
+    int vh;
+};
+
+constexpr int kMsFlushThreads = 256;
+
+__global__ void __launch_bounds__(kMsFlushThreads) ms_flush_kernel(MsFlushArg a)
+{
+    __shared__ float cxs[kMaxShifts][kMsWin + 1], cps[kMaxShifts][kMsWin + 1];
+    __shared__ int fl[kMaxShifts];
+    __shared__ float4 *xp[kMaxShifts], *pp[kMaxShifts], *rp[kMsWin];
+    const MultishiftState *s = a.s;
+    const int m = s->win;
+    if (m == 0) return;
+    const int k0 = s->iter - m;
+    for (int t = threadIdx.x; t < a.nshift * (kMsWin + 1); t += blockDim.x) {
+        const int i = t / (kMsWin + 1), j = t % (kMsWin + 1);
+        cxs[i][j] = (float)s->cx[i][j];
+        cps[i][j] = (float)s->cp[i][j];
+    }
+    for (int i = threadIdx.x; i < a.nshift; i += blockDim.x) {
+        fl[i] = (s->xupd[i] ? 1 : 0) | ((s->pupd[i] && s->active[i] == 1) ? 2 : 0);
+        xp[i] = a.x[i].v;
+        pp[i] = a.p[i].v;
+    }
+    for (int j = threadIdx.x; j < m; j += blockDim.x) rp[j] = a.ring[(k0 + 1 + j) % (kMsWin + 1)].v;
+    __syncthreads();
+    const int stride = a.ring[0].stride;
+    for (int h = blockIdx.x * blockDim.x + threadIdx.x; h < a.vh; h += gridDim.x * blockDim.x) {
+        for (int w = 0; w < 6; ++w) {
+            const size_t o = (size_t)w * stride + h;
+            float4 R[kMsWin];
+#pragma unroll
+            for (int j = 0; j < kMsWin; ++j)
+                if (j < m) R[j] = rp[j][o];
+            for (int i = 0; i < a.nshift; ++i) {
+                const int f = fl[i];
+                if (!f) continue;
+                const float4 P = pp[i][o];
+                float4 X = xp[i][o], Q;
+                const float c0 = cxs[i][0], d0 = cps[i][0];
+                X.x += c0 * P.x; X.y += c0 * P.y; X.z += c0 * P.z; X.w += c0 * P.w;
+                Q.x = d0 * P.x; Q.y = d0 * P.y; Q.z = d0 * P.z; Q.w = d0 * P.w;
+#pragma unroll
+                for (int j = 0; j < kMsWin; ++j) {
+                    if (j < m) {
+                        const float c = cxs[i][j + 1], d = cps[i][j + 1];
+                        X.x += c * R[j].x; X.y += c * R[j].y; X.z += c * R[j].z; X.w += c * R[j].w;
+                        Q.x += d * R[j].x; Q.y += d * R[j].y; Q.z += d * R[j].z; Q.w += d * R[j].w;
+                    }
+                }
+                xp[i][o] = X;
+                if (f & 2) pp[i][o] = Q;
+            }
+        }
+    }
+}
+
+// start a new window (after the flush)
+__global__ void ms_window_reset_kernel(MultishiftState *s, int nshift)
+{
+    const int i = threadIdx.x;
+    if (i < nshift) {
+        s->xupd[i] = s->pupd[i] = 0;
+        for (int j = 0; j <= kMsWin; ++j) s->cx[i][j] = s->cp[i][j] = 0.0;
+        s->cp[i][0] = 1.0;
+    }
+    if (i == 0) s->win = 0;
+}
 
 // per shift: x_i += alpha_i p_i ; p_i = zeta_i r + beta_i p_i  (one launch over all shifts;
 // a step that asks for a reliable update leaves the directions to OpMsDirection)
