@@ -888,12 +888,32 @@ __global__ void __launch_bounds__(kBlasThreads) site_batch_kernel(Op op, int vh,
         __syncthreads();
         if (last) {
             __threadfence();
+            // every thread sums a fixed chunk of the blocks for one RHS (thread = chunk * nb + r),
+            // then thread r adds the chunks in order: deterministic, and the block partials are
+            // read by all threads instead of nb
+            const int nchunk = blockDim.x / nb, G = gridDim.x;
+            double(*red)[NR] = &smem[0][0];  // [nchunk * nb][NR], the same storage
+            if ((int)threadIdx.x < nchunk * nb) {
+                const int r = threadIdx.x % nb, ch = threadIdx.x / nb;
+                const int b0 = (int)((long)ch * G / nchunk), b1 = (int)((long)(ch + 1) * G / nchunk);
+                double part[NR];
+#pragma unroll
+                for (int k = 0; k < NR; ++k) part[k] = 0.0;
+                for (int b = b0; b < b1; ++b) {
+                    const double *src = partials + ((size_t)b * kMaxBatch + r) * NR;
+#pragma unroll
+                    for (int k = 0; k < NR; ++k) part[k] += __ldcg(src + k);
+                }
+#pragma unroll
+                for (int k = 0; k < NR; ++k) red[threadIdx.x][k] = part[k];
+            }
+            __syncthreads();
             if (threadIdx.x < nb) {
                 double tot[NR];
+#pragma unroll
                 for (int k = 0; k < NR; ++k) {
                     double s = 0.0;
-                    for (int b = 0; b < (int)gridDim.x; ++b)
-                        s += ((volatile double *)partials)[((size_t)b * kMaxBatch + threadIdx.x) * NR + k];
+                    for (int ch = 0; ch < nchunk; ++ch) s += red[ch * nb + threadIdx.x][k];
                     tot[k] = s;
                 }
                 op.finalize(threadIdx.x, tot);
