@@ -620,6 +620,31 @@ def run_rhmc(args, world, rank, local, dims=RHMC_DIMS):
     for p in [hsrc] + hsol:
         lib.lym_host_free(p)
 
+    # the RHMC consumers on the same system (RationalApproximation::evaluate and the solves of
+    # NFlavorFermionAction::updateForce), device buffers, one call each after a warm-up call
+    alphas = np.ascontiguousarray(np.linspace(0.05, 0.6, nsh)[::-1], dtype=np.float64)
+    r_out = torch.empty_like(b)
+    ys = [torch.empty_like(b) for _ in range(nsh)]
+    yptrs = (C.c_void_p * nsh)(*[y.data_ptr() for y in ys])
+    dop = C.c_int(0)
+    lib.lym_operator_create(ctx, 1, 2, RHMC_KAPPA, RHMC_CSW, 1, C.byref(dop))
+    consumer = {}
+    for _ in range(2):
+        t0 = time.perf_counter()
+        if lib.lym_rational_evaluate_device(ctx, opid, algo, nsh, alphas.ctypes.data_as(C.c_void_p),
+                                            sh.ctypes.data_as(C.c_void_p), eps, 20000, C.c_void_p(b.data_ptr()),
+                                            C.c_void_p(r_out.data_ptr()), C.byref(st)) != 0:
+            raise RuntimeError(lib.lym_last_error(ctx))
+        consumer["rational_evaluate_s"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        if lib.lym_rhmc_force_solves_device(ctx, opid, dop.value, algo, nsh, sh.ctypes.data_as(C.c_void_p), eps,
+                                            20000, C.c_void_p(b.data_ptr()), ptrs, yptrs, C.byref(st)) != 0:
+            raise RuntimeError(lib.lym_last_error(ctx))
+        consumer["force_solves_s"] = time.perf_counter() - t0
+    consumer["energy"] = float(torch.vdot(b.flatten(), r_out.flatten()).real)
+    del ys, r_out
+    torch.cuda.empty_cache()
+
     # the plain FP64 multishift CG on the same system (one solve)
     log("rhmc: FP64 multishift CG")
     fp64 = solve(algorithm=MULTISHIFT["multishift_cg"])
@@ -645,6 +670,7 @@ def run_rhmc(args, world, rank, local, dims=RHMC_DIMS):
                    "parallelism": "replicas (one independent solve stream per GPU)"},
         "multishift_steps": [r[1] for r in rec], "total_iterations": [r[2] for r in rec],
         "worst_true_residual": worst,
+        "rhmc_consumers": consumer,
         "fp64_multishift_cg_solves_per_s": 1.0 / fp64[0], "fp64_multishift_cg_iterations": fp64[2],
         "mixed_over_fp64": value / world * fp64[0],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",

@@ -230,6 +230,29 @@ int lym_multishift_device(lym_context *ctx, int op_id, int algorithm, int nshift
                           double precision, int max_steps, const double *source, double **solutions,
                           lym_solve_stats *stats);
 
+/* ---- RHMC consumers of the multishift (dirac_functions/RationalApproximation.cpp,
+ * actions/NFlavorFermionAction.cpp) -----------------------------------------------------
+ * RationalApproximation::evaluate(dirac, output, input) (RationalApproximation.cpp:18-42):
+ * output = sum_i alphas[i] (A + betas[i])^{-1} input with the multishift `algorithm` (a
+ * lym_multishift_solver value; precision and max_steps as the approximation's
+ * setPrecision / setMaximumRecursion), solutions and their combination on the device. */
+int lym_rational_evaluate(lym_context *ctx, int op_id, int algorithm, int n, const double *alphas,
+                          const double *betas, double precision, int max_steps, const double *input,
+                          double *output, lym_solve_stats *stats);
+int lym_rational_evaluate_device(lym_context *ctx, int op_id, int algorithm, int n, const double *alphas,
+                                 const double *betas, double precision, int max_steps, const double *input,
+                                 double *output, lym_solve_stats *stats);
+/* The solves of NFlavorFermionAction::updateForce (NFlavorFermionAction.cpp:76-96) for one
+ * pseudofermion phi: x[i] = (A + betas[i])^{-1} phi with the multishift on square_op_id, then
+ * y[i] = D x[i] with dirac_op_id (DiracOperator::multiply); both operators on one gauge field.
+ * x[i], y[i]: n caller buffers of full spinors (device pointers for the _device form). */
+int lym_rhmc_force_solves(lym_context *ctx, int square_op_id, int dirac_op_id, int algorithm, int n,
+                          const double *betas, double precision, int max_steps, const double *phi, double **x,
+                          double **y, lym_solve_stats *stats);
+int lym_rhmc_force_solves_device(lym_context *ctx, int square_op_id, int dirac_op_id, int algorithm, int n,
+                                 const double *betas, double precision, int max_steps, const double *phi,
+                                 double **x, double **y, lym_solve_stats *stats);
+
 /* ---- solve server (no reference counterpart: the reference has no serving mode) -------
  * Keeps gauge fields resident by key (one context, CUDA stream and worker thread per
  * field, so work on different fields overlaps on the device) and serves solve requests

@@ -8,6 +8,7 @@ from ._lib import LymError, SolveStats, build, declared_symbols, lib
 from .dirac import (DiracOperator, DiracWilsonOperator, EvenOddImprovedDiracWilsonOperator,
                     ImprovedDiracWilsonOperator, Lattice, SquareDiracWilsonOperator,
                     SquareEvenOddImprovedDiracWilsonOperator, SquareImprovedDiracWilsonOperator)
+from .rhmc import NFlavorFermionAction, RationalApproximation
 from .solvers import (BiConjugateGradient, ConjugateGradient, EvenOddBiCGStab, EvenOddConjugateGradient,
                       MultishiftSolver, PreconditionedBiCGStab, Solver)
 
@@ -17,5 +18,5 @@ __all__ = [
     "SquareDiracWilsonOperator", "SquareImprovedDiracWilsonOperator", "SquareEvenOddImprovedDiracWilsonOperator",
     "Solver", "ConjugateGradient", "BiConjugateGradient", "PreconditionedBiCGStab", "EvenOddConjugateGradient",
     "EvenOddBiCGStab",
-    "MultishiftSolver",
+    "MultishiftSolver", "RationalApproximation", "NFlavorFermionAction",
 ]

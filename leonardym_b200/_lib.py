@@ -94,6 +94,10 @@ def lib():
         "lym_solve_block_device": (i, [vp, i, i, dp, i, i, C.POINTER(vp), C.POINTER(vp), i, sp]),
         "lym_multishift": (i, [vp, i, i, i, vp, dp, i, vp, C.POINTER(vp), sp]),
         "lym_multishift_device": (i, [vp, i, i, i, vp, dp, i, vp, C.POINTER(vp), sp]),
+        "lym_rational_evaluate": (i, [vp, i, i, i, vp, vp, dp, i, vp, vp, sp]),
+        "lym_rational_evaluate_device": (i, [vp, i, i, i, vp, vp, dp, i, vp, vp, sp]),
+        "lym_rhmc_force_solves": (i, [vp, i, i, i, i, vp, dp, i, vp, C.POINTER(vp), C.POINTER(vp), sp]),
+        "lym_rhmc_force_solves_device": (i, [vp, i, i, i, i, vp, dp, i, vp, C.POINTER(vp), C.POINTER(vp), sp]),
         "lym_neighbour_tables": (i, [vp, ip, ip]),
         "lym_stencil_indices": (i, [vp, ip]),
         "lym_context_kernel_launches": (C.c_ulonglong, [vp]),

@@ -2816,6 +2816,73 @@ int lym_solve_preconditioned(lym_context *c, int op_id, int preconditioner_op_id
     });
 }
 
+// The multishift solvers on device spinors: xv[i] receives (A + shifts[i])^{-1} b.  For the
+// chronological solver xv[i] (i >= 1) holds the guess of shift i on entry.
+static int run_multishift(lym_context *c, OpEntry &op, int algorithm, int nshift, const double *shifts,
+                          double precision, int max_steps, const Spinor &b, std::vector<Spinor> &xv,
+                          lym_solve_stats &local)
+{
+    int rc = LYM_OK;
+    if (algorithm == LYM_MULTISHIFT_CG) {
+        rc = multishift_cg(c, op, nshift, shifts, precision, max_steps, b, xv, &local);
+    } else if (algorithm == LYM_MULTISHIFT_ME) {
+        // MEMultishiftSolver::solve: CG per shift, warm-started from the previous shift
+        int total = 0;
+        bool ok = true;
+        for (int i = 0; i < nshift; ++i) {
+            const double sh = shifts[i];
+            auto mv = [&](const Spinor &out, const Spinor &in, const int *skip) {
+                op_apply(c, op, PREC_D, out, in, &in, C2(sh), skip);
+            };
+            lym_solve_stats s1;
+            memset(&s1, 0, sizeof(s1));
+            if (i == 0) {
+                Vec z(c, PREC_D, 2);
+                zero(c, *z);
+                rc = cg_solve(c, mv, 2, b, xv[0], &*z, precision, max_steps, &s1);
+            } else {
+                rc = cg_solve(c, mv, 2, b, xv[i], &xv[i - 1], precision, max_steps, &s1);
+            }
+            ok = ok && rc == LYM_OK;
+            total += s1.iterations;
+        }
+        local.iterations = total;
+        local.steps = total;
+        local.converged = ok;
+        rc = ok ? LYM_OK : LYM_NOT_CONVERGED;
+    } else if (algorithm == LYM_MULTISHIFT_MMMR) {
+        rc = multishift_mmmr(c, op, nshift, shifts, precision, max_steps, b, xv, &local);
+    } else if (algorithm == LYM_MULTISHIFT_CG_MIXED_SINGLE || algorithm == LYM_MULTISHIFT_CG_MIXED_HALF) {
+        // the shared Krylov space runs in FP32 for both: the precision of its operator
+        // bounds the accuracy of every shifted solution (FP16 leaves them near 1e-3, FP32
+        // near 1e-7), and the refinement from there is what the storage choice saves on
+        const int rp = algorithm == LYM_MULTISHIFT_CG_MIXED_SINGLE ? PREC_F : PREC_H;
+        rc = multishift_cg_mixed(c, op, rp, nshift, shifts, precision, max_steps, b, xv, &local);
+    } else if (algorithm == LYM_MULTISHIFT_CHRONOLOGICAL) {
+        rc = multishift_chrono(c, op, nshift, shifts, precision, max_steps, b, xv, &local);
+    } else {
+        fail(c, LYM_ERR_UNSUPPORTED, "multishift algorithm %d", algorithm);
+    }
+    return rc;
+}
+
+// Device spinors owned for the length of one call.
+struct VecSet {
+    std::vector<Vec *> v;
+    std::vector<Spinor> s;
+    VecSet(lym_context *c, int n, int prec, int nparity)
+    {
+        for (int i = 0; i < n; ++i) {
+            v.push_back(new Vec(c, prec, nparity));
+            s.push_back(**v.back());
+        }
+    }
+    ~VecSet()
+    {
+        for (auto p : v) delete p;
+    }
+};
+
 static int do_multishift(lym_context *c, int op_id, int algorithm, int nshift, const double *shifts, double precision,
                          int max_steps, const double *source, double **solutions, lym_solve_stats *stats,
                          bool device_ptr)
@@ -2829,65 +2896,87 @@ static int do_multishift(lym_context *c, int op_id, int algorithm, int nshift, c
         memset(&local, 0, sizeof(local));
         Vec b(c, PREC_D, 2);
         upload_vec(c, *b, source, device_ptr, 0);
-        std::vector<Vec *> xs;
-        std::vector<Spinor> xv;
-        for (int i = 0; i < nshift; ++i) {
-            xs.push_back(new Vec(c, PREC_D, 2));
-            xv.push_back(**xs.back());
-        }
+        VecSet xs(c, nshift, PREC_D, 2);
         CK(cudaEventRecord(c->ev0, c->st));
-        int rc = LYM_OK;
-        try {
-            if (algorithm == LYM_MULTISHIFT_CG) {
-                rc = multishift_cg(c, op, nshift, shifts, precision, max_steps, *b, xv, &local);
-            } else if (algorithm == LYM_MULTISHIFT_ME) {
-                // MEMultishiftSolver::solve: CG per shift, warm-started from the previous shift
-                int total = 0;
-                bool ok = true;
-                for (int i = 0; i < nshift; ++i) {
-                    const double sh = shifts[i];
-                    auto mv = [&](const Spinor &out, const Spinor &in, const int *skip) {
-                        op_apply(c, op, PREC_D, out, in, &in, C2(sh), skip);
-                    };
-                    lym_solve_stats s1;
-                    memset(&s1, 0, sizeof(s1));
-                    if (i == 0) {
-                        Vec z(c, PREC_D, 2);
-                        zero(c, *z);
-                        rc = cg_solve(c, mv, 2, *b, xv[0], &*z, precision, max_steps, &s1);
-                    } else {
-                        rc = cg_solve(c, mv, 2, *b, xv[i], &xv[i - 1], precision, max_steps, &s1);
-                    }
-                    ok = ok && rc == LYM_OK;
-                    total += s1.iterations;
-                }
-                local.iterations = total;
-                local.steps = total;
-                local.converged = ok;
-                rc = ok ? LYM_OK : LYM_NOT_CONVERGED;
-            } else if (algorithm == LYM_MULTISHIFT_MMMR) {
-                rc = multishift_mmmr(c, op, nshift, shifts, precision, max_steps, *b, xv, &local);
-            } else if (algorithm == LYM_MULTISHIFT_CG_MIXED_SINGLE || algorithm == LYM_MULTISHIFT_CG_MIXED_HALF) {
-                // the shared Krylov space runs in FP32 for both: the precision of its operator
-                // bounds the accuracy of every shifted solution (FP16 leaves them near 1e-3, FP32
-                // near 1e-7), and the refinement from there is what the storage choice saves on
-                const int rp = algorithm == LYM_MULTISHIFT_CG_MIXED_SINGLE ? PREC_F : PREC_H;
-                rc = multishift_cg_mixed(c, op, rp, nshift, shifts, precision, max_steps, *b, xv, &local);
-            } else if (algorithm == LYM_MULTISHIFT_CHRONOLOGICAL) {
-                // solutions[i] (i >= 1) hold the chronological guesses on entry
-                for (int i = 1; i < nshift; ++i) upload_vec(c, xv[i], solutions[i], device_ptr, 1);
-                rc = multishift_chrono(c, op, nshift, shifts, precision, max_steps, *b, xv, &local);
-            } else {
-                fail(c, LYM_ERR_UNSUPPORTED, "multishift algorithm %d", algorithm);
-            }
-        } catch (...) {
-            for (auto v : xs) delete v;
-            throw;
+        // solutions[i] (i >= 1) hold the chronological guesses on entry
+        if (algorithm == LYM_MULTISHIFT_CHRONOLOGICAL)
+            for (int i = 1; i < nshift; ++i) upload_vec(c, xs.s[i], solutions[i], device_ptr, 1);
+        const int rc = run_multishift(c, op, algorithm, nshift, shifts, precision, max_steps, *b, xs.s, local);
+        CK(cudaEventRecord(c->ev1, c->st));
+        for (int i = 0; i < nshift; ++i) download_vec(c, solutions[i], xs.s[i], device_ptr, 2), CK(cudaStreamSynchronize(c->st));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        local.seconds = ms * 1e-3;
+        if (stats) *stats = local;
+        CK(cudaGetLastError());
+        return rc;
+    });
+}
+
+// RationalApproximation::evaluate (dirac_functions/RationalApproximation.cpp:18-42):
+// output = sum_i alphas[i] (A + betas[i])^{-1} input, everything on the device.
+static int do_rational(lym_context *c, int op_id, int algorithm, int n, const double *alphas, const double *betas,
+                       double precision, int max_steps, const double *input, double *output, lym_solve_stats *stats,
+                       bool device_ptr)
+{
+    if (!alphas || !betas || !input || !output || n < 1 || n > kMaxShifts) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        OpEntry &op = op_of(c, op_id);
+        lym_solve_stats local;
+        memset(&local, 0, sizeof(local));
+        Vec b(c, PREC_D, 2), out(c, PREC_D, 2);
+        upload_vec(c, *b, input, device_ptr, 0);
+        VecSet xs(c, n, PREC_D, 2);
+        for (int i = 1; i < n; ++i) zero(c, xs.s[i]);  // no chronological history
+        CK(cudaEventRecord(c->ev0, c->st));
+        const int rc = run_multishift(c, op, algorithm, n, betas, precision, max_steps, *b, xs.s, local);
+        zero(c, *out);
+        for (int i = 0; i < n; ++i) axpby(c, xs.s[i], *out, C2(alphas[i]), C2(1.0));
+        CK(cudaEventRecord(c->ev1, c->st));
+        download_vec(c, output, *out, device_ptr, 2);
+        CK(cudaStreamSynchronize(c->st));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        local.seconds = ms * 1e-3;
+        if (stats) *stats = local;
+        CK(cudaGetLastError());
+        return rc;
+    });
+}
+
+// The solves of NFlavorFermionAction::updateForce (actions/NFlavorFermionAction.cpp:76-96)
+// for one pseudofermion: x_i = (A + betas[i])^{-1} phi with the multishift on square_op_id,
+// then y_i = D x_i with dirac_op_id (DiracOperator::multiply), on the device.
+static int do_rhmc_force_solves(lym_context *c, int square_op_id, int dirac_op_id, int algorithm, int n,
+                                const double *betas, double precision, int max_steps, const double *phi, double **x,
+                                double **y, lym_solve_stats *stats, bool device_ptr)
+{
+    if (!betas || !phi || !x || !y || n < 1 || n > kMaxShifts) return LYM_ERR_ARGUMENT;
+    for (int i = 0; i < n; ++i)
+        if (!x[i] || !y[i]) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        OpEntry &sq = op_of(c, square_op_id);
+        OpEntry &dop = op_of(c, dirac_op_id);
+        if (dop.gauge_id != sq.gauge_id)
+            fail(c, LYM_ERR_ARGUMENT, "the Dirac and squared operators act on different gauge fields");
+        lym_solve_stats local;
+        memset(&local, 0, sizeof(local));
+        Vec b(c, PREC_D, 2), yv(c, PREC_D, 2);
+        upload_vec(c, *b, phi, device_ptr, 0);
+        VecSet xs(c, n, PREC_D, 2);
+        for (int i = 1; i < n; ++i) zero(c, xs.s[i]);
+        CK(cudaEventRecord(c->ev0, c->st));
+        const int rc = run_multishift(c, sq, algorithm, n, betas, precision, max_steps, *b, xs.s, local);
+        for (int i = 0; i < n; ++i) {
+            op_apply(c, dop, PREC_D, *yv, xs.s[i], nullptr, C2(0.0));
+            download_vec(c, x[i], xs.s[i], device_ptr, 2);
+            CK(cudaStreamSynchronize(c->st));
+            download_vec(c, y[i], *yv, device_ptr, 2);
+            CK(cudaStreamSynchronize(c->st));
         }
         CK(cudaEventRecord(c->ev1, c->st));
-        for (int i = 0; i < nshift; ++i) download_vec(c, solutions[i], xv[i], device_ptr, 2), CK(cudaStreamSynchronize(c->st));
-        for (auto v : xs) delete v;
         float ms = 0.f;
+        CK(cudaEventSynchronize(c->ev1));
         cudaEventElapsedTime(&ms, c->ev0, c->ev1);
         local.seconds = ms * 1e-3;
         if (stats) *stats = local;
@@ -2906,6 +2995,35 @@ int lym_multishift_device(lym_context *c, int op_id, int algorithm, int nshift, 
                           int max_steps, const double *source, double **solutions, lym_solve_stats *stats)
 {
     return do_multishift(c, op_id, algorithm, nshift, shifts, precision, max_steps, source, solutions, stats, true);
+}
+
+int lym_rational_evaluate(lym_context *c, int op_id, int algorithm, int n, const double *alphas, const double *betas,
+                          double precision, int max_steps, const double *input, double *output, lym_solve_stats *stats)
+{
+    return do_rational(c, op_id, algorithm, n, alphas, betas, precision, max_steps, input, output, stats, false);
+}
+
+int lym_rational_evaluate_device(lym_context *c, int op_id, int algorithm, int n, const double *alphas,
+                                 const double *betas, double precision, int max_steps, const double *input,
+                                 double *output, lym_solve_stats *stats)
+{
+    return do_rational(c, op_id, algorithm, n, alphas, betas, precision, max_steps, input, output, stats, true);
+}
+
+int lym_rhmc_force_solves(lym_context *c, int square_op_id, int dirac_op_id, int algorithm, int n, const double *betas,
+                          double precision, int max_steps, const double *phi, double **x, double **y,
+                          lym_solve_stats *stats)
+{
+    return do_rhmc_force_solves(c, square_op_id, dirac_op_id, algorithm, n, betas, precision, max_steps, phi, x, y,
+                                stats, false);
+}
+
+int lym_rhmc_force_solves_device(lym_context *c, int square_op_id, int dirac_op_id, int algorithm, int n,
+                                 const double *betas, double precision, int max_steps, const double *phi, double **x,
+                                 double **y, lym_solve_stats *stats)
+{
+    return do_rhmc_force_solves(c, square_op_id, dirac_op_id, algorithm, n, betas, precision, max_steps, phi, x, y,
+                                stats, true);
 }
 
 int lym_neighbour_tables(lym_context *c, int *sup, int *sdn)

@@ -261,6 +261,45 @@ def mmmr_multishift(op, src, shifts, eps, max_steps=3000):
     return _multishift(lib().orc_mmmr_multishift, op, src, shifts, eps, max_steps, True)
 
 
+def rational_evaluate(op, alphas, betas, src, precision=1e-12, max_steps=3000, algorithm="mass_estrapolation"):
+    """RationalApproximation::evaluate (dirac_functions/RationalApproximation.cpp:18-42): the
+    multishift solutions x_i = (A + beta_i)^{-1} src, then output = sum_i alpha_i x_i
+    (zeroed, then accumulated in the order of the approximation's terms)."""
+    fn = {"mass_estrapolation": me_multishift, "minimal_residual": mmmr_multishift}[algorithm]
+    rc, xs, _ = fn(op, src, list(betas), precision, max_steps)
+    out = np.zeros_like(xs[0])
+    for a, x in zip(alphas, xs):
+        out += float(a) * x
+    return rc, out
+
+
+def rational_value(alphas, betas, x):
+    """RationalApproximation::evaluate(const complex&) (RationalApproximation.cpp:44-52):
+    sum_i alpha_i / (x + beta_i)."""
+    r = 0j
+    for a, b in zip(alphas, betas):
+        r += a / (x + b)
+    return r
+
+
+def rhmc_energy(op, approximations, pseudofermions, precision=1e-12, max_steps=3000):
+    """NFlavorFermionAction::energy (actions/NFlavorFermionAction.cpp:193-207): the sum over
+    the (alphas, betas) approximations of Re <phi_k, r_k(A) phi_k> on the squared operator."""
+    e = 0.0
+    for (alphas, betas), phi in zip(approximations, pseudofermions):
+        _, out = rational_evaluate(op, alphas, betas, phi, precision, max_steps)
+        e += float(np.vdot(phi, out).real)
+    return e
+
+
+def rhmc_force_solves(square_op, dirac_op, betas, phi, precision=1e-12, max_steps=3000):
+    """The solves of NFlavorFermionAction::updateForce (NFlavorFermionAction.cpp:76-96) for
+    one pseudofermion: x_i = (A + beta_i)^{-1} phi (mass-estrapolation multishift on the
+    squared operator), y_i = D x_i."""
+    rc, xs, _ = me_multishift(square_op, phi, list(betas), precision, max_steps)
+    return rc, xs, [dirac_op.multiply(x) for x in xs]
+
+
 def squared_norm(v):
     return float(np.vdot(v, v).real)
 

@@ -21,6 +21,7 @@ TUS=(
   dirac_operators/SquareEvenOddImprovedDiracWilsonOperator.cpp
   dirac_operators/OverlapOperator.cpp dirac_operators/SquareOverlapOperator.cpp dirac_operators/ExactOverlapOperator.cpp
   dirac_functions/Polynomial.cpp dirac_functions/ChebyshevRecursion.cpp fermion_measurements/DiracEigenSolver.cpp
+  dirac_functions/RationalApproximation.cpp
   inverters/ConjugateGradient.cpp inverters/BiConjugateGradient.cpp inverters/PreconditionedBiCGStab.cpp
   inverters/MultishiftSolver.cpp inverters/MEMultishiftSolver.cpp inverters/MMMRMultishiftSolver.cpp
   inverters/ChronologicalMultishiftSolver.cpp

@@ -36,6 +36,7 @@ def lib(rep):
         L.ref_solve.argtypes = [ip, i, dp, dp, i, vp, i, dp, i, dp, dp, vp, vp, ip]
         L.ref_solve2.argtypes = [ip, i, dp, dp, i, vp, i, dp, i, i, i, dp, dp, vp, vp, ip]
         L.ref_multishift.argtypes = [ip, i, dp, dp, i, vp, i, i, vp, dp, i, vp, C.POINTER(C.c_void_p)]
+        L.ref_rational_evaluate.argtypes = [ip, i, dp, dp, i, vp, i, i, vp, vp, dp, i, vp, vp]
         L.ref_neighbours.argtypes = [ip, ip, ip]
         L.ref_antiperiodic.argtypes = [ip, vp]
         if hasattr(L, "ref_to_adjoint"):
@@ -118,6 +119,20 @@ class Reference:
         rc = self.L.ref_multishift(_d(self.dims), KIND[kind], kappa, csw, int(gamma5), _p(self.links), alg,
                                    len(shifts), _p(sh), float(epsilon), int(max_steps), _p(b), ptrs)
         return rc, sols
+
+
+def _rational(self, kind, algorithm, alphas, betas, b, precision, max_steps, kappa, csw=0.0, gamma5=True):
+    b = np.ascontiguousarray(b, np.complex128)
+    out = self._vec()
+    a = np.ascontiguousarray(alphas, np.float64)
+    be = np.ascontiguousarray(betas, np.float64)
+    alg = {"mass_estrapolation": 0, "minimal_residual": 1}[algorithm]
+    rc = self.L.ref_rational_evaluate(_d(self.dims), KIND[kind], kappa, csw, int(gamma5), _p(self.links), alg,
+                                      len(a), _p(a), _p(be), float(precision), int(max_steps), _p(b), _p(out))
+    return rc, out
+
+
+Reference.rational_evaluate = _rational
 
 
 def neighbours(dims, rep="su3"):

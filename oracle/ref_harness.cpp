@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "algebra_utils/AlgebraUtils.h"
+#include "dirac_functions/RationalApproximation.h"
 #include "dirac_operators/DiracWilsonOperator.h"
 #include "dirac_operators/EvenOddImprovedDiracWilsonOperator.h"
 #include "dirac_operators/ImprovedDiracWilsonOperator.h"
@@ -269,6 +270,31 @@ int ref_multishift(const int dims[4], int kind, double kappa, double csw, int ga
     delete ms;
     delete op;
     return ok ? 1 : 0;
+}
+
+// RationalApproximation::evaluate with MEMultishiftSolver (algorithm 0) or
+// MMMRMultishiftSolver (1); precision / max_steps through setPrecision / setMaximumRecursion
+int ref_rational_evaluate(const int dims[4], int kind, double kappa, double csw, int gamma5, const double *links,
+                          int algorithm, int n, const double *alphas, const double *betas, double precision,
+                          int max_steps, const double *src, double *out)
+{
+    init_layout(dims);
+    extended_fermion_lattice_t L;
+    load(L, links);
+    DiracOperator *op = make_operator(kind, kappa, csw, gamma5, L);
+    if (!op) return -1;
+    extended_dirac_vector_t b, o;
+    load(b, src);
+    MultishiftSolver *ms = algorithm == 0 ? (MultishiftSolver *)new MEMultishiftSolver(precision, max_steps)
+                                          : (MultishiftSolver *)new MMMRMultishiftSolver(precision, max_steps);
+    RationalApproximation ra(std::vector<real_t>(alphas, alphas + n), std::vector<real_t>(betas, betas + n), ms);
+    ra.setPrecision(precision);
+    ra.setMaximumRecursion(max_steps);
+    ra.evaluate(op, o, b);
+    store(o, out);
+    delete ms;
+    delete op;
+    return 1;
 }
 
 }  // extern "C"

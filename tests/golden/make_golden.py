@@ -53,6 +53,15 @@ def make(rep):
         rc, sols = ref.multishift("SquareImproved", alg, x, shifts, prec, 5000, kappa, csw, True)
         assert rc == 1, alg
         out[f"multishift/{alg}"] = np.stack(sols)
+    # RationalApproximation::evaluate (RationalApproximation.cpp:18-42) with the
+    # mass-estrapolation multishift, on the squared full and even-odd operators
+    out["rational/alphas"] = np.array([0.31, 0.12, 0.047, 0.011])
+    out["rational/betas"] = np.array([0.9, 0.17, 0.03, 0.004])
+    for kind in ("SquareImproved", "SquareEvenOddImproved"):
+        rc, r = ref.rational_evaluate(kind, "mass_estrapolation", out["rational/alphas"], out["rational/betas"], x,
+                                      prec, 5000, kappa, csw, True)
+        assert rc == 1
+        out[f"rational/{kind}"] = r
     # BiCGStab(l) and BiCGStab with a preconditioner operator (BiConjugateGradient.cpp:11-317)
     for l in (2, 4):
         rc, sol, steps = ref.solve2("SquareImproved", "bicgstab_l", x, prec, 5000, kappa, csw, True, l=l)

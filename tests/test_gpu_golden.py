@@ -86,3 +86,16 @@ def test_solvers_against_reference(gold):
         assert ms.solve(make(gold, "SquareImproved"), x, sols, list(gold["shifts"]))
         for a, b in zip(sols, gold[f"multishift/{alg}"]):
             assert rel(a, b) < 1e-8
+
+
+def test_rational_evaluate_golden(gold):
+    # RationalApproximation::evaluate against the compiled reference's own output
+    x = gold["x"]
+    prec = 1e-20 * float(np.vdot(x, x).real)
+    for kind in ("SquareImproved", "SquareEvenOddImproved"):
+        ra = L.RationalApproximation(gold["rational/alphas"], gold["rational/betas"])
+        ra.setPrecision(prec)
+        ra.setMaximumRecursion(5000)
+        out = gold["lat"].new_vector()
+        ra.evaluate(make(gold, kind), out, x)
+        assert rel(out, gold[f"rational/{kind}"]) < 1e-8

@@ -310,3 +310,60 @@ def test_multishift_cg_mixed_needs_rhmc_operator(setup):
     op = gpu_op(setup, L.SquareEvenOddImprovedDiracWilsonOperator)
     with pytest.raises(L.LymError):
         ms.solve(op, setup["b"], [], [-1.0, 0.01])
+
+
+@pytest.mark.parametrize("kind,alg", [("SquareImproved", "mass_estrapolation"),
+                                      ("SquareImproved", "minimal_residual"),
+                                      ("SquareEvenOddImproved", "mass_estrapolation"),
+                                      ("SquareEvenOddImproved", "multishift_cg_mixed_half")])
+def test_rational_evaluate(setup, oracle, kind, alg):
+    # RationalApproximation::evaluate: sum_i alpha_i (A + beta_i)^{-1} b, against the oracle's
+    # restatement (FP64 mass-estrapolation multishift)
+    b = setup["b"]
+    alphas, betas = [0.31, 0.12, 0.047, 0.011], [0.9, 0.17, 0.03, 0.004]
+    eps = (1e-11) ** 2 * float(np.vdot(b, b).real)
+    cls = L.SquareImprovedDiracWilsonOperator if kind == "SquareImproved" else L.SquareEvenOddImprovedDiracWilsonOperator
+    ra = L.RationalApproximation(alphas, betas, L.MultishiftSolver.getInstance(alg))
+    ra.setPrecision(eps)
+    ra.setMaximumRecursion(10000)
+    out = setup["lat"].new_vector()
+    ra.evaluate(gpu_op(setup, cls), out, b)
+    orc = oracle.Operator(setup["geom"], setup["links"], kind, setup["kappa"], setup["csw"], True)
+    rc, ref = oracle.rational_evaluate(orc, alphas, betas, b, eps, 10000)
+    assert rc == 1
+    assert rel(out, ref) < 1e-8
+    assert abs(ra.evaluate(0.25) - oracle.rational_value(alphas, betas, 0.25)) < 1e-14
+
+
+def test_rhmc_action_energy_and_force_solves(setup, oracle):
+    # NFlavorFermionAction: energy = sum_k Re <phi_k, r_k(A) phi_k>; updateForce's solves
+    # x_i = (A + beta_i)^{-1} phi, y_i = D x_i, on the even-odd RHMC operator
+    b = setup["b"]
+    phi2 = synth.gaussian_spinor(setup["dims"], 3, 23)
+    approx = [([0.31, 0.12, 0.047], [0.9, 0.17, 0.03]), ([0.5, 0.2], [0.4, 0.05])]
+    eps = (1e-11) ** 2 * float(np.vdot(b, b).real)
+    sq = gpu_op(setup, L.SquareEvenOddImprovedDiracWilsonOperator)
+    D = gpu_op(setup, L.EvenOddImprovedDiracWilsonOperator)
+    ras = []
+    for al, be in approx:
+        ms = L.MultishiftSolver.getInstance("mass_estrapolation")
+        ms.setPrecision(eps)
+        ms.setMaxSteps(10000)
+        ra = L.RationalApproximation(al, be, ms)
+        ra.setPrecision(eps)
+        ra.setMaximumRecursion(10000)
+        ras.append(ra)
+    act = L.NFlavorFermionAction(D, sq, ras)
+    act.addPseudoFermion(b)
+    act.addPseudoFermion(phi2)
+    A = oracle.Operator(setup["geom"], setup["links"], "SquareEvenOddImproved", setup["kappa"], setup["csw"], True)
+    Do = oracle.Operator(setup["geom"], setup["links"], "EvenOddImproved", setup["kappa"], setup["csw"], True)
+    e_ref = oracle.rhmc_energy(A, approx, [b, phi2], eps, 10000)
+    assert abs(act.energy() - e_ref) <= 1e-9 * abs(e_ref)
+    Xs, Ys = act.solves()
+    for (al, be), phi, X, Y in zip(approx, [b, phi2], Xs, Ys):
+        rc, xo, yo = oracle.rhmc_force_solves(A, Do, be, phi, eps, 10000)
+        assert rc == 1
+        for x, y, xr, yr in zip(X, Y, xo, yo):
+            assert rel(x, xr) < 1e-8
+            assert rel(y, yr) < 1e-8

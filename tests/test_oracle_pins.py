@@ -135,3 +135,17 @@ def test_chronological_multishift_pinned(gold, oracle):
     for s, sh in zip(sols, shifts):
         r = x - A.multiply(s) - sh * s
         assert float(np.vdot(r, r).real) < 4 * prec
+
+
+def test_rational_evaluate_pinned(gold, oracle):
+    # RationalApproximation::evaluate (RationalApproximation.cpp:18-42) on the squared full and
+    # even-odd operators, mass-estrapolation multishift
+    x = gold["x"]
+    prec = 1e-20 * float(np.vdot(x, x).real)
+    alphas, betas = list(gold["rational/alphas"]), list(gold["rational/betas"])
+    for kind in ("SquareImproved", "SquareEvenOddImproved"):
+        rc, out = oracle.rational_evaluate(op(oracle, gold, kind), alphas, betas, x, prec, 5000)
+        assert rc == 1
+        assert rel(out, gold[f"rational/{kind}"]) < 1e-10
+    assert abs(oracle.rational_value(alphas, betas, 0.5 + 0.1j) -
+               sum(a / (0.5 + 0.1j + b) for a, b in zip(alphas, betas))) < 1e-15
