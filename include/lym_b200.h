@@ -253,6 +253,45 @@ int lym_rhmc_force_solves_device(lym_context *ctx, int square_op_id, int dirac_o
                                  const double *betas, double precision, int max_steps, const double *phi,
                                  double **x, double **y, lym_solve_stats *stats);
 
+/* ---- propagator consumers (correlators/MesonCorrelator.cpp,
+ * fermion_measurements/ChiralCondensate.cpp) ---------------------------------------------
+ * The connected contractions of MesonCorrelator::execute (MesonCorrelator.cpp:98-157) of
+ * the 12 point-source propagators (propagators[c * 4 + alpha]: the solution of D x = b for
+ * the source of spin alpha and colour c at the origin, StochasticEstimator.cpp:100-112), in
+ * the reference's layout: per time slice t the summator results pion[t], scalar[t], ps[t]
+ * (Lt doubles each; the reference's output multiplies them by 4 kappa^2, :163).  Both
+ * representations have 3 colour components.  _device: device pointers. */
+int lym_meson_contractions(lym_context *ctx, const double *const *propagators, double *pion, double *scalar,
+                           double *ps);
+int lym_meson_contractions_device(lym_context *ctx, const double *const *propagators, double *pion,
+                                  double *scalar, double *ps);
+/* out[2k], out[2k+1] = <a[k], b[k]> (gamma5 = 0, AlgebraUtils::dot, AlgebraUtils.h:17-27) or
+ * <a[k], gamma5 b[k]> (gamma5 = 1, AlgebraUtils::gamma5dot, :219-238) for n pairs of full
+ * spinors in device memory (the dot products of ChiralCondensate::execute, :92-105); out on
+ * the host. */
+int lym_dots_device(lym_context *ctx, int n, const double *const *a, const double *const *b, int gamma5,
+                    double *out);
+/* Real Z2 noise (StochasticEstimator::generateRandomNoise, StochasticEstimator.h:16-31: every
+ * spin-colour component +-1) from a counter-based generator instead of the reference's
+ * time-seeded one: component j of vector `stream` is +1 when the top bit of
+ * splitmix64(seed + 0x9E3779B97F4A7C15 (stream 12 V + j + 1)) is set, else -1.  out: a full
+ * AoS spinor in device memory. */
+int lym_noise_z2_device(lym_context *ctx, unsigned long long seed, unsigned long long stream, double *out);
+/* MesonCorrelator::execute (MesonCorrelator.cpp:22-157) for the operator op_id (a
+ * DiracWilson / Improved kind, gamma5 off as the reference sets it): the 12 point sources
+ * solved with the block solver `solver` (lym_solve_block's solvers, precision and batch as
+ * there), then lym_meson_contractions; stats: 12 entries or NULL.  Without the reference's
+ * stout smearing, source shift and stochastic disconnected part. */
+int lym_meson_correlator(lym_context *ctx, int op_id, int solver, double precision, int max_steps, int batch,
+                         double *pion, double *scalar, double *ps, lym_solve_stats *stats);
+/* ChiralCondensate::execute (ChiralCondensate.cpp:84-118) for n stochastic estimators:
+ * eta_k = lym_noise_z2_device(seed, k), x_k = D^-1 eta_k and with `connected` y_k = D^-1 x_k
+ * (block solver `solver`); out[8k .. 8k+7] = <eta,x>/V, <eta,gamma5 x>/V, <x,x>/V,
+ * <eta,y>/V as (re, im) (the last pair 0 without `connected`); stats: n (2n with
+ * `connected`) entries or NULL. */
+int lym_chiral_condensate(lym_context *ctx, int op_id, int solver, double precision, int max_steps, int batch,
+                          int n, unsigned long long seed, int connected, double *out, lym_solve_stats *stats);
+
 /* ---- solve server (no reference counterpart: the reference has no serving mode) -------
  * Keeps gauge fields resident by key (one context, CUDA stream and worker thread per
  * field, so work on different fields overlaps on the device) and serves solve requests

@@ -8,6 +8,7 @@ from ._lib import LymError, SolveStats, build, declared_symbols, lib
 from .dirac import (DiracOperator, DiracWilsonOperator, EvenOddImprovedDiracWilsonOperator,
                     ImprovedDiracWilsonOperator, Lattice, SquareDiracWilsonOperator,
                     SquareEvenOddImprovedDiracWilsonOperator, SquareImprovedDiracWilsonOperator)
+from .measurements import ChiralCondensate, MesonCorrelator
 from .rhmc import NFlavorFermionAction, RationalApproximation
 from .solvers import (BiConjugateGradient, ConjugateGradient, EvenOddBiCGStab, EvenOddConjugateGradient,
                       MultishiftSolver, PreconditionedBiCGStab, Solver)
@@ -18,5 +19,5 @@ __all__ = [
     "SquareDiracWilsonOperator", "SquareImprovedDiracWilsonOperator", "SquareEvenOddImprovedDiracWilsonOperator",
     "Solver", "ConjugateGradient", "BiConjugateGradient", "PreconditionedBiCGStab", "EvenOddConjugateGradient",
     "EvenOddBiCGStab",
-    "MultishiftSolver", "RationalApproximation", "NFlavorFermionAction",
+    "MultishiftSolver", "RationalApproximation", "NFlavorFermionAction", "MesonCorrelator", "ChiralCondensate",
 ]

@@ -95,6 +95,12 @@ def lib():
         "lym_multishift": (i, [vp, i, i, i, vp, dp, i, vp, C.POINTER(vp), sp]),
         "lym_multishift_device": (i, [vp, i, i, i, vp, dp, i, vp, C.POINTER(vp), sp]),
         "lym_rational_evaluate": (i, [vp, i, i, i, vp, vp, dp, i, vp, vp, sp]),
+        "lym_meson_contractions": (i, [vp, C.POINTER(vp), vp, vp, vp]),
+        "lym_meson_contractions_device": (i, [vp, C.POINTER(vp), vp, vp, vp]),
+        "lym_dots_device": (i, [vp, i, C.POINTER(vp), C.POINTER(vp), i, vp]),
+        "lym_noise_z2_device": (i, [vp, C.c_ulonglong, C.c_ulonglong, vp]),
+        "lym_meson_correlator": (i, [vp, i, i, dp, i, i, vp, vp, vp, sp]),
+        "lym_chiral_condensate": (i, [vp, i, i, dp, i, i, i, C.c_ulonglong, i, vp, sp]),
         "lym_rational_evaluate_device": (i, [vp, i, i, i, vp, vp, dp, i, vp, vp, sp]),
         "lym_rhmc_force_solves": (i, [vp, i, i, i, i, vp, dp, i, vp, C.POINTER(vp), C.POINTER(vp), sp]),
         "lym_rhmc_force_solves_device": (i, [vp, i, i, i, i, vp, dp, i, vp, C.POINTER(vp), C.POINTER(vp), sp]),

@@ -57,7 +57,7 @@ struct lym_context {
     int rep = REP_SU3;
     int device = 0;
     cudaStream_t st = nullptr;
-    std::mutex mu;
+    std::recursive_mutex mu;  // entry points may call other entry points on the same thread
     std::string err;
     std::map<int, GaugeEntry> gauges;
     std::map<int, OpEntry> ops;
@@ -112,7 +112,7 @@ void ck(lym_context *c, cudaError_t e, const char *what)
 template <class F> int guarded(lym_context *c, F f)
 {
     if (!c) return LYM_ERR_ARGUMENT;
-    std::lock_guard<std::mutex> lock(c->mu);
+    std::lock_guard<std::recursive_mutex> lock(c->mu);
     try {
         cudaSetDevice(c->device);
         return f();
@@ -3024,6 +3024,196 @@ int lym_rhmc_force_solves_device(lym_context *c, int square_op_id, int dirac_op_
 {
     return do_rhmc_force_solves(c, square_op_id, dirac_op_id, algorithm, n, betas, precision, max_steps, phi, x, y,
                                 stats, true);
+}
+
+// device memory for the length of one call
+struct DevBuf {
+    lym_context *c;
+    void *p = nullptr;
+    size_t n = 0;
+    DevBuf(lym_context *ctx, size_t bytes) : c(ctx), p(dev_alloc(ctx, bytes)), n(bytes) {}
+    ~DevBuf()
+    {
+        if (p) dev_free(c, p, n);
+    }
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+};
+
+static int do_meson(lym_context *c, const double *const *props, double *pion, double *scalar, double *ps,
+                    bool device_ptr)
+{
+    if (!props || !pion || !scalar || !ps) return LYM_ERR_ARGUMENT;
+    for (int k = 0; k < 12; ++k)
+        if (!props[k]) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        const size_t vb = (size_t)c->g.V * 24 * sizeof(double);
+        const int Lt = c->g.L[3];
+        MesonProps P;
+        std::vector<std::unique_ptr<DevBuf>> staged;
+        for (int k = 0; k < 12; ++k) {
+            if (device_ptr) {
+                P.p[k] = (const double2 *)props[k];
+            } else {
+                staged.emplace_back(new DevBuf(c, vb));
+                CK(cudaMemcpyAsync(staged.back()->p, props[k], vb, cudaMemcpyHostToDevice, c->st));
+                P.p[k] = (const double2 *)staged.back()->p;
+            }
+        }
+        DevBuf scratch(c, meson_scratch_bytes(c->g)), res(c, 3 * (size_t)Lt * sizeof(double));
+        launch_meson_contractions(c->g, P, (double *)scratch.p, (double *)res.p, c->st);
+        count(c, 2);
+        std::vector<double> h(3 * (size_t)Lt);
+        CK(cudaMemcpyAsync(h.data(), res.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        CK(cudaGetLastError());
+        for (int t = 0; t < Lt; ++t) {
+            pion[t] = h[t];
+            scalar[t] = h[Lt + t];
+            ps[t] = h[2 * Lt + t];
+        }
+        return LYM_OK;
+    });
+}
+
+int lym_meson_contractions(lym_context *c, const double *const *propagators, double *pion, double *scalar, double *ps)
+{
+    return do_meson(c, propagators, pion, scalar, ps, false);
+}
+
+int lym_meson_contractions_device(lym_context *c, const double *const *propagators, double *pion, double *scalar,
+                                  double *ps)
+{
+    return do_meson(c, propagators, pion, scalar, ps, true);
+}
+
+int lym_dots_device(lym_context *c, int n, const double *const *a, const double *const *b, int gamma5, double *out)
+{
+    if (n < 0 || (n > 0 && (!a || !b || !out))) return LYM_ERR_ARGUMENT;
+    for (int k = 0; k < n; ++k)
+        if (!a[k] || !b[k]) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        const int nblk = dot_blocks(c->g);
+        DevBuf partials(c, (size_t)kMaxDots * nblk * sizeof(double2)), res(c, (size_t)kMaxDots * sizeof(double2));
+        for (int k0 = 0; k0 < n; k0 += kMaxDots) {
+            const int m = std::min(kMaxDots, n - k0);
+            DotPairs D;
+            for (int k = 0; k < m; ++k) {
+                D.a[k] = (const double2 *)a[k0 + k];
+                D.b[k] = (const double2 *)b[k0 + k];
+            }
+            launch_dots(c->g, D, m, gamma5 ? 1 : 0, (double2 *)partials.p, (double2 *)res.p, c->st);
+            count(c, 2);
+            CK(cudaMemcpyAsync(out + 2 * (size_t)k0, res.p, m * sizeof(double2), cudaMemcpyDeviceToHost, c->st));
+            CK(cudaStreamSynchronize(c->st));
+        }
+        CK(cudaGetLastError());
+        return LYM_OK;
+    });
+}
+
+int lym_noise_z2_device(lym_context *c, unsigned long long seed, unsigned long long stream, double *out)
+{
+    if (!out) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        launch_z2_noise(c->g, out, seed, stream, c->st);
+        count(c, 1);
+        CK(cudaStreamSynchronize(c->st));
+        CK(cudaGetLastError());
+        return LYM_OK;
+    });
+}
+
+// MesonCorrelator::execute (correlators/MesonCorrelator.cpp:22-157) on the device: the 12
+// point sources (StochasticEstimator.cpp:100-112), their block solve, the contractions.
+int lym_meson_correlator(lym_context *c, int op_id, int solver, double precision, int max_steps, int batch,
+                         double *pion, double *scalar, double *ps, lym_solve_stats *stats)
+{
+    if (!pion || !scalar || !ps) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        const size_t vb = (size_t)c->g.V * 24 * sizeof(double);
+        std::vector<std::unique_ptr<DevBuf>> bufs;
+        std::vector<const double *> src(12);
+        std::vector<double *> sol(12);
+        const double2 one = make_double2(1.0, 0.0);
+        for (int k = 0; k < 12; ++k) {
+            const int alpha = k % 4, col = k / 4;
+            bufs.emplace_back(new DevBuf(c, vb));
+            CK(cudaMemsetAsync(bufs.back()->p, 0, vb, c->st));
+            CK(cudaMemcpyAsync((double2 *)bufs.back()->p + alpha * 3 + col, &one, sizeof(one), cudaMemcpyHostToDevice,
+                               c->st));
+            src[k] = (const double *)bufs.back()->p;
+            bufs.emplace_back(new DevBuf(c, vb));
+            sol[k] = (double *)bufs.back()->p;
+        }
+        CK(cudaStreamSynchronize(c->st));
+        const int rc = do_solve_block(c, op_id, solver, precision, max_steps, 12, src.data(), sol.data(), batch,
+                                      stats, true);
+        if (rc < 0) return rc;
+        const int rm = do_meson(c, sol.data(), pion, scalar, ps, true);
+        return rm < 0 ? rm : rc;
+    });
+}
+
+// ChiralCondensate::execute (fermion_measurements/ChiralCondensate.cpp:84-118) on the
+// device: n real Z2 noise vectors eta_k (lym_noise_z2_device streams 0..n-1 of `seed`), the
+// block solve D x_k = eta_k and, with `connected`, D y_k = x_k; per estimator k, out[8k..8k+7]
+// = <eta,x>/V, <eta,g5 x>/V, <x,x>/V, <eta,y>/V as (re, im) pairs (0 without `connected`).
+int lym_chiral_condensate(lym_context *c, int op_id, int solver, double precision, int max_steps, int batch,
+                          int n, unsigned long long seed, int connected, double *out, lym_solve_stats *stats)
+{
+    if (n < 1 || !out) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        const size_t vb = (size_t)c->g.V * 24 * sizeof(double);
+        std::vector<std::unique_ptr<DevBuf>> bufs;
+        std::vector<const double *> eta(n), xc(n);
+        std::vector<double *> x(n), y(connected ? n : 0);
+        for (int k = 0; k < n; ++k) {
+            bufs.emplace_back(new DevBuf(c, vb));
+            launch_z2_noise(c->g, (double *)bufs.back()->p, seed, (unsigned long long)k, c->st);
+            count(c, 1);
+            eta[k] = (const double *)bufs.back()->p;
+            bufs.emplace_back(new DevBuf(c, vb));
+            x[k] = (double *)bufs.back()->p;
+            xc[k] = x[k];
+            if (connected) {
+                bufs.emplace_back(new DevBuf(c, vb));
+                y[k] = (double *)bufs.back()->p;
+            }
+        }
+        CK(cudaStreamSynchronize(c->st));
+        int rc = do_solve_block(c, op_id, solver, precision, max_steps, n, eta.data(), x.data(), batch, stats, true);
+        if (rc < 0) return rc;
+        if (connected) {
+            const int rc2 = do_solve_block(c, op_id, solver, precision, max_steps, n, xc.data(), y.data(), batch,
+                                           stats ? stats + n : nullptr, true);
+            if (rc2 < 0) return rc2;
+            if (rc2 != LYM_OK) rc = rc2;
+        }
+        std::vector<double> d(2 * (size_t)n);
+        const double V = (double)c->g.V;
+        auto put = [&](int slot) {
+            for (int k = 0; k < n; ++k) {
+                out[8 * (size_t)k + 2 * slot] = d[2 * k] / V;
+                out[8 * (size_t)k + 2 * slot + 1] = d[2 * k + 1] / V;
+            }
+        };
+        int r;
+        if ((r = lym_dots_device(c, n, eta.data(), xc.data(), 0, d.data())) < 0) return r;
+        put(0);
+        if ((r = lym_dots_device(c, n, eta.data(), xc.data(), 1, d.data())) < 0) return r;
+        put(1);
+        if ((r = lym_dots_device(c, n, xc.data(), xc.data(), 0, d.data())) < 0) return r;
+        put(2);
+        if (connected) {
+            std::vector<const double *> yc(y.begin(), y.end());
+            if ((r = lym_dots_device(c, n, eta.data(), yc.data(), 0, d.data())) < 0) return r;
+            put(3);
+        } else {
+            for (int k = 0; k < n; ++k) out[8 * (size_t)k + 6] = out[8 * (size_t)k + 7] = 0.0;
+        }
+        return rc;
+    });
 }
 
 int lym_neighbour_tables(lym_context *c, int *sup, int *sdn)

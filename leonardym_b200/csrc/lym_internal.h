@@ -119,4 +119,22 @@ void launch_nbr_table(const Geom &g, int *nbr, cudaStream_t st);
 void launch_order_table(const Geom &g, int by, int bz, int *order, cudaStream_t st);
 extern const int kBatchMinBlocks[];  // the compiled variants of the batched stencil
 extern const int kBatchMinBlocksCount;
+
+// measurements on AoS spinors in device memory (lym_measure.cu)
+struct MesonProps {
+    const double2 *p[12];  // the propagator of the point source of spin a, colour c at c * 4 + a
+};
+constexpr int kMaxDots = 64;
+struct DotPairs {
+    const double2 *a[kMaxDots];
+    const double2 *b[kMaxDots];
+};
+size_t meson_scratch_bytes(const Geom &g);
+// result: [3][Lt] per time slice sums (pion, scalar, PS)
+void launch_meson_contractions(const Geom &g, const MesonProps &P, double *scratch, double *result, cudaStream_t st);
+int dot_blocks(const Geom &g);
+void launch_dots(const Geom &g, const DotPairs &D, int n, int gamma5, double2 *partials, double2 *out,
+                 cudaStream_t st);
+// real Z2 noise vector `stream` of generator `seed` (AoS full spinor)
+void launch_z2_noise(const Geom &g, double *out, unsigned long long seed, unsigned long long stream, cudaStream_t st);
 }  // namespace lym

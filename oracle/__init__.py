@@ -300,6 +300,113 @@ def rhmc_force_solves(square_op, dirac_op, betas, phi, precision=1e-12, max_step
     return rc, xs, [dirac_op.multiply(x) for x in xs]
 
 
+# gamma_t and gamma5 of the chiral basis (the reference's Gamma tables gammamu[3] and
+# _gamma5, utils/Gamma.cpp:9-11)
+GAMMA_T = np.array([[0, 0, 1, 0], [0, 0, 0, 1], [1, 0, 0, 0], [0, 1, 0, 0]], dtype=np.complex128)
+GAMMA5 = np.diag([1.0, 1.0, -1.0, -1.0]).astype(np.complex128)
+GAMMA5_GAMMA_T = GAMMA5 @ GAMMA_T
+
+
+def point_sources(dims, nc=3):
+    """StochasticEstimator::generateSource (StochasticEstimator.cpp:100-112) for every spin
+    alpha and colour c, in MesonCorrelator's order c * 4 + alpha."""
+    V = int(np.prod(dims))
+    out = []
+    for c in range(nc):
+        for alpha in range(4):
+            v = np.zeros((V, 4, nc), dtype=np.complex128)
+            v[0, alpha, c] = 1.0
+            out.append(v)
+    return out
+
+
+def meson_contractions(props, dims):
+    """The connected correlators of MesonCorrelator::execute (MesonCorrelator.cpp:98-157) of
+    the 12 point-source propagators props[c * 4 + alpha] (V, 4, 3): per time slice the pion,
+    scalar and PS summator results (before the 4 kappa^2 of the output)."""
+    V, Lt = int(np.prod(dims)), int(dims[3])
+    P = np.stack(props).reshape(3, 4, V, 4, 3)  # [c][alpha][site][mu][d]
+    t = np.arange(V) % Lt
+    G, g = GAMMA5_GAMMA_T, GAMMA_T
+    pion = np.einsum("casmd,casmd->s", P.conj(), P).real
+    scalar = np.einsum("mn,ab,casmd,cbsnd->s", G, G, P.conj(), P).real
+    ps = (-np.einsum("ab,casmd,cbsmd->s", g, P.conj(), P) + np.einsum("ab,cmsad,cmsbd->s", g, P.conj(), P)).real
+    return tuple(np.bincount(t, weights=w, minlength=Lt) for w in (pion, scalar, ps))
+
+
+def meson_contractions_loops(props, dims):
+    """meson_contractions loop for loop as MesonCorrelator.cpp:98-157 (small lattices only)."""
+    V, Lt = int(np.prod(dims)), int(dims[3])
+    pion, scalar, ps = np.zeros(Lt), np.zeros(Lt), np.zeros(Lt)
+    for alpha in range(4):
+        for c in range(3):
+            for site in range(V):
+                for mu in range(4):
+                    for d in range(3):
+                        v = props[c * 4 + alpha][site, mu, d]
+                        pion[site % Lt] += (v.conjugate() * v).real
+    for alpha in range(4):
+        for beta in range(4):
+            for c in range(3):
+                for site in range(V):
+                    for mu in range(4):
+                        for nu in range(4):
+                            for d in range(3):
+                                z = (GAMMA5_GAMMA_T[mu, nu] * GAMMA5_GAMMA_T[alpha, beta] *
+                                     props[c * 4 + alpha][site, mu, d].conjugate() * props[c * 4 + beta][site, nu, d])
+                                scalar[site % Lt] += z.real
+    for alpha in range(4):
+        for beta in range(4):
+            for c in range(3):
+                for site in range(V):
+                    for mu in range(4):
+                        for d in range(3):
+                            z = -GAMMA_T[alpha, beta] * (props[c * 4 + alpha][site, mu, d].conjugate() *
+                                                          props[c * 4 + beta][site, mu, d])
+                            z += GAMMA_T[alpha, beta] * (props[c * 4 + mu][site, alpha, d].conjugate() *
+                                                         props[c * 4 + mu][site, beta, d])
+                            ps[site % Lt] += z.real
+    return pion, scalar, ps
+
+
+def meson_output(pion, scalar, ps, kappa):
+    """The normalised correlators and PCAC mass MesonCorrelator writes (MesonCorrelator.cpp:160-193)."""
+    Lt = len(pion)
+    f = 4.0 * kappa * kappa
+    pcac = [(ps[(t - 1) % Lt] - ps[(t + 1) % Lt]) / (4.0 * pion[t]) for t in range(Lt)]
+    return {"pion_exact": list(f * np.asarray(pion)), "scalar_exact": list(f * np.asarray(scalar)),
+            "ps_exact": list(f * np.asarray(ps)), "pcac_mass": pcac}
+
+
+def _splitmix64(z):
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def z2_noise(dims, seed, stream, nc=3):
+    """The library's real Z2 noise (lym_noise_z2_device): component j of vector `stream` is
+    +1 where the top bit of splitmix64(seed + 0x9E3779B97F4A7C15 (stream 12 V + j + 1)) is
+    set, else -1 (StochasticEstimator.h:16-31 draws +-1 from a time-seeded generator)."""
+    V = int(np.prod(dims))
+    n = V * 4 * nc
+    with np.errstate(over="ignore"):
+        j = np.arange(n, dtype=np.uint64)
+        z = np.uint64(seed) + np.uint64(0x9E3779B97F4A7C15) * (np.uint64(stream) * np.uint64(n) + j + np.uint64(1))
+        z = _splitmix64(z)
+    return np.where((z >> np.uint64(63)) == 1, 1.0, -1.0).astype(np.complex128).reshape(V, 4, nc)
+
+
+def condensate_estimator(eta, x, y=None):
+    """One estimator of ChiralCondensate::execute (ChiralCondensate.cpp:92-118): <eta,x>/V,
+    <eta,gamma5 x>/V, <x,x>/V and <eta,y>/V (x = D^-1 eta, y = D^-1 x)."""
+    V = eta.shape[0]
+    g5x = x.copy()
+    g5x[:, 2:, :] *= -1
+    out = [np.vdot(eta, x) / V, np.vdot(eta, g5x) / V, np.vdot(x, x) / V, (np.vdot(eta, y) / V) if y is not None else 0j]
+    return np.array([[z.real, z.imag] for z in out]).reshape(8)
+
+
 def squared_norm(v):
     return float(np.vdot(v, v).real)
 

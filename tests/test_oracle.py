@@ -94,3 +94,23 @@ def test_solvers_converge(cfg, oracle):
     for s, a, c in zip(shifts, sols, sols2):
         assert np.linalg.norm(b - Q2.multiply_add(a, a, s)) / np.linalg.norm(b) < 2e-10
         assert np.linalg.norm(b - Q2.multiply_add(c, c, s)) / np.linalg.norm(b) < 2e-10
+
+
+def test_meson_contractions_restatements(oracle):
+    # the vectorised contraction equals the loop-for-loop restatement of MesonCorrelator.cpp:98-157
+    rng = np.random.default_rng(3)
+    dims = (2, 2, 2, 4)
+    V = 32
+    props = [rng.standard_normal((V, 4, 3)) + 1j * rng.standard_normal((V, 4, 3)) for _ in range(12)]
+    for a, b in zip(oracle.meson_contractions(props, dims), oracle.meson_contractions_loops(props, dims)):
+        assert np.max(np.abs(a - b)) <= 1e-13 * np.max(np.abs(b))
+    src = oracle.point_sources(dims)
+    assert len(src) == 12 and all(s[0, k % 4, k // 4] == 1 and np.count_nonzero(s) == 1 for k, s in enumerate(src))
+
+
+def test_z2_noise_restatement(oracle):
+    n = oracle.z2_noise((4, 4, 4, 8), 11, 2)
+    assert n.shape == (4 * 4 * 4 * 8, 4, 3) and set(np.unique(n.real)) == {-1.0, 1.0} and not n.imag.any()
+    assert abs(n.real.mean()) < 0.1
+    assert not np.array_equal(n, oracle.z2_noise((4, 4, 4, 8), 11, 3))
+    assert np.array_equal(n, oracle.z2_noise((4, 4, 4, 8), 11, 2))
