@@ -476,6 +476,20 @@ def run_ours(args, world, rank, local):
                           f"iterations (set-up {info['setup']:.2f} s, {info['t_iter']:.3f} s/iteration, "
                           f"{info['sample_seconds']:.1f} s of CPU work), extrapolated to the {n_iter} iterations "
                           f"its GPU mirror needs on the same system")}
+    # the propagator consumers of this workload's sources, after the timed region on their own
+    # clock: MesonCorrelator (the 12 point sources) and ChiralCondensate (32 Z2 noise vectors)
+    consumers = None
+    if rank == 0:
+        consumers = {}
+        for name, fn in (("meson_correlator", lambda: L.MesonCorrelator(op, tolerance=TOL, batch=args.batch)),
+                         ("chiral_condensate", lambda: L.ChiralCondensate(op, number_stochastic_estimators=N_NOISE,
+                                                                          seed=SEED, tolerance=TOL,
+                                                                          batch=args.batch))):
+            t0 = time.perf_counter()
+            res = fn().execute()
+            consumers[f"{name}_s"] = time.perf_counter() - t0
+            consumers[f"{name}_converged"] = bool(res["converged"])
+        consumers["sources"] = {"meson_correlator": 12, "chiral_condensate": N_NOISE}
     lat.close()
     serving = None
     if rank == 0 and args.serve_window > 0:  # after the timed region: its own clock
@@ -508,6 +522,7 @@ def run_ours(args, world, rank, local):
                 "d2h_bytes_per_step": nrhs * nbytes},
         "cpu_baseline": cpu,
         "serving": serving,
+        "consumers": consumers,
     }
     print(json.dumps(line), flush=True)
 
