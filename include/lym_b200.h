@@ -292,6 +292,30 @@ int lym_meson_correlator(lym_context *ctx, int op_id, int solver, double precisi
 int lym_chiral_condensate(lym_context *ctx, int op_id, int solver, double precision, int max_steps, int batch,
                           int n, unsigned long long seed, int connected, double *out, lym_solve_stats *stats);
 
+/* ---- gauge-configuration files (io/OutputSweep.cpp, starters/ReadStartGaugeConfiguration.cpp)
+ * Fundamental links (nc = 3: SU(3); nc = 2: SU(2)) in the layout of lym_gauge_upload_fundamental.
+ * LYM_GAUGE_LEONARD ("leonard_format", ReadStartGaugeConfiguration.cpp:51-130): the text
+ * descriptor <directory><name>_<number>.descriptor.txt (extents, process grid, processes,
+ * sites per process, plaquette) and one XDR file <directory><name>_<number>_<proc>.txt per
+ * process (per site x y z t and U(i,j) row by row as double pairs).  LYM_GAUGE_MUENSTER
+ * ("muenster_format"): SU(2) <directory>0:<number>:<name> (U^+ as float pairs plus the
+ * run-parameter trailer, :131-300), SU(3) <directory><name>.config-<number> (two columns of
+ * U^* as float pairs, re-orthonormalised on reading, :300-480).  Readers return
+ * LYM_ERR_NOT_FOUND for a missing file and LYM_ERR_ARGUMENT for other extents or a short
+ * file; plaquette (may be NULL) receives the value stored in the file.  Writers write one
+ * process's files (OutputSweep.cpp:32-440); beta and kappa go into the muenster trailers.
+ * Host code: usable without a GPU. */
+enum lym_gauge_format { LYM_GAUGE_LEONARD = 0, LYM_GAUGE_MUENSTER = 1 };
+int lym_gauge_file_read(int format, const int dims[4], int nc, const char *directory, const char *name, int number,
+                        double *links, double *plaquette);
+int lym_gauge_file_write(int format, const int dims[4], int nc, const double *links, const char *directory,
+                         const char *name, int number, double plaquette, double beta, double kappa);
+/* ReadStartGaugeConfiguration::readConfiguration then Environment::synchronize: read a file
+ * of the context's extents and make its fermion links resident under gauge_id, as
+ * lym_gauge_upload_fundamental with `boundary`. */
+int lym_gauge_read(lym_context *ctx, int gauge_id, int format, const char *directory, const char *name, int number,
+                   int boundary, double *plaquette);
+
 /* ---- solve server (no reference counterpart: the reference has no serving mode) -------
  * Keeps gauge fields resident by key (one context, CUDA stream and worker thread per
  * field, so work on different fields overlaps on the device) and serves solve requests

@@ -99,6 +99,9 @@ def lib():
         "lym_meson_contractions_device": (i, [vp, C.POINTER(vp), vp, vp, vp]),
         "lym_dots_device": (i, [vp, i, C.POINTER(vp), C.POINTER(vp), i, vp]),
         "lym_noise_z2_device": (i, [vp, C.c_ulonglong, C.c_ulonglong, vp]),
+        "lym_gauge_file_read": (i, [i, ip, i, C.c_char_p, C.c_char_p, i, vp, vp]),
+        "lym_gauge_file_write": (i, [i, ip, i, vp, C.c_char_p, C.c_char_p, i, dp, dp, dp]),
+        "lym_gauge_read": (i, [vp, i, i, C.c_char_p, C.c_char_p, i, i, vp]),
         "lym_meson_correlator": (i, [vp, i, i, dp, i, i, vp, vp, vp, sp]),
         "lym_chiral_condensate": (i, [vp, i, i, dp, i, i, i, C.c_ulonglong, i, vp, sp]),
         "lym_rational_evaluate_device": (i, [vp, i, i, i, vp, vp, dp, i, vp, vp, sp]),

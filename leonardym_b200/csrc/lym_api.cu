@@ -3216,6 +3216,25 @@ int lym_chiral_condensate(lym_context *c, int op_id, int solver, double precisio
     });
 }
 
+int lym_gauge_read(lym_context *c, int gauge_id, int format, const char *directory, const char *name, int number,
+                   int boundary, double *plaquette)
+{
+    if (!c) return LYM_ERR_ARGUMENT;
+    const int nc = c->rep == REP_SU3 ? 3 : 2;
+    std::vector<double> links;
+    try {
+        links.resize((size_t)c->g.V * 4 * nc * nc * 2);
+    } catch (const std::bad_alloc &) {
+        return LYM_ERR_MEMORY;
+    }
+    const int rc = lym_gauge_file_read(format, c->g.L, nc, directory, name, number, links.data(), plaquette);
+    if (rc != LYM_OK) {
+        c->err = "gauge configuration file could not be read";
+        return rc;
+    }
+    return lym_gauge_upload_fundamental(c, gauge_id, links.data(), boundary);
+}
+
 int lym_neighbour_tables(lym_context *c, int *sup, int *sdn)
 {
     if (!sup || !sdn) return LYM_ERR_ARGUMENT;
