@@ -1992,8 +1992,8 @@ private:
     void reliable_update_bicg(int j)
     {
         Slot &s = slot[j];
-        if (hs.restart[j] != 2) axpby_views(c, xs.f().slot(j), s.X.parity(1).d(), C2(1.0), C2(1.0));
-        axpby_views(c, xs.f().slot(j), xs.f().slot(j), C2(0.0), C2(0.0));
+        if (hs.restart[j] != 2) run_site(c, OpFoldClear<SlotF, SpinorD>{xs.f().slot(j), s.X.parity(1).d()}, 1);
+        else axpby_views(c, xs.f().slot(j), xs.f().slot(j), C2(0.0), C2(0.0));
         double rrS;
         true_res_S(j, rrS);
         ++s.updates;
@@ -2019,18 +2019,18 @@ private:
                 // the recursion goes on with the true residual in place of the recursive
                 // one: p += r_true - r_rec (p was formed from r_rec), r = r_true,
                 // rho = <rhat, r>, alpha = rho / <what, p>
-                double2 wp;
-                if (sprec == PREC_F) {
-                    axpby_views(c, rs.f().slot(j), ps.f().slot(j), C2(-1.0), C2(1.0));
-                    axpby_views(c, (*rS).d(), ps.f().slot(j), C2(1.0), C2(1.0));
-                } else {
-                    axpby_views(c, rs.f().slot(j), ps.h().slot(j), C2(-1.0), C2(1.0));
-                    axpby_views(c, (*rS).d(), ps.h().slot(j), C2(1.0), C2(1.0));
-                }
-                axpby_views(c, (*rS).d(), rs.f().slot(j), C2(1.0), C2(0.0));
-                hs.rho[j] = slot_dot(rhat->f().slot(j), (*rS).d());
-                if (sprec == PREC_F) wp = slot_dot(what->f().slot(j), ps.f().slot(j));
-                else wp = slot_dot(what->f().slot(j), ps.h().slot(j));
+                if (sprec == PREC_F)
+                    run_site(c, OpBiContinue<SlotF, SlotF, SpinorD, SlotF, SlotF>{
+                                    rs.f().slot(j), ps.f().slot(j), (*rS).d(), rhat->f().slot(j), what->f().slot(j),
+                                    c->d_scal}, 1);
+                else
+                    run_site(c, OpBiContinue<SlotF, SlotH, SpinorD, SlotF, SlotF>{
+                                    rs.f().slot(j), ps.h().slot(j), (*rS).d(), rhat->f().slot(j), what->f().slot(j),
+                                    c->d_scal}, 1);
+                CK(cudaMemcpyAsync(c->h_scal, c->d_scal, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+                CK(cudaStreamSynchronize(c->st));
+                hs.rho[j] = make_double2(c->h_scal[0], c->h_scal[1]);
+                const double2 wp = make_double2(c->h_scal[2], c->h_scal[3]);
                 hs.alpha[j] = cdiv(hs.rho[j], wp);
                 hs.rr[j] = hs.rr_max[j] = rrS;
                 hs.active[j] = 1;
@@ -2094,8 +2094,7 @@ private:
             return;
         }
         Slot &s = slot[j];
-        axpby_views(c, xs.f().slot(j), s.X.parity(1).d(), C2(1.0), C2(1.0));
-        axpby_views(c, xs.f().slot(j), xs.f().slot(j), C2(0.0), C2(0.0));
+        run_site(c, OpFoldClear<SlotF, SpinorD>{xs.f().slot(j), s.X.parity(1).d()}, 1);
         double rrS, rrN;
         true_res(j, rrS, rrN);
         ++s.updates;
@@ -2104,8 +2103,11 @@ private:
             finish(j);
         } else {
             if (hs.converged[j]) hs.eps[j] = std::max(hs.eps[j] * 0.5 * s.epsS / rrS, 1e-300);
-            axpby_views(c, (*rN).d(), rs.f().slot(j), C2(1.0), C2(0.0));
-            set_direction(j, rrN / hs.rr_prev[j]);
+            const double b = rrN / hs.rr_prev[j];
+            if (sprec == PREC_F)
+                run_site(c, OpCGContinue<SlotF, SlotF, SpinorD>{rs.f().slot(j), ps.f().slot(j), (*rN).d(), b}, 1);
+            else
+                run_site(c, OpCGContinue<SlotF, SlotH, SpinorD>{rs.f().slot(j), ps.h().slot(j), (*rN).d(), b}, 1);
             hs.rr[j] = hs.rr_max[j] = rrN;
             hs.active[j] = 1;  // back into the iteration
         }

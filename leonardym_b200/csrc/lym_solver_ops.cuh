@@ -61,6 +61,77 @@ template <class SA, class SB> struct OpDot {  // sum conj(a) b -> out[0..1]
     }
 };
 
+// x += a, a = 0: a reduced-precision solution accumulator folded into the FP64 solution
+template <class SA, class SX> struct OpFoldClear {
+    static constexpr int NRED = 0;
+    SA a;
+    SX x;
+    LYM_D void site(int p, int h, double *) const
+    {
+        cx<double> av[12], xv[12];
+        a.par(p).template load<double>(h, av);
+        x.par(p).template load<double>(h, xv);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+            xv[k] = xv[k] + av[k];
+            av[k] = cx<double>{0.0, 0.0};
+        }
+        x.par(p).template store<double>(h, xv);
+        a.par(p).template store<double>(h, av);
+    }
+};
+
+// BiCGStab going on after a reliable update with the true residual rt in place of the
+// recursive r: p += rt - r, r = rt; out = (<rh, rt>, <w, p>) with p as stored
+template <class SR, class SP, class ST, class SH, class SW> struct OpBiContinue {
+    static constexpr int NRED = 4;
+    SR r;
+    SP p;
+    ST rt;
+    SH rh;
+    SW w;
+    double *out;
+    LYM_D void site(int q, int h, double *acc) const
+    {
+        cx<double> rv[12], pv[12], tv[12];
+        r.par(q).template load<double>(h, rv);
+        p.par(q).template load<double>(h, pv);
+        rt.par(q).template load<double>(h, tv);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) pv[k] = pv[k] + tv[k] - rv[k];
+        p.par(q).template store<double>(h, pv);
+        r.par(q).template store<double>(h, tv);
+        p.par(q).template load<double>(h, pv);  // the stored direction
+        rh.par(q).template load<double>(h, rv);
+        dotc(rv, tv, acc[0], acc[1]);
+        w.par(q).template load<double>(h, rv);
+        dotc(rv, pv, acc[2], acc[3]);
+    }
+    LYM_D void finalize(const double *t) const
+    {
+        for (int k = 0; k < 4; ++k) out[k] = t[k];
+    }
+};
+
+// CG going on after a reliable update: r = rt, p = rt + b p
+template <class SR, class SP, class ST> struct OpCGContinue {
+    static constexpr int NRED = 0;
+    SR r;
+    SP p;
+    ST rt;
+    double b;
+    LYM_D void site(int q, int h, double *) const
+    {
+        cx<double> pv[12], tv[12];
+        p.par(q).template load<double>(h, pv);
+        rt.par(q).template load<double>(h, tv);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) pv[k] = tv[k] + b * pv[k];
+        p.par(q).template store<double>(h, pv);
+        r.par(q).template store<double>(h, tv);
+    }
+};
+
 template <class SA> struct OpNorm {
     static constexpr int NRED = 1;
     SA a;
