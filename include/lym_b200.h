@@ -253,6 +253,18 @@ int lym_rhmc_force_solves_device(lym_context *ctx, int square_op_id, int dirac_o
                                  const double *betas, double precision, int max_steps, const double *phi,
                                  double **x, double **y, lym_solve_stats *stats);
 
+/* FermionForce::derivative (hmc_forces/FermionForce.cpp:11-20) for the operator op_id:
+ * force[x][mu] -= weight * F_mu(x), F the per-link matrix of ImprovedFermionForce
+ * (hmc_forces/ImprovedFermionForce.cpp:11-223: the clover-leaf terms / 4 plus the Wilson part;
+ * the kinds with a clover term, at the operator's kappa and c_sw) or DiracWilsonFermionForce
+ * (hmc_forces/DiracWilsonFermionForce.cpp:10-53; DiracWilson kinds), from the spinors X, Y
+ * (NFlavorFermionAction's x_i and y_i = D x_i) on the operator's gauge field.  force: the
+ * fermion force field in the reference's layout, double[V][4][3][3][2] (complex 3x3 matrices,
+ * column-major), read and updated in place.  _device: device pointers. */
+int lym_fermion_force(lym_context *ctx, int op_id, const double *X, const double *Y, double weight, double *force);
+int lym_fermion_force_device(lym_context *ctx, int op_id, const double *X, const double *Y, double weight,
+                             double *force);
+
 /* ---- propagator consumers (correlators/MesonCorrelator.cpp,
  * fermion_measurements/ChiralCondensate.cpp) ---------------------------------------------
  * The connected contractions of MesonCorrelator::execute (MesonCorrelator.cpp:98-157) of

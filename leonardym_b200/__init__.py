@@ -9,7 +9,7 @@ from .dirac import (DiracOperator, DiracWilsonOperator, EvenOddImprovedDiracWils
                     ImprovedDiracWilsonOperator, Lattice, SquareDiracWilsonOperator,
                     SquareEvenOddImprovedDiracWilsonOperator, SquareImprovedDiracWilsonOperator)
 from .measurements import ChiralCondensate, MesonCorrelator
-from .rhmc import NFlavorFermionAction, RationalApproximation
+from .rhmc import FermionForce, NFlavorFermionAction, RationalApproximation
 from .solvers import (BiConjugateGradient, ConjugateGradient, EvenOddBiCGStab, EvenOddConjugateGradient,
                       MultishiftSolver, PreconditionedBiCGStab, Solver)
 
@@ -19,5 +19,5 @@ __all__ = [
     "SquareDiracWilsonOperator", "SquareImprovedDiracWilsonOperator", "SquareEvenOddImprovedDiracWilsonOperator",
     "Solver", "ConjugateGradient", "BiConjugateGradient", "PreconditionedBiCGStab", "EvenOddConjugateGradient",
     "EvenOddBiCGStab",
-    "MultishiftSolver", "RationalApproximation", "NFlavorFermionAction", "MesonCorrelator", "ChiralCondensate",
+    "MultishiftSolver", "RationalApproximation", "NFlavorFermionAction", "MesonCorrelator", "ChiralCondensate", "FermionForce",
 ]

@@ -100,6 +100,8 @@ def lib():
         "lym_dots_device": (i, [vp, i, C.POINTER(vp), C.POINTER(vp), i, vp]),
         "lym_noise_z2_device": (i, [vp, C.c_ulonglong, C.c_ulonglong, vp]),
         "lym_gauge_file_read": (i, [i, ip, i, C.c_char_p, C.c_char_p, i, vp, vp]),
+        "lym_fermion_force": (i, [vp, i, vp, vp, dp, vp]),
+        "lym_fermion_force_device": (i, [vp, i, vp, vp, dp, vp]),
         "lym_gauge_file_write": (i, [i, ip, i, vp, C.c_char_p, C.c_char_p, i, dp, dp, dp]),
         "lym_gauge_read": (i, [vp, i, i, C.c_char_p, C.c_char_p, i, i, vp]),
         "lym_meson_correlator": (i, [vp, i, i, dp, i, i, vp, vp, vp, sp]),

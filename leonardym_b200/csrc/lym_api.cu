@@ -3237,6 +3237,51 @@ int lym_gauge_read(lym_context *c, int gauge_id, int format, const char *directo
     return lym_gauge_upload_fundamental(c, gauge_id, links.data(), boundary);
 }
 
+// FermionForce::derivative (hmc_forces/FermionForce.cpp:11-20) of the operator's force:
+// ImprovedFermionForce for the kinds with the clover term, DiracWilsonFermionForce otherwise
+static int do_fermion_force(lym_context *c, int op_id, const double *X, const double *Y, double weight,
+                            double *force, bool device_ptr)
+{
+    if (!X || !Y || !force) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        OpEntry &op = op_of(c, op_id);
+        GaugeEntry &ge = gauge_of(c, op.gauge_id);
+        const size_t vb = (size_t)c->g.V * 24 * sizeof(double), fb = (size_t)c->g.V * 4 * 9 * sizeof(double2);
+        std::unique_ptr<DevBuf> bx, by, bf;
+        const double *dX = X, *dY = Y;
+        double *dF = force;
+        if (!device_ptr) {
+            bx.reset(new DevBuf(c, vb));
+            by.reset(new DevBuf(c, vb));
+            bf.reset(new DevBuf(c, fb));
+            CK(cudaMemcpyAsync(bx->p, X, vb, cudaMemcpyHostToDevice, c->st));
+            CK(cudaMemcpyAsync(by->p, Y, vb, cudaMemcpyHostToDevice, c->st));
+            CK(cudaMemcpyAsync(bf->p, force, fb, cudaMemcpyHostToDevice, c->st));
+            dX = (const double *)bx->p;
+            dY = (const double *)by->p;
+            dF = (double *)bf->p;
+        }
+        launch_fermion_force(c->g, ge.dev, (const double2 *)dX, (const double2 *)dY, op.kappa, op.csw,
+                             kind_has_clover(op.kind) ? 1 : 0, weight, (double2 *)dF, c->st);
+        count(c, 1);
+        if (!device_ptr) CK(cudaMemcpyAsync(force, dF, fb, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        CK(cudaGetLastError());
+        return LYM_OK;
+    });
+}
+
+int lym_fermion_force(lym_context *c, int op_id, const double *X, const double *Y, double weight, double *force)
+{
+    return do_fermion_force(c, op_id, X, Y, weight, force, false);
+}
+
+int lym_fermion_force_device(lym_context *c, int op_id, const double *X, const double *Y, double weight,
+                             double *force)
+{
+    return do_fermion_force(c, op_id, X, Y, weight, force, true);
+}
+
 int lym_neighbour_tables(lym_context *c, int *sup, int *sdn)
 {
     if (!sup || !sdn) return LYM_ERR_ARGUMENT;

@@ -164,6 +164,11 @@ class DiracOperator:
     def getKappa(self):
         return self._kappa
 
+    def getForce(self):
+        """DiracOperator::getForce: the fermion force of this operator (on the GPU)."""
+        from .rhmc import FermionForce
+        return FermionForce(self)
+
     def setCSW(self, csw):
         self._csw = float(csw)
         if self._op is not None:

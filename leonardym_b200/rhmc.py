@@ -1,7 +1,7 @@
 """RHMC consumers of the multishift solvers, on the GPU through the C ABI:
-RationalApproximation (dirac_functions/RationalApproximation.{h,cpp}) and the solve and
-energy parts of NFlavorFermionAction (actions/NFlavorFermionAction.cpp:76-96,193-207).
-The fermion force derivative itself (hmc_forces/) is not part of this module."""
+RationalApproximation (dirac_functions/RationalApproximation.{h,cpp}), the fermion force
+(hmc_forces/FermionForce, DiracWilsonFermionForce, ImprovedFermionForce) and the solve, force
+and energy parts of NFlavorFermionAction (actions/NFlavorFermionAction.cpp:76-117,193-207)."""
 from __future__ import annotations
 
 import ctypes as C
@@ -81,6 +81,28 @@ class RationalApproximation:
         return self.maximumSteps
 
 
+class FermionForce:
+    """The fermion force of an operator (DiracOperator::getForce): ImprovedFermionForce at the
+    operator's kappa and c_sw for the kinds with a clover term, DiracWilsonFermionForce
+    otherwise, on the operator's gauge field."""
+
+    def __init__(self, diracOperator):
+        self.diracOperator = diracOperator
+
+    def derivative(self, fermionForce, X, Y, weight):
+        """FermionForce::derivative (FermionForce.cpp:11-20): fermionForce[x][mu] -=
+        weight * F_mu(x); fermionForce complex128[V, 4, 3, 3] (column-major matrices), in place."""
+        op = self.diracOperator
+        x, y = op._vec(X), op._vec(Y)
+        if fermionForce.dtype != np.complex128 or not fermionForce.flags.c_contiguous:
+            raise LymError(-1, "the force field must be a contiguous complex128 array")
+        rc = lib().lym_fermion_force(op.lattice.handle, op.op_id, _p(x), _p(y), float(weight),
+                                     _p(fermionForce))
+        if rc < 0:
+            raise LymError(rc, lib().lym_last_error(op.lattice.handle).decode())
+        return fermionForce
+
+
 class NFlavorFermionAction:
     """The multishift parts of NFlavorFermionAction: one RationalApproximation per
     pseudofermion, `squareDiracOperator` the operator A of the approximations and
@@ -132,3 +154,23 @@ class NFlavorFermionAction:
             Xs.append(X)
             Ys.append(Y)
         return Xs, Ys
+
+    def fermionForce(self, boundary_conditions="fermion_antiperiodic"):
+        """The fermion force lattice of NFlavorFermionAction::updateForce / derivative
+        (NFlavorFermionAction.cpp:53-117): for every approximation and shift,
+        force -= alpha_i F(x_i, y_i), then with antiperiodic boundary conditions the sign of
+        the t links at t = Lt - 1 (the projection onto the gauge algebra, FermionForce::force,
+        is not included)."""
+        lat = self.diracOperator.lattice
+        force = np.zeros((lat.V, 4, 3, 3), np.complex128)
+        ff = FermionForce(self.diracOperator)
+        Xs, Ys = self.solves()
+        for approx, X, Y in zip(self.rationalApproximations, Xs, Ys):
+            for alpha, x, y in zip(approx.alphas, X, Y):
+                ff.derivative(force, x, y, alpha)
+        if boundary_conditions == "fermion_antiperiodic":
+            Lt = lat.dims[3]
+            force.reshape(-1, Lt, 4, 3, 3)[:, Lt - 1, 3] *= -1
+        elif boundary_conditions != "fermion_periodic":
+            raise LymError(-4, f"boundary conditions {boundary_conditions!r}")
+        return force

@@ -37,6 +37,7 @@ def lib(rep):
         L.ref_solve2.argtypes = [ip, i, dp, dp, i, vp, i, dp, i, i, i, dp, dp, vp, vp, ip]
         L.ref_multishift.argtypes = [ip, i, dp, dp, i, vp, i, i, vp, dp, i, vp, C.POINTER(C.c_void_p)]
         L.ref_rational_evaluate.argtypes = [ip, i, dp, dp, i, vp, i, i, vp, vp, dp, i, vp, vp]
+        L.ref_fermion_force.argtypes = [ip, i, dp, dp, vp, vp, vp, dp, vp]
         L.ref_neighbours.argtypes = [ip, ip, ip]
         L.ref_antiperiodic.argtypes = [ip, vp]
         if hasattr(L, "ref_to_adjoint"):
@@ -133,6 +134,20 @@ def _rational(self, kind, algorithm, alphas, betas, b, precision, max_steps, kap
 
 
 Reference.rational_evaluate = _rational
+
+
+def _fermion_force(self, kind, kappa, csw, X, Y, weight, force):
+    """FermionForce::derivative of DiracWilsonFermionForce ("DiracWilson") or
+    ImprovedFermionForce ("Improved"); returns force - weight * derivative."""
+    X = np.ascontiguousarray(X, np.complex128)
+    Y = np.ascontiguousarray(Y, np.complex128)
+    out = np.ascontiguousarray(force, np.complex128).copy()
+    self.L.ref_fermion_force(_d(self.dims), {"DiracWilson": 0, "Improved": 1}[kind], kappa, csw, _p(self.links),
+                             _p(X), _p(Y), float(weight), _p(out))
+    return out
+
+
+Reference.fermion_force = _fermion_force
 
 
 def neighbours(dims, rep="su3"):

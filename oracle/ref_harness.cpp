@@ -11,6 +11,8 @@
 
 #include "algebra_utils/AlgebraUtils.h"
 #include "dirac_functions/RationalApproximation.h"
+#include "hmc_forces/DiracWilsonFermionForce.h"
+#include "hmc_forces/ImprovedFermionForce.h"
 #include "dirac_operators/DiracWilsonOperator.h"
 #include "dirac_operators/EvenOddImprovedDiracWilsonOperator.h"
 #include "dirac_operators/ImprovedDiracWilsonOperator.h"
@@ -294,6 +296,34 @@ int ref_rational_evaluate(const int dims[4], int kind, double kappa, double csw,
     store(o, out);
     delete ms;
     delete op;
+    return 1;
+}
+
+// FermionForce::derivative of DiracWilsonFermionForce (kind 0) or ImprovedFermionForce (1):
+// force[x][mu] -= weight * derivative(x, mu), force read and written in place
+int ref_fermion_force(const int dims[4], int kind, double kappa, double csw, const double *links, const double *X,
+                      const double *Y, double weight, double *force)
+{
+    init_layout(dims);
+    extended_fermion_lattice_t L;
+    load(L, links);
+    extended_dirac_vector_t x, y;
+    load(x, X);
+    load(y, Y);
+    extended_fermion_force_lattice_t F;
+    load(F, force);
+    // the derived classes' per-link derivative(...) hides the base class's field overload
+    if (kind == 0) {
+        DiracWilsonFermionForce f(kappa);
+        FermionForce &base = f;
+        base.derivative(F, L, x, y, weight);
+    } else {
+        ImprovedFermionForce f(kappa, csw);
+        f.setLattice(L);
+        FermionForce &base = f;
+        base.derivative(F, L, x, y, weight);
+    }
+    store(F, force);
     return 1;
 }
 

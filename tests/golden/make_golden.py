@@ -62,6 +62,12 @@ def make(rep):
                                       prec, 5000, kappa, csw, True)
         assert rc == 1
         out[f"rational/{kind}"] = r
+    # FermionForce::derivative of the Wilson and improved forces (hmc_forces/), weight 0.7 on a
+    # zero field; the first 64 sites are kept
+    V = int(np.prod(DIMS))
+    zero = np.zeros((V, 4, 3, 3), np.complex128)
+    for kind in ("DiracWilson", "Improved"):
+        out[f"force/{kind}"] = ref.fermion_force(kind, kappa, csw, x, y, 0.7, zero)[:64]
     # BiCGStab(l) and BiCGStab with a preconditioner operator (BiConjugateGradient.cpp:11-317)
     for l in (2, 4):
         rc, sol, steps = ref.solve2("SquareImproved", "bicgstab_l", x, prec, 5000, kappa, csw, True, l=l)

@@ -99,3 +99,17 @@ def test_rational_evaluate_golden(gold):
         out = gold["lat"].new_vector()
         ra.evaluate(make(gold, kind), out, x)
         assert rel(out, gold[f"rational/{kind}"]) < 1e-8
+
+
+def test_fermion_force_golden(gold):
+    # the GPU fermion force against the compiled reference's FermionForce::derivative
+    dims = gold["lat"].dims
+    for kind, cls in (("DiracWilson", L.DiracWilsonOperator), ("Improved", L.ImprovedDiracWilsonOperator)):
+        op = cls(gold["lat"], float(gold["kappa"]))
+        if kind == "Improved":
+            op.setCSW(float(gold["csw"]))
+        op.setLattice(gold["gid"])
+        f = np.zeros((int(np.prod(dims)), 4, 3, 3), np.complex128)
+        op.getForce().derivative(f, gold["x"], gold["y"], 0.7)
+        ref = gold[f"force/{kind}"]
+        assert np.max(np.abs(f[:64] - ref)) <= 1e-13 * np.max(np.abs(ref))

@@ -149,3 +149,15 @@ def test_rational_evaluate_pinned(gold, oracle):
         assert rel(out, gold[f"rational/{kind}"]) < 1e-10
     assert abs(oracle.rational_value(alphas, betas, 0.5 + 0.1j) -
                sum(a / (0.5 + 0.1j + b) for a, b in zip(alphas, betas))) < 1e-15
+
+
+def test_fermion_force_pinned(gold, oracle):
+    # FermionForce::derivative of DiracWilsonFermionForce / ImprovedFermionForce (hmc_forces/)
+    from oracle import force as OF
+    dims = tuple(int(d) for d in gold["dims"])
+    zero = np.zeros((int(np.prod(dims)), 4, 3, 3), np.complex128)
+    for kind, clover in (("DiracWilson", False), ("Improved", True)):
+        f = OF.fermion_force(dims, gold["links"], gold["x"], gold["y"], float(gold["kappa"]), float(gold["csw"]),
+                             clover, 0.7, zero)
+        ref = gold[f"force/{kind}"]
+        assert np.max(np.abs(f[:64] - ref)) <= 1e-13 * np.max(np.abs(ref))
