@@ -657,7 +657,26 @@ def run_rhmc(args, world, rank, local, dims=RHMC_DIMS):
             raise RuntimeError(lib.lym_last_error(ctx))
         consumer["force_solves_s"] = time.perf_counter() - t0
     consumer["energy"] = float(torch.vdot(b.flatten(), r_out.flatten()).real)
-    del ys, r_out
+    # the fermion force of one shift's (x, y) pair on the whole field (FermionForce::derivative)
+    fop = C.c_int(0)
+    lib.lym_operator_create(ctx, 1, 1, RHMC_KAPPA, RHMC_CSW, 1, C.byref(fop))
+    force = torch.zeros((lat.V, 4, 3, 3), dtype=torch.complex128, device=dev)
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if lib.lym_fermion_force_device(ctx, fop.value, C.c_void_p(sols[0].data_ptr()), C.c_void_p(ys[0].data_ptr()),
+                                        float(alphas[0]), C.c_void_p(force.data_ptr())) != 0:
+            raise RuntimeError(lib.lym_last_error(ctx))
+        consumer["fermion_force_s"] = time.perf_counter() - t0
+    # all 12 shifts' pairs in one pass (NFlavorFermionAction's sum over the shifts)
+    for _ in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if lib.lym_fermion_force_multi_device(ctx, fop.value, nsh, ptrs, yptrs, alphas.ctypes.data_as(C.c_void_p),
+                                              C.c_void_p(force.data_ptr())) != 0:
+            raise RuntimeError(lib.lym_last_error(ctx))
+        consumer["fermion_force_12_pairs_s"] = time.perf_counter() - t0
+    del ys, r_out, force
     torch.cuda.empty_cache()
 
     # the plain FP64 multishift CG on the same system (one solve)

@@ -116,6 +116,10 @@ const char *lym_last_error(lym_context *ctx);
 int lym_context_volume(lym_context *ctx);
 /* bytes of device memory held by the context (gauge fields, clover terms, work vectors) */
 size_t lym_context_device_bytes(lym_context *ctx);
+/* Frees the context's cache of idle work spinors and host-transfer staging buffers (they are
+ * allocated again when needed).  A device allocation that fails trims the cache and retries
+ * once by itself. */
+int lym_context_trim(lym_context *ctx);
 int lym_synchronize(lym_context *ctx);
 
 /* ---- gauge fields, resident by id ----------------------------------------------
@@ -264,6 +268,13 @@ int lym_rhmc_force_solves_device(lym_context *ctx, int square_op_id, int dirac_o
 int lym_fermion_force(lym_context *ctx, int op_id, const double *X, const double *Y, double weight, double *force);
 int lym_fermion_force_device(lym_context *ctx, int op_id, const double *X, const double *Y, double weight,
                              double *force);
+/* The same for n pairs at once, force -= sum_i weights[i] F(X[i], Y[i]) (NFlavorFermionAction's
+ * sum over the shifts, NFlavorFermionAction.cpp:53-75): the link products of each clover leaf
+ * are formed once for all pairs. */
+int lym_fermion_force_multi(lym_context *ctx, int op_id, int n, const double *const *X, const double *const *Y,
+                            const double *weights, double *force);
+int lym_fermion_force_multi_device(lym_context *ctx, int op_id, int n, const double *const *X,
+                                   const double *const *Y, const double *weights, double *force);
 
 /* ---- propagator consumers (correlators/MesonCorrelator.cpp,
  * fermion_measurements/ChiralCondensate.cpp) ---------------------------------------------

@@ -67,6 +67,7 @@ def lib():
         "lym_last_error": (C.c_char_p, [vp]),
         "lym_context_volume": (i, [vp]),
         "lym_context_device_bytes": (C.c_size_t, [vp]),
+        "lym_context_trim": (i, [vp]),
         "lym_synchronize": (i, [vp]),
         "lym_gauge_upload": (i, [vp, i, vp]),
         "lym_gauge_upload_device": (i, [vp, i, vp]),
@@ -102,6 +103,8 @@ def lib():
         "lym_gauge_file_read": (i, [i, ip, i, C.c_char_p, C.c_char_p, i, vp, vp]),
         "lym_fermion_force": (i, [vp, i, vp, vp, dp, vp]),
         "lym_fermion_force_device": (i, [vp, i, vp, vp, dp, vp]),
+        "lym_fermion_force_multi": (i, [vp, i, i, C.POINTER(vp), C.POINTER(vp), vp, vp]),
+        "lym_fermion_force_multi_device": (i, [vp, i, i, C.POINTER(vp), C.POINTER(vp), vp, vp]),
         "lym_gauge_file_write": (i, [i, ip, i, vp, C.c_char_p, C.c_char_p, i, dp, dp, dp]),
         "lym_gauge_read": (i, [vp, i, i, C.c_char_p, C.c_char_p, i, i, vp]),
         "lym_meson_correlator": (i, [vp, i, i, dp, i, i, vp, vp, vp, sp]),

@@ -124,10 +124,35 @@ template <class F> int guarded(lym_context *c, F f)
     }
 }
 
+size_t spinor_bytes(const Geom &g, int prec, int nparity);
+
+// frees the idle spinors of the pool and the host-transfer staging buffers
+void trim_pool(lym_context *c)
+{
+    if (c->st) cudaStreamSynchronize(c->st);
+    for (auto &s : c->pool) {
+        cudaFree(s.v);
+        c->bytes -= spinor_bytes(c->g, s.prec, s.nparity);
+    }
+    c->pool.clear();
+    for (int k = 0; k < 3; ++k)
+        if (c->aos[k]) {
+            cudaFree(c->aos[k]);
+            c->bytes -= (size_t)c->g.V * 24 * sizeof(double);
+            c->aos[k] = nullptr;
+        }
+}
+
 void *dev_alloc(lym_context *c, size_t bytes)
 {
     void *p = nullptr;
     cudaError_t e = cudaMalloc(&p, bytes);
+    if (e == cudaErrorMemoryAllocation && !c->capturing && (!c->pool.empty() || c->aos[0] || c->aos[1] || c->aos[2])) {
+        // the idle pooled spinors are a cache: give them back and try once more
+        cudaGetLastError();
+        trim_pool(c);
+        e = cudaMalloc(&p, bytes);
+    }
     if (e != cudaSuccess) {
         cudaGetLastError();
         fail(c, LYM_ERR_MEMORY, "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
@@ -2294,6 +2319,14 @@ int lym_context_volume(lym_context *c) { return c ? c->g.V : 0; }
 
 size_t lym_context_device_bytes(lym_context *c) { return c ? c->bytes : 0; }
 
+int lym_context_trim(lym_context *c)
+{
+    return guarded(c, [&]() {
+        trim_pool(c);
+        return LYM_OK;
+    });
+}
+
 int lym_synchronize(lym_context *c)
 {
     return guarded(c, [&]() {
@@ -3237,33 +3270,52 @@ int lym_gauge_read(lym_context *c, int gauge_id, int format, const char *directo
     return lym_gauge_upload_fundamental(c, gauge_id, links.data(), boundary);
 }
 
-// FermionForce::derivative (hmc_forces/FermionForce.cpp:11-20) of the operator's force:
-// ImprovedFermionForce for the kinds with the clover term, DiracWilsonFermionForce otherwise
-static int do_fermion_force(lym_context *c, int op_id, const double *X, const double *Y, double weight,
-                            double *force, bool device_ptr)
+// FermionForce::derivative (hmc_forces/FermionForce.cpp:11-20) of the operator's force for n
+// weighted pairs: ImprovedFermionForce for the kinds with the clover term,
+// DiracWilsonFermionForce otherwise
+static int do_fermion_force(lym_context *c, int op_id, int n, const double *const *X, const double *const *Y,
+                            const double *weights, double *force, bool device_ptr)
 {
-    if (!X || !Y || !force) return LYM_ERR_ARGUMENT;
+    if (n < 1 || !X || !Y || !weights || !force) return LYM_ERR_ARGUMENT;
+    for (int i = 0; i < n; ++i)
+        if (!X[i] || !Y[i]) return LYM_ERR_ARGUMENT;
     return guarded(c, [&]() {
         OpEntry &op = op_of(c, op_id);
         GaugeEntry &ge = gauge_of(c, op.gauge_id);
         const size_t vb = (size_t)c->g.V * 24 * sizeof(double), fb = (size_t)c->g.V * 4 * 9 * sizeof(double2);
-        std::unique_ptr<DevBuf> bx, by, bf;
-        const double *dX = X, *dY = Y;
+        std::vector<std::unique_ptr<DevBuf>> bufs;
+        std::vector<const double2 *> hx(n), hy(n);
         double *dF = force;
-        if (!device_ptr) {
-            bx.reset(new DevBuf(c, vb));
-            by.reset(new DevBuf(c, vb));
-            bf.reset(new DevBuf(c, fb));
-            CK(cudaMemcpyAsync(bx->p, X, vb, cudaMemcpyHostToDevice, c->st));
-            CK(cudaMemcpyAsync(by->p, Y, vb, cudaMemcpyHostToDevice, c->st));
-            CK(cudaMemcpyAsync(bf->p, force, fb, cudaMemcpyHostToDevice, c->st));
-            dX = (const double *)bx->p;
-            dY = (const double *)by->p;
-            dF = (double *)bf->p;
+        for (int i = 0; i < n; ++i) {
+            if (device_ptr) {
+                hx[i] = (const double2 *)X[i];
+                hy[i] = (const double2 *)Y[i];
+                continue;
+            }
+            bufs.emplace_back(new DevBuf(c, vb));
+            CK(cudaMemcpyAsync(bufs.back()->p, X[i], vb, cudaMemcpyHostToDevice, c->st));
+            hx[i] = (const double2 *)bufs.back()->p;
+            bufs.emplace_back(new DevBuf(c, vb));
+            CK(cudaMemcpyAsync(bufs.back()->p, Y[i], vb, cudaMemcpyHostToDevice, c->st));
+            hy[i] = (const double2 *)bufs.back()->p;
         }
-        launch_fermion_force(c->g, ge.dev, (const double2 *)dX, (const double2 *)dY, op.kappa, op.csw,
-                             kind_has_clover(op.kind) ? 1 : 0, weight, (double2 *)dF, c->st);
-        count(c, 1);
+        if (!device_ptr) {
+            bufs.emplace_back(new DevBuf(c, fb));
+            CK(cudaMemcpyAsync(bufs.back()->p, force, fb, cudaMemcpyHostToDevice, c->st));
+            dF = (double *)bufs.back()->p;
+        }
+        DevBuf tab(c, (size_t)n * (2 * sizeof(void *) + sizeof(double)));
+        char *t = (char *)tab.p;
+        CK(cudaMemcpyAsync(t, hx.data(), n * sizeof(void *), cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(t + n * sizeof(void *), hy.data(), n * sizeof(void *), cudaMemcpyHostToDevice, c->st));
+        CK(cudaMemcpyAsync(t + 2 * n * sizeof(void *), weights, n * sizeof(double), cudaMemcpyHostToDevice, c->st));
+        const int clover = kind_has_clover(op.kind) ? 1 : 0;
+        std::unique_ptr<DevBuf> scratch;
+        if (clover) scratch.reset(new DevBuf(c, fermion_force_scratch_bytes(c->g)));
+        launch_fermion_force(c->g, ge.dev, n, (const double2 *const *)t, (const double2 *const *)(t + n * sizeof(void *)),
+                             (const double *)(t + 2 * n * sizeof(void *)), op.kappa, op.csw, clover, (double2 *)dF,
+                             clover ? (double2 *)scratch->p : nullptr, c->st);
+        count(c, 1 + clover);
         if (!device_ptr) CK(cudaMemcpyAsync(force, dF, fb, cudaMemcpyDeviceToHost, c->st));
         CK(cudaStreamSynchronize(c->st));
         CK(cudaGetLastError());
@@ -3273,13 +3325,25 @@ static int do_fermion_force(lym_context *c, int op_id, const double *X, const do
 
 int lym_fermion_force(lym_context *c, int op_id, const double *X, const double *Y, double weight, double *force)
 {
-    return do_fermion_force(c, op_id, X, Y, weight, force, false);
+    return do_fermion_force(c, op_id, 1, &X, &Y, &weight, force, false);
 }
 
 int lym_fermion_force_device(lym_context *c, int op_id, const double *X, const double *Y, double weight,
                              double *force)
 {
-    return do_fermion_force(c, op_id, X, Y, weight, force, true);
+    return do_fermion_force(c, op_id, 1, &X, &Y, &weight, force, true);
+}
+
+int lym_fermion_force_multi(lym_context *c, int op_id, int n, const double *const *X, const double *const *Y,
+                            const double *weights, double *force)
+{
+    return do_fermion_force(c, op_id, n, X, Y, weights, force, false);
+}
+
+int lym_fermion_force_multi_device(lym_context *c, int op_id, int n, const double *const *X, const double *const *Y,
+                                   const double *weights, double *force)
+{
+    return do_fermion_force(c, op_id, n, X, Y, weights, force, true);
 }
 
 int lym_neighbour_tables(lym_context *c, int *sup, int *sdn)

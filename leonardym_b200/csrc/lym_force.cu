@@ -82,13 +82,92 @@ LYM_D void add_tensor(M3 &F, double s, const C x[3], const C y[3])
 
 struct ForceArg {
     Geom g;
-    const void *links;  // FP64 fermion links [2][4][9][stride] (complex, or real for the adjoint)
-    int rep;
-    const double2 *X, *Y;
+    int n;                     // pairs (x_i, y_i) with weights w_i
+    const double2 *const *X;   // device array [n] of AoS spinors
+    const double2 *const *Y;
+    const double *w;           // device array [n]
     double2 *force;
-    double kappa, csw, weight;
+    const double2 *N;  // [V][6][3][3] plane matrices (clover only)
+    double kappa, csw;
     int clover;
 };
+
+// planes (mu < nu): 01 02 03 12 13 23
+LYM_D int plane_index(int mu, int nu)
+{
+    const int a = mu < nu ? mu : nu, b = mu < nu ? nu : mu;
+    return a == 0 ? b - 1 : (a == 1 ? b + 1 : 5);
+}
+LYM_D M3 load_plane(const double2 *N, int site, int plane)
+{
+    M3 M;
+    const double2 *b = N + ((size_t)site * 6 + plane) * 9;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        const double2 w = __ldg(b + k);
+        M.a[k / 3][k % 3] = C{w.x, w.y};
+    }
+    return M;
+}
+
+// N^{mu nu}(x) = i kappa c_sw sum_i w_i sum_{ab} (gamma5 sigma_{mu nu})_{ab} (Y_b X_a^+ + X_b Y_a^+) at
+// every site, for the six planes mu < nu: the spinor part of ImprovedFermionForce's terms, whose
+// term k is then sign_k L_k N(x_k) R_k^+ (tensor(R X_a, L P_Y[a]) + tensor(R Y_a, L P_X[a]) summed
+// over a)
+__global__ void __launch_bounds__(128) clover_outer_kernel(ForceArg a, double2 *N)
+{
+    const int site = blockIdx.x * blockDim.x + threadIdx.x;
+    if (site >= a.g.V) return;
+#pragma unroll 1
+    for (int p = 0; p < 6; ++p) {
+        const int mu = p < 3 ? 0 : (p < 5 ? 1 : 2), nu = p < 3 ? p + 1 : (p < 5 ? p - 1 : 3);
+        M3 acc;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) acc.a[i][j] = C{0.0, 0.0};
+#pragma unroll 1
+        for (int k = 0; k < a.n; ++k) {
+            const double2 *Xp = a.X[k] + (size_t)site * 12, *Yp = a.Y[k] + (size_t)site * 12;
+            const C ikc{0.0, a.kappa * a.csw * a.w[k]};
+#pragma unroll 1
+            for (int al = 0; al < 4; ++al) {
+                C xa[3], ya[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const double2 x = __ldg(Xp + al * 3 + d), y = __ldg(Yp + al * 3 + d);
+                    xa[d] = C{x.x, x.y};
+                    ya[d] = C{y.x, y.y};
+                }
+#pragma unroll 1
+                for (int be = 0; be < 4; ++be) {
+                    const C g = c_ft.g5s[mu][nu][al][be];
+                    if (g.re == 0.0 && g.im == 0.0) continue;
+                    const C c = ikc * g;
+                    C xb[3], yb[3];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        const double2 x = __ldg(Xp + be * 3 + d), y = __ldg(Yp + be * 3 + d);
+                        xb[d] = C{x.x, x.y};
+                        yb[d] = C{y.x, y.y};
+                    }
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int j = 0; j < 3; ++j) {
+                            C t{0.0, 0.0};
+                            fma_cc(t, xa[j], yb[i]);
+                            fma_cc(t, ya[j], xb[i]);
+                            fma_c(acc.a[i][j], c, t);
+                        }
+                }
+            }
+        }
+        double2 *o = N + ((size_t)site * 6 + p) * 9;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) o[k] = make_double2(acc.a[k / 3][k % 3].re, acc.a[k / 3][k % 3].im);
+    }
+}
 
 template <class Gauge> struct Ctx {
     const ForceArg &a;
@@ -131,29 +210,122 @@ template <class Gauge> struct Ctx {
     }
     LYM_D static C as_c(cx<double> z) { return z; }
     LYM_D static C as_c(double z) { return C{z, 0.0}; }
-    LYM_D void spinor(const double2 *V, int s, C v[4][3]) const
+    LYM_D static void colour(const double2 *V, int s, int al, C v[3])
     {
 #pragma unroll
-        for (int al = 0; al < 4; ++al)
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const double2 w = __ldg(V + (size_t)s * 12 + al * 3 + d);
-                v[al][d] = C{w.x, w.y};
-            }
+        for (int d = 0; d < 3; ++d) {
+            const double2 w = __ldg(V + (size_t)s * 12 + al * 3 + d);
+            v[d] = C{w.x, w.y};
+        }
     }
 };
 
-// sum over beta of coef * T[alpha][beta] * v[beta] for one alpha
-LYM_D void spin_comb(const C T[4][4], int al, C coef, const C v[4][3], C out[3])
+// out = coef * sum_beta T[al][beta] V(s, beta), the non-zero entries only
+LYM_D void spin_comb(const C T[4][4], int al, C coef, const double2 *V, int s, C out[3])
 {
 #pragma unroll
     for (int d = 0; d < 3; ++d) out[d] = C{0.0, 0.0};
-#pragma unroll
+#pragma unroll 1
     for (int be = 0; be < 4; ++be) {
         const C w = coef * T[al][be];
         if (w.re == 0.0 && w.im == 0.0) continue;
+        C v[3];
 #pragma unroll
-        for (int d = 0; d < 3; ++d) fma_c(out[d], w, v[be][d]);
+        for (int d = 0; d < 3; ++d) {
+            const double2 z = __ldg(V + (size_t)s * 12 + be * 3 + d);
+            v[d] = C{z.x, z.y};
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) fma_c(out[d], w, v[d]);
+    }
+}
+// the same of U^+ V(s, beta)
+LYM_D void spin_comb_dag(const C T[4][4], int al, C coef, const M3 &U, const double2 *V, int s, C out[3])
+{
+#pragma unroll
+    for (int d = 0; d < 3; ++d) out[d] = C{0.0, 0.0};
+#pragma unroll 1
+    for (int be = 0; be < 4; ++be) {
+        const C w = coef * T[al][be];
+        if (w.re == 0.0 && w.im == 0.0) continue;
+        C v[3], u[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double2 z = __ldg(V + (size_t)s * 12 + be * 3 + d);
+            v[d] = C{z.x, z.y};
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            C t{0.0, 0.0};
+#pragma unroll
+            for (int k = 0; k < 3; ++k) fma_cc(t, U.a[k][i], v[k]);
+            u[i] = t;
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) fma_c(out[d], w, u[d]);
+    }
+}
+
+// the link matrices L, R of clover term `term` (ImprovedFermionForce::setLattice,
+// ImprovedFermionForce.cpp:225-268) and the site its spinors are taken at; hasL / hasR false
+// for an identity
+template <class Gauge>
+LYM_D void clover_term(const Ctx<Gauge> &cx_, int term, int x, int mu, int nu, const M3 &Umu, M3 &L, bool &hasL,
+                       M3 &R, bool &hasR, int &ps)
+{
+    const int xp = cx_.shift(x, mu, +1);
+    hasL = hasR = true;
+    switch (term) {
+    case 0:  // L = U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+
+        L = mul(mul(cx_.link(xp, nu), dag(cx_.link(cx_.shift(x, nu, +1), mu))), dag(cx_.link(x, nu)));
+        hasR = false;
+        ps = x;
+        break;
+    case 1: {  // L = U_mu(x)^+, R = U_mu(x) U_nu(x+mu-nu)^+ U_mu(x-nu)^+ U_nu(x-nu)
+        const int xmn = cx_.shift(x, nu, -1);
+        L = dag(Umu);
+        R = mul(mul(mul(Umu, dag(cx_.link(cx_.shift(x, mu, +1, nu, -1), nu))), dag(cx_.link(xmn, mu))),
+                cx_.link(xmn, nu));
+        ps = x;
+        break;
+    }
+    case 2:  // L = U_nu(x+mu) U_mu(x+nu)^+, R = U_nu(x)
+        L = mul(cx_.link(xp, nu), dag(cx_.link(cx_.shift(x, nu, +1), mu)));
+        R = cx_.link(x, nu);
+        ps = cx_.shift(x, nu, +1);
+        break;
+    case 3: {  // L = U_mu(x)^+ U_nu(x-nu)^+, R = U_mu(x) U_nu(x+mu-nu)^+ U_mu(x-nu)^+
+        const int xmn = cx_.shift(x, nu, -1);
+        L = mul(dag(Umu), dag(cx_.link(xmn, nu)));
+        R = mul(mul(Umu, dag(cx_.link(cx_.shift(x, mu, +1, nu, -1), nu))), dag(cx_.link(xmn, mu)));
+        ps = xmn;
+        break;
+    }
+    case 4:  // R = U_nu(x) U_mu(x+nu) U_nu(x+mu)^+
+        hasL = false;
+        R = mul(mul(cx_.link(x, nu), cx_.link(cx_.shift(x, nu, +1), mu)), dag(cx_.link(xp, nu)));
+        ps = xp;
+        break;
+    case 5: {  // L = U_mu(x)^+ U_nu(x-nu)^+ U_mu(x-nu) U_nu(x+mu-nu), R = U_mu(x)
+        const int xmn = cx_.shift(x, nu, -1);
+        L = mul(mul(mul(dag(Umu), dag(cx_.link(xmn, nu))), cx_.link(xmn, mu)),
+                cx_.link(cx_.shift(x, mu, +1, nu, -1), nu));
+        R = Umu;
+        ps = xp;
+        break;
+    }
+    case 6:  // L = U_nu(x+mu), R = U_nu(x) U_mu(x+nu)
+        L = cx_.link(xp, nu);
+        R = mul(cx_.link(x, nu), cx_.link(cx_.shift(x, nu, +1), mu));
+        ps = cx_.shift(x, mu, +1, nu, +1);
+        break;
+    default: {  // L = U_mu(x)^+ U_nu(x-nu)^+ U_mu(x-nu), R = U_mu(x) U_nu(x+mu-nu)^+
+        const int xmn = cx_.shift(x, nu, -1);
+        L = mul(mul(dag(Umu), dag(cx_.link(xmn, nu))), cx_.link(xmn, mu));
+        R = mul(Umu, dag(cx_.link(cx_.shift(x, mu, +1, nu, -1), nu)));
+        ps = cx_.shift(x, mu, +1, nu, -1);
+        break;
+    }
     }
 }
 
@@ -163,138 +335,62 @@ template <class Gauge> __global__ void __launch_bounds__(128) fermion_force_kern
     if (tid >= 4L * a.g.V) return;
     const int site = (int)(tid >> 2), mu = (int)(tid & 3);
     const Ctx<Gauge> cx_{a, U};
-    M3 F;
+    M3 F;  // sum_i w_i F_i, Wilson part first
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) F.a[i][j] = C{0.0, 0.0};
-    const C mk{-a.kappa, 0.0};
     const int xp = cx_.shift(site, mu, +1);
-    {
-        // DiracWilsonFermionForce::derivative
-        C Xs[4][3], Ys[4][3], Xp[4][3], Yp[4][3];
-        cx_.spinor(a.X, site, Xs);
-        cx_.spinor(a.Y, site, Ys);
-        cx_.spinor(a.X, xp, Xp);
-        cx_.spinor(a.Y, xp, Yp);
-        const M3 Um = cx_.link(site, mu), Ud = dag(Um);
-        C UdXs[4][3], UdYs[4][3];
-#pragma unroll
-        for (int al = 0; al < 4; ++al) {
-            mv(Ud, Xs[al], UdXs[al]);
-            mv(Ud, Ys[al], UdYs[al]);
-        }
+    const M3 Um = cx_.link(site, mu);
+    // DiracWilsonFermionForce::derivative
 #pragma unroll 1
-        for (int al = 0; al < 4; ++al) {
-            C t[3], u[3];
-            spin_comb(c_ft.mg[mu], al, mk, Yp, t);
-            add_tensor(F, 1.0, Xs[al], t);
-            spin_comb(c_ft.pg[mu], al, mk, UdYs, t);
-            mv(Um, Xp[al], u);
-            add_tensor(F, -1.0, u, t);
-            spin_comb(c_ft.mg[mu], al, mk, Xp, t);
-            add_tensor(F, 1.0, Ys[al], t);
-            spin_comb(c_ft.pg[mu], al, mk, UdXs, t);
-            mv(Um, Yp[al], u);
-            add_tensor(F, -1.0, u, t);
+    for (int i = 0; i < a.n; ++i) {
+        const double2 *X = a.X[i], *Y = a.Y[i];
+        const C mk{-a.kappa * a.w[i], 0.0};
+#pragma unroll 1
+        for (int pass = 0; pass < 2; ++pass) {  // (X, Y), then X and Y exchanged
+            const double2 *A = pass ? Y : X, *B = pass ? X : Y;
+#pragma unroll 1
+            for (int al = 0; al < 4; ++al) {
+                C t[3], u[3], v[3];
+                spin_comb(c_ft.mg[mu], al, mk, B, xp, t);
+                Ctx<Gauge>::colour(A, site, al, v);
+                add_tensor(F, 1.0, v, t);
+                spin_comb_dag(c_ft.pg[mu], al, mk, Um, B, site, t);
+                Ctx<Gauge>::colour(A, xp, al, v);
+                mv(Um, v, u);
+                add_tensor(F, -1.0, u, t);
+            }
         }
     }
     if (a.clover) {
-        // ImprovedFermionForce::derivative, terms 1-8 for every nu != mu
+        // ImprovedFermionForce::derivative: term k of plane (mu, nu) adds sign_k L_k N^{mu nu}(x_k) R_k^+
+        // (N from clover_outer_kernel: the spin traces of both pair orders, weights included);
+        // the clover sum / 4
         M3 Fc;
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
             for (int j = 0; j < 3; ++j) Fc.a[i][j] = C{0.0, 0.0};
-        const C ikc{0.0, a.kappa * a.csw};
-        const M3 Umu_x = cx_.link(site, mu);
 #pragma unroll 1
         for (int nu = 0; nu < 4; ++nu) {
             if (nu == mu) continue;
-            const int xpn = cx_.shift(site, nu, +1), xmn = cx_.shift(site, nu, -1);
-            const int xpm_mn = cx_.shift(site, mu, +1, nu, -1), xpm_pn = cx_.shift(site, mu, +1, nu, +1);
-            const M3 Unu_x = cx_.link(site, nu), Unu_xpm = cx_.link(xp, nu), Umu_xpn = cx_.link(xpn, mu);
-            const M3 Unu_xpm_mn = cx_.link(xpm_mn, nu), Umu_xmn = cx_.link(xmn, mu), Unu_xmn = cx_.link(xmn, nu);
-            const M3 Umu_xd = dag(Umu_x);
+            const int plane = plane_index(mu, nu);
+            const double ps_sign = mu < nu ? 1.0 : -1.0;  // N^{nu mu} = -N^{mu nu}
 #pragma unroll 1
             for (int term = 0; term < 8; ++term) {
                 M3 L, R;
-                bool hasL = true, hasR = true;
+                bool hasL, hasR;
                 int ps;
-                switch (term) {
-                case 0:  // L = U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+
-                    L = mul(mul(Unu_xpm, dag(Umu_xpn)), dag(Unu_x));
-                    hasR = false;
-                    ps = site;
-                    break;
-                case 1:  // L = U_mu(x)^+, R = U_mu(x) U_nu(x+mu-nu)^+ U_mu(x-nu)^+ U_nu(x-nu)
-                    L = Umu_xd;
-                    R = mul(mul(mul(Umu_x, dag(Unu_xpm_mn)), dag(Umu_xmn)), Unu_xmn);
-                    ps = site;
-                    break;
-                case 2:  // L = U_nu(x+mu) U_mu(x+nu)^+, R = U_nu(x)
-                    L = mul(Unu_xpm, dag(Umu_xpn));
-                    R = Unu_x;
-                    ps = xpn;
-                    break;
-                case 3:  // L = U_mu(x)^+ U_nu(x-nu)^+, R = U_mu(x) U_nu(x+mu-nu)^+ U_mu(x-nu)^+
-                    L = mul(Umu_xd, dag(Unu_xmn));
-                    R = mul(mul(Umu_x, dag(Unu_xpm_mn)), dag(Umu_xmn));
-                    ps = xmn;
-                    break;
-                case 4:  // R = U_nu(x) U_mu(x+nu) U_nu(x+mu)^+
-                    hasL = false;
-                    R = mul(mul(Unu_x, Umu_xpn), dag(Unu_xpm));
-                    ps = xp;
-                    break;
-                case 5:  // L = U_mu(x)^+ U_nu(x-nu)^+ U_mu(x-nu) U_nu(x+mu-nu), R = U_mu(x)
-                    L = mul(mul(mul(Umu_xd, dag(Unu_xmn)), Umu_xmn), Unu_xpm_mn);
-                    R = Umu_x;
-                    ps = xp;
-                    break;
-                case 6:  // L = U_nu(x+mu), R = U_nu(x) U_mu(x+nu)
-                    L = Unu_xpm;
-                    R = mul(Unu_x, Umu_xpn);
-                    ps = xpm_pn;
-                    break;
-                default:  // L = U_mu(x)^+ U_nu(x-nu)^+ U_mu(x-nu), R = U_mu(x) U_nu(x+mu-nu)^+
-                    L = mul(mul(Umu_xd, dag(Unu_xmn)), Umu_xmn);
-                    R = mul(Umu_x, dag(Unu_xpm_mn));
-                    ps = xpm_mn;
-                    break;
-                }
-                const double sg = (term & 1) ? -1.0 : 1.0;
-                C Xq[4][3], Yq[4][3];
-                cx_.spinor(a.X, ps, Xq);
-                cx_.spinor(a.Y, ps, Yq);
-#pragma unroll 1
-                for (int al = 0; al < 4; ++al) {
-                    C pX[3], pY[3], lX[3], lY[3], rX[3], rY[3];
-                    spin_comb(c_ft.g5s[mu][nu], al, ikc, Xq, pX);
-                    spin_comb(c_ft.g5s[mu][nu], al, ikc, Yq, pY);
-                    if (hasL) {
-                        mv(L, pY, lY);
-                        mv(L, pX, lX);
-                    } else {
+                clover_term(cx_, term, site, mu, nu, Um, L, hasL, R, hasR, ps);
+                M3 Nm = load_plane(a.N, ps, plane);
+                if (hasL) Nm = mul(L, Nm);
+                if (hasR) Nm = mul(Nm, dag(R));
+                const double sg = ((term & 1) ? -1.0 : 1.0) * ps_sign;
 #pragma unroll
-                        for (int d = 0; d < 3; ++d) {
-                            lY[d] = pY[d];
-                            lX[d] = pX[d];
-                        }
-                    }
-                    if (hasR) {
-                        mv(R, Xq[al], rX);
-                        mv(R, Yq[al], rY);
-                    } else {
+                for (int i = 0; i < 3; ++i)
 #pragma unroll
-                        for (int d = 0; d < 3; ++d) {
-                            rX[d] = Xq[al][d];
-                            rY[d] = Yq[al][d];
-                        }
-                    }
-                    add_tensor(Fc, sg, rX, lY);
-                    add_tensor(Fc, sg, rY, lX);
-                }
+                    for (int j = 0; j < 3; ++j) Fc.a[i][j] = Fc.a[i][j] + sg * Nm.a[i][j];
             }
         }
 #pragma unroll
@@ -308,8 +404,8 @@ template <class Gauge> __global__ void __launch_bounds__(128) fermion_force_kern
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
             double2 w = out[j * 3 + i];
-            w.x -= a.weight * F.a[i][j].re;
-            w.y -= a.weight * F.a[i][j].im;
+            w.x -= F.a[i][j].re;
+            w.y -= F.a[i][j].im;
             out[j * 3 + i] = w;
         }
 }
@@ -357,13 +453,17 @@ void upload_tables(cudaStream_t st)
 
 }  // namespace
 
-void launch_fermion_force(const Geom &g, const GaugeDev &U, const double2 *X, const double2 *Y, double kappa,
-                          double csw, int clover, double weight, double2 *force, cudaStream_t st)
+size_t fermion_force_scratch_bytes(const Geom &g) { return (size_t)g.V * 6 * 9 * sizeof(double2); }
+
+void launch_fermion_force(const Geom &g, const GaugeDev &U, int n, const double2 *const *X, const double2 *const *Y,
+                          const double *weights, double kappa, double csw, int clover, double2 *force,
+                          double2 *scratch, cudaStream_t st)
 {
     upload_tables(st);
-    ForceArg a{g, U.d64, U.rep, X, Y, force, kappa, csw, weight, clover};
-    const long n = 4L * g.V;
-    const int grid = (int)((n + 127) / 128);
+    ForceArg a{g, n, X, Y, weights, force, scratch, kappa, csw, clover};
+    if (clover) clover_outer_kernel<<<(g.V + 127) / 128, 128, 0, st>>>(a, scratch);
+    const long threads = 4L * g.V;
+    const int grid = (int)((threads + 127) / 128);
     if (U.rep == REP_SU3)
         fermion_force_kernel<GaugeD18><<<grid, 128, 0, st>>>(a, GaugeD18{(const double2 *)U.d64, g.stride});
     else

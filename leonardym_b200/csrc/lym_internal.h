@@ -135,9 +135,13 @@ void launch_meson_contractions(const Geom &g, const MesonProps &P, double *scrat
 int dot_blocks(const Geom &g);
 void launch_dots(const Geom &g, const DotPairs &D, int n, int gamma5, double2 *partials, double2 *out,
                  cudaStream_t st);
-// force[x][mu] -= weight * F_mu(x) of the Wilson (clover = 0) or Wilson-clover fermion force
-void launch_fermion_force(const Geom &g, const GaugeDev &U, const double2 *X, const double2 *Y, double kappa,
-                          double csw, int clover, double weight, double2 *force, cudaStream_t st);
+// force[x][mu] -= sum_i w_i F_mu(x; X_i, Y_i) of the Wilson (clover = 0) or Wilson-clover fermion
+// force; X, Y, weights: device arrays of n entries
+// scratch: fermion_force_scratch_bytes (the per-site plane matrices of the clover part)
+size_t fermion_force_scratch_bytes(const Geom &g);
+void launch_fermion_force(const Geom &g, const GaugeDev &U, int n, const double2 *const *X, const double2 *const *Y,
+                          const double *weights, double kappa, double csw, int clover, double2 *force,
+                          double2 *scratch, cudaStream_t st);
 // real Z2 noise vector `stream` of generator `seed` (AoS full spinor)
 void launch_z2_noise(const Geom &g, double *out, unsigned long long seed, unsigned long long stream, cudaStream_t st);
 }  // namespace lym

@@ -102,6 +102,25 @@ class FermionForce:
             raise LymError(rc, lib().lym_last_error(op.lattice.handle).decode())
         return fermionForce
 
+    def derivative_many(self, fermionForce, Xs, Ys, weights):
+        """fermionForce -= sum_i weights[i] F(Xs[i], Ys[i]) in one pass (the link products of
+        every clover leaf formed once)."""
+        op = self.diracOperator
+        xs = [op._vec(x) for x in Xs]
+        ys = [op._vec(y) for y in Ys]
+        n = len(xs)
+        if n == 0:
+            return fermionForce
+        if fermionForce.dtype != np.complex128 or not fermionForce.flags.c_contiguous:
+            raise LymError(-1, "the force field must be a contiguous complex128 array")
+        w = np.ascontiguousarray(weights, np.float64)
+        xp = (C.c_void_p * n)(*[x.ctypes.data for x in xs])
+        yp = (C.c_void_p * n)(*[y.ctypes.data for y in ys])
+        rc = lib().lym_fermion_force_multi(op.lattice.handle, op.op_id, n, xp, yp, _p(w), _p(fermionForce))
+        if rc < 0:
+            raise LymError(rc, lib().lym_last_error(op.lattice.handle).decode())
+        return fermionForce
+
 
 class NFlavorFermionAction:
     """The multishift parts of NFlavorFermionAction: one RationalApproximation per
@@ -166,8 +185,7 @@ class NFlavorFermionAction:
         ff = FermionForce(self.diracOperator)
         Xs, Ys = self.solves()
         for approx, X, Y in zip(self.rationalApproximations, Xs, Ys):
-            for alpha, x, y in zip(approx.alphas, X, Y):
-                ff.derivative(force, x, y, alpha)
+            ff.derivative_many(force, X, Y, approx.alphas)
         if boundary_conditions == "fermion_antiperiodic":
             Lt = lat.dims[3]
             force.reshape(-1, Lt, 4, 3, 3)[:, Lt - 1, 3] *= -1

@@ -77,3 +77,21 @@ def test_action_force(setup, oracle):
     Lt = dims[3]
     ref.reshape(-1, Lt, 4, 3, 3)[:, Lt - 1, 3] *= -1
     assert np.max(np.abs(f - ref)) <= 1e-9 * np.max(np.abs(ref))
+
+
+def test_force_many_pairs(setup):
+    # one pass over n weighted pairs equals n single-pair passes
+    dims, lat = setup["dims"], setup["lat"]
+    op = L.ImprovedDiracWilsonOperator(lat, setup["kappa"], setup["csw"])
+    op.setLattice(setup["gid"])
+    ff = op.getForce()
+    Xs = [synth.gaussian_spinor(dims, 3, 60 + k) for k in range(3)]
+    Ys = [synth.gaussian_spinor(dims, 3, 70 + k) for k in range(3)]
+    w = [0.3, -0.1, 0.05]
+    V = int(np.prod(dims))
+    a = np.zeros((V, 4, 3, 3), np.complex128)
+    b = np.zeros_like(a)
+    ff.derivative_many(a, Xs, Ys, w)
+    for x, y, wi in zip(Xs, Ys, w):
+        ff.derivative(b, x, y, wi)
+    assert np.max(np.abs(a - b)) <= 1e-13 * np.max(np.abs(b))
