@@ -729,6 +729,8 @@ def run_profile(args):
     lib = L.lib()
     if args.workload.startswith("rhmc"):
         return run_profile_rhmc(args)
+    if args.workload == "consumers":
+        return run_profile_consumers(args)
     lat = L.Lattice(DIMS, "su3", device=0)
     op = L.ImprovedDiracWilsonOperator(lat, KAPPA, CSW, gamma5=False)
     op.setLattice(workload_links())
@@ -753,6 +755,43 @@ def run_profile(args):
     print(f"profile case: rc {rc}, block solve {t_solve:.3f} s, updates {st.reliable_updates}, "
           f"iterations {st.iterations}, true residual {st.true_residual:.2e}, "
           f"stencil {ms.value * 1e3:.1f} us, batched stencil ({args.batch}) {msb.value * 1e3:.1f} us")
+    lat.close()
+    if rc != 0:
+        sys.exit(1)
+
+
+def run_profile_consumers(args):
+    """Small case for ncu captures of the consumer kernels on 24^3x48 (links and sources
+    seeded on the device, a few GB on the device): one fermion force over 12 weighted pairs,
+    the meson contractions of 12 spinors, the condensate dot products of 32 pairs."""
+    import torch
+
+    import leonardym_b200 as L
+    from leonardym_b200 import synth
+    lib = L.lib()
+    lat = L.Lattice(DIMS, "su3", device=0)
+    ctx = lat.handle
+    links = synth.su3_fermion_links_device(DIMS, RHMC_EPS, RHMC_SEED, "cuda:0")
+    lib.lym_gauge_upload_device(ctx, 1, C.c_void_p(links.data_ptr()))
+    del links
+    opid = C.c_int(0)
+    lib.lym_operator_create(ctx, 1, 1, KAPPA, CSW, 0, C.byref(opid))
+    vecs = [synth.gaussian_spinor_device(DIMS, 3, 100 + k, "cuda:0") for k in range(24)]
+    X, Y = vecs[:12], vecs[12:]
+    w = np.linspace(0.05, 0.6, 12)
+    xp = (C.c_void_p * 12)(*[v.data_ptr() for v in X])
+    yp = (C.c_void_p * 12)(*[v.data_ptr() for v in Y])
+    force = torch.zeros((lat.V, 4, 3, 3), dtype=torch.complex128, device="cuda:0")
+    t0 = time.perf_counter()
+    rc = lib.lym_fermion_force_multi_device(ctx, opid.value, 12, xp, yp, w.ctypes.data_as(C.c_void_p),
+                                            C.c_void_p(force.data_ptr()))
+    t_force = time.perf_counter() - t0
+    Lt = DIMS[3]
+    pion, scalar, ps = np.zeros(Lt), np.zeros(Lt), np.zeros(Lt)
+    rc |= lib.lym_meson_contractions_device(ctx, xp, pion.ctypes.data, scalar.ctypes.data, ps.ctypes.data)
+    d = np.zeros(2 * 12)
+    rc |= lib.lym_dots_device(ctx, 12, xp, yp, 1, d.ctypes.data)
+    print(f"consumers profile case: rc {rc}, fermion force (12 pairs) {t_force:.3f} s, pion[0] {pion[0]:.6e}")
     lat.close()
     if rc != 0:
         sys.exit(1)
@@ -799,7 +838,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default=None, choices=["single", "half"],
                     help="inner storage (default: single for the propagator solves, half for rhmc)")
-    ap.add_argument("--workload", default="propagators", choices=["propagators", "rhmc", "rhmc-small"],
+    ap.add_argument("--workload", default="propagators", choices=["propagators", "rhmc", "rhmc-small", "consumers"],
                     help="propagators: the 24^3x48 block solves (the headline); rhmc: the 48^3x96 multishift; "
                          "rhmc-small: the same at 24^3x48")
     ap.add_argument("--solver", default="bicgstab", choices=["cg", "bicgstab"],

@@ -116,10 +116,12 @@ LYM_D M3 load_plane(const double2 *N, int site, int plane)
 // over a)
 __global__ void __launch_bounds__(128) clover_outer_kernel(ForceArg a, double2 *N)
 {
-    const int site = blockIdx.x * blockDim.x + threadIdx.x;
-    if (site >= a.g.V) return;
-#pragma unroll 1
-    for (int p = 0; p < 6; ++p) {
+    // one thread per (site, plane): the six threads of a site are neighbours in the warp, so
+    // each spinor word comes from DRAM once and from L1 for the other five
+    const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= 6L * a.g.V) return;
+    const int site = (int)(tid / 6), p = (int)(tid % 6);
+    {
         const int mu = p < 3 ? 0 : (p < 5 ? 1 : 2), nu = p < 3 ? p + 1 : (p < 5 ? p - 1 : 3);
         M3 acc;
 #pragma unroll
@@ -266,69 +268,6 @@ LYM_D void spin_comb_dag(const C T[4][4], int al, C coef, const M3 &U, const dou
     }
 }
 
-// the link matrices L, R of clover term `term` (ImprovedFermionForce::setLattice,
-// ImprovedFermionForce.cpp:225-268) and the site its spinors are taken at; hasL / hasR false
-// for an identity
-template <class Gauge>
-LYM_D void clover_term(const Ctx<Gauge> &cx_, int term, int x, int mu, int nu, const M3 &Umu, M3 &L, bool &hasL,
-                       M3 &R, bool &hasR, int &ps)
-{
-    const int xp = cx_.shift(x, mu, +1);
-    hasL = hasR = true;
-    switch (term) {
-    case 0:  // L = U_nu(x+mu) U_mu(x+nu)^+ U_nu(x)^+
-        L = mul(mul(cx_.link(xp, nu), dag(cx_.link(cx_.shift(x, nu, +1), mu))), dag(cx_.link(x, nu)));
-        hasR = false;
-        ps = x;
-        break;
-    case 1: {  // L = U_mu(x)^+, R = U_mu(x) U_nu(x+mu-nu)^+ U_mu(x-nu)^+ U_nu(x-nu)
-        const int xmn = cx_.shift(x, nu, -1);
-        L = dag(Umu);
-        R = mul(mul(mul(Umu, dag(cx_.link(cx_.shift(x, mu, +1, nu, -1), nu))), dag(cx_.link(xmn, mu))),
-                cx_.link(xmn, nu));
-        ps = x;
-        break;
-    }
-    case 2:  // L = U_nu(x+mu) U_mu(x+nu)^+, R = U_nu(x)
-        L = mul(cx_.link(xp, nu), dag(cx_.link(cx_.shift(x, nu, +1), mu)));
-        R = cx_.link(x, nu);
-        ps = cx_.shift(x, nu, +1);
-        break;
-    case 3: {  // L = U_mu(x)^+ U_nu(x-nu)^+, R = U_mu(x) U_nu(x+mu-nu)^+ U_mu(x-nu)^+
-        const int xmn = cx_.shift(x, nu, -1);
-        L = mul(dag(Umu), dag(cx_.link(xmn, nu)));
-        R = mul(mul(Umu, dag(cx_.link(cx_.shift(x, mu, +1, nu, -1), nu))), dag(cx_.link(xmn, mu)));
-        ps = xmn;
-        break;
-    }
-    case 4:  // R = U_nu(x) U_mu(x+nu) U_nu(x+mu)^+
-        hasL = false;
-        R = mul(mul(cx_.link(x, nu), cx_.link(cx_.shift(x, nu, +1), mu)), dag(cx_.link(xp, nu)));
-        ps = xp;
-        break;
-    case 5: {  // L = U_mu(x)^+ U_nu(x-nu)^+ U_mu(x-nu) U_nu(x+mu-nu), R = U_mu(x)
-        const int xmn = cx_.shift(x, nu, -1);
-        L = mul(mul(mul(dag(Umu), dag(cx_.link(xmn, nu))), cx_.link(xmn, mu)),
-                cx_.link(cx_.shift(x, mu, +1, nu, -1), nu));
-        R = Umu;
-        ps = xp;
-        break;
-    }
-    case 6:  // L = U_nu(x+mu), R = U_nu(x) U_mu(x+nu)
-        L = cx_.link(xp, nu);
-        R = mul(cx_.link(x, nu), cx_.link(cx_.shift(x, nu, +1), mu));
-        ps = cx_.shift(x, mu, +1, nu, +1);
-        break;
-    default: {  // L = U_mu(x)^+ U_nu(x-nu)^+ U_mu(x-nu), R = U_mu(x) U_nu(x+mu-nu)^+
-        const int xmn = cx_.shift(x, nu, -1);
-        L = mul(mul(dag(Umu), dag(cx_.link(xmn, nu))), cx_.link(xmn, mu));
-        R = mul(Umu, dag(cx_.link(cx_.shift(x, mu, +1, nu, -1), nu)));
-        ps = cx_.shift(x, mu, +1, nu, -1);
-        break;
-    }
-    }
-}
-
 template <class Gauge> __global__ void __launch_bounds__(128) fermion_force_kernel(ForceArg a, Gauge U)
 {
     const long tid = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -376,21 +315,41 @@ template <class Gauge> __global__ void __launch_bounds__(128) fermion_force_kern
         for (int nu = 0; nu < 4; ++nu) {
             if (nu == mu) continue;
             const int plane = plane_index(mu, nu);
-            const double ps_sign = mu < nu ? 1.0 : -1.0;  // N^{nu mu} = -N^{mu nu}
-#pragma unroll 1
-            for (int term = 0; term < 8; ++term) {
-                M3 L, R;
-                bool hasL, hasR;
-                int ps;
-                clover_term(cx_, term, site, mu, nu, Um, L, hasL, R, hasR, ps);
-                M3 Nm = load_plane(a.N, ps, plane);
-                if (hasL) Nm = mul(L, Nm);
-                if (hasR) Nm = mul(Nm, dag(R));
-                const double sg = ((term & 1) ? -1.0 : 1.0) * ps_sign;
+            const double sgn = mu < nu ? 1.0 : -1.0;  // N^{nu mu} = -N^{mu nu}
+            const int xpn = cx_.shift(site, nu, +1), xmn = cx_.shift(site, nu, -1);
+            const int xpm_mn = cx_.shift(site, mu, +1, nu, -1), xpm_pn = cx_.shift(site, mu, +1, nu, +1);
+            auto add = [&](double sg, const M3 &M) {
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
 #pragma unroll
-                    for (int j = 0; j < 3; ++j) Fc.a[i][j] = Fc.a[i][j] + sg * Nm.a[i][j];
+                    for (int j = 0; j < 3; ++j) Fc.a[i][j] = Fc.a[i][j] + (sg * sgn) * M.a[i][j];
+            };
+            // the terms in an order that shares their link products (k = term of
+            // ImprovedFermionForce.cpp; L_k, R_k its matrices): A = U_nu(x+mu) U_mu(x+nu)^+
+            {
+                const M3 Unu_x = cx_.link(site, nu);
+                const M3 A = mul(cx_.link(xp, nu), dag(cx_.link(xpn, mu)));
+                add(+1.0, mul(mul(A, load_plane(a.N, xpn, plane)), dag(Unu_x)));  // k=2: L=A, R=U_nu(x)
+                add(+1.0, mul(mul(A, dag(Unu_x)), load_plane(a.N, site, plane)));  // k=0: L=A U_nu(x)^+
+            }
+            {
+                // D = U_nu(x) U_mu(x+nu)
+                const M3 Unu_xpm = cx_.link(xp, nu);
+                const M3 D = mul(cx_.link(site, nu), cx_.link(xpn, mu));
+                add(+1.0, mul(mul(Unu_xpm, load_plane(a.N, xpm_pn, plane)), dag(D)));  // k=6: L=U_nu(x+mu), R=D
+                add(+1.0, mul(load_plane(a.N, xp, plane), dag(mul(D, dag(Unu_xpm)))));  // k=4: R=D U_nu(x+mu)^+
+            }
+            {
+                // C = U_mu(x)^+ U_nu(x-nu)^+, R7 = U_mu(x) U_nu(x+mu-nu)^+, B = R7 U_mu(x-nu)^+
+                const M3 Umu_xmn = cx_.link(xmn, mu), Unu_xmn = cx_.link(xmn, nu), Unu_xpm_mn = cx_.link(xpm_mn, nu);
+                const M3 C = mul(dag(Um), dag(Unu_xmn));
+                const M3 R7 = mul(Um, dag(Unu_xpm_mn));
+                const M3 L7 = mul(C, Umu_xmn);
+                add(-1.0, mul(mul(L7, load_plane(a.N, xpm_mn, plane)), dag(R7)));  // k=7
+                add(-1.0, mul(mul(mul(L7, Unu_xpm_mn), load_plane(a.N, xp, plane)), dag(Um)));  // k=5: L=L7 U_nu(x+mu-nu), R=U_mu(x)
+                const M3 B = mul(R7, dag(Umu_xmn));
+                add(-1.0, mul(mul(C, load_plane(a.N, xmn, plane)), dag(B)));  // k=3: L=C, R=B
+                add(-1.0, mul(mul(dag(Um), load_plane(a.N, site, plane)), dag(mul(B, Unu_xmn))));  // k=1: L=U_mu(x)^+, R=B U_nu(x-nu)
             }
         }
 #pragma unroll
@@ -461,7 +420,7 @@ void launch_fermion_force(const Geom &g, const GaugeDev &U, int n, const double2
 {
     upload_tables(st);
     ForceArg a{g, n, X, Y, weights, force, scratch, kappa, csw, clover};
-    if (clover) clover_outer_kernel<<<(g.V + 127) / 128, 128, 0, st>>>(a, scratch);
+    if (clover) clover_outer_kernel<<<(int)((6L * g.V + 127) / 128), 128, 0, st>>>(a, scratch);
     const long threads = 4L * g.V;
     const int grid = (int)((threads + 127) / 128);
     if (U.rep == REP_SU3)
