@@ -57,6 +57,7 @@ struct lym_context {
     int rep = REP_SU3;
     int device = 0;
     cudaStream_t st = nullptr;
+    cudaStream_t st_copy = nullptr;  // host <-> device copies that overlap the solves
     std::recursive_mutex mu;  // entry points may call other entry points on the same thread
     std::string err;
     std::map<int, GaugeEntry> gauges;
@@ -169,6 +170,20 @@ void dev_free(lym_context *c, void *p, size_t bytes)
         c->bytes -= bytes;
     }
 }
+
+// device memory for the length of one call
+struct DevBuf {
+    lym_context *c;
+    void *p = nullptr;
+    size_t n = 0;
+    DevBuf(lym_context *ctx, size_t bytes) : c(ctx), p(dev_alloc(ctx, bytes)), n(bytes) {}
+    ~DevBuf()
+    {
+        if (p) dev_free(c, p, n);
+    }
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+};
 
 size_t spinor_bytes(const Geom &g, int prec, int nparity)
 {
@@ -2255,6 +2270,7 @@ int lym_context_create(const int dims[4], int rep, int device, lym_context **out
     int rc = guarded(c, [&]() {
         CK(cudaSetDevice(device));
         CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&c->st_copy, cudaStreamNonBlocking));
         c->partials = (double *)dev_alloc(c, (size_t)kBlasGridMax * kMaxRed * sizeof(double));
         c->bpartials = (double *)dev_alloc(c, (size_t)kBlasGridMax * kMaxBatch * kBatchMaxRed * sizeof(double));
         c->nbr = (int *)dev_alloc(c, (size_t)16 * c->g.stride * sizeof(int));
@@ -2283,6 +2299,7 @@ void lym_context_destroy(lym_context *c)
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->st) cudaStreamSynchronize(c->st);
+    if (c->st_copy) cudaStreamSynchronize(c->st_copy);
     for (auto &kv : c->ops)
         for (int p = 0; p < 3; ++p) {
             cudaFree(kv.second.clover.T[p]);
@@ -2310,6 +2327,7 @@ void lym_context_destroy(lym_context *c)
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->st) cudaStreamDestroy(c->st);
+    if (c->st_copy) cudaStreamDestroy(c->st_copy);
     delete c;
 }
 
@@ -2717,14 +2735,64 @@ static int run_block(lym_context *c, OpEntry &op, int sp, int algo, double tol, 
     int rc_all = LYM_OK;
     auto now = []() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
     std::vector<double> t_start(tags.size(), 0.0);
+    // host buffers: the sources' H2D copies run ahead on the copy stream through a ring of
+    // device staging buffers, and every solution's D2H copy runs there while the solves go on
+    const size_t vb = (size_t)c->g.V * 24 * sizeof(double);
+    const int K = device_ptr ? 0 : (int)std::min<size_t>(4, tags.size());
+    std::vector<std::unique_ptr<DevBuf>> up, down;
+    struct Events {
+        std::vector<cudaEvent_t> e;
+        ~Events()
+        {
+            for (auto x : e) cudaEventDestroy(x);
+        }
+        cudaEvent_t make()
+        {
+            cudaEvent_t x;
+            cudaEventCreateWithFlags(&x, cudaEventDisableTiming);
+            e.push_back(x);
+            return x;
+        }
+    } events;
+    std::vector<cudaEvent_t> ev_up(K), ev_used(K), ev_unpacked(K), ev_down(K);
+    for (int r = 0; r < K; ++r) {
+        up.emplace_back(new DevBuf(c, vb));
+        down.emplace_back(new DevBuf(c, vb));
+        ev_up[r] = events.make();
+        ev_used[r] = events.make();
+        ev_unpacked[r] = events.make();
+        ev_down[r] = events.make();
+    }
+    auto issue_up = [&](size_t k) {
+        const int r = (int)(k % K);
+        if (k >= (size_t)K) CK(cudaStreamWaitEvent(c->st_copy, ev_used[r], 0));
+        CK(cudaMemcpyAsync(up[r]->p, sources[tags[k]], vb, cudaMemcpyHostToDevice, c->st_copy));
+        CK(cudaEventRecord(ev_up[r], c->st_copy));
+    };
+    size_t ndown = 0;
+    struct CopyDrain {
+        lym_context *c;
+        ~CopyDrain() { cudaStreamSynchronize(c->st_copy); }
+    } drain{c};
+    for (int k = 0; k < K; ++k) issue_up(k);
     auto collect = [&](int f) {
         const auto &s = engine.info(f);
         const int tag = tags[s.tag];
         if (s.gave_up) {
             gave_up.push_back(tag);
         } else {
-            download_vec(c, solutions[tag], s.X, device_ptr, 2);
-            CK(cudaStreamSynchronize(c->st));
+            if (device_ptr) {
+                download_vec(c, solutions[tag], s.X, true, 2);
+            } else {
+                const int r = (int)(ndown % K);
+                if (ndown >= (size_t)K) CK(cudaEventSynchronize(ev_down[r]));  // the buffer's last copy is done
+                launch_unpack(c->g, s.X, (double *)down[r]->p, c->st);
+                CK(cudaEventRecord(ev_unpacked[r], c->st));
+                CK(cudaStreamWaitEvent(c->st_copy, ev_unpacked[r], 0));
+                CK(cudaMemcpyAsync(solutions[tag], down[r]->p, vb, cudaMemcpyDeviceToHost, c->st_copy));
+                CK(cudaEventRecord(ev_down[r], c->st_copy));
+                ++ndown;
+            }
             if (stats) {
                 stats[tag].iterations = stats[tag].steps = s.iters;
                 stats[tag].reliable_updates = s.updates;
@@ -2743,7 +2811,15 @@ static int run_block(lym_context *c, OpEntry &op, int sp, int algo, double tol, 
             int j;
             while (next < tags.size() && (j = engine.free_slot()) >= 0) {
                 const Spinor B = **bufs[2 * j], X = **bufs[2 * j + 1];
-                upload_vec(c, B, sources[tags[next]], device_ptr, 0);
+                if (device_ptr) {
+                    upload_vec(c, B, sources[tags[next]], true, 0);
+                } else {
+                    const int r = (int)(next % K);
+                    CK(cudaStreamWaitEvent(c->st, ev_up[r], 0));
+                    launch_pack(c->g, (const double *)up[r]->p, B, c->st);
+                    CK(cudaEventRecord(ev_used[r], c->st));
+                    if (next + K < tags.size()) issue_up(next + K);
+                }
                 t_start[next] = now();
                 engine.add(j, op, B, X, tol, max_steps, (long long)next);
                 ++next;
@@ -2755,9 +2831,11 @@ static int run_block(lym_context *c, OpEntry &op, int sp, int algo, double tol, 
             }
         }
     } catch (...) {
+        cudaStreamSynchronize(c->st_copy);
         for (auto v : bufs) delete v;
         throw;
     }
+    CK(cudaStreamSynchronize(c->st_copy));
     for (auto v : bufs) delete v;
     return rc_all;
 }
@@ -3061,19 +3139,6 @@ int lym_rhmc_force_solves_device(lym_context *c, int square_op_id, int dirac_op_
                                 stats, true);
 }
 
-// device memory for the length of one call
-struct DevBuf {
-    lym_context *c;
-    void *p = nullptr;
-    size_t n = 0;
-    DevBuf(lym_context *ctx, size_t bytes) : c(ctx), p(dev_alloc(ctx, bytes)), n(bytes) {}
-    ~DevBuf()
-    {
-        if (p) dev_free(c, p, n);
-    }
-    DevBuf(const DevBuf &) = delete;
-    DevBuf &operator=(const DevBuf &) = delete;
-};
 
 static int do_meson(lym_context *c, const double *const *props, double *pion, double *scalar, double *ps,
                     bool device_ptr)
