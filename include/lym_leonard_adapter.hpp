@@ -10,6 +10,8 @@
 //     multiply / multiplyAdd -> lym_multiply / lym_multiply_add on the raw vector storage
 //   GpuSolver       : Solver            -> lym_solve     (inverters/Solver.h:13)
 //   GpuMultishiftSolver : MultishiftSolver -> lym_multishift (inverters/MultishiftSolver.h:28)
+//   GpuFermionForce : ImprovedFermionForce, what GpuDiracOperator::getForce returns
+//     derivative(force, lattice, X, Y, weight) -> lym_fermion_force (hmc_forces/FermionForce.h:15)
 //
 // Requirements: single process (no ENABLE_MPI), LocalLayout initialised, even glob_t.
 // Errors: the reference calls exit() on misuse; these adapters print the library's
@@ -18,6 +20,8 @@
 #define LYM_LEONARD_ADAPTER_HPP
 
 #include <iostream>
+#include <stdexcept>
+#include <string>
 #include <vector>
 
 #include "dirac_operators/DiracWilsonOperator.h"
@@ -26,6 +30,7 @@
 #include "dirac_operators/SquareDiracWilsonOperator.h"
 #include "dirac_operators/SquareEvenOddImprovedDiracWilsonOperator.h"
 #include "dirac_operators/SquareImprovedDiracWilsonOperator.h"
+#include "hmc_forces/ImprovedFermionForce.h"
 #include "inverters/MultishiftSolver.h"
 #include "inverters/Solver.h"
 #include "lym_b200.h"
@@ -63,6 +68,8 @@ inline int lym_next_gauge_id()
     static int next = 1;
     return next++;
 }
+
+class GpuFermionForce;
 
 template <class Base, int Kind> class GpuDiracOperator : public Base {
 public:
@@ -107,6 +114,10 @@ public:
 
     int operatorId() { return sync() ? op_ : -1; }
 
+    // DiracOperator::getForce (dirac_operators/DiracOperator.h:101): the fermion force of this
+    // operator on the GPU (the library picks the Wilson or the improved force by the kind)
+    virtual FermionForce *getForce() const;
+
 protected:
     // kappa, csw and gamma5 are plain members of the reference classes (setGamma5 and
     // setCSW are not virtual), so they are pushed to the library before every use.
@@ -147,6 +158,34 @@ inline int lym_operator_of(DiracOperator *d)
     if (auto o = dynamic_cast<GpuSquareImprovedDiracWilsonOperator *>(d)) return o->operatorId();
     if (auto o = dynamic_cast<GpuSquareEvenOddImprovedDiracWilsonOperator *>(d)) return o->operatorId();
     return -1;
+}
+
+// FermionForce::derivative (hmc_forces/FermionForce.cpp:11-20) on the GPU for the operator
+// that created it: force[x][mu] -= weight * F_mu(x) on the raw force-lattice storage.
+class GpuFermionForce : public ImprovedFermionForce {
+public:
+    GpuFermionForce(DiracOperator *op, real_t kappa, real_t csw) : ImprovedFermionForce(kappa, csw), op_(op) {}
+    using ImprovedFermionForce::derivative;
+    virtual void derivative(extended_fermion_force_lattice_t &fermionForce, const extended_fermion_lattice_t &,
+                            const extended_dirac_vector_t &X, const extended_dirac_vector_t &Y, real_t weight)
+    {
+        lym_context *c = lym_global_context();
+        const int op = lym_operator_of(op_);
+        if (!c || op < 0)
+            throw std::runtime_error("GpuFermionForce needs the Gpu* DiracOperator that created it");
+        if (lym_fermion_force(c, op, reinterpret_cast<const double *>(X.getRawData()),
+                              reinterpret_cast<const double *>(Y.getRawData()), weight,
+                              reinterpret_cast<double *>(fermionForce.getRawData())) != LYM_OK)
+            throw std::runtime_error(std::string("liblym_b200: ") + lym_last_error(c));
+    }
+
+private:
+    DiracOperator *op_;
+};
+
+template <class Base, int Kind> FermionForce *GpuDiracOperator<Base, Kind>::getForce() const
+{
+    return new GpuFermionForce(const_cast<GpuDiracOperator *>(this), this->kappa, csw_of());
 }
 
 // Solver::solve on the GPU; `algorithm` is a lym_solver value.

@@ -51,3 +51,8 @@ COMMON=(-O2 -fPIC -fopenmp -std=c++17 -w -include ctime -include cstring -I"$HER
         -DMBE="\"$REF/utils/MatrixBaseExtension.h\"" -DEIGEN -DMULTITHREADING)
 build su3 "${COMMON[@]}" -DNUMCOLORS=3
 build su2adj "${COMMON[@]}" -DNUMCOLORS=2 -DADJOINT
+# the C++ adapter of include/ must compile against the reference's own headers
+for flags in "-DNUMCOLORS=3" "-DNUMCOLORS=2 -DADJOINT"; do
+  # shellcheck disable=SC2086
+  g++ "${COMMON[@]}" $flags -fsyntax-only -I"$HERE/../include" -x c++ "$HERE/../include/lym_leonard_adapter.hpp"
+done
