@@ -1405,10 +1405,12 @@ std::vector<BatchTile> tile_candidates(const Geom &g)
 // Schur complement on a batch whose slots share the gauge field and may carry their own
 // kappa and clover terms (per-slot tables b_slot = -kappa^2, T, Tinv in device memory):
 //   out_r = G5^g (T_oo,r in_r - kappa_r^2 H_oe T_ee,r^-1 H_eo in_r)
+// res_r, res_s, res_alpha (optional): with the second launch, s = r - alpha out per RHS
 void apply_schur_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, const SpinorBatch &out,
                        const SpinorBatch &in, const SpinorBatch &tmp, int gamma5, const int *skip, const int *active,
                        const double *b_slot, const void *const *T_slot, const void *const *Ti_slot,
-                       const BatchTile &tile, const int *uniform)
+                       const BatchTile &tile, const int *uniform, const SpinorBatch *res_r = nullptr,
+                       const SpinorBatch *res_s = nullptr, const double2 *res_alpha = nullptr)
 {
     DslashBatchParams P;
     P.g = c->g;
@@ -1430,7 +1432,7 @@ void apply_schur_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, c
     P.clover_slot = clov ? Ti_slot : nullptr;
     P.a = 1.0;
     launch_dslash_batch(P, c->st);
-    P.epi = EPI_XPAY_;
+    P.epi = res_r ? EPI_XPAY_RES_ : EPI_XPAY_;
     P.parity = 1;
     P.in = tmp;
     P.out = out;
@@ -1438,6 +1440,11 @@ void apply_schur_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, c
     P.clover_slot = clov ? T_slot : nullptr;
     P.b_slot = b_slot;
     P.gamma5 = gamma5;
+    if (res_r) {
+        P.res_r = *res_r;
+        P.res_s = *res_s;
+        P.res_alpha = res_alpha;
+    }
     launch_dslash_batch(P, c->st);
     count(c, 2);
 }
@@ -2177,9 +2184,9 @@ private:
         Gate gate{&S->pause, nullptr};
         const int lognb = xs.s.lognb;
         // alpha is known when the iteration starts (<rhat, S p> = <S^+ rhat, p>, reduced with p)
+        // v = S p, and s = r - alpha v in the same launch's epilogue
         apply_schur_batch(c, U, has_clover, sprec, aps.s, ps.s, tes.s, 0, &S->pause, S->active, d_b, d_T, d_Ti, tile,
-                          d_uniform);
-        run_batch(c, OpBBResidualS<BatchF, SP, SP>{rs.f(), v, sv, S}, lognb, gate);
+                          d_uniform, &rs.s, &svec->s, S->alpha);
         apply_schur_batch(c, U, has_clover, sprec, tos.s, svec->s, tes.s, 0, &S->pause, S->active, d_b, d_T, d_Ti,
                           tile, d_uniform);
         run_batch(c, OpBBOmega<SP, SP, BatchF>{t, sv, rhat->f(), S}, lognb, gate);

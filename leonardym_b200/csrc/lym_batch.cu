@@ -27,6 +27,8 @@ static void launch_staged(const DslashBatchArg<SB, G> &a, int nblk, cudaStream_t
 
 static BatchF fview(const SpinorBatch &s) { return BatchF{(float4 *)s.v, s.stride, s.lognb - 1}; }
 static BatchH hview(const SpinorBatch &s) { return BatchH{(int4 *)s.v, (float2 *)s.norm, s.stride, s.lognb - 1}; }
+static void view_as(const SpinorBatch &s, BatchF &v) { v = s.v ? fview(s) : BatchF{}; }
+static void view_as(const SpinorBatch &s, BatchH &v) { v = s.v ? hview(s) : BatchH{}; }
 
 template <int EPI, class SB, class G>
 static void launch_minb(const DslashBatchParams &P, const DslashBatchArg<SB, G> &a, cudaStream_t st)
@@ -45,13 +47,17 @@ static void launch_minb(const DslashBatchParams &P, const DslashBatchArg<SB, G> 
 template <class SB, class G>
 static void run(const DslashBatchParams &P, const SB &in, const SB &out, const SB &y, const G &U, cudaStream_t st)
 {
+    SB res_s;
+    view_as(P.res_s, res_s);
     DslashBatchArg<SB, G> a{P.g,       in,          out,       y,         U,
                             P.parity,  P.gamma5,    P.has_clover, in.lognp, (float)P.a,
                             (float)P.b, NbrTable{P.nbr, P.g.stride}, P.order, P.skip_if, P.active,
-                            P.b_slot,  P.clover_slot, P.uniform};
+                            P.b_slot,  P.clover_slot, P.uniform, P.res_r.v ? fview(P.res_r) : BatchF{},
+                            res_s,     P.res_alpha};
     switch (P.epi) {
     case EPI_SCALE_: launch_minb<EPI_SCALE>(P, a, st); break;
     case EPI_CLOVINV_: launch_minb<EPI_CLOVINV>(P, a, st); break;
+    case EPI_XPAY_RES_: launch_minb<EPI_XPAY_RES>(P, a, st); break;
     default: launch_minb<EPI_XPAY>(P, a, st); break;
     }
 }

@@ -606,6 +606,11 @@ template <class SB, class GaugeT> struct DslashBatchArg {
     const double *b_slot;
     const void *const *clover_slot;
     const int *uniform;  // device flag: every slot on one operator (nullptr: not known)
+    // EPI_XPAY_RES: the BiCGStab residual s = r - alpha out of every active RHS (an inactive
+    // lane copies r), written next to out
+    BatchF res_r;
+    SB res_s;
+    const double2 *res_alpha;
 };
 
 // The epilogue on H x (acc) for the pair q at half-site h, written to out.  ysrc(blk, y6)
@@ -662,6 +667,21 @@ LYM_D void batch_epilogue(const DslashBatchArg<SB, GaugeT> &arg, int h, int q, b
         }
     }
     arg.out.store(h, q, acc);
+    if constexpr (EPI == EPI_XPAY_RES) {
+        c2 r[12];
+        arg.res_r.load(h, q, r);
+        const double2 aa = act_a ? arg.res_alpha[ra] : make_double2(0.0, 0.0);
+        const double2 ab = act_b ? arg.res_alpha[rb] : make_double2(0.0, 0.0);
+        const float2 are = make_float2((float)aa.x, (float)ab.x), aim = make_float2((float)aa.y, (float)ab.y);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+            // s = r - alpha v:  re -= are v.re - aim v.im,  im -= are v.im + aim v.re
+            const float2 sre = fma2(aim, acc[k].im, sub2(r[k].re, mul2(are, acc[k].re)));
+            const float2 sim = sub2(sub2(r[k].im, mul2(are, acc[k].im)), mul2(aim, acc[k].re));
+            r[k] = c2{sre, sim};
+        }
+        arg.res_s.store(h, q, r);
+    }
 }
 
 template <int EPI, class SB, class GaugeT>
@@ -701,7 +721,7 @@ __global__ void __launch_bounds__(128, MINB) dslash_batch_kernel(const DslashBat
     c2 acc[12];
     hopping_pair<GaugeT::kReal>(nf, nbk, arg.in, arg.U, arg.parity, h, q, acc);
     const CloverWordsGlobal cw = clover_global<EPI>(arg, h, q, act_a, act_b);
-    if (EPI == EPI_XPAY) {
+    if (EPI == EPI_XPAY || EPI == EPI_XPAY_RES) {
         c2 yv[12];
         arg.y.load_cs(h, q, yv);
         batch_epilogue<EPI>(arg, h, q, act_a, act_b, acc, [&](int blk, c2 y6[6]) {
@@ -797,7 +817,7 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
         act_b = arg.active[2 * q + 1] != 0;
     }
     const int np = 1 << arg.lognp;
-    StagedHop<EPI == EPI_XPAY, SB, GaugeT> s{arg, stage_smem, 0, q, np, (int)threadIdx.x >> arg.lognp,
+    StagedHop<EPI == EPI_XPAY || EPI == EPI_XPAY_RES, SB, GaugeT> s{arg, stage_smem, 0, q, np, (int)threadIdx.x >> arg.lognp,
                                              (int)threadIdx.x & (np - 1)};
     s.h = arg.order ? __ldg(arg.order + wi) : wi;
 #pragma unroll
@@ -1125,35 +1145,6 @@ template <class SP, class SR> struct OpBDirection {
 
 LYM_D double2 as_d2(cx<double> z) { return make_double2(z.re, z.im); }
 LYM_D cx<double> as_cx(double2 z) { return cx<double>{z.x, z.y}; }
-
-// s_r = r_r - alpha_r v_r
-template <class SR, class SV, class SS> struct OpBBResidualS {
-    static constexpr int NRED = 0;
-    SR rv;
-    SV v;
-    SS sv;
-    BatchCGState *s;
-    LYM_D void site(int h, int q, double *) const
-    {
-        const bool act[2] = {s->active[2 * q] != 0, s->active[2 * q + 1] != 0};
-        if (!act[0] && !act[1]) return;
-        const cx<double> al[2] = {as_cx(s->alpha[2 * q]), as_cx(s->alpha[2 * q + 1])};
-        auto so = pair_out(sv, h, q);
-#pragma unroll 2
-        for (int c = 0; c < 12; ++c) {
-            cx<double> r[2], w[2];
-            rv.get(h, q, c, r[0], r[1]);
-            v.get(h, q, c, w[0], w[1]);
-#pragma unroll
-            for (int l = 0; l < 2; ++l)
-                if (act[l]) r[l] = r[l] - al[l] * w[l];
-            so.put(c, r[0], r[1]);
-        }
-        so.finish();
-    }
-    LYM_D void finalize(int, const double *) const {}
-    LYM_D void finalize_all() const {}
-};
 
 // omega_r = <t_r, s_r> / |t_r|^2;  rho'_r = <rhat_r, r'_r> = <rhat_r, s_r> - omega_r <rhat_r, t_r>;
 // beta_r = (rho'_r / rho_r) (alpha_r / omega_r).  A zero |t|^2 or rho' marks the slot for a

@@ -155,6 +155,7 @@ enum Epilogue : int {
     EPI_CLOVINV = 1,    // out = Tinv (a * Hx)        (Tinv of the output parity)
     EPI_XPAY = 2,       // out = G5^g (T y + b Hx) + alpha v2   (T = 1 without clover)
     EPI_XPAY_INV = 3,   // out = Tinv (y + b Hx)
+    EPI_XPAY_RES = 4,   // EPI_XPAY, then s = r - alpha out per RHS (batched BiCGStab)
 };
 
 template <class SpinorT, class GaugeT, class CloverT>

@@ -47,7 +47,7 @@ struct CloverDev {
     void *Tinv[3] = {nullptr, nullptr, nullptr};
 };
 
-enum Epi : int { EPI_SCALE_ = 0, EPI_CLOVINV_ = 1, EPI_XPAY_ = 2, EPI_XPAY_INV_ = 3 };
+enum Epi : int { EPI_SCALE_ = 0, EPI_CLOVINV_ = 1, EPI_XPAY_ = 2, EPI_XPAY_INV_ = 3, EPI_XPAY_RES_ = 4 };
 
 struct DslashParams {
     Geom g;
@@ -110,6 +110,9 @@ struct DslashBatchParams {
     const double *b_slot = nullptr;            // device array [nb] or nullptr
     const void *const *clover_slot = nullptr;  // device array [nb] of FP32 clover bases (T or Tinv)
     const int *uniform = nullptr;              // device flag: every slot on one operator
+    // EPI_XPAY_RES: s = r - alpha out with r FP32, s in the precision of out, alpha per RHS
+    SpinorBatch res_r, res_s;
+    const double2 *res_alpha = nullptr;
 };
 
 void launch_dslash_batch(const DslashBatchParams &P, cudaStream_t st);
