@@ -1406,11 +1406,14 @@ std::vector<BatchTile> tile_candidates(const Geom &g)
 // kappa and clover terms (per-slot tables b_slot = -kappa^2, T, Tinv in device memory):
 //   out_r = G5^g (T_oo,r in_r - kappa_r^2 H_oe T_ee,r^-1 H_eo in_r)
 // res_r, res_s, res_alpha (optional): with the second launch, s = r - alpha out per RHS
+// om_rhat, om_scratch, om_state (optional, batch_omega_fusable variants): with the second
+// launch, the BiCGStab omega sums of out, in and rhat, then the omega update of the state
 void apply_schur_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, const SpinorBatch &out,
                        const SpinorBatch &in, const SpinorBatch &tmp, int gamma5, const int *skip, const int *active,
                        const double *b_slot, const void *const *T_slot, const void *const *Ti_slot,
                        const BatchTile &tile, const int *uniform, const SpinorBatch *res_r = nullptr,
-                       const SpinorBatch *res_s = nullptr, const double2 *res_alpha = nullptr)
+                       const SpinorBatch *res_s = nullptr, const double2 *res_alpha = nullptr,
+                       const SpinorBatch *om_rhat = nullptr, double *om_scratch = nullptr, void *om_state = nullptr)
 {
     DslashBatchParams P;
     P.g = c->g;
@@ -1445,8 +1448,19 @@ void apply_schur_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, c
         P.res_s = *res_s;
         P.res_alpha = res_alpha;
     }
+    if (om_rhat) {
+        if (!batch_omega_fusable(tile.minb, prec) || res_r || gamma5)
+            fail(c, LYM_ERR_ARGUMENT, "the omega sums need the FP32 staged stencil without other fusions");
+        P.epi = EPI_XPAY_OMEGA_;
+        P.om_rhat = *om_rhat;
+        P.om_partials = om_scratch;
+    }
     launch_dslash_batch(P, c->st);
     count(c, 2);
+    if (om_rhat) {
+        launch_omega_finalize(om_scratch, c->g, out.lognb, om_state, c->st);
+        count(c, 2);
+    }
 }
 
 // Autotuner of the batched stencil: times one batched Schur application for every
@@ -1841,6 +1855,8 @@ public:
             has_clover = clov;
             for (int k = 0; k < nb; ++k) set_tables(k, b, T, Ti);
             tile = tune_batch(c, gauge_of(c, gauge_id).dev, clov, sprec, tos.s, ps.s, tes.s, d_b, d_T, d_Ti, d_uniform);
+            if (algo == ALGO_BICGSTAB && batch_omega_fusable(tile.minb, sprec))
+                om_scratch.reset(new DevBuf(c, omega_scratch_doubles(c->g, xs.s.lognb) * sizeof(double)));
         }
         Slot &s = slot[j];
         delete s.bp;
@@ -1935,6 +1951,7 @@ private:
     Vec te, t1, rS, rN;
     BVec xs, rs, ps, aps, tes, tos;       // CG: p, S^+S p (aps), tmp, S p (tos); BiCGStab: p, v, tmp, t
     std::unique_ptr<BVec> svec, rhat, what;  // BiCGStab only: s, the shadow residual rhat, S^+ rhat
+    std::unique_ptr<DevBuf> om_scratch;      // BiCGStab: partial omega sums of the fused stencil epilogue
     static constexpr size_t kTableBytes = 3 * kMaxBatch * sizeof(double) + 16;
     char *tables = nullptr;
     double *d_b = nullptr;
@@ -2187,9 +2204,15 @@ private:
         // v = S p, and s = r - alpha v in the same launch's epilogue
         apply_schur_batch(c, U, has_clover, sprec, aps.s, ps.s, tes.s, 0, &S->pause, S->active, d_b, d_T, d_Ti, tile,
                           d_uniform, &rs.s, &svec->s, S->alpha);
-        apply_schur_batch(c, U, has_clover, sprec, tos.s, svec->s, tes.s, 0, &S->pause, S->active, d_b, d_T, d_Ti,
-                          tile, d_uniform);
-        run_batch(c, OpBBOmega<SP, SP, BatchF>{t, sv, rhat->f(), S}, lognb, gate);
+        if (om_scratch) {  // t = S s with the omega sums in its epilogue
+            apply_schur_batch(c, U, has_clover, sprec, tos.s, svec->s, tes.s, 0, &S->pause, S->active, d_b, d_T,
+                              d_Ti, tile, d_uniform, nullptr, nullptr, nullptr, &rhat->s,
+                              (double *)om_scratch->p, S);
+        } else {
+            apply_schur_batch(c, U, has_clover, sprec, tos.s, svec->s, tes.s, 0, &S->pause, S->active, d_b, d_T,
+                              d_Ti, tile, d_uniform);
+            run_batch(c, OpBBOmega<SP, SP, BatchF>{t, sv, rhat->f(), S}, lognb, gate);
+        }
         run_batch(c, OpBBUpdate<BatchF, SP, SP, SP, SP, BatchF, BatchF>{xs.f(), p, sv, t, v, rs.f(), what->f(), S},
                   lognb, gate);
     }

@@ -53,13 +53,81 @@ static void run(const DslashBatchParams &P, const SB &in, const SB &out, const S
                             P.parity,  P.gamma5,    P.has_clover, in.lognp, (float)P.a,
                             (float)P.b, NbrTable{P.nbr, P.g.stride}, P.order, P.skip_if, P.active,
                             P.b_slot,  P.clover_slot, P.uniform, P.res_r.v ? fview(P.res_r) : BatchF{},
-                            res_s,     P.res_alpha};
+                            res_s,     P.res_alpha, P.om_rhat.v ? fview(P.om_rhat) : BatchF{}, P.om_partials};
     switch (P.epi) {
     case EPI_SCALE_: launch_minb<EPI_SCALE>(P, a, st); break;
     case EPI_CLOVINV_: launch_minb<EPI_CLOVINV>(P, a, st); break;
     case EPI_XPAY_RES_: launch_minb<EPI_XPAY_RES>(P, a, st); break;
+    case EPI_XPAY_OMEGA_: {  // staged variants only (batch_omega_fusable)
+        const int nblk = (int)batch_stencil_blocks(P.g, in.lognp + 1);
+        if (P.minb == 19) launch_staged<EPI_XPAY_OMEGA, 3>(a, nblk, st);
+        else launch_staged<EPI_XPAY_OMEGA, 4>(a, nblk, st);
+        break;
+    }
     default: launch_minb<EPI_XPAY>(P, a, st); break;
     }
+}
+
+// The omega sums of the staged stencil's blocks (EPI_XPAY_OMEGA), [block][nb][7], added in a
+// fixed order: kOmegaChunks blocks each add a fixed range of stencil blocks, then one block per
+// RHS adds the chunk sums and applies omega_finalize.
+constexpr int kOmegaThreads = 256;
+constexpr int kOmegaChunks = 256;
+__global__ void __launch_bounds__(kOmegaThreads) omega_chunk_kernel(const double *partials, int nblk, int nb,
+                                                                    double *chunks, const BatchCGState *S)
+{
+    if (S->pause) return;
+    const int w = nb * 7, j = threadIdx.x;
+    if (j >= w) return;
+    const long per = (nblk + kOmegaChunks - 1) / kOmegaChunks;
+    const long b0 = blockIdx.x * per, b1 = min((long)nblk, b0 + per);
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+    long b = b0;
+    for (; b + 4 <= b1; b += 4) {
+        t0 += __ldcg(partials + b * w + j);
+        t1 += __ldcg(partials + (b + 1) * w + j);
+        t2 += __ldcg(partials + (b + 2) * w + j);
+        t3 += __ldcg(partials + (b + 3) * w + j);
+    }
+    for (; b < b1; ++b) t0 += __ldcg(partials + b * w + j);
+    chunks[(long)blockIdx.x * w + j] = (t0 + t1) + (t2 + t3);
+}
+
+__global__ void __launch_bounds__(kOmegaThreads) omega_finalize_kernel(const double *chunks, int nb, BatchCGState *S)
+{
+    if (S->pause) return;
+    __shared__ double sm[kOmegaThreads][7];
+    const int r = blockIdx.x, w = nb * 7;
+    double t[7] = {0, 0, 0, 0, 0, 0, 0};
+    for (int b = threadIdx.x; b < kOmegaChunks; b += blockDim.x)
+#pragma unroll
+        for (int j = 0; j < 7; ++j) t[j] += chunks[(long)b * w + r * 7 + j];
+#pragma unroll
+    for (int j = 0; j < 7; ++j) sm[threadIdx.x][j] = t[j];
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o)
+#pragma unroll
+            for (int j = 0; j < 7; ++j) sm[threadIdx.x][j] += sm[threadIdx.x + o][j];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) omega_finalize(S, r, sm[0]);
+}
+
+bool batch_omega_fusable(int minb, int prec) { return prec == PREC_F && (minb == 19 || minb == 20); }
+
+long omega_scratch_doubles(const Geom &g, int lognb)
+{
+    return (batch_stencil_blocks(g, lognb) + kOmegaChunks) * (7L << lognb);
+}
+
+void launch_omega_finalize(double *scratch, const Geom &g, int lognb, void *state, cudaStream_t st)
+{
+    const long nblk = batch_stencil_blocks(g, lognb);
+    const int nb = 1 << lognb;
+    double *chunks = scratch + nblk * 7 * nb;
+    omega_chunk_kernel<<<kOmegaChunks, kOmegaThreads, 0, st>>>(scratch, (int)nblk, nb, chunks, (BatchCGState *)state);
+    omega_finalize_kernel<<<nb, kOmegaThreads, 0, st>>>(chunks, nb, (BatchCGState *)state);
 }
 
 void launch_dslash_batch(const DslashBatchParams &P, cudaStream_t st)

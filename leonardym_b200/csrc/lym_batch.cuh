@@ -611,6 +611,9 @@ template <class SB, class GaugeT> struct DslashBatchArg {
     BatchF res_r;
     SB res_s;
     const double2 *res_alpha;
+    // EPI_XPAY_OMEGA: rhat and the per-block partial sums [block][nb][7]
+    BatchF om_rhat;
+    double *om_partials;
 };
 
 // The epilogue on H x (acc) for the pair q at half-site h, written to out.  ysrc(blk, y6)
@@ -800,59 +803,126 @@ template <bool STAGE_Y, class SB, class GaugeT> struct StagedHop {
     }
 };
 
+// EPI_XPAY_OMEGA: the sums of one thread's pair are reduced over the block in a fixed order
+// (warp shuffles, then the four warps in shared memory) and written as the block's partial
+// sums [block][nb][7]; every thread of the block takes part.
+template <class SB, class GaugeT>
+LYM_D void omega_block_reduce(const DslashBatchArg<SB, GaugeT> &arg, float4 *smem, double v[14])
+{
+    __syncthreads();  // every thread is done with the staging buffers
+    double *sm = reinterpret_cast<double *>(smem);  // [4 warps][kMaxBatch][7]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int np = 1 << arg.lognp, nb = 2 * np;
+#pragma unroll
+    for (int k = 0; k < 14; ++k)
+        for (int o = 16; o >= np; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    if (lane < np) {
+#pragma unroll
+        for (int j = 0; j < 7; ++j) {
+            sm[(warp * kMaxBatch + 2 * lane) * 7 + j] = v[j];
+            sm[(warp * kMaxBatch + 2 * lane + 1) * 7 + j] = v[7 + j];
+        }
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < nb) {
+        for (int j = 0; j < 7; ++j) {
+            double t = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sm[(w * kMaxBatch + threadIdx.x) * 7 + j];
+            arg.om_partials[((size_t)blockIdx.x * nb + threadIdx.x) * 7 + j] = t;
+        }
+    }
+}
+
 template <int EPI, int MINB, class SB, class GaugeT>
 __global__ void __launch_bounds__(kStagedThreads, MINB)
     dslash_batch_staged_kernel(const DslashBatchArg<SB, GaugeT> arg)
 {
     extern __shared__ float4 stage_smem[];
     if (arg.skip_if && *arg.skip_if) return;
+    constexpr bool RED = EPI == EPI_XPAY_OMEGA;
+    double red[RED ? 14 : 1];
+#pragma unroll
+    for (int k = 0; k < (RED ? 14 : 1); ++k) red[k] = 0.0;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int wi = tid >> arg.lognp, q = tid & ((1 << arg.lognp) - 1);
     const bool valid = wi < arg.g.Vh;  // equal for all lanes of a half-site
     const unsigned vmask = __ballot_sync(0xffffffffu, valid);
-    if (!valid) return;
-    bool act_a = true, act_b = true;
-    if (arg.active) {
-        act_a = arg.active[2 * q] != 0;
-        act_b = arg.active[2 * q + 1] != 0;
-    }
-    const int np = 1 << arg.lognp;
-    StagedHop<EPI == EPI_XPAY || EPI == EPI_XPAY_RES, SB, GaugeT> s{arg, stage_smem, 0, q, np, (int)threadIdx.x >> arg.lognp,
-                                             (int)threadIdx.x & (np - 1)};
-    s.h = arg.order ? __ldg(arg.order + wi) : wi;
+    auto work = [&]() {
+        if (!valid) return;
+        bool act_a = true, act_b = true;
+        if (arg.active) {
+            act_a = arg.active[2 * q] != 0;
+            act_b = arg.active[2 * q + 1] != 0;
+        }
+        const int np = 1 << arg.lognp;
+        StagedHop<EPI == EPI_XPAY || EPI == EPI_XPAY_RES || EPI == EPI_XPAY_OMEGA, SB, GaugeT> s{
+            arg, stage_smem, 0, q, np, (int)threadIdx.x >> arg.lognp, (int)threadIdx.x & (np - 1)};
+        s.h = arg.order ? __ldg(arg.order + wi) : wi;
 #pragma unroll
-    for (int mu = 0; mu < 4; ++mu) {
-        s.nf[mu] = arg.nbr.get(arg.parity, mu, 0, s.h);
-        s.nbk[mu] = arg.nbr.get(arg.parity, mu, 1, s.h);
-    }
-    s.live = act_a || act_b;  // idle pairs still copy their share of the link words
-    s.vmask = vmask;
-    s.clov_smem = EPI != EPI_SCALE && arg.has_clover && arg.uniform && *arg.uniform;
-    s.clov = s.clov_smem ? (const float4 *)arg.clover_slot[0] : nullptr;
-    c2 acc[12];
+        for (int mu = 0; mu < 4; ++mu) {
+            s.nf[mu] = arg.nbr.get(arg.parity, mu, 0, s.h);
+            s.nbk[mu] = arg.nbr.get(arg.parity, mu, 1, s.h);
+        }
+        s.live = act_a || act_b;  // idle pairs still copy their share of the link words
+        s.vmask = vmask;
+        s.clov_smem = EPI != EPI_SCALE && arg.has_clover && arg.uniform && *arg.uniform;
+        s.clov = s.clov_smem ? (const float4 *)arg.clover_slot[0] : nullptr;
+        c2 acc[12];
 #pragma unroll
-    for (int k = 0; k < 12; ++k) acc[k] = c2{make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
-    s.template issue<0>();
-    cp_async_commit();
-    s.template step<0>(acc);
-    s.template step<1>(acc);
-    s.template step<2>(acc);
-    s.template step<3>(acc);
-    s.template step<4>(acc);
-    s.template step<5>(acc);
-    s.template step<6>(acc);
-    s.template step<7>(acc);
-    if (s.clov_smem) s.stage_clover(1);  // link buffer 1 is free after the last direction
-    cp_async_commit();
-    cp_async_wait<0>();
-    __syncwarp(vmask);
-    if (!s.live) return;
-    auto ysrc = [&](int blk, c2 y6[6]) { arg.y.unstage_block(s.sx(0), kStagedThreads, blk, y6); };
-    if (s.clov_smem) {
-        batch_epilogue<EPI>(arg, s.h, q, act_a, act_b, acc, ysrc, CloverWordsSmem{s.sl(0), s.sl(1)});
-    } else {
-        batch_epilogue<EPI>(arg, s.h, q, act_a, act_b, acc, ysrc, clover_global<EPI>(arg, s.h, q, act_a, act_b));
-    }
+        for (int k = 0; k < 12; ++k) acc[k] = c2{make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+        s.template issue<0>();
+        cp_async_commit();
+        s.template step<0>(acc);
+        s.template step<1>(acc);
+        s.template step<2>(acc);
+        s.template step<3>(acc);
+        s.template step<4>(acc);
+        s.template step<5>(acc);
+        s.template step<6>(acc);
+        s.template step<7>(acc);
+        if (s.clov_smem) s.stage_clover(1);  // link buffer 1 is free after the last direction
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncwarp(vmask);
+        if (!s.live) return;
+        auto ysrc = [&](int blk, c2 y6[6]) { arg.y.unstage_block(s.sx(0), kStagedThreads, blk, y6); };
+        if (s.clov_smem) {
+            batch_epilogue<EPI>(arg, s.h, q, act_a, act_b, acc, ysrc, CloverWordsSmem{s.sl(0), s.sl(1)});
+        } else {
+            batch_epilogue<EPI>(arg, s.h, q, act_a, act_b, acc, ysrc, clover_global<EPI>(arg, s.h, q, act_a, act_b));
+        }
+        if constexpr (RED) {
+            // the omega sums of the two lanes: <t, s>, |t|^2, <rhat, s>, <rhat, t> (t = out, s = y)
+#pragma unroll
+            for (int blk = 0; blk < 2; ++blk) {
+                c2 y6[6];
+                ysrc(blk, y6);
+#pragma unroll
+                for (int k = 0; k < 6; ++k) {
+                    const c2 t = acc[6 * blk + k], sv = y6[k];
+                    cx<double> ra, rb;
+                    arg.om_rhat.get(s.h, q, 6 * blk + k, ra, rb);
+                    const double tr[2] = {t.re.x, t.re.y}, ti[2] = {t.im.x, t.im.y};
+                    const double sr[2] = {sv.re.x, sv.re.y}, si[2] = {sv.im.x, sv.im.y};
+                    const double rr[2] = {ra.re, rb.re}, ri[2] = {ra.im, rb.im};
+#pragma unroll
+                    for (int l = 0; l < 2; ++l) {
+                        if (l == 0 ? !act_a : !act_b) continue;
+                        double *a = red + 7 * l;
+                        a[0] += tr[l] * sr[l] + ti[l] * si[l];
+                        a[1] += tr[l] * si[l] - ti[l] * sr[l];
+                        a[2] += tr[l] * tr[l] + ti[l] * ti[l];
+                        a[3] += rr[l] * sr[l] + ri[l] * si[l];
+                        a[4] += rr[l] * si[l] - ri[l] * sr[l];
+                        a[5] += rr[l] * tr[l] + ri[l] * ti[l];
+                        a[6] += rr[l] * ti[l] - ri[l] * tr[l];
+                    }
+                }
+            }
+        }
+    };
+    work();
+    if constexpr (RED) omega_block_reduce(arg, stage_smem, red);
 }
 
 // --------------------------------------------------- batch site kernels ----
@@ -1149,6 +1219,19 @@ LYM_D cx<double> as_cx(double2 z) { return cx<double>{z.x, z.y}; }
 // omega_r = <t_r, s_r> / |t_r|^2;  rho'_r = <rhat_r, r'_r> = <rhat_r, s_r> - omega_r <rhat_r, t_r>;
 // beta_r = (rho'_r / rho_r) (alpha_r / omega_r).  A zero |t|^2 or rho' marks the slot for a
 // restart (the update parks it).
+// omega, rho' and beta of RHS r from t[7] = <t,s>, |t|^2, <rhat,s>, <rhat,t>
+LYM_D void omega_finalize(BatchCGState *s, int r, const double *t)
+{
+    if (!s->active[r]) return;
+    const double2 om = t[2] > 0.0 ? make_double2(t[0] / t[2], t[1] / t[2]) : make_double2(0.0, 0.0);
+    const double2 rho_new = csub(make_double2(t[3], t[4]), cmul(om, make_double2(t[5], t[6])));
+    const bool stalled = (om.x == 0.0 && om.y == 0.0) || (rho_new.x == 0.0 && rho_new.y == 0.0);
+    s->omega[r] = om;
+    s->bbeta[r] = stalled ? make_double2(0.0, 0.0) : cmul(cdiv(rho_new, s->rho[r]), cdiv(s->alpha[r], om));
+    s->rho[r] = rho_new;
+    if (stalled) s->restart[r] = 1;
+}
+
 template <class ST, class SS, class SRh> struct OpBBOmega {
     static constexpr int NRED = 7;
     ST tv;
@@ -1176,17 +1259,7 @@ template <class ST, class SS, class SRh> struct OpBBOmega {
             }
         }
     }
-    LYM_D void finalize(int r, const double *t) const
-    {
-        if (!s->active[r]) return;
-        const double2 om = t[2] > 0.0 ? make_double2(t[0] / t[2], t[1] / t[2]) : make_double2(0.0, 0.0);
-        const double2 rho_new = csub(make_double2(t[3], t[4]), cmul(om, make_double2(t[5], t[6])));
-        const bool stalled = (om.x == 0.0 && om.y == 0.0) || (rho_new.x == 0.0 && rho_new.y == 0.0);
-        s->omega[r] = om;
-        s->bbeta[r] = stalled ? make_double2(0.0, 0.0) : cmul(cdiv(rho_new, s->rho[r]), cdiv(s->alpha[r], om));
-        s->rho[r] = rho_new;
-        if (stalled) s->restart[r] = 1;
-    }
+    LYM_D void finalize(int r, const double *t) const { omega_finalize(s, r, t); }
     LYM_D void finalize_all() const {}
 };
 

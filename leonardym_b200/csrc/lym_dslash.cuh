@@ -156,6 +156,7 @@ enum Epilogue : int {
     EPI_XPAY = 2,       // out = G5^g (T y + b Hx) + alpha v2   (T = 1 without clover)
     EPI_XPAY_INV = 3,   // out = Tinv (y + b Hx)
     EPI_XPAY_RES = 4,   // EPI_XPAY, then s = r - alpha out per RHS (batched BiCGStab)
+    EPI_XPAY_OMEGA = 5, // EPI_XPAY, then the BiCGStab omega sums of out, y and rhat per RHS
 };
 
 template <class SpinorT, class GaugeT, class CloverT>

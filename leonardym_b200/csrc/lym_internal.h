@@ -47,7 +47,7 @@ struct CloverDev {
     void *Tinv[3] = {nullptr, nullptr, nullptr};
 };
 
-enum Epi : int { EPI_SCALE_ = 0, EPI_CLOVINV_ = 1, EPI_XPAY_ = 2, EPI_XPAY_INV_ = 3, EPI_XPAY_RES_ = 4 };
+enum Epi : int { EPI_SCALE_ = 0, EPI_CLOVINV_ = 1, EPI_XPAY_ = 2, EPI_XPAY_INV_ = 3, EPI_XPAY_RES_ = 4, EPI_XPAY_OMEGA_ = 5 };
 
 struct DslashParams {
     Geom g;
@@ -113,9 +113,21 @@ struct DslashBatchParams {
     // EPI_XPAY_RES: s = r - alpha out with r FP32, s in the precision of out, alpha per RHS
     SpinorBatch res_r, res_s;
     const double2 *res_alpha = nullptr;
+    // EPI_XPAY_OMEGA (staged kernel variants only): rhat (FP32) and the per-block partial sums
+    // [block][nb][7] of <out, y>, |out|^2, <rhat, y>, <rhat, out>
+    SpinorBatch om_rhat;
+    double *om_partials = nullptr;
 };
+// blocks of the batched stencil launch (the size of the EPI_XPAY_OMEGA partials)
+inline long batch_stencil_blocks(const Geom &g, int lognb) { return (((long)g.Vh << (lognb - 1)) + 127) / 128; }
 
 void launch_dslash_batch(const DslashBatchParams &P, cudaStream_t st);
+// the BiCGStab omega sums fused into the second stencil launch of a block Schur product
+// (EPI_XPAY_OMEGA_): the variants that support it, the scratch it needs (per-block partial
+// sums, then chunk sums) and the launches that add them up and apply the omega update
+bool batch_omega_fusable(int minb, int prec);
+long omega_scratch_doubles(const Geom &g, int lognb);
+void launch_omega_finalize(double *scratch, const Geom &g, int lognb, void *state, cudaStream_t st);
 void launch_nbr_table(const Geom &g, int *nbr, cudaStream_t st);
 // traversal of the half-sites in by * bz columns of the (y, z) plane, t fastest
 // (by | Ly, bz | Lz)

@@ -50,3 +50,33 @@ def test_block_rejects_bad_batch(setup):
     s = L.EvenOddConjugateGradient("single", 1e-10)
     with pytest.raises(L.LymError):
         s.solve_block(setup["op"], setup["srcs"], batch=3)
+
+
+@pytest.mark.parametrize("minb", [19, 20])
+def test_block_bicgstab_fused_omega_matches_separate_pass(setup, minb):
+    """The staged stencil variants fold the BiCGStab omega sums into the epilogue of the
+    t = S s launch; a direct variant keeps them in a separate pass.  Both meet the 1e-10
+    true residual and agree, and the fused sums are added in a fixed order (a second
+    solve repeats the first bit for bit)."""
+    from leonardym_b200.dirac import set_batch_tile
+    lat = setup["lat"]
+    srcs = setup["srcs"]
+    out = {}
+    try:
+        for variant in (minb, minb, 1):
+            set_batch_tile(lat, 0, 0, variant)
+            s = L.EvenOddBiCGStab("single", 1e-10)
+            ok, sols = s.solve_block(setup["op"], srcs, batch=8)
+            assert ok
+            for j, (b, x) in enumerate(zip(srcs, sols)):
+                r = np.linalg.norm(b - setup["D"].multiply(x)) / np.linalg.norm(b)
+                assert r <= 1e-10, (variant, j, r)
+            out.setdefault(variant, []).append((sols, [st.iterations for st in s.block_stats]))
+    finally:
+        set_batch_tile(lat, -1, 0)
+    (a, ia), (b, ib) = out[minb]
+    assert ia == ib
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+    for x, y in zip(a, out[1][0][0]):
+        assert rel(x, y) < 1e-8
