@@ -343,6 +343,17 @@ def block_solver(args):
 SOLVER_NAMES = {"cg": "block even-odd CG on (gamma5 S)^2", "bicgstab": "block even-odd BiCGStab on S"}
 
 
+ENGINE_KEYS = ("iterating_s", "reliable_updates_s", "adding_s", "collecting_s", "graph_replays", "pauses",
+               "reliable_updates")
+
+
+def engine_stats(lib, ctx):
+    out = (C.c_double * len(ENGINE_KEYS))()
+    if lib.lym_context_engine_stats(ctx, out, len(ENGINE_KEYS)) != 0:
+        raise RuntimeError("lym_context_engine_stats failed")
+    return list(out)
+
+
 def config_dict(solver):
     return {"workload": "su3-clover-24^3x48-kappa0.137-csw1.7-44rhs-tol1e-10", "lattice": "24x24x24x48",
             "representation": "SU(3) fundamental", "kappa": KAPPA, "csw": CSW, "links": "exp(i 0.25 H), seeded",
@@ -398,6 +409,7 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     lib.lym_synchronize(ctx)
     launches0 = lib.lym_context_kernel_launches(ctx)
+    eng0 = engine_stats(lib, ctx)
     sampler.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record()
@@ -409,6 +421,7 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     clocks = sampler.stop()
     launches = int(lib.lym_context_kernel_launches(ctx) - launches0)
+    eng = [(b - a) / args.steps for a, b in zip(eng0, engine_stats(lib, ctx))]
     elapsed = max_over_ranks(world, ev0.elapsed_time(ev1) / 1e3)
     barrier(world)
     value = world * nrhs * args.steps / elapsed
@@ -507,6 +520,7 @@ def run_ours(args, world, rank, local):
         "mixed_over_fp64": value / world / (fp64_value / world),
         "latency_ms": {"p50": lat_ms[len(lat_ms) // 2], "p99": lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))]},
         "iterations": {"median": statistics.median(iters), "max": max(iters)},
+        "engine_per_step": {k: round(v, 4) for k, v in zip(ENGINE_KEYS, eng)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
                      "kernel": (f"batched Schur stencil with clover, {args.batch} right-hand sides, "

@@ -384,6 +384,12 @@ int lym_stencil_indices(lym_context *ctx, int *out);
  * warm-up launches): which 0 = odd-parity output with the clover term and xpay epilogue
  * (second half of the Schur operator), 1 = even-parity output with T_ee^-1 (first half). */
 unsigned long long lym_context_kernel_launches(lym_context *ctx);
+/* where the block solves of this context spent their host wall time so far (seconds, and
+ * counts as doubles): out[0] iterating (graph replays of the batched loop, host waiting),
+ * out[1] reliable updates and restarts of parked slots, out[2] adding sources (Schur source,
+ * first true residual), out[3] collecting solutions (reconstruction, true residual,
+ * download), out[4] graph replays, out[5] loop pauses, out[6] reliable updates; n = 7 */
+int lym_context_engine_stats(lym_context *ctx, double *out, int n);
 int lym_time_stencil(lym_context *ctx, int op_id, int prec, int which, int iters, double *ms_per_launch);
 /* the same for the batched stencil of the block solves (prec 1 or 2, batch a power of 2,
  * 2 <= batch <= 32), in the configuration the autotuner picks (tuned on first use) */

@@ -115,6 +115,7 @@ def lib():
         "lym_neighbour_tables": (i, [vp, ip, ip]),
         "lym_stencil_indices": (i, [vp, ip]),
         "lym_context_kernel_launches": (C.c_ulonglong, [vp]),
+        "lym_context_engine_stats": (i, [vp, C.POINTER(C.c_double), i]),
         "lym_time_stencil": (i, [vp, i, i, i, i, C.POINTER(C.c_double)]),
         "lym_time_stencil_batch": (i, [vp, i, i, i, i, i, C.POINTER(C.c_double)]),
         "lym_multiply_batch": (i, [vp, i, i, C.POINTER(C.c_int), C.POINTER(vp), C.POINTER(vp)]),

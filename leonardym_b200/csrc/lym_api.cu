@@ -80,8 +80,12 @@ struct lym_context {
     // host-layout staging buffers (V * 24 doubles)
     double *aos[3] = {nullptr, nullptr, nullptr};
     std::vector<Spinor> pool;
+    // idle per-call device buffers (batched vectors, staging rings, scratch) kept for the
+    // next call of the same size, like the spinor pool: given back by trim_pool
+    std::vector<std::pair<size_t, void *>> blocks;
     size_t bytes = 0;
     unsigned long long launches = 0;  // kernels enqueued (graph replays count their nodes)
+    double engine_stats[7] = {};      // block solves: lym_context_engine_stats
     bool capturing = false;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
@@ -136,6 +140,11 @@ void trim_pool(lym_context *c)
         c->bytes -= spinor_bytes(c->g, s.prec, s.nparity);
     }
     c->pool.clear();
+    for (auto &b : c->blocks) {
+        cudaFree(b.second);
+        c->bytes -= b.first;
+    }
+    c->blocks.clear();
     for (int k = 0; k < 3; ++k)
         if (c->aos[k]) {
             cudaFree(c->aos[k]);
@@ -148,7 +157,8 @@ void *dev_alloc(lym_context *c, size_t bytes)
 {
     void *p = nullptr;
     cudaError_t e = cudaMalloc(&p, bytes);
-    if (e == cudaErrorMemoryAllocation && !c->capturing && (!c->pool.empty() || c->aos[0] || c->aos[1] || c->aos[2])) {
+    if (e == cudaErrorMemoryAllocation && !c->capturing &&
+        (!c->pool.empty() || !c->blocks.empty() || c->aos[0] || c->aos[1] || c->aos[2])) {
         // the idle pooled spinors are a cache: give them back and try once more
         cudaGetLastError();
         trim_pool(c);
@@ -171,15 +181,35 @@ void dev_free(lym_context *c, void *p, size_t bytes)
     }
 }
 
+// a zeroed buffer of the given size from the idle blocks, else newly allocated
+void *block_alloc(lym_context *c, size_t bytes)
+{
+    for (size_t i = 0; i < c->blocks.size(); ++i)
+        if (c->blocks[i].first == bytes) {
+            void *p = c->blocks[i].second;
+            c->blocks.erase(c->blocks.begin() + i);
+            CK(cudaMemsetAsync(p, 0, bytes, c->st));
+            return p;
+        }
+    return dev_alloc(c, bytes);
+}
+
+// back to the idle blocks (its last uses are ordered before any later use on the
+// context's stream; copies on the copy stream are drained by their owners first)
+void block_free(lym_context *c, void *p, size_t bytes)
+{
+    if (p) c->blocks.emplace_back(bytes, p);
+}
+
 // device memory for the length of one call
 struct DevBuf {
     lym_context *c;
     void *p = nullptr;
     size_t n = 0;
-    DevBuf(lym_context *ctx, size_t bytes) : c(ctx), p(dev_alloc(ctx, bytes)), n(bytes) {}
+    DevBuf(lym_context *ctx, size_t bytes) : c(ctx), p(block_alloc(ctx, bytes)), n(bytes) {}
     ~DevBuf()
     {
-        if (p) dev_free(c, p, n);
+        if (p) block_free(c, p, n);
     }
     DevBuf(const DevBuf &) = delete;
     DevBuf &operator=(const DevBuf &) = delete;
@@ -1349,11 +1379,11 @@ struct BVec {
         while ((1 << s.lognb) < nb) ++s.lognb;
         s.stride = c->g.stride;
         bytes = batch_bytes(c->g, prec, nb);
-        char *base = (char *)dev_alloc(c, bytes);
+        char *base = (char *)block_alloc(c, bytes);
         s.v = base;
         if (prec == PREC_H) s.norm = (float *)(base + (size_t)3 * s.stride * nb * sizeof(int4));
     }
-    ~BVec() { dev_free(c, s.v, bytes); }
+    ~BVec() { block_free(c, s.v, bytes); }
     BVec(const BVec &) = delete;
     BVec &operator=(const BVec &) = delete;
     BatchF f() const { return BatchF{(float4 *)s.v, s.stride, s.lognb - 1}; }
@@ -1462,6 +1492,16 @@ void apply_schur_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, c
         count(c, 2);
     }
 }
+
+// the squared fall of the recursive residual that triggers a block solve's FP64 reliable
+// update with FP32 inner storage, and the fraction (1/n) of busy slots parked for their
+// updates that pauses the batched loop
+#ifndef LYM_BLOCK_DELTA2_F
+#define LYM_BLOCK_DELTA2_F 1e-4
+#endif
+#ifndef LYM_BLOCK_PARK_FRACTION
+#define LYM_BLOCK_PARK_FRACTION 8
+#endif
 
 // Autotuner of the batched stencil: times one batched Schur application for every
 // traversal column and kernel variant on the caller's fields (in is read, tmp and out
@@ -1815,7 +1855,7 @@ public:
         hs.nb = nb;
         // reliable update when the recursive residual fell by 10x (FP16 inner storage) or
         // by 100x (FP32, whose rounding drift stays far below that between updates)
-        hs.delta2 = sprec == PREC_H ? 0.01 : 1e-4;
+        hs.delta2 = sprec == PREC_H ? 0.01 : LYM_BLOCK_DELTA2_F;
         static_assert(sizeof(BatchCGState) <= kStateBytes, "state buffer too small");
     }
     ~BlockEngine()
@@ -1899,6 +1939,7 @@ public:
         }
     }
 
+    static double wall() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); }
     // Iterates the running slots until the captured loop pauses (slots parked for their
     // FP64 reliable update, iteration limit, nothing left running), then services the
     // parked slots.  Returns the slots that finished since the last call.
@@ -1919,7 +1960,10 @@ public:
             *(BatchCGState *)c->h_state = hs;
             CK(cudaMemcpyAsync(c->d_state, c->h_state, sizeof(BatchCGState), cudaMemcpyHostToDevice, c->st));
             BatchCGState *S = (BatchCGState *)c->d_state;
+            const double t0 = wall();
             run_loop(S, (long)left + kGraphIters);
+            c->engine_stats[0] += wall() - t0;
+            c->engine_stats[5] += 1;
             hs = *(BatchCGState *)c->h_state;
             if (hs.failed) fail(c, LYM_ERR_NUMERIC, "block CG produced a non-finite residual");
             direction_rest(S);
@@ -1965,7 +2009,7 @@ private:
     size_t nodes = 0;
     static constexpr int kGraphIters = 8;
     // the loop pauses once a kParkFraction-th of the busy slots waits for its update
-    static constexpr int kParkFraction = 8;
+    static constexpr int kParkFraction = LYM_BLOCK_PARK_FRACTION;
     // BiCGStab gives a source up after kMaxStalls reliable updates in a row that did not
     // halve its best true residual, or after kMaxRestarts breakdowns
     static constexpr int kMaxStalls = 3, kMaxRestarts = 3;
@@ -2112,12 +2156,15 @@ private:
     // the reliable updates of the parked slots; a slot past its iteration limit finishes
     void service()
     {
+        const double t0 = wall();
         for (int j = 0; j < nb; ++j) {
             Slot &s = slot[j];
             if (!s.busy || s.finished || !hs.need_update[j]) continue;
             reliable_update(j);
+            c->engine_stats[6] += 1;
             if (!s.finished && hs.its[j] >= s.max_iter) finish(j);
         }
+        c->engine_stats[1] += wall() - t0;
     }
     // captures kGraphIters iterations once, then replays them until the state pauses
     void run_loop(BatchCGState *S, long max_iterations)
@@ -2145,6 +2192,7 @@ private:
         for (long l = 0; l < max_launches; ++l) {
             CK(cudaGraphLaunch(exec, c->st));
             c->launches += nodes;
+            c->engine_stats[4] += 1;
             CK(cudaMemcpyAsync(c->h_state, S, sizeof(BatchCGState), cudaMemcpyDeviceToHost, c->st));
             CK(cudaStreamSynchronize(c->st));
             if (((BatchCGState *)c->h_state)->pause) return;
@@ -2343,6 +2391,7 @@ void lym_context_destroy(lym_context *c)
         cudaFree(kv.second.dev.f32dup);
     }
     for (auto &s : c->pool) cudaFree(s.v);
+    for (auto &b : c->blocks) cudaFree(b.second);
     for (int k = 0; k < 3; ++k) cudaFree(c->aos[k]);
     cudaFree(c->partials);
     cudaFree(c->bpartials);
@@ -2806,6 +2855,7 @@ static int run_block(lym_context *c, OpEntry &op, int sp, int algo, double tol, 
     } drain{c};
     for (int k = 0; k < K; ++k) issue_up(k);
     auto collect = [&](int f) {
+        const double t_collect = now();
         const auto &s = engine.info(f);
         const int tag = tags[s.tag];
         if (s.gave_up) {
@@ -2833,6 +2883,7 @@ static int run_block(lym_context *c, OpEntry &op, int sp, int algo, double tol, 
             if (!s.converged) rc_all = LYM_NOT_CONVERGED;
         }
         engine.release(f);
+        c->engine_stats[3] += now() - t_collect;
     };
     try {
         for (int j = 0; j < 2 * width; ++j) bufs.push_back(new Vec(c, PREC_D, 2));
@@ -2851,7 +2902,9 @@ static int run_block(lym_context *c, OpEntry &op, int sp, int algo, double tol, 
                     if (next + K < tags.size()) issue_up(next + K);
                 }
                 t_start[next] = now();
+                const double t0 = now();
                 engine.add(j, op, B, X, tol, max_steps, (long long)next);
+                c->engine_stats[2] += now() - t0;
                 ++next;
             }
             for (int f : engine.advance()) collect(f);
@@ -3471,6 +3524,14 @@ int lym_stencil_indices(lym_context *c, int *out)
 }
 
 unsigned long long lym_context_kernel_launches(lym_context *c) { return c ? c->launches : 0ull; }
+
+int lym_context_engine_stats(lym_context *c, double *out, int n)
+{
+    if (!c || !out || n < 0) return LYM_ERR_ARGUMENT;
+    std::lock_guard<std::recursive_mutex> g(c->mu);
+    for (int k = 0; k < n && k < 7; ++k) out[k] = c->engine_stats[k];
+    return LYM_OK;
+}
 
 int lym_time_stencil(lym_context *c, int op_id, int prec, int which, int iters, double *ms_per_launch)
 {
