@@ -1454,6 +1454,8 @@ void apply_schur_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, c
     P.active = active;
     P.nbr = c->nbr;
     P.order = order_table(c, tile.by, tile.bz);
+    P.walk_by = tile.by;
+    P.walk_bz = tile.bz;
     P.minb = tile.minb;
     P.has_clover = clov;
     P.uniform = uniform;
@@ -3599,6 +3601,8 @@ int lym_time_stencil_batch(lym_context *c, int op_id, int prec, int which, int b
         P.U = &ge.dev;
         P.nbr = c->nbr;
         P.order = order_table(c, tile.by, tile.bz);
+        P.walk_by = tile.by;
+        P.walk_bz = tile.bz;
         P.minb = tile.minb;
         P.has_clover = clov;
         P.uniform = tab.uniform;

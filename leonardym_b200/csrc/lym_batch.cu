@@ -44,6 +44,34 @@ static void launch_minb(const DslashBatchParams &P, const DslashBatchArg<SB, G> 
     }
 }
 
+static unsigned walk_magic(int d) { return d == 1 ? 0u : (unsigned)(((1ull << 32) + d - 1) / d); }
+
+// the arithmetic walk of the traversal (by, bz) when its divisions are exact (ColumnWalk)
+ColumnWalk column_walk(const Geom &g, int by, int bz)
+{
+    ColumnWalk w{};
+    if (by == 0) {  // h order: one column of Ly x Lz
+        by = g.L[1];
+        bz = g.L[2];
+    }
+    if (bz < 1 || by < 1 || g.L[1] % by || g.L[2] % bz || g.L[3] % 2 || g.Vh >= (1 << 24)) return w;
+    const int div[5] = {g.L[3] / 2, bz, by, g.L[0], g.L[2] / bz};
+    for (int d : div)
+        if (d < 1 || d > 256) return w;
+    for (int k = 0; k < 4; ++k) w.L[k] = g.L[k];
+    w.lth = div[0];
+    w.bz = bz;
+    w.by = by;
+    w.nzb = div[4];
+    w.m_lth = walk_magic(div[0]);
+    w.m_bz = walk_magic(bz);
+    w.m_by = walk_magic(by);
+    w.m_lx = walk_magic(g.L[0]);
+    w.m_nzb = walk_magic(div[4]);
+    w.on = 1;
+    return w;
+}
+
 template <class SB, class G>
 static void run(const DslashBatchParams &P, const SB &in, const SB &out, const SB &y, const G &U, cudaStream_t st)
 {
@@ -53,7 +81,8 @@ static void run(const DslashBatchParams &P, const SB &in, const SB &out, const S
                             P.parity,  P.gamma5,    P.has_clover, in.lognp, (float)P.a,
                             (float)P.b, NbrTable{P.nbr, P.g.stride}, P.order, P.skip_if, P.active,
                             P.b_slot,  P.clover_slot, P.uniform, P.res_r.v ? fview(P.res_r) : BatchF{},
-                            res_s,     P.res_alpha, P.om_rhat.v ? fview(P.om_rhat) : BatchF{}, P.om_partials};
+                            res_s,     P.res_alpha, P.om_rhat.v ? fview(P.om_rhat) : BatchF{}, P.om_partials,
+                            column_walk(P.g, P.walk_by, P.walk_bz)};
     switch (P.epi) {
     case EPI_SCALE_: launch_minb<EPI_SCALE>(P, a, st); break;
     case EPI_CLOVINV_: launch_minb<EPI_CLOVINV>(P, a, st); break;

@@ -591,6 +591,53 @@ LYM_D void hopping_pair(const int nf[4], const int nbk[4], const SB &in, const G
     hopping_mu<REAL, 3>(nf, nbk, in, U, p, h, q, acc);
 }
 
+// Work item -> half-site and its 8 neighbours by arithmetic, for the traversal in (y, z)
+// columns of by x bz (the order of order_table_kernel; h order is the column Ly x Lz):
+// w = th + lth (zi + bz (yi + by (x + Lx (zb + nzb yb)))), th = t / 2, lth = Lt / 2.
+// Divisions are multiply-high by m = ceil(2^32 / d), exact for w < 2^24 and d <= 256
+// (the host checks both before it enables the walk).
+struct ColumnWalk {
+    int on;                           // 0: use the order and neighbour tables
+    int L[4], lth, by, bz, nzb;
+    unsigned m_lth, m_bz, m_by, m_lx, m_nzb;  // 0 for a divisor of 1
+};
+
+LYM_D unsigned walk_div(unsigned n, unsigned m) { return m ? __umulhi(n, m) : n; }
+
+// h and the neighbour half-sites nf (+mu) and nbk (-mu) of work item w at output parity p
+LYM_D int walk_site(const ColumnWalk &cw, int p, unsigned w, int nf[4], int nbk[4])
+{
+    unsigned u = w, q;
+    q = walk_div(u, cw.m_lth);
+    const int th = (int)(u - q * cw.lth);
+    u = q;
+    q = walk_div(u, cw.m_bz);
+    const int zi = (int)(u - q * cw.bz);
+    u = q;
+    q = walk_div(u, cw.m_by);
+    const int yi = (int)(u - q * cw.by);
+    u = q;
+    q = walk_div(u, cw.m_lx);
+    const int x = (int)(u - q * cw.L[0]);
+    u = q;
+    q = walk_div(u, cw.m_nzb);
+    const int zb = (int)(u - q * cw.nzb), yb = (int)q;
+    const int y = yb * cw.by + yi, z = zb * cw.bz + zi;
+    const int t = 2 * th + ((p + x + y + z) & 1);
+    const int sx = cw.lth * cw.L[2] * cw.L[1], sy = cw.lth * cw.L[2], sz = cw.lth;
+    const int h = th + sz * z + sy * y + sx * x;
+    nf[0] = h + (x + 1 == cw.L[0] ? -x * sx : sx);
+    nbk[0] = h + (x == 0 ? (cw.L[0] - 1) * sx : -sx);
+    nf[1] = h + (y + 1 == cw.L[1] ? -y * sy : sy);
+    nbk[1] = h + (y == 0 ? (cw.L[1] - 1) * sy : -sy);
+    nf[2] = h + (z + 1 == cw.L[2] ? -z * sz : sz);
+    nbk[2] = h + (z == 0 ? (cw.L[2] - 1) * sz : -sz);
+    const int base = h - th;
+    nf[3] = base + ((t + 1 == cw.L[3] ? 0 : t + 1) >> 1);
+    nbk[3] = base + ((t == 0 ? cw.L[3] - 1 : t - 1) >> 1);
+    return h;
+}
+
 template <class SB, class GaugeT> struct DslashBatchArg {
     Geom g;
     SB in, out, y;
@@ -614,6 +661,7 @@ template <class SB, class GaugeT> struct DslashBatchArg {
     // EPI_XPAY_OMEGA: rhat and the per-block partial sums [block][nb][7]
     BatchF om_rhat;
     double *om_partials;
+    ColumnWalk walk;  // the staged kernel's indices without tables (walk.on)
 };
 
 // The epilogue on H x (acc) for the pair q at half-site h, written to out.  ysrc(blk, y6)
@@ -857,11 +905,15 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
         const int np = 1 << arg.lognp;
         StagedHop<EPI == EPI_XPAY || EPI == EPI_XPAY_RES || EPI == EPI_XPAY_OMEGA, SB, GaugeT> s{
             arg, stage_smem, 0, q, np, (int)threadIdx.x >> arg.lognp, (int)threadIdx.x & (np - 1)};
-        s.h = arg.order ? __ldg(arg.order + wi) : wi;
+        if (arg.walk.on) {
+            s.h = walk_site(arg.walk, arg.parity, (unsigned)wi, s.nf, s.nbk);
+        } else {
+            s.h = arg.order ? __ldg(arg.order + wi) : wi;
 #pragma unroll
-        for (int mu = 0; mu < 4; ++mu) {
-            s.nf[mu] = arg.nbr.get(arg.parity, mu, 0, s.h);
-            s.nbk[mu] = arg.nbr.get(arg.parity, mu, 1, s.h);
+            for (int mu = 0; mu < 4; ++mu) {
+                s.nf[mu] = arg.nbr.get(arg.parity, mu, 0, s.h);
+                s.nbk[mu] = arg.nbr.get(arg.parity, mu, 1, s.h);
+            }
         }
         s.live = act_a || act_b;  // idle pairs still copy their share of the link words
         s.vmask = vmask;

@@ -106,6 +106,7 @@ struct DslashBatchParams {
     const int *active = nullptr;
     const int *nbr = nullptr;                  // neighbour table [2][8][stride]
     const int *order = nullptr;                // traversal table [stride] or nullptr (h order)
+    int walk_by = 0, walk_bz = 0;              // the column of that traversal (0: h order)
     int minb = 1;                              // kernel variant: minimum resident blocks per SM
     const double *b_slot = nullptr;            // device array [nb] or nullptr
     const void *const *clover_slot = nullptr;  // device array [nb] of FP32 clover bases (T or Tinv)
