@@ -886,22 +886,30 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
     dslash_batch_staged_kernel(const DslashBatchArg<SB, GaugeT> arg)
 {
     extern __shared__ float4 stage_smem[];
-    if (arg.skip_if && *arg.skip_if) return;
-    constexpr bool RED = EPI == EPI_XPAY_OMEGA;
-    double red[RED ? 14 : 1];
-#pragma unroll
-    for (int k = 0; k < (RED ? 14 : 1); ++k) red[k] = 0.0;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int wi = tid >> arg.lognp, q = tid & ((1 << arg.lognp) - 1);
     const bool valid = wi < arg.g.Vh;  // equal for all lanes of a half-site
+    constexpr bool RED = EPI == EPI_XPAY_OMEGA;
+    // the flags of the launch and of this pair, loaded together: one memory latency before
+    // the first copy is issued (the omega variant reads the pair's flags later: its
+    // registers are taken by the sums)
+    const int skip = arg.skip_if ? *arg.skip_if : 0;
+    const bool uniform = !RED && EPI != EPI_SCALE && arg.has_clover && arg.uniform && *arg.uniform;
+    int flag_a = 1, flag_b = 1;
+    if (!RED && arg.active && valid) {
+        flag_a = arg.active[2 * q];
+        flag_b = arg.active[2 * q + 1];
+    }
+    if (skip) return;
+    double red[RED ? 14 : 1];  // set by work() when it returns true
     const unsigned vmask = __ballot_sync(0xffffffffu, valid);
-    auto work = [&]() {
-        if (!valid) return;
-        bool act_a = true, act_b = true;
-        if (arg.active) {
-            act_a = arg.active[2 * q] != 0;
-            act_b = arg.active[2 * q + 1] != 0;
+    auto work = [&]() -> bool {
+        if (!valid) return false;
+        if (RED && arg.active) {
+            flag_a = arg.active[2 * q];
+            flag_b = arg.active[2 * q + 1];
         }
+        const bool act_a = flag_a != 0, act_b = flag_b != 0;
         const int np = 1 << arg.lognp;
         StagedHop<EPI == EPI_XPAY || EPI == EPI_XPAY_RES || EPI == EPI_XPAY_OMEGA, SB, GaugeT> s{
             arg, stage_smem, 0, q, np, (int)threadIdx.x >> arg.lognp, (int)threadIdx.x & (np - 1)};
@@ -917,7 +925,7 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
         }
         s.live = act_a || act_b;  // idle pairs still copy their share of the link words
         s.vmask = vmask;
-        s.clov_smem = EPI != EPI_SCALE && arg.has_clover && arg.uniform && *arg.uniform;
+        s.clov_smem = RED ? arg.has_clover && arg.uniform && *arg.uniform : uniform;
         s.clov = s.clov_smem ? (const float4 *)arg.clover_slot[0] : nullptr;
         c2 acc[12];
 #pragma unroll
@@ -936,7 +944,7 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
         cp_async_commit();
         cp_async_wait<0>();
         __syncwarp(vmask);
-        if (!s.live) return;
+        if (!s.live) return false;
         auto ysrc = [&](int blk, c2 y6[6]) { arg.y.unstage_block(s.sx(0), kStagedThreads, blk, y6); };
         if (s.clov_smem) {
             batch_epilogue<EPI>(arg, s.h, q, act_a, act_b, acc, ysrc, CloverWordsSmem{s.sl(0), s.sl(1)});
@@ -945,6 +953,8 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
         }
         if constexpr (RED) {
             // the omega sums of the two lanes: <t, s>, |t|^2, <rhat, s>, <rhat, t> (t = out, s = y)
+#pragma unroll
+            for (int k = 0; k < 14; ++k) red[k] = 0.0;
 #pragma unroll
             for (int blk = 0; blk < 2; ++blk) {
                 c2 y6[6];
@@ -972,9 +982,15 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
                 }
             }
         }
+        return true;
     };
-    work();
-    if constexpr (RED) omega_block_reduce(arg, stage_smem, red);
+    const bool summed = work();
+    if constexpr (RED) {
+        if (!summed)
+#pragma unroll
+            for (int k = 0; k < 14; ++k) red[k] = 0.0;
+        omega_block_reduce(arg, stage_smem, red);
+    }
 }
 
 // --------------------------------------------------- batch site kernels ----
