@@ -463,6 +463,9 @@ def run_ours(args, world, rank, local):
     # stencil of the block solve) on the library stream
     ms = C.c_double(0)
     lib.lym_time_stencil_batch(ctx, opid, sprec, 0, args.batch, 30, C.byref(ms))
+    tby, tbz, tminb = C.c_int(), C.c_int(), C.c_int()
+    if lib.lym_get_batch_tile(ctx, sprec, args.batch, 1, C.byref(tby), C.byref(tbz), C.byref(tminb)) != 0:
+        raise RuntimeError(f"lym_get_batch_tile failed: {lib.lym_last_error(ctx)}")
     Vh = V // 2
     bytes_launch = (STENCIL_SITE_BYTES[sprec] + args.batch * STENCIL_RHS_BYTES[sprec]) * Vh
     achieved = bytes_launch / (ms.value * 1e-3) / 1e9
@@ -526,6 +529,9 @@ def run_ours(args, world, rank, local):
                      "kernel": (f"batched Schur stencil with clover, {args.batch} right-hand sides, "
                                 f"{args.precision} storage, {ms.value * 1e3:.1f} us/launch"),
                      "algorithmic_bytes_per_launch": bytes_launch,
+                     "variant": (f"column {tby.value}x{tbz.value}, "
+                                 + ("staged" if tminb.value >= 16 else "direct")
+                                 + f" kernel, {tminb.value % 16} blocks/SM"),
                      "peak_source": f"{pk['which']} hbm_gbs",
                      "gflops": STENCIL_FLOPS * Vh * args.batch / (ms.value * 1e-3) / 1e9,
                      "single_rhs_kernel_gbs": STENCIL_BYTES[sprec] * Vh / (ms1.value * 1e-3) / 1e9,
@@ -766,9 +772,12 @@ def run_profile(args):
     lib.lym_time_stencil(lat.handle, op.op_id, sp, 0, 10, C.byref(ms))
     msb = C.c_double(0)
     lib.lym_time_stencil_batch(lat.handle, op.op_id, sp, 0, args.batch, 10, C.byref(msb))
+    tby, tbz, tminb = C.c_int(), C.c_int(), C.c_int()
+    lib.lym_get_batch_tile(lat.handle, sp, args.batch, 1, C.byref(tby), C.byref(tbz), C.byref(tminb))
     print(f"profile case: rc {rc}, block solve {t_solve:.3f} s, updates {st.reliable_updates}, "
           f"iterations {st.iterations}, true residual {st.true_residual:.2e}, "
-          f"stencil {ms.value * 1e3:.1f} us, batched stencil ({args.batch}) {msb.value * 1e3:.1f} us")
+          f"stencil {ms.value * 1e3:.1f} us, batched stencil ({args.batch}) {msb.value * 1e3:.1f} us, "
+          f"tile {tby.value},{tbz.value},{tminb.value}")
     lat.close()
     if rc != 0:
         sys.exit(1)
