@@ -591,6 +591,9 @@ LYM_D void hopping_pair(const int nf[4], const int nbk[4], const SB &in, const G
     hopping_mu<REAL, 3>(nf, nbk, in, U, p, h, q, acc);
 }
 
+// threads per block of the shared-memory staged stencil (dslash_batch_staged_kernel)
+constexpr int kStagedThreads = 128;
+
 // Work item -> half-site and its 8 neighbours by arithmetic, for the traversal in (y, z)
 // columns of by x bz (the order of order_table_kernel; h order is the column Ly x Lz):
 // w = th + lth (zi + bz (yi + by (x + Lx (zb + nzb yb)))), th = t / 2, lth = Lt / 2.
@@ -668,7 +671,7 @@ template <class SB, class GaugeT> struct DslashBatchArg {
 // gives the 6 same-parity input components of block blk (EPI_XPAY); cw the clover words.
 template <int EPI, class SB, class GaugeT, class YSrc, class CW>
 LYM_D void batch_epilogue(const DslashBatchArg<SB, GaugeT> &arg, int h, int q, bool act_a, bool act_b, c2 acc[12],
-                          const YSrc &ysrc, const CW &cw)
+                          const YSrc &ysrc, const CW &cw, const float4 *r_smem = nullptr)
 {
     const int ra = 2 * q, rb = 2 * q + 1;
     if (EPI == EPI_SCALE || EPI == EPI_CLOVINV) {
@@ -719,8 +722,9 @@ LYM_D void batch_epilogue(const DslashBatchArg<SB, GaugeT> &arg, int h, int q, b
     }
     arg.out.store(h, q, acc);
     if constexpr (EPI == EPI_XPAY_RES) {
-        c2 r[12];
-        arg.res_r.load(h, q, r);
+        c2 r[12];  // r from this thread's shared-memory slots (staged kernel) or from memory
+        if (r_smem) arg.res_r.unstage(r_smem, kStagedThreads, r);
+        else arg.res_r.load(h, q, r);
         const double2 aa = act_a ? arg.res_alpha[ra] : make_double2(0.0, 0.0);
         const double2 ab = act_b ? arg.res_alpha[rb] : make_double2(0.0, 0.0);
         const float2 are = make_float2((float)aa.x, (float)ab.x), aim = make_float2((float)aa.y, (float)ab.y);
@@ -791,7 +795,6 @@ __global__ void __launch_bounds__(128, MINB) dslash_batch_kernel(const DslashBat
 // per block of 128 threads: two buffers of 12 words per thread (the thread's own
 // spinor words) and two buffers of 9 link words per half-site; the np threads of a
 // half-site copy its link words between them and meet at __syncwarp before reading.
-constexpr int kStagedThreads = 128;
 LYM_HD int staged_smem_bytes(int lognp)
 {
     return (2 * 12 * kStagedThreads + 2 * (kStagedThreads >> lognp) * 9) * 16;
@@ -941,15 +944,22 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
         s.template step<6>(acc);
         s.template step<7>(acc);
         if (s.clov_smem) s.stage_clover(1);  // link buffer 1 is free after the last direction
+        // the own-site operand of a fused epilogue (r, rhat) into this thread's slots of
+        // spinor buffer 1, free after the last direction as well
+        if constexpr (EPI == EPI_XPAY_RES)
+            if (s.live) arg.res_r.stage(smem_u32(s.sx(1)), kStagedThreads * 16, s.h, q);
+        if constexpr (RED)
+            if (s.live) arg.om_rhat.stage(smem_u32(s.sx(1)), kStagedThreads * 16, s.h, q);
         cp_async_commit();
         cp_async_wait<0>();
         __syncwarp(vmask);
         if (!s.live) return false;
         auto ysrc = [&](int blk, c2 y6[6]) { arg.y.unstage_block(s.sx(0), kStagedThreads, blk, y6); };
         if (s.clov_smem) {
-            batch_epilogue<EPI>(arg, s.h, q, act_a, act_b, acc, ysrc, CloverWordsSmem{s.sl(0), s.sl(1)});
+            batch_epilogue<EPI>(arg, s.h, q, act_a, act_b, acc, ysrc, CloverWordsSmem{s.sl(0), s.sl(1)}, s.sx(1));
         } else {
-            batch_epilogue<EPI>(arg, s.h, q, act_a, act_b, acc, ysrc, clover_global<EPI>(arg, s.h, q, act_a, act_b));
+            batch_epilogue<EPI>(arg, s.h, q, act_a, act_b, acc, ysrc, clover_global<EPI>(arg, s.h, q, act_a, act_b),
+                                s.sx(1));
         }
         if constexpr (RED) {
             // the omega sums of the two lanes: <t, s>, |t|^2, <rhat, s>, <rhat, t> (t = out, s = y)
@@ -957,16 +967,15 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
             for (int k = 0; k < 14; ++k) red[k] = 0.0;
 #pragma unroll
             for (int blk = 0; blk < 2; ++blk) {
-                c2 y6[6];
+                c2 y6[6], r6[6];
                 ysrc(blk, y6);
+                arg.om_rhat.unstage_block(s.sx(1), kStagedThreads, blk, r6);
 #pragma unroll
                 for (int k = 0; k < 6; ++k) {
-                    const c2 t = acc[6 * blk + k], sv = y6[k];
-                    cx<double> ra, rb;
-                    arg.om_rhat.get(s.h, q, 6 * blk + k, ra, rb);
+                    const c2 t = acc[6 * blk + k], sv = y6[k], rh = r6[k];
                     const double tr[2] = {t.re.x, t.re.y}, ti[2] = {t.im.x, t.im.y};
                     const double sr[2] = {sv.re.x, sv.re.y}, si[2] = {sv.im.x, sv.im.y};
-                    const double rr[2] = {ra.re, rb.re}, ri[2] = {ra.im, rb.im};
+                    const double rr[2] = {rh.re.x, rh.re.y}, ri[2] = {rh.im.x, rh.im.y};
 #pragma unroll
                     for (int l = 0; l < 2; ++l) {
                         if (l == 0 ? !act_a : !act_b) continue;
