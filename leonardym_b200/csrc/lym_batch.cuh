@@ -766,12 +766,16 @@ __global__ void __launch_bounds__(128, MINB) dslash_batch_kernel(const DslashBat
         act_b = arg.active[2 * q + 1] != 0;
         if (!act_a && !act_b) return;
     }
-    const int h = arg.order ? __ldg(arg.order + wi) : wi;
-    int nf[4], nbk[4];
+    int h, nf[4], nbk[4];
+    if (arg.walk.on) {
+        h = walk_site(arg.walk, arg.parity, (unsigned)wi, nf, nbk);
+    } else {
+        h = arg.order ? __ldg(arg.order + wi) : wi;
 #pragma unroll
-    for (int mu = 0; mu < 4; ++mu) {
-        nf[mu] = arg.nbr.get(arg.parity, mu, 0, h);
-        nbk[mu] = arg.nbr.get(arg.parity, mu, 1, h);
+        for (int mu = 0; mu < 4; ++mu) {
+            nf[mu] = arg.nbr.get(arg.parity, mu, 0, h);
+            nbk[mu] = arg.nbr.get(arg.parity, mu, 1, h);
+        }
     }
     c2 acc[12];
     hopping_pair<GaugeT::kReal>(nf, nbk, arg.in, arg.U, arg.parity, h, q, acc);
