@@ -83,10 +83,22 @@ template <int N> LYM_D void cp_async_wait() { asm volatile("cp.async.wait_group 
 struct SlotF {
     float *f;
     int stride, lognp, r;
+    static constexpr bool kPerComponent = true;  // get / put one component at a time
     LYM_HD SlotF par(int) const { return *this; }
     LYM_D size_t base(int c, int h) const
     {
         return (((((size_t)c * stride + h) << lognp) + (r >> 1)) << 2) + (r & 1);
+    }
+    LYM_D cx<double> get(int c, int h) const
+    {
+        const size_t b = base(c, h);
+        return cx<double>{(double)f[b], (double)f[b + 2]};
+    }
+    LYM_D void put(int c, int h, cx<double> s) const
+    {
+        const size_t b = base(c, h);
+        f[b] = (float)s.re;
+        f[b + 2] = (float)s.im;
     }
     template <typename R> LYM_D void load(int h, cx<R> s[12]) const
     {
@@ -197,6 +209,7 @@ struct SlotH {
     __half *hv;
     float *norm;
     int stride, lognp, r;
+    static constexpr bool kPerComponent = false;  // a store needs the whole site (its norm)
     LYM_HD SlotH par(int) const { return *this; }
     LYM_D size_t base(int w, int h) const
     {

@@ -106,6 +106,13 @@ struct SpinorD {  // FP64: 12 x double2 words
     int stride;
     static constexpr int kWords = 12;
     LYM_HD SpinorD par(int p) const { return SpinorD{v + (size_t)p * 12 * stride, stride}; }
+    // component k of half-site h (vector steps that stream one component at a time)
+    LYM_D cx<double> get(int k, int h) const
+    {
+        const double2 w = __ldg(v + (size_t)k * stride + h);
+        return cx<double>{w.x, w.y};
+    }
+    LYM_D void put(int k, int h, cx<double> s) const { v[(size_t)k * stride + h] = make_double2(s.re, s.im); }
     template <typename R> LYM_D void load(int h, cx<R> s[12]) const
     {
 #pragma unroll

@@ -66,18 +66,16 @@ template <class SA, class SX> struct OpFoldClear {
     static constexpr int NRED = 0;
     SA a;
     SX x;
-    LYM_D void site(int p, int h, double *) const
+    LYM_D void site(int p, int h, double *) const  // one component at a time
     {
-        cx<double> av[12], xv[12];
-        a.par(p).template load<double>(h, av);
-        x.par(p).template load<double>(h, xv);
-#pragma unroll
+        const SA ap = a.par(p);
+        const SX xp = x.par(p);
+#pragma unroll 4
         for (int k = 0; k < 12; ++k) {
-            xv[k] = xv[k] + av[k];
-            av[k] = cx<double>{0.0, 0.0};
+            const cx<double> av = ap.get(k, h);
+            xp.put(k, h, xp.get(k, h) + av);
+            ap.put(k, h, cx<double>{0.0, 0.0});
         }
-        x.par(p).template store<double>(h, xv);
-        a.par(p).template store<double>(h, av);
     }
 };
 
@@ -93,6 +91,24 @@ template <class SR, class SP, class ST, class SH, class SW> struct OpBiContinue 
     double *out;
     LYM_D void site(int q, int h, double *acc) const
     {
+        if constexpr (SP::kPerComponent) {
+            // FP32 direction: one component at a time; the stored direction is pn rounded
+            // to FP32, formed in registers
+#pragma unroll 2
+            for (int k = 0; k < 12; ++k) {
+                const cx<double> rv = r.par(q).get(k, h), tv = rt.par(q).get(k, h);
+                const cx<double> pn = p.par(q).get(k, h) + tv - rv;
+                p.par(q).put(k, h, pn);
+                r.par(q).put(k, h, tv);
+                const cx<double> ps{(double)(float)pn.re, (double)(float)pn.im};
+                const cx<double> hv = rh.par(q).get(k, h), wv = w.par(q).get(k, h);
+                acc[0] += hv.re * tv.re + hv.im * tv.im;
+                acc[1] += hv.re * tv.im - hv.im * tv.re;
+                acc[2] += wv.re * ps.re + wv.im * ps.im;
+                acc[3] += wv.re * ps.im - wv.im * ps.re;
+            }
+            return;
+        }
         cx<double> rv[12], pv[12], tv[12];
         r.par(q).template load<double>(h, rv);
         p.par(q).template load<double>(h, pv);
