@@ -114,11 +114,13 @@ int lym_context_create(const int dims[4], int rep, int device, lym_context **ctx
 void lym_context_destroy(lym_context *ctx);
 const char *lym_last_error(lym_context *ctx);
 int lym_context_volume(lym_context *ctx);
-/* bytes of device memory held by the context (gauge fields, clover terms, work vectors) */
+/* bytes of device memory held by the context (gauge fields, clover terms, work vectors,
+ * and the idle cached buffers below) */
 size_t lym_context_device_bytes(lym_context *ctx);
-/* Frees the context's cache of idle work spinors and host-transfer staging buffers (they are
- * allocated again when needed).  A device allocation that fails trims the cache and retries
- * once by itself. */
+/* Frees the context's cache of idle work spinors, host-transfer staging buffers and the
+ * per-call buffers of the block solves (batch vectors, staging rings, scratch), which are kept
+ * for the next call of the same size; they are allocated again when needed.  A device
+ * allocation that fails trims the cache and retries once by itself. */
 int lym_context_trim(lym_context *ctx);
 int lym_synchronize(lym_context *ctx);
 
