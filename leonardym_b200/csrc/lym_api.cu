@@ -2855,6 +2855,14 @@ static int run_block(lym_context *c, OpEntry &op, int sp, int algo, double tol, 
         lym_context *c;
         ~CopyDrain() { cudaStreamSynchronize(c->st_copy); }
     } drain{c};
+    if (K > 0) {
+        // the staging buffers are zeroed on the context's stream when they are handed out:
+        // the copy stream starts its first uploads only after that (and after the engine's
+        // own set-up), so that no zeroing lands on a source that has already arrived
+        cudaEvent_t ready = events.make();
+        CK(cudaEventRecord(ready, c->st));
+        CK(cudaStreamWaitEvent(c->st_copy, ready, 0));
+    }
     for (int k = 0; k < K; ++k) issue_up(k);
     auto collect = [&](int f) {
         const double t_collect = now();
