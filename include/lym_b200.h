@@ -14,7 +14,10 @@
  *   links   extended_fermion_lattice_t : per site 4 links, Eigen column-major,
  *           complex double[3][3] (SU(3) fundamental) or double[3][3] (SU(2) adjoint)
  *   site    t + Lt*(z + Lz*(y + Ly*x))            (MPILattice/LocalLayout.h:149-163)
- * "_device" variants take device pointers with the same layout.
+ * "_device" variants take device pointers with the same layout.  The context's stream does
+ * not wait for other streams: device inputs must be fully written before the call (for
+ * example, synchronise the stream that produced them); every call has finished with its
+ * device outputs when it returns.
  */
 #ifndef LYM_B200_H
 #define LYM_B200_H
