@@ -383,6 +383,7 @@ def run_ours(args, world, rank, local):
     V = lat.V
     dev_src = torch.from_numpy(np.stack(srcs).view(np.float64).reshape(nrhs, V * 24)).to(f"cuda:{local}")
     dev_sol = torch.zeros_like(dev_src)
+    torch.cuda.synchronize()  # the library's stream does not wait for torch's
     stats = L.SolveStats()
     bstats = (L.SolveStats * nrhs)()
     src_ptrs = (C.c_void_p * nrhs)(*[dev_src[k].data_ptr() for k in range(nrhs)])
@@ -587,6 +588,7 @@ def run_rhmc(args, world, rank, local, dims=RHMC_DIMS):
     nsh = len(RHMC_SHIFTS)
     sh = np.ascontiguousarray(RHMC_SHIFTS, dtype=np.float64)
     sols = [torch.zeros_like(b) for _ in range(nsh)]
+    torch.cuda.synchronize()  # the library's stream does not wait for torch's
     ptrs = (C.c_void_p * nsh)(*[x.data_ptr() for x in sols])
     st = L.SolveStats()
 
@@ -681,6 +683,7 @@ def run_rhmc(args, world, rank, local, dims=RHMC_DIMS):
     fop = C.c_int(0)
     lib.lym_operator_create(ctx, 1, 1, RHMC_KAPPA, RHMC_CSW, 1, C.byref(fop))
     force = torch.zeros((lat.V, 4, 3, 3), dtype=torch.complex128, device=dev)
+    torch.cuda.synchronize()  # the library's stream does not wait for torch's
     for _ in range(2):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -805,6 +808,7 @@ def run_profile_consumers(args):
     xp = (C.c_void_p * 12)(*[v.data_ptr() for v in X])
     yp = (C.c_void_p * 12)(*[v.data_ptr() for v in Y])
     force = torch.zeros((lat.V, 4, 3, 3), dtype=torch.complex128, device="cuda:0")
+    torch.cuda.synchronize()  # the library's stream does not wait for torch's
     t0 = time.perf_counter()
     rc = lib.lym_fermion_force_multi_device(ctx, opid.value, 12, xp, yp, w.ctypes.data_as(C.c_void_p),
                                             C.c_void_p(force.data_ptr()))
@@ -840,6 +844,7 @@ def run_profile_rhmc(args):
     b = synth.gaussian_spinor_device(DIMS, 3, RHMC_SEED + 1, "cuda:0")
     bb = float(torch.vdot(b.flatten(), b.flatten()).real)
     sols = [torch.zeros_like(b) for _ in RHMC_SHIFTS]
+    torch.cuda.synchronize()  # the library's stream does not wait for torch's
     ptrs = (C.c_void_p * len(sols))(*[x.data_ptr() for x in sols])
     sh = np.ascontiguousarray(RHMC_SHIFTS, dtype=np.float64)
     st = L.SolveStats()

@@ -219,15 +219,19 @@ def su3_fermion_links_device(dims, eps, seed, device, chunk=1 << 22):
         del h, H, U
     Lt = int(dims[3])
     out.view(-1, Lt, 4, 3, 3)[:, Lt - 1, 3] *= -1
+    torch.cuda.synchronize(device)  # written before the library's stream reads it
     return out
 
 
 def gaussian_spinor_device(dims, nc, seed, device):
     """Complex-normal spinor (E|z|^2 = 1 per component) from torch's seeded device generator,
-    as a torch complex128 tensor [V, 4, nc]."""
+    as a torch complex128 tensor [V, 4, nc] (the device is synchronised before it returns: the
+    library's stream does not wait for torch's)."""
     import torch
 
     g = torch.Generator(device=device)
     g.manual_seed(int(seed))
     a = torch.randn((volume(dims), 4, nc, 2), generator=g, device=device, dtype=torch.float64) * np.sqrt(0.5)
-    return torch.view_as_complex(a).contiguous()
+    out = torch.view_as_complex(a).contiguous()
+    torch.cuda.synchronize(device)  # written before the library's stream reads it
+    return out

@@ -43,6 +43,7 @@ def test_force_field(setup, kind):
     import torch
     dX, dY = (torch.from_numpy(v).to("cuda:0") for v in (X, Y))
     df = torch.from_numpy(f0).to("cuda:0")
+    torch.cuda.synchronize()  # the library's stream does not wait for torch's
     for _ in range(2):
         assert L.lib().lym_fermion_force_device(lat.handle, op.op_id, C.c_void_p(dX.data_ptr()),
                                                 C.c_void_p(dY.data_ptr()), 0.35, C.c_void_p(df.data_ptr())) == 0

@@ -43,6 +43,7 @@ def test_noise_matches_oracle(setup, oracle):
     import torch
     lat = setup["lat"]
     out = torch.zeros((lat.V, 4, 3), dtype=torch.complex128, device="cuda:0")
+    torch.cuda.synchronize()  # the library's stream does not wait for torch's
     for seed, stream in ((7, 0), (7, 5), (123456789, 2)):
         assert L.lib().lym_noise_z2_device(lat.handle, seed, stream, C.c_void_p(out.data_ptr())) == 0
         assert np.array_equal(out.cpu().numpy(), oracle.z2_noise(setup["dims"], seed, stream))

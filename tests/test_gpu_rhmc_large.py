@@ -36,6 +36,7 @@ def test_rhmc_multishift_48c96_half():
         assert lib.lym_operator_create(h, 1, 5, KAPPA, CSW, 1, C.byref(op)) == 0, lib.lym_last_error(h)
         b = synth.gaussian_spinor_device(DIMS, 3, SEED + 1, "cuda:0")
         sols = [torch.zeros_like(b) for _ in SHIFTS]
+        torch.cuda.synchronize()  # the library's stream does not wait for torch's
         sh = np.ascontiguousarray(SHIFTS, dtype=np.float64)
         bb = float(torch.vdot(b.flatten(), b.flatten()).real)
         ptrs = (C.c_void_p * len(SHIFTS))(*[s.data_ptr() for s in sols])

@@ -35,6 +35,7 @@ def test_noalloc_matches_multiply_device(rep, kappa, csw, gamma5):
             dx = torch.from_numpy(x.view(np.float64).reshape(-1)).cuda()
             ref = torch.zeros_like(dx)
             out = torch.full_like(dx, float("nan"))
+            torch.cuda.synchronize()  # the library's stream does not wait for torch's
             rc = lib.lym_multiply_device(lat.handle, op.op_id, C.c_void_p(ref.data_ptr()), C.c_void_p(dx.data_ptr()))
             assert rc == 0, lib.lym_last_error(lat.handle)
             rc = lib.lym_multiply_device_noalloc(lat.handle, op.op_id, C.c_void_p(out.data_ptr()),
