@@ -75,6 +75,30 @@ def test_even_odd_schur_relations(cfg, oracle):
     assert np.array_equal(Sx[~odd], x[~odd])
 
 
+def test_schur_shadow_identity(cfg, oracle):
+    # S^+ = g5 S g5 on the odd sites (S is gamma5-hermitian, as D is): <rhat, S p> equals
+    # <g5 S g5 rhat, p>, which is how the block BiCGStab knows alpha = rho / <rhat, S p> from
+    # the update pass that forms p, before S p is formed
+    dims = cfg["dims"]
+    E = oracle.Operator(cfg["geom"], cfg["links"], "EvenOddImproved", cfg["kappa"], cfg["csw"], False)
+    odd = synth.lex_coords(dims).sum(axis=1) % 2 == 1
+    rhat = synth.gaussian_spinor(dims, 3, 7)
+    p = synth.gaussian_spinor(dims, 3, 8)
+    rhat[~odd] = 0
+    p[~odd] = 0
+
+    def g5(v):
+        w = v.copy()
+        w[:, 2:] *= -1
+        return w
+
+    Sp = E.multiply(p)
+    what = g5(E.multiply(g5(rhat)))
+    lhs = np.vdot(rhat[odd], Sp[odd])
+    rhs = np.vdot(what[odd], p[odd])
+    assert abs(lhs - rhs) < 1e-12 * np.linalg.norm(rhat) * np.linalg.norm(Sp)
+
+
 def test_solvers_converge(cfg, oracle):
     b = synth.gaussian_spinor(cfg["dims"], 3, 6)
     eps = 1e-20 * float(np.vdot(b, b).real)
