@@ -25,3 +25,12 @@ def test_context_create_rejects_bad_geometry():
     bad_rep = (ctypes.c_int * 4)(4, 4, 4, 4)
     assert lib.lym_context_create(bad_rep, 7, 0, ctypes.byref(ptr)) == -1
     assert lib.lym_context_create(None, 0, 0, ctypes.byref(ptr)) == -1
+
+
+def test_every_declared_symbol_has_a_typed_binding():
+    # ctypes signatures for the whole C ABI: the context entry points in _lib.py, the
+    # server's in server.py (without them ctypes would pass 64-bit values as int)
+    here = os.path.dirname(L.__file__)
+    src = "".join(open(os.path.join(here, f)).read() for f in ("_lib.py", "server.py"))
+    untyped = [n for n in L.declared_symbols() if f'"{n}"' not in src and f"L.{n}.argtypes" not in src]
+    assert not untyped, untyped
