@@ -1445,6 +1445,8 @@ void apply_schur_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, c
                        const SpinorBatch *res_s = nullptr, const double2 *res_alpha = nullptr,
                        const SpinorBatch *om_rhat = nullptr, double *om_scratch = nullptr, void *om_state = nullptr)
 {
+    if (!U.recon_ok)  // the batched stencil reads the 12-real FP32 links
+        fail(c, LYM_ERR_UNSUPPORTED, "batched solves need +-SU(3) / +-SO(3) links (their FP32 links are reconstructed)");
     DslashBatchParams P;
     P.g = c->g;
     P.prec = prec;
@@ -2390,7 +2392,6 @@ void lym_context_destroy(lym_context *c)
         cudaFree(kv.second.dev.f32);
         cudaFree(kv.second.dev.h16);
         cudaFree(kv.second.dev.sign);
-        cudaFree(kv.second.dev.f32dup);
     }
     for (auto &s : c->pool) cudaFree(s.v);
     for (auto &b : c->blocks) cudaFree(b.second);
@@ -2450,7 +2451,6 @@ static int gauge_store(lym_context *c, int id, const double *links, bool device_
         e.dev.f32 = dev_alloc(c, f32);
         e.dev.h16 = dev_alloc(c, h16);
         e.dev.sign = (uint8_t *)dev_alloc(c, 2 * s);
-        e.dev.f32dup = dev_alloc(c, c->rep == REP_SU3 ? 2 * 4 * 9 * s * sizeof(float4) : 2 * 4 * 9 * s * sizeof(float2));
         ge = &(c->gauges[id] = e);
     } else {
         ge = &it->second;
@@ -2523,7 +2523,6 @@ int lym_gauge_evict(lym_context *c, int id)
         dev_free(c, it->second.dev.f32, su3 ? 2 * 4 * 3 * s * sizeof(float4) : 2 * 4 * 3 * s * sizeof(float2));
         dev_free(c, it->second.dev.h16, su3 ? 2 * 4 * 3 * s * sizeof(uint2) : 2 * 4 * 3 * s * sizeof(__half2));
         dev_free(c, it->second.dev.sign, 2 * s);
-        dev_free(c, it->second.dev.f32dup, su3 ? 2 * 4 * 9 * s * sizeof(float4) : 2 * 4 * 9 * s * sizeof(float2));
         c->gauges.erase(it);
         return LYM_OK;
     });
@@ -3744,28 +3743,27 @@ void lym_host_free(void *p)
 }  // extern "C"
 
 // ------------------------------------------------- allocation-free variant --
-namespace lym {
-int noalloc_schur(const Geom &g, int rep, int device, cudaStream_t st, const GaugeDev &U, const CloverDev *C,
-                  double kappa, int gamma5, double *out, const double *in);
-}
-
 extern "C" int lym_multiply_device_noalloc(lym_context *c, int op_id, double *out, const double *in)
 {
-    if (!out || !in || out == in) return LYM_ERR_ARGUMENT;
     return guarded(c, [&]() {
+        if (!out || !in || out == in)
+            fail(c, LYM_ERR_ARGUMENT, "lym_multiply_device_noalloc: out and in must be distinct device vectors");
         OpEntry &op = op_of(c, op_id);
         if (op.kind != LYM_OP_EVEN_ODD_IMPROVED)
             fail(c, LYM_ERR_UNSUPPORTED, "lym_multiply_device_noalloc applies EvenOddImproved operators only");
-        if (c->g.Vh > 65536)
-            fail(c, LYM_ERR_ARGUMENT, "lym_multiply_device_noalloc: volume %d exceeds its maximum of 131072 sites",
-                 c->g.V);
+        if (c->g.Vh > kNoallocMaxHalfSites)
+            fail(c, LYM_ERR_ARGUMENT, "lym_multiply_device_noalloc: volume %d exceeds its maximum of %d sites",
+                 c->g.V, 2 * kNoallocMaxHalfSites);
         if (!op.clover_ok)
             fail(c, LYM_ERR_ARGUMENT,
                  "lym_multiply_device_noalloc: the operator's clover term is not built yet (building it allocates); "
                  "apply the operator once through lym_multiply or lym_multiply_device first");
         GaugeEntry &ge = gauge_of(c, op.gauge_id);
-        const int rc = noalloc_schur(c->g, c->rep, c->device, c->st, ge.dev, &op.clover, op.kappa, op.gamma5, out, in);
-        if (rc != LYM_OK) fail(c, rc, "lym_multiply_device_noalloc: CUDA error %s", cudaGetErrorString(cudaGetLastError()));
+        cudaError_t ce = cudaSuccess;
+        const int rc =
+            noalloc_schur(c->g, c->rep, c->device, c->st, ge.dev, &op.clover, op.kappa, op.gamma5, out, in, &ce);
+        if (rc != LYM_OK)
+            fail(c, rc, "lym_multiply_device_noalloc: CUDA error %s", cudaGetErrorString(ce));
         CK(cudaStreamSynchronize(c->st));
         count(c, 2);
         return LYM_OK;

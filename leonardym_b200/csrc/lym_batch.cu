@@ -163,12 +163,14 @@ void launch_dslash_batch(const DslashBatchParams &P, cudaStream_t st)
 {
     const GaugeDev &U = *P.U;
     const int s = P.g.stride;
+    const GaugeC12P c12{(const float4 *)U.f32, U.sign, s};
+    const GaugeR6P r6{(const float2 *)U.f32, U.sign, s};
     if (P.prec == PREC_F) {
-        if (P.rep == REP_SU3) run(P, fview(P.in), fview(P.out), fview(P.y), GaugeDupC{(const float4 *)U.f32dup, s}, st);
-        else run(P, fview(P.in), fview(P.out), fview(P.y), GaugeDupR{(const float2 *)U.f32dup, s}, st);
+        if (P.rep == REP_SU3) run(P, fview(P.in), fview(P.out), fview(P.y), c12, st);
+        else run(P, fview(P.in), fview(P.out), fview(P.y), r6, st);
     } else {
-        if (P.rep == REP_SU3) run(P, hview(P.in), hview(P.out), hview(P.y), GaugeDupC{(const float4 *)U.f32dup, s}, st);
-        else run(P, hview(P.in), hview(P.out), hview(P.y), GaugeDupR{(const float2 *)U.f32dup, s}, st);
+        if (P.rep == REP_SU3) run(P, hview(P.in), hview(P.out), hview(P.y), c12, st);
+        else run(P, hview(P.in), hview(P.out), hview(P.y), r6, st);
     }
 }
 

@@ -16,9 +16,7 @@
 //         norm n[h * np + q] = (max |.| of RHS 2q, of RHS 2q+1).
 // Link, clover and neighbour-index words of a half-site are read by all np threads
 // of that half-site (broadcast), so their bytes are shared by the whole batch; the
-// batched stencil therefore reads links stored without reconstruction and with each
-// component duplicated into both lanes, (re, re, im, im), ready for the packed
-// multiply.
+// links are read in the 12-real format and expanded in registers.
 #pragma once
 
 #include "lym_blas.cuh"
@@ -353,57 +351,100 @@ struct LinkP {  // a link with every component duplicated into both lanes
 // Links and clover words are read by exactly one warp instruction per launch (all np
 // lanes of the half-site at once), so they are loaded with the evict-first hint and
 // leave L2 to the neighbour spinors, which are read eight times.
-struct GaugeDupC {  // SU(3): float4 (re, re, im, im) per component, [parity][mu][9][stride]
+//
+// The links are the 12-real FP32 words of the single-RHS stencils (GaugeF12 / GaugeF6:
+// rows 0 and 1, row 2 = s conj(row0 x row1), s = -1 where bit mu of the site's sign byte
+// is set) and are expanded in registers into lane-duplicated components for the packed
+// arithmetic.  Staged through shared memory, a link takes kStageWords slots: its 3 words
+// and the aligned 32-bit word of the sign table that holds its sign byte.
+LYM_D void cp_async4(unsigned saddr, const void *g)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(saddr), "l"(g) : "memory");
+}
+
+struct GaugeC12P {  // SU(3)
     static constexpr bool kReal = false;
-    const float4 *u;
+    static constexpr int kStageWords = 4;
+    const float4 *u;       // [parity][mu][3][stride]
+    const uint8_t *sign;   // [parity][stride]
     int stride;
+    LYM_D static void expand(const float4 w0, const float4 w1, const float4 w2, unsigned neg, LinkP &L)
+    {
+        const float r[2][3] = {{w0.x, w0.z, w1.x}, {w1.z, w2.x, w2.z}};
+        const float i[2][3] = {{w0.y, w0.w, w1.y}, {w1.w, w2.y, w2.w}};
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                L.ur[a][b] = make_float2(r[a][b], r[a][b]);
+                L.ui[a][b] = make_float2(i[a][b], i[a][b]);
+            }
+        const float s = neg ? -1.f : 1.f;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {  // row 2 = s conj(r0_a r1_c - r0_c r1_a)
+            const int a = (j + 1) % 3, c = (j + 2) % 3;
+            const float vr = (r[0][a] * r[1][c] - i[0][a] * i[1][c]) - (r[0][c] * r[1][a] - i[0][c] * i[1][a]);
+            const float vi = (r[0][a] * i[1][c] + i[0][a] * r[1][c]) - (r[0][c] * i[1][a] + i[0][c] * r[1][a]);
+            L.ur[2][j] = make_float2(s * vr, s * vr);
+            L.ui[2][j] = make_float2(-s * vi, -s * vi);
+        }
+    }
     LYM_D void load(int p, int mu, int h, LinkP &L) const
     {
-        const float4 *b = u + ((unsigned)(p * 4 + mu) * 9 * stride + h);
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            const float4 w = __ldcs(b + k * stride);
-            L.ur[k / 3][k % 3] = make_float2(w.x, w.y);
-            L.ui[k / 3][k % 3] = make_float2(w.z, w.w);
-        }
+        const float4 *b = u + ((unsigned)(p * 4 + mu) * 3 * stride + h);
+        const float4 w0 = __ldcs(b), w1 = __ldcs(b + stride), w2 = __ldcs(b + 2 * stride);
+        expand(w0, w1, w2, (__ldg(sign + (unsigned)p * stride + h) >> mu) & 1u, L);
     }
-    // word k of link (p, mu, h) copied to shared memory / a link read from 9 staged words
+    // slot k of link (p, mu, h): words 0..2, then the sign word
     LYM_D void stage(int p, int mu, int k, int h, unsigned saddr) const
     {
-        cp_async16(saddr, u + ((unsigned)((p * 4 + mu) * 9 + k) * stride + h));
+        if (k < 3) cp_async16(saddr, u + ((unsigned)((p * 4 + mu) * 3 + k) * stride + h));
+        else cp_async4(saddr, sign + (((unsigned)p * stride + h) & ~3u));
     }
-    LYM_D void unstage(const float4 *w9, LinkP &L) const
+    LYM_D void unstage(const float4 *w4, int mu, int h, LinkP &L) const
     {
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            const float4 w = w9[k];
-            L.ur[k / 3][k % 3] = make_float2(w.x, w.y);
-            L.ui[k / 3][k % 3] = make_float2(w.z, w.w);
-        }
+        const unsigned word = *reinterpret_cast<const unsigned *>(w4 + 3);
+        expand(w4[0], w4[1], w4[2], (word >> (8 * (h & 3) + mu)) & 1u, L);
     }
 };
 
-struct GaugeDupR {  // real adjoint links: float2 (u, u) per component, [parity][mu][9][stride]
+struct GaugeR6P {  // real adjoint links: 3 float2 words (rows 0 and 1), row 2 = s (row0 x row1)
     static constexpr bool kReal = true;
-    const float2 *u;
+    static constexpr int kStageWords = 4;
+    const float2 *u;       // [parity][mu][3][stride]
+    const uint8_t *sign;   // [parity][stride]
     int stride;
+    LYM_D static void expand(const float2 w0, const float2 w1, const float2 w2, unsigned neg, LinkP &L)
+    {
+        const float r[2][3] = {{w0.x, w0.y, w1.x}, {w1.y, w2.x, w2.y}};
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) L.ur[a][b] = make_float2(r[a][b], r[a][b]);
+        const float s = neg ? -1.f : 1.f;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const int a = (j + 1) % 3, c = (j + 2) % 3;
+            const float v = s * (r[0][a] * r[1][c] - r[0][c] * r[1][a]);
+            L.ur[2][j] = make_float2(v, v);
+        }
+    }
     LYM_D void load(int p, int mu, int h, LinkP &L) const
     {
-        const float2 *b = u + ((unsigned)(p * 4 + mu) * 9 * stride + h);
-#pragma unroll
-        for (int k = 0; k < 9; ++k) L.ur[k / 3][k % 3] = __ldcs(b + k * stride);
+        const float2 *b = u + ((unsigned)(p * 4 + mu) * 3 * stride + h);
+        const float2 w0 = __ldcs(b), w1 = __ldcs(b + stride), w2 = __ldcs(b + 2 * stride);
+        expand(w0, w1, w2, (__ldg(sign + (unsigned)p * stride + h) >> mu) & 1u, L);
     }
     LYM_D void stage(int p, int mu, int k, int h, unsigned saddr) const
     {
-        cp_async8(saddr, u + ((unsigned)((p * 4 + mu) * 9 + k) * stride + h));
+        if (k < 3) cp_async8(saddr, u + ((unsigned)((p * 4 + mu) * 3 + k) * stride + h));
+        else cp_async4(saddr, sign + (((unsigned)p * stride + h) & ~3u));
     }
-    LYM_D void unstage(const float4 *w9, LinkP &L) const
+    LYM_D void unstage(const float4 *w4, int mu, int h, LinkP &L) const
     {
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            const float4 w = w9[k];
-            L.ur[k / 3][k % 3] = make_float2(w.x, w.y);
-        }
+        const unsigned word = *reinterpret_cast<const unsigned *>(w4 + 3);
+        expand(make_float2(w4[0].x, w4[0].y), make_float2(w4[1].x, w4[1].y), make_float2(w4[2].x, w4[2].y),
+               (word >> (8 * (h & 3) + mu)) & 1u, L);
     }
 };
 
@@ -810,8 +851,9 @@ __global__ void __launch_bounds__(128, MINB) dslash_batch_kernel(const DslashBat
 // shared memory (cp.async) while direction d is computed, so the loads of the next
 // term overlap the arithmetic of this one without holding registers.  Shared memory
 // per block of 128 threads: two buffers of 12 words per thread (the thread's own
-// spinor words) and two buffers of 9 link words per half-site; the np threads of a
-// half-site copy its link words between them and meet at __syncwarp before reading.
+// spinor words) and two buffers of 9 words per half-site (a link's kStageWords words, or
+// the clover words of a batch on one operator); the np threads of a half-site copy its
+// link words between them and meet at __syncwarp before reading.
 LYM_HD int staged_smem_bytes(int lognp)
 {
     return (2 * 12 * kStagedThreads + 2 * (kStagedThreads >> lognp) * 9) * 16;
@@ -847,7 +889,7 @@ template <bool STAGE_Y, class SB, class GaugeT> struct StagedHop {
         if (live) arg.in.stage(smem_u32(sx(D & 1)), kStagedThreads * 16, n, q);
         const int lp = DIR == 0 ? arg.parity : 1 - arg.parity, lh = DIR == 0 ? h : n;
         float4 *L = sl(D & 1);
-        for (int k = lane_in; k < 9; k += np) arg.U.stage(lp, MU, k, lh, smem_u32(L + k));
+        for (int k = lane_in; k < GaugeT::kStageWords; k += np) arg.U.stage(lp, MU, k, lh, smem_u32(L + k));
     }
     template <int D> LYM_D void step(c2 acc[12]) const
     {
@@ -864,7 +906,7 @@ template <bool STAGE_Y, class SB, class GaugeT> struct StagedHop {
             c2 x[12];
             arg.in.unstage(sx(D & 1), kStagedThreads, x);
             LinkP L;
-            arg.U.unstage(sl(D & 1), L);
+            arg.U.unstage(sl(D & 1), D / 2, D % 2 == 0 ? h : nbk[D / 2], L);
             accumulate_dir<GaugeT::kReal, D / 2, D % 2>(x, L, acc);
         }
         __syncwarp(vmask);  // every lane is done with buffer D & 1 before it is refilled

@@ -35,11 +35,6 @@ struct GaugeDev {
     void *h16 = nullptr;       // FP16 reconstructed: uint2[2][4][3][stride] or half2[2][4][3][stride]
     uint8_t *sign = nullptr;   // [2][stride]
     bool recon_ok = false;
-    // FP32 without reconstruction and with every component duplicated into both lanes of
-    // a float2 pair, for the batched stencil (link bytes are shared by the batch, the
-    // reconstruction arithmetic would not be): float4 (re, re, im, im)[2][4][9][stride]
-    // (SU3) or float2 (u, u)[2][4][9][stride] (adjoint)
-    void *f32dup = nullptr;
 };
 
 struct CloverDev {
@@ -123,6 +118,13 @@ struct DslashBatchParams {
 inline long batch_stencil_blocks(const Geom &g, int lognb) { return (((long)g.Vh << (lognb - 1)) + 127) / 128; }
 
 void launch_dslash_batch(const DslashBatchParams &P, cudaStream_t st);
+// lym_multiply_device_noalloc (lym_noalloc.cu): half-sites of its fixed scratch array, the
+// lattice size limit of that entry point (V <= 2 * kNoallocMaxHalfSites, e.g. 16^3 x 32)
+constexpr int kNoallocMaxHalfSites = 65536;
+// the even-odd operator on AoS device vectors through that array; returns a LYM_* status
+// and, on LYM_ERR_CUDA, the CUDA error it saw in *cuda_err
+int noalloc_schur(const Geom &g, int rep, int device, cudaStream_t st, const GaugeDev &U, const CloverDev *C,
+                  double kappa, int gamma5, double *out, const double *in, cudaError_t *cuda_err);
 // the BiCGStab omega sums fused into the second stencil launch of a block Schur product
 // (EPI_XPAY_OMEGA_): the variants that support it, the scratch it needs (per-block partial
 // sums, then chunk sums) and the launches that add them up and apply the omega update

@@ -161,8 +161,7 @@ LYM_D void load_link_d(const Geom &g, int rep, const void *d64, int p, int mu, i
 // Compress the FP64 links to the reconstructed FP32 / FP16 formats.  A link is
 // accepted when it is +-V with V special unitary (SU(3)) or special orthogonal
 // (adjoint); the sign goes to the sign table.
-__global__ void compress_gauge_kernel(Geom g, int rep, const void *d64, void *f32, void *h16, uint8_t *sign, int *err,
-                                      void *f32dup)
+__global__ void compress_gauge_kernel(Geom g, int rep, const void *d64, void *f32, void *h16, uint8_t *sign, int *err)
 {
     const int h = blockIdx.x * blockDim.x + threadIdx.x;
     const int p = blockIdx.y;
@@ -188,12 +187,6 @@ __global__ void compress_gauge_kernel(Geom g, int rep, const void *d64, void *f3
         else atomicOr(err, 1);
         if (dev > 1e-8) atomicOr(err, 2);
         bits |= (uint8_t)(neg << mu);
-        for (int kk = 0; kk < 9; ++kk) {
-            const size_t wf = ((size_t)(p * 4 + mu) * 9 + kk) * g.stride + h;
-            const float ure = (float)u[kk / 3][kk % 3].re, uim = (float)u[kk / 3][kk % 3].im;
-            if (rep == REP_SU3) ((float4 *)f32dup)[wf] = make_float4(ure, ure, uim, uim);
-            else ((float2 *)f32dup)[wf] = make_float2(ure, ure);
-        }
         const size_t w0 = (size_t)(p * 4 + mu) * 3 * g.stride + h;
         if (rep == REP_SU3) {
             float4 *F = (float4 *)f32;
@@ -227,7 +220,7 @@ __global__ void compress_gauge_kernel(Geom g, int rep, const void *d64, void *f3
 void launch_compress_gauge(const Geom &g, GaugeDev &U, int *err, cudaStream_t st)
 {
     dim3 grid(nblocks(g.Vh, 128), 2);
-    compress_gauge_kernel<<<grid, 128, 0, st>>>(g, U.rep, U.d64, U.f32, U.h16, U.sign, err, U.f32dup);
+    compress_gauge_kernel<<<grid, 128, 0, st>>>(g, U.rep, U.d64, U.f32, U.h16, U.sign, err);
 }
 
 // Fundamental gauge links -> fermion links: the adjoint map for SU(2)

@@ -8,8 +8,8 @@
 // (EvenOddImprovedDiracWilsonOperator.cpp:26-47) to caller-owned device vectors in the
 // reference's layout; its one intermediate vector, the even-site half spinor
 // T_ee^-1 H_eo x_o, lives in the file-scope array below instead of memory the library
-// allocates.  The array is kNoallocMaxHalfSites half-sites of FP64 (12 MiB), held by
-// every GPU that loads the library until the process exits.
+// allocates.  The array is kNoallocMaxHalfSites (lym_internal.h) half-sites of FP64
+// (12 MiB), held by every GPU that loads the library until the process exits.
 #include <mutex>
 
 #include "../../include/lym_b200.h"
@@ -17,8 +17,6 @@
 #include "lym_internal.h"
 
 namespace lym {
-
-constexpr int kNoallocMaxHalfSites = 65536;  // V <= 131072 sites, e.g. 16^3 x 32
 
 static __device__ __align__(256) double2 g_noalloc_half_spinor[12 * kNoallocMaxHalfSites];
 
@@ -54,12 +52,17 @@ struct SpinorAoS {
     }
 };
 
+// tmp = T_ee^-1 H_eo x_o, and the even sites of the output are those of the input
+// (EvenOddImprovedDiracWilsonOperator.cpp:38-41), copied by the same threads
 template <class GaugeT>
-__global__ void noalloc_schur_even(Geom g, SpinorAoS in_odd, SpinorD tmp, GaugeT U, CloverD Tinv, int clover)
+__global__ void noalloc_schur_even(Geom g, SpinorAoS in_odd, SpinorAoS in_even, SpinorAoS out_even, SpinorD tmp,
+                                   GaugeT U, CloverD Tinv, int clover)
 {
     const int h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= g.Vh) return;
     cx<double> acc[12], res[12];
+    in_even.load<double>(h, res);
+    out_even.store<double>(h, res);
     hopping<double>(g, in_odd, U, 0, h, acc);
     if (clover) clover_apply<double>(Tinv, 0, h, acc, res);
     else
@@ -110,17 +113,14 @@ static double2 *scratch_address(int device, cudaError_t *err)
 }
 
 int noalloc_schur(const Geom &g, int rep, int device, cudaStream_t st, const GaugeDev &U, const CloverDev *C,
-                  double kappa, int gamma5, double *out, const double *in)
+                  double kappa, int gamma5, double *out, const double *in, cudaError_t *cuda_err)
 {
+    *cuda_err = cudaSuccess;
     if (g.Vh > kNoallocMaxHalfSites) return LYM_ERR_ARGUMENT;
-    cudaError_t e;
-    double2 *scratch = scratch_address(device, &e);
+    double2 *scratch = scratch_address(device, cuda_err);
     if (!scratch) return LYM_ERR_CUDA;
-    // even sites of the output are the input's (EvenOddImprovedDiracWilsonOperator.cpp:38-41);
-    // the odd sites are overwritten below
-    if (cudaMemcpyAsync(out, in, (size_t)g.V * 24 * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-        return LYM_ERR_CUDA;
     SpinorAoS in_odd{(double2 *)in, g, 1}, out_odd{(double2 *)out, g, 1};
+    SpinorAoS in_even{(double2 *)in, g, 0}, out_even{(double2 *)out, g, 0};
     SpinorD tmp{scratch, kNoallocMaxHalfSites};
     const int clover = C != nullptr;
     CloverD T{clover ? (const double2 *)C->T[PREC_D] : nullptr, g.stride};
@@ -128,15 +128,15 @@ int noalloc_schur(const Geom &g, int rep, int device, cudaStream_t st, const Gau
     const int nb = (g.Vh + 127) / 128;
     if (rep == REP_SU3) {
         GaugeD18 G{(const double2 *)U.d64, g.stride};
-        noalloc_schur_even<<<nb, 128, 0, st>>>(g, in_odd, tmp, G, Ti, clover);
+        noalloc_schur_even<<<nb, 128, 0, st>>>(g, in_odd, in_even, out_even, tmp, G, Ti, clover);
         noalloc_schur_odd<<<nb, 128, 0, st>>>(g, tmp, in_odd, out_odd, G, T, clover, kappa * kappa, gamma5);
     } else {
         GaugeD9 G{(const double *)U.d64, g.stride};
-        noalloc_schur_even<<<nb, 128, 0, st>>>(g, in_odd, tmp, G, Ti, clover);
+        noalloc_schur_even<<<nb, 128, 0, st>>>(g, in_odd, in_even, out_even, tmp, G, Ti, clover);
         noalloc_schur_odd<<<nb, 128, 0, st>>>(g, tmp, in_odd, out_odd, G, T, clover, kappa * kappa, gamma5);
     }
-    if (cudaGetLastError() != cudaSuccess) return LYM_ERR_CUDA;
-    return LYM_OK;
+    *cuda_err = cudaGetLastError();
+    return *cuda_err == cudaSuccess ? LYM_OK : LYM_ERR_CUDA;
 }
 
 }  // namespace lym

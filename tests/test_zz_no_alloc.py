@@ -66,6 +66,10 @@ def test_noalloc_rejects_what_it_cannot_do():
         w.setLattice(op._gauge)
         assert lib.lym_multiply_device_noalloc(lat.handle, w.op_id, C.c_void_p(e.data_ptr()),
                                                C.c_void_p(d.data_ptr())) == -4
+        # the output may not alias the input; the reason is kept for lym_last_error
+        assert lib.lym_multiply_device_noalloc(lat.handle, op.op_id, C.c_void_p(d.data_ptr()),
+                                               C.c_void_p(d.data_ptr())) == -1
+        assert b"distinct" in lib.lym_last_error(lat.handle)
     finally:
         lat.close()
     big = L.Lattice((16, 16, 16, 64), "su3")  # 262144 sites: beyond the fixed scratch
@@ -77,5 +81,6 @@ def test_noalloc_rejects_what_it_cannot_do():
         assert lib.lym_multiply_device(big.handle, op.op_id, C.c_void_p(e.data_ptr()), C.c_void_p(d.data_ptr())) == 0
         assert lib.lym_multiply_device_noalloc(big.handle, op.op_id, C.c_void_p(e.data_ptr()),
                                                C.c_void_p(d.data_ptr())) == -1
+        assert b"131072" in lib.lym_last_error(big.handle)
     finally:
         big.close()
