@@ -5,11 +5,11 @@ Wilson-clover operator on a 24^3 x 48 lattice, kappa = 0.137, c_sw = 1.7, seeded
 near-unit links U = exp(i 0.25 H), antiperiodic in time; 44 right-hand sides
 (12 spin-colour point sources at the origin + 32 Z2 x Z2 noise sources).  One
 step solves all 44 systems D x = b to a true residual ||b - D x|| / ||b|| <= 1e-10
-with the even-odd mixed-precision CG (FP32 stencil, FP64 reliable updates,
-re-measured with the FP64 operator).
+with the block even-odd mixed-precision BiCGStab (FP32 batched stencil, FP64 reliable
+updates, every solution re-measured with the FP64 operator).
 
-Prints one JSON line (rank 0).  --impl reference times the reference algorithm on
-the host cores instead (see cpu_reference()).
+Prints one JSON line (rank 0).  --impl reference times the reference's own solver,
+compiled from its sources, on the host cores instead (see ReferenceCPU).
 """
 from __future__ import annotations
 
@@ -58,18 +58,31 @@ def peaks():
 
 
 _LINKS = None
+_SYNTH = None
+
+
+def synth_module():
+    """leonardym_b200/synth.py (seeded host generators, numpy only) loaded on its own, so
+    that the reference arm draws the same inputs without importing the package."""
+    global _SYNTH
+    if _SYNTH is None:
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("lym_synth_standalone",
+                                                      os.path.join(ROOT, "leonardym_b200", "synth.py"))
+        _SYNTH = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(_SYNTH)
+    return _SYNTH
 
 
 def workload_links():
     global _LINKS
     if _LINKS is None:
-        from leonardym_b200 import synth
-        _LINKS = synth.fermion_links(DIMS, "su3", EPS, SEED)
+        _LINKS = synth_module().fermion_links(DIMS, "su3", EPS, SEED)
     return _LINKS
 
 
 def workload_sources(nc=3):
-    from leonardym_b200 import synth
+    synth = synth_module()
     srcs = []
     for alpha in range(4):
         for c in range(nc):
@@ -216,37 +229,58 @@ class quiet_stdout:
         os.close(self.null)
 
 
-def cpu_reference(sample_iters=(4, 8)):
-    """The reference's FP64 even-odd BiCGStab (PreconditionedBiCGStab.cpp:33-100) on the
-    host cores (OpenMP, all threads), on the benchmark's lattice and first noise source.
-    A bounded sample: the solver runs with max_steps = 4 and 8; the difference gives the
-    time per iteration, the first run the set-up (field strength + 12x12 inverses).
-    Solves/s = 1 / (setup + iterations x time per iteration) with the iteration count the
-    reference algorithm needs on this system.  Runs the reference's own code compiled
-    from its sources (oracle/_ref) when present, else the oracle's restatement."""
-    import oracle as O
-    from oracle import ref as R
-    links = workload_links()
-    b = workload_sources()[N_POINT]
-    prec = (TOL ** 2) * float(np.vdot(b, b).real)
-    if R.available("su3"):
-        kind = "reference"
-        ref = R.Reference(DIMS, links, "su3")
-        run = lambda n: ref.solve("Improved", "preconditioned_bicgstab", b, prec, n, KAPPA, CSW, False)
-    else:
-        kind = "port"
-        D = O.Operator(O.Geometry(DIMS), links, "Improved", KAPPA, CSW, False)
-        run = lambda n: O.preconditioned_bicgstab(D, b, prec, n)
-    ts = []
-    with quiet_stdout():
-        for n in sample_iters:
+def host_threads():
+    n = os.environ.get("OMP_NUM_THREADS")
+    return int(n) if n else len(os.sched_getaffinity(0))
+
+
+class ReferenceCPU:
+    """The reference's own FP64 even-odd BiCGStab, PreconditionedBiCGStab::solve
+    (inverters/PreconditionedBiCGStab.cpp:33-100), compiled from its sources into
+    oracle/_ref, on the host cores (OpenMP, every thread this process may use), on the
+    benchmark's lattice and its first Z2 x Z2 noise source.  The Improved operator is held
+    across solves (field strength built once, as a caller solving many sources on one
+    gauge field holds it); every solve then pays the reference's own per-solve set-up
+    (the even-odd operators' field strength and 12x12 inverses) and its iterations.  The
+    reference stops on the squared residual of its Schur system, ||r||^2 < precision,
+    with precision = (1e-10 ||b||)^2; the true residual of the converged solve is
+    re-measured with the reference's FP64 Improved operator.  The -march=native build
+    is used when a probe of it succeeds on this host, else the portable one."""
+
+    def __init__(self):
+        from oracle import ref as R
+        self.build = "su3_native" if R.runs_here("su3_native") else "su3"
+        self.links = workload_links()
+        self.b = workload_sources()[N_POINT]
+        self.precision = (TOL ** 2) * float(np.vdot(self.b, self.b).real)
+        self.ref = R.Reference(DIMS, self.links, self.build)
+        t0 = time.perf_counter()
+        with quiet_stdout():
+            self.ref.bench_prepare(KAPPA, CSW)
+        self.prepare_s = time.perf_counter() - t0
+        self.cores = host_threads()
+
+    def full_solve(self):
+        """One solve to convergence: wall time, the reference's own getLastSteps(), the
+        re-measured true residual."""
+        with quiet_stdout():
             t0 = time.perf_counter()
-            run(n)
-            ts.append(time.perf_counter() - t0)
-    t_iter = (ts[1] - ts[0]) / (sample_iters[1] - sample_iters[0])
-    setup = max(ts[0] - sample_iters[0] * t_iter, 0.0)
-    return {"t_iter": t_iter, "setup": setup, "kind": kind, "sample_seconds": sum(ts),
-            "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))}
+            rc, x, steps = self.ref.bench_solve(self.b, self.precision, 5000)
+            seconds = time.perf_counter() - t0
+            y = self.ref.multiply("Improved", x, KAPPA, CSW, False)
+        res = float(np.linalg.norm(self.b - y) / np.linalg.norm(self.b))
+        return {"seconds": seconds, "steps": steps, "converged": rc == 1, "true_residual": res,
+                "solves_per_s": 1.0 / seconds}
+
+    def sample(self, max_steps):
+        """The same solve stopped after max_steps iterations (its set-up included)."""
+        with quiet_stdout():
+            t0 = time.perf_counter()
+            self.ref.bench_solve(self.b, self.precision, max_steps, keep_solution=False)
+            return time.perf_counter() - t0
+
+    def close(self):
+        self.ref.bench_release()
 
 
 def dist_setup():
@@ -277,58 +311,50 @@ def max_over_ranks(world, x):
     return float(t.item())
 
 
+REF_SAMPLE_STEPS = 8  # iterations of one bounded sample of the reference solve
+
+
 def run_reference(args, world, rank):
+    """The reference arm: only the reference's own code (oracle/_ref), no GPU.  First one
+    solve to convergence (its wall time, iteration count and re-measured true residual go
+    into the line as full_solve); then every step is a bounded sample, the same solve
+    stopped after REF_SAMPLE_STEPS iterations.  A step's solves/s is
+    1 / (setup + steps x per-iteration time), with setup the solve stopped at 0 iterations
+    (timed twice before the warm-up), the per-iteration time from the step's sample and
+    steps the converged solve's own count."""
     if rank != 0:
         return
-    steps = []
-    info = None
-    # solve iteration count of the reference algorithm on this system: the GPU mirror of
-    # PreconditionedBiCGStab when a GPU is present
-    n_iter = gpu_eo_bicgstab_iterations()
-    for s in range(args.warmup + args.steps):
-        info = cpu_reference()
-        per_solve = info["setup"] + n_iter * info["t_iter"]
-        if s >= args.warmup:
-            steps.append(per_solve)
-    per_solve = statistics.median(steps)
-    value = 1.0 / per_solve
+    ref = ReferenceCPU()
+    try:
+        full = ref.full_solve()
+        if not full["converged"] or full["true_residual"] > TOL:
+            log(f"reference: solve did not reach the tolerance: {full}")
+        setup = min(ref.sample(0) for _ in range(2))
+        per_solve, sample_s = [], []
+        for s in range(args.warmup + args.steps):
+            t = ref.sample(REF_SAMPLE_STEPS)
+            if s >= args.warmup:
+                sample_s.append(t)
+                per_solve.append(setup + full["steps"] * max(t - setup, 0.0) / REF_SAMPLE_STEPS)
+    finally:
+        ref.close()
+    value = 1.0 / statistics.median(per_solve)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 0,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_solve * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(sample_s) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded)", "config": config_dict("reference-fp64-eo-bicgstab"),
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": info["cores"], "kind": info["kind"],
-                         "sample": (f"per step: the reference's FP64 even-odd BiCGStab run for 4 and 8 iterations on "
-                                    f"the 24^3x48 system (set-up {info['setup']:.2f} s, {info['t_iter']:.3f} s/iteration), "
-                                    f"extrapolated to its {n_iter} iterations to converge")},
+        "data": "synthetic (seeded)", "config": config_dict("reference-fp64-eo-bicgstab (PreconditionedBiCGStab)"),
+        "full_solve": {**full, "build": ref.build, "cores": ref.cores},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": ref.cores, "kind": "reference",
+                         "sample": (f"the reference's PreconditionedBiCGStab::solve (oracle/_ref {ref.build} build) on "
+                                    f"the 24^3x48 system of the first Z2 source: one converged solve "
+                                    f"({full['seconds']:.1f} s, {full['steps']} steps by its getLastSteps(), true "
+                                    f"residual {full['true_residual']:.2e}), then per step the same solve stopped "
+                                    f"after {REF_SAMPLE_STEPS} iterations ({statistics.mean(sample_s):.2f} s; set-up "
+                                    f"{setup:.2f} s), scaled to the converged solve's {full['steps']} steps")},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
-
-
-def gpu_eo_bicgstab_iterations():
-    try:
-        import leonardym_b200 as L
-        links = workload_links()
-        lat = L.Lattice(DIMS, "su3", device=0)
-        op = L.ImprovedDiracWilsonOperator(lat, KAPPA, CSW, gamma5=False)
-        op.setLattice(links)
-        b = workload_sources()[N_POINT]
-        s = L.PreconditionedBiCGStab()
-        s.setPrecision((TOL ** 2) * float(np.vdot(b, b).real))
-        s.setMaximumSteps(5000)
-        x = lat.new_vector()
-        s.solve(op, b, x)
-        n = s.stats.iterations
-        lat.close()
-        return n
-    except Exception:
-        import oracle as O
-        links = workload_links()
-        b = workload_sources()[N_POINT]
-        D = O.Operator(O.Geometry(DIMS), links, "Improved", KAPPA, CSW, False)
-        _, _, n = O.preconditioned_bicgstab(D, b, (TOL ** 2) * float(np.vdot(b, b).real), 5000)
-        return n
 
 
 def block_solver(args):
@@ -478,21 +504,15 @@ def run_ours(args, world, rank, local):
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
-        n_iter = None
-        s = L.PreconditionedBiCGStab()
-        b = srcs[N_POINT]
-        s.setPrecision((TOL ** 2) * float(np.vdot(b, b).real))
-        s.setMaximumSteps(5000)
-        x = lat.new_vector()
-        s.solve(op, b, x)
-        n_iter = s.stats.iterations
-        info = cpu_reference()
-        per_solve = info["setup"] + n_iter * info["t_iter"]
-        cpu = {"value": 1.0 / per_solve, "unit": "solves/s", "cores": info["cores"], "kind": info["kind"],
-               "sample": (f"the reference's FP64 even-odd BiCGStab on this lattice and source run for 4 and 8 "
-                          f"iterations (set-up {info['setup']:.2f} s, {info['t_iter']:.3f} s/iteration, "
-                          f"{info['sample_seconds']:.1f} s of CPU work), extrapolated to the {n_iter} iterations "
-                          f"its GPU mirror needs on the same system")}
+        ref = ReferenceCPU()
+        try:
+            full = ref.full_solve()
+        finally:
+            ref.close()
+        cpu = {"value": full["solves_per_s"], "unit": "solves/s", "cores": ref.cores, "kind": "reference",
+               "sample": (f"one solve to convergence of the reference's PreconditionedBiCGStab::solve (oracle/_ref "
+                          f"{ref.build} build) on this lattice and the first Z2 source: {full['seconds']:.1f} s, "
+                          f"{full['steps']} steps by its getLastSteps(), true residual {full['true_residual']:.2e}")}
     # the propagator consumers of this workload's sources, after the timed region on their own
     # clock: MesonCorrelator (the 12 point sources) and ChiralCondensate (32 Z2 noise vectors)
     consumers = None

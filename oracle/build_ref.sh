@@ -4,8 +4,14 @@
 # oracle/eigen_shim, plus oracle/ref_harness.cpp, into oracle/_ref/:
 #   libleonard_ref_su3.so     NUMCOLORS=3            (SU(3) fundamental)
 #   libleonard_ref_su2adj.so  NUMCOLORS=2 -DADJOINT  (SU(2) adjoint)
+#   libleonard_ref_su3_native.so  the SU(3) build again with -march=native (the CPU
+#                             baseline of bench.py; the two builds above, for any x86-64,
+#                             pin the oracle and make the golden fixtures)
 # Flags follow the reference's Makefile.mth (-DEIGEN -DMULTITHREADING -fopenmp, the
-# MatrixBase plugin), with -std=c++17 because program_options uses <any>.
+# MatrixBase plugin) and Makefile.mpi (-march=native, native build only), with
+# -std=c++17 because program_options uses <any>.  -march=native targets the CPU of the
+# machine that runs this script; bench.py runs the native build only after a probe of it
+# on the host that runs the benchmark succeeds.
 set -euo pipefail
 REF=${LYM_REFERENCE:-/root/reference}/source
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
@@ -38,7 +44,7 @@ build() {
   local objs=()
   for tu in "${TUS[@]}" ; do
     local o="$objdir/$(echo "$tu" | tr '/' '_' | sed 's/\.cpp$/.o/')"
-    if [ ! -f "$o" ] || [ "$REF/$tu" -nt "$o" ] || [ "$HERE/eigen_shim/Eigen/Dense" -nt "$o" ]; then
+    if [ ! -f "$o" ] || [ "$REF/$tu" -nt "$o" ] || [ "$HERE/eigen_shim/Eigen/Dense" -nt "$o" ] || [ "$HERE/build_ref.sh" -nt "$o" ]; then
       g++ "${flags[@]}" -c "$REF/$tu" -o "$o" &
     fi
     objs+=("$o")
@@ -51,6 +57,8 @@ COMMON=(-O2 -fPIC -fopenmp -std=c++17 -w -include ctime -include cstring -I"$HER
         -DMBE="\"$REF/utils/MatrixBaseExtension.h\"" -DEIGEN -DMULTITHREADING)
 build su3 "${COMMON[@]}" -DNUMCOLORS=3
 build su2adj "${COMMON[@]}" -DNUMCOLORS=2 -DADJOINT
+build su3_native "${COMMON[@]}" -march=native -DNUMCOLORS=3
+gcc -march=native -Q --help=target 2>/dev/null | grep -E '^\s+-march=' | head -1 | awk '{print $2}' > "$OUT/native_arch.txt"
 # the C++ adapter of include/ must compile against the reference's own headers
 for flags in "-DNUMCOLORS=3" "-DNUMCOLORS=2 -DADJOINT"; do
   # shellcheck disable=SC2086

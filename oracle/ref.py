@@ -19,11 +19,46 @@ SOLVER = {"cg": 0, "bicgstab": 1, "preconditioned_bicgstab": 2, "bicgstab_shifte
 
 
 def path(rep):
+    """rep: "su3", "su2adj" (portable builds) or "su3_native" (-march=native)."""
     return os.path.join(_HERE, "_ref", f"libleonard_ref_{rep}.so")
 
 
 def available(rep="su3"):
     return os.path.exists(path(rep))
+
+
+_PROBE = """
+import sys, numpy as np
+sys.path.insert(0, sys.argv[1])
+from oracle import ref as R
+dims = (4, 4, 4, 4)
+rng = np.random.default_rng(5)
+links = np.empty((256, 4, 3, 3), np.complex128)
+for k in range(256 * 4):
+    q, _ = np.linalg.qr(rng.normal(size=(3, 3)) + 1j * rng.normal(size=(3, 3)))
+    links.reshape(-1, 3, 3)[k] = q
+x = rng.normal(size=(256, 4, 3)) + 1j * rng.normal(size=(256, 4, 3))
+ref = R.Reference(dims, links, sys.argv[2])
+y = ref.multiply("EvenOddImproved", x, 0.13, 1.0, False)
+z = R.Reference(dims, links, "su3").multiply("EvenOddImproved", x, 0.13, 1.0, False)
+assert np.linalg.norm(y - z) <= 1e-12 * np.linalg.norm(z)
+"""
+
+
+def runs_here(rep):
+    """True when the build `rep` loads and computes correctly on this host, tried in a
+    child process (a build for another CPU ends the child, not the caller)."""
+    import subprocess
+    import sys
+    if not available(rep):
+        return False
+    root = os.path.dirname(_HERE)
+    try:
+        r = subprocess.run([sys.executable, "-c", _PROBE, root, rep], capture_output=True, timeout=300,
+                           env={**os.environ, "OMP_NUM_THREADS": "1"})
+    except subprocess.TimeoutExpired:
+        return False
+    return r.returncode == 0
 
 
 def lib(rep):
@@ -42,6 +77,9 @@ def lib(rep):
         L.ref_antiperiodic.argtypes = [ip, vp]
         if hasattr(L, "ref_to_adjoint"):
             L.ref_to_adjoint.argtypes = [i, vp, vp]
+        L.ref_bench_prepare.argtypes = [ip, dp, dp, vp]
+        L.ref_bench_solve.argtypes = [dp, i, vp, vp, ip]
+        L.ref_bench_release.argtypes = []
         _LIBS[rep] = L
     return _LIBS[rep]
 
@@ -98,6 +136,22 @@ class Reference:
         rc = self.L.ref_solve(_d(self.dims), KIND[kind], kappa, csw, int(gamma5), _p(self.links), SOLVER[solver],
                               float(precision), int(max_steps), s.real, s.imag, _p(b), _p(x), C.byref(steps))
         return rc, x, steps.value
+
+    # the benchmark's CPU baseline: PreconditionedBiCGStab::solve on one held Improved operator
+    def bench_prepare(self, kappa, csw):
+        rc = self.L.ref_bench_prepare(_d(self.dims), float(kappa), float(csw), _p(self.links))
+        assert rc == 0
+
+    def bench_solve(self, b, precision, max_steps, keep_solution=True):
+        b = np.ascontiguousarray(b, np.complex128)
+        x = self._vec() if keep_solution else None
+        steps = C.c_int(0)
+        rc = self.L.ref_bench_solve(float(precision), int(max_steps), _p(b), _p(x) if x is not None else None,
+                                    C.byref(steps))
+        return rc, x, steps.value
+
+    def bench_release(self):
+        self.L.ref_bench_release()
 
     def solve2(self, kind, solver, b, precision, max_steps, kappa, csw=0.0, gamma5=True, l=2, pre_kind="DiracWilson",
                pre_kappa=0.1, pre_csw=0.0):

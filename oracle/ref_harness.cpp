@@ -327,4 +327,46 @@ int ref_fermion_force(const int dims[4], int kind, double kappa, double csw, con
     return 1;
 }
 
+// ---- CPU baseline of the benchmark --------------------------------------------------
+// One ImprovedDiracWilsonOperator held on one link field, as a caller that solves many
+// sources on one gauge configuration holds it (the field strength is built once), and
+// PreconditionedBiCGStab::solve on it: per call the reference builds its even-odd
+// operators (field strength and the 12x12 inverses of every site) and runs BiCGStab on
+// the Schur system (inverters/PreconditionedBiCGStab.cpp:33-100).
+static extended_fermion_lattice_t *g_bench_links = nullptr;
+static ImprovedDiracWilsonOperator *g_bench_op = nullptr;
+
+void ref_bench_release()
+{
+    delete g_bench_op;
+    delete g_bench_links;
+    g_bench_op = nullptr;
+    g_bench_links = nullptr;
+}
+
+int ref_bench_prepare(const int dims[4], double kappa, double csw, const double *links)
+{
+    ref_bench_release();
+    init_layout(dims);
+    g_bench_links = new extended_fermion_lattice_t;
+    load(*g_bench_links, links);
+    g_bench_op = static_cast<ImprovedDiracWilsonOperator *>(make_operator(1, kappa, csw, 0, *g_bench_links));
+    return g_bench_op ? 0 : -1;
+}
+
+// returns 1 when the solver reports convergence, 0 when not, -1 without a prepared operator
+int ref_bench_solve(double precision, int max_steps, const double *src, double *sol, int *steps)
+{
+    if (!g_bench_op) return -1;
+    reduced_dirac_vector_t b, x;
+    load(b, src);
+    PreconditionedBiCGStab pb;
+    pb.setPrecision(precision);
+    pb.setMaximumSteps(max_steps);
+    const bool ok = pb.solve(g_bench_op, b, x);
+    *steps = pb.getLastSteps();
+    if (sol) store(x, sol);
+    return ok ? 1 : 0;
+}
+
 }  // extern "C"
