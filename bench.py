@@ -229,6 +229,11 @@ class quiet_stdout:
         os.close(self.null)
 
 
+# the reference's Schur-residual precision, in units of (1e-10 ||b||)^2, that gives a true
+# residual <= 1e-10 on the benchmark's system (see ReferenceCPU)
+REF_PRECISION_FACTOR = 7e-4
+
+
 def host_threads():
     n = os.environ.get("OMP_NUM_THREADS")
     return int(n) if n else len(os.sched_getaffinity(0))
@@ -243,16 +248,20 @@ class ReferenceCPU:
     gauge field holds it); every solve then pays the reference's own per-solve set-up
     (the even-odd operators' field strength and 12x12 inverses) and its iterations.  The
     reference stops on the squared residual of its Schur system, ||r||^2 < precision,
-    with precision = (1e-10 ||b||)^2; the true residual of the converged solve is
-    re-measured with the reference's FP64 Improved operator.  The -march=native build
-    is used when a probe of it succeeds on this host, else the portable one."""
+    which is not the true residual of D x = b: at precision (1e-10 ||b||)^2 it stops after
+    263 steps at a true residual of 3.3e-9.  To reach the same 1e-10 true residual as the
+    GPU solves, precision is REF_PRECISION_FACTOR (1e-10 ||b||)^2 (measured: 286 steps,
+    9.2e-11); the converged solve's true residual is re-measured with the reference's FP64
+    Improved operator and, should it miss 1e-10, the factor is tightened and the solve
+    repeated.  The -march=native build is used when a probe of it succeeds on this host,
+    else the portable one."""
 
     def __init__(self):
         from oracle import ref as R
         self.build = "su3_native" if R.runs_here("su3_native") else "su3"
         self.links = workload_links()
         self.b = workload_sources()[N_POINT]
-        self.precision = (TOL ** 2) * float(np.vdot(self.b, self.b).real)
+        self.precision = REF_PRECISION_FACTOR * (TOL ** 2) * float(np.vdot(self.b, self.b).real)
         self.ref = R.Reference(DIMS, self.links, self.build)
         t0 = time.perf_counter()
         with quiet_stdout():
@@ -261,16 +270,21 @@ class ReferenceCPU:
         self.cores = host_threads()
 
     def full_solve(self):
-        """One solve to convergence: wall time, the reference's own getLastSteps(), the
-        re-measured true residual."""
-        with quiet_stdout():
-            t0 = time.perf_counter()
-            rc, x, steps = self.ref.bench_solve(self.b, self.precision, 5000)
-            seconds = time.perf_counter() - t0
-            y = self.ref.multiply("Improved", x, KAPPA, CSW, False)
-        res = float(np.linalg.norm(self.b - y) / np.linalg.norm(self.b))
+        """One solve to a true residual <= 1e-10: wall time, the reference's own
+        getLastSteps(), the re-measured true residual (at most two tighter repeats)."""
+        for _ in range(3):
+            with quiet_stdout():
+                t0 = time.perf_counter()
+                rc, x, steps = self.ref.bench_solve(self.b, self.precision, 5000)
+                seconds = time.perf_counter() - t0
+                y = self.ref.multiply("Improved", x, KAPPA, CSW, False)
+            res = float(np.linalg.norm(self.b - y) / np.linalg.norm(self.b))
+            if res <= TOL or rc != 1:
+                break
+            self.precision *= 0.5 * (TOL / res) ** 2
         return {"seconds": seconds, "steps": steps, "converged": rc == 1, "true_residual": res,
-                "solves_per_s": 1.0 / seconds}
+                "solves_per_s": 1.0 / seconds,
+                "precision_factor": self.precision / ((TOL ** 2) * float(np.vdot(self.b, self.b).real))}
 
     def sample(self, max_steps):
         """The same solve stopped after max_steps iterations (its set-up included)."""

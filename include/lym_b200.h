@@ -423,6 +423,14 @@ int lym_multiply_batch(lym_context *ctx, int prec, int nrhs, const int *op_ids, 
 int lym_set_batch_tile(lym_context *ctx, int by, int bz, int minb);
 int lym_get_batch_tile(lym_context *ctx, int prec, int batch, int has_clover, int *by, int *bz, int *minb);
 
+/* ---- fault injection on the host (no reference counterpart: a test hook) -----------
+ * The next n device allocations of the context (of the server lane holding gauge field
+ * `key`) report failure as a cudaMalloc that returned cudaErrorMemoryAllocation would:
+ * the call that needed the memory returns LYM_ERR_MEMORY.  No device memory or kernel is
+ * involved.  A server lane fails only the request whose admission met the failure. */
+int lym_context_inject_alloc_failures(lym_context *ctx, int n);
+int lym_server_inject_alloc_failures(lym_server *server, int key, int n);
+
 /* ---- pinned host memory for callers that want fast transfers ---------------------- */
 void *lym_host_alloc(size_t bytes);
 void lym_host_free(void *p);

@@ -9,6 +9,9 @@
 //     setLattice -> lym_gauge_upload of the raw extended_fermion_lattice_t storage
 //     multiply / multiplyAdd -> lym_multiply / lym_multiply_add on the raw vector storage
 //   GpuSolver       : Solver            -> lym_solve     (inverters/Solver.h:13)
+//   GpuPreconditionedBiCGStab : PreconditionedBiCGStab -> lym_solve (LYM_SOLVER_EO_BICGSTAB), for
+//                       the callers that build that solver themselves (MesonCorrelator.cpp:70,
+//                       ChiralCondensate.cpp:51); any ImprovedDiracWilsonOperator, GPU or not
 //   GpuMultishiftSolver : MultishiftSolver -> lym_multishift (inverters/MultishiftSolver.h:28)
 //   GpuFermionForce : ImprovedFermionForce, what GpuDiracOperator::getForce returns
 //     derivative(force, lattice, X, Y, weight) -> lym_fermion_force (hmc_forces/FermionForce.h:15)
@@ -32,6 +35,7 @@
 #include "dirac_operators/SquareImprovedDiracWilsonOperator.h"
 #include "hmc_forces/ImprovedFermionForce.h"
 #include "inverters/MultishiftSolver.h"
+#include "inverters/PreconditionedBiCGStab.h"
 #include "inverters/Solver.h"
 #include "lym_b200.h"
 
@@ -215,6 +219,71 @@ public:
 
 private:
     int algorithm_;
+};
+
+// PreconditionedBiCGStab::solve (inverters/PreconditionedBiCGStab.cpp:33-100) with the whole
+// solve on the GPU: source preparation, BiCGStab on the even-odd Schur system and the
+// reconstruction run in the library (LYM_SOLVER_EO_BICGSTAB, the reference's iteration step
+// for step in FP64; getLastSteps() is the inner BiCGStab's step count, as the reference's).
+// The callers that create this solver themselves (MesonCorrelator.cpp:70,
+// ChiralCondensate.cpp:51) switch to it by changing that one `new`.  A Gpu* Improved operator
+// is solved as it is; any other ImprovedDiracWilsonOperator has its links, kappa and c_sw
+// uploaded for the call (and released after it).  With even-odd preconditioning switched
+// off through this class, the plain BiCGStab on D (PreconditionedBiCGStab.cpp:94-96,
+// LYM_SOLVER_BICGSTAB).  Operators that are not ImprovedDiracWilsonOperator go to the
+// reference's own solver, as before.
+class GpuPreconditionedBiCGStab : public PreconditionedBiCGStab {
+public:
+    GpuPreconditionedBiCGStab() : PreconditionedBiCGStab(), even_odd_(true) {}
+    using PreconditionedBiCGStab::solve;
+
+    // PreconditionedBiCGStab::setUseEvenOddPreconditioning is not virtual: call it on this type
+    void setUseEvenOddPreconditioning(bool eo)
+    {
+        even_odd_ = eo;
+        PreconditionedBiCGStab::setUseEvenOddPreconditioning(eo);
+    }
+
+    virtual bool solve(DiracOperator *dirac, const reduced_dirac_vector_t &source, reduced_dirac_vector_t &solution,
+                       reduced_dirac_vector_t const *initial_guess = 0)
+    {
+        ImprovedDiracWilsonOperator *imp = dynamic_cast<ImprovedDiracWilsonOperator *>(dirac);
+        lym_context *c = imp ? lym_global_context() : nullptr;
+        if (!c) return PreconditionedBiCGStab::solve(dirac, source, solution, 0, initial_guess);
+        int op = lym_operator_of(dirac);
+        int tmp_gauge = -1, tmp_op = -1;
+        if (op < 0) {  // a CPU operator: its links, kappa, c_sw and gamma5 for this call
+            tmp_gauge = lym_next_gauge_id();
+            if (lym_gauge_upload(c, tmp_gauge, reinterpret_cast<const double *>(imp->getLattice()->getRawData())) !=
+                    LYM_OK ||
+                lym_operator_create(c, tmp_gauge, LYM_OP_IMPROVED, imp->getKappa(), imp->getCSW(), imp->getGamma5(),
+                                    &tmp_op) != LYM_OK) {
+                std::cerr << "liblym_b200: " << lym_last_error(c) << std::endl;
+                release(c, tmp_gauge, tmp_op);
+                return false;
+            }
+            op = tmp_op;
+        }
+        lym_solve_stats st;
+        const int rc = lym_solve(c, op, even_odd_ ? LYM_SOLVER_EO_BICGSTAB : LYM_SOLVER_BICGSTAB, precision,
+                                 (int)maxSteps, reinterpret_cast<const double *>(source.getRawData()),
+                                 reinterpret_cast<double *>(solution.getRawData()),
+                                 initial_guess ? reinterpret_cast<const double *>(initial_guess->getRawData()) : 0,
+                                 &st);
+        lastSteps = st.steps;
+        lastError = st.last_error;
+        if (rc < 0) std::cerr << "liblym_b200: " << lym_last_error(c) << std::endl;
+        release(c, tmp_gauge, tmp_op);
+        return rc == LYM_OK;
+    }
+
+private:
+    static void release(lym_context *c, int gauge, int op)
+    {
+        if (op >= 0) lym_operator_destroy(c, op);
+        if (gauge >= 0) lym_gauge_evict(c, gauge);
+    }
+    bool even_odd_;
 };
 
 // MultishiftSolver::solve on the GPU; `algorithm` is a lym_multishift_solver value.

@@ -121,6 +121,7 @@ def lib():
         "lym_multiply_batch": (i, [vp, i, i, C.POINTER(C.c_int), C.POINTER(vp), C.POINTER(vp)]),
         "lym_set_batch_tile": (i, [vp, i, i, i]),
         "lym_get_batch_tile": (i, [vp, i, i, i, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "lym_context_inject_alloc_failures": (i, [vp, i]),
         "lym_host_alloc": (vp, [C.c_size_t]),
         "lym_host_free": (None, [vp]),
     }

@@ -7,6 +7,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -87,6 +88,7 @@ struct lym_context {
     unsigned long long launches = 0;  // kernels enqueued (graph replays count their nodes)
     double engine_stats[7] = {};      // block solves: lym_context_engine_stats
     bool capturing = false;
+    int inject_alloc_failures = 0;  // the next n device allocations report failure (tests)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -155,6 +157,10 @@ void trim_pool(lym_context *c)
 
 void *dev_alloc(lym_context *c, size_t bytes)
 {
+    if (c->inject_alloc_failures > 0) {  // host-side fault injection (lym_context_inject_alloc_failures)
+        --c->inject_alloc_failures;
+        fail(c, LYM_ERR_MEMORY, "device allocation of %zu bytes failed: injected failure", bytes);
+    }
     void *p = nullptr;
     cudaError_t e = cudaMalloc(&p, bytes);
     if (e == cudaErrorMemoryAllocation && !c->capturing &&
@@ -1833,6 +1839,9 @@ public:
         double best_rr = 0.0;
         int stalls = 0, restarts = 0;
         bool gave_up = false;
+        // the source or the FP64 true residual is not finite: the slot stops unconverged,
+        // alone (its batch mates go on), and is not handed to another solver
+        bool nonfinite = false;
     };
 
     // algo ALGO_CG: CG on (gamma5 S)^2 (per iteration S^+ S p); ALGO_BICGSTAB: BiCGStab on S
@@ -1894,13 +1903,16 @@ public:
         const void *T = clov ? op.clover.T[PREC_F] : nullptr, *Ti = clov ? op.clover.Tinv[PREC_F] : nullptr;
         if (gauge_id < 0) {
             // first operator: every slot's table entry points at it (an idle lane of a pair
-            // borrows valid operator data), then the batched stencil is tuned on it
+            // borrows valid operator data), then the batched stencil is tuned on it; the
+            // engine takes the operator only once that has succeeded
+            for (int k = 0; k < nb; ++k) set_tables(k, b, T, Ti);
+            const BatchTile t =
+                tune_batch(c, gauge_of(c, op.gauge_id).dev, clov, sprec, tos.s, ps.s, tes.s, d_b, d_T, d_Ti, d_uniform);
+            if (algo == ALGO_BICGSTAB && batch_omega_fusable(t.minb, sprec))
+                om_scratch.reset(new DevBuf(c, omega_scratch_doubles(c->g, xs.s.lognb) * sizeof(double)));
+            tile = t;
             gauge_id = op.gauge_id;
             has_clover = clov;
-            for (int k = 0; k < nb; ++k) set_tables(k, b, T, Ti);
-            tile = tune_batch(c, gauge_of(c, gauge_id).dev, clov, sprec, tos.s, ps.s, tes.s, d_b, d_T, d_Ti, d_uniform);
-            if (algo == ALGO_BICGSTAB && batch_omega_fusable(tile.minb, sprec))
-                om_scratch.reset(new DevBuf(c, omega_scratch_doubles(c->g, xs.s.lognb) * sizeof(double)));
         }
         Slot &s = slot[j];
         delete s.bp;
@@ -1916,6 +1928,12 @@ public:
         s.bp = new Vec(c, PREC_D, 1);
         schur_source(c, op, B, **s.bp);
         s.bb = norm2_now(c, B);
+        if (!std::isfinite(s.bb)) {
+            s.nonfinite = true;
+            zero(c, X);
+            finish(j);
+            return;
+        }
         s.epsS = tol * tol * s.bb;
         zero(c, X.parity(1));
         set_tables(j, b, T, Ti);
@@ -1928,7 +1946,7 @@ public:
             finish(j);
             return;
         }
-        hs.converged[j] = hs.need_update[j] = 0;
+        hs.converged[j] = hs.need_update[j] = hs.restart[j] = 0;
         hs.last_update_its[j] = 0;
         if (algo == ALGO_BICGSTAB) {
             s.best_rr = rrS;
@@ -2117,7 +2135,10 @@ private:
             ++s.stalls;
         }
         if (hs.restart[j]) ++s.restarts;
-        if (rrS < s.epsS) {
+        if (!std::isfinite(rrS)) {
+            s.nonfinite = true;
+            finish(j);
+        } else if (rrS < s.epsS) {
             s.converged = 1;
             finish(j);
         } else if (s.stalls >= kMaxStalls || s.restarts >= kMaxRestarts) {
@@ -2210,13 +2231,25 @@ private:
             return;
         }
         Slot &s = slot[j];
-        run_site(c, OpFoldClear<SlotF, SpinorD>{xs.f().slot(j), s.X.parity(1).d()}, 1);
+        // a non-finite recursion (restart 2) drops its FP32 accumulator
+        if (hs.restart[j] != 2) run_site(c, OpFoldClear<SlotF, SpinorD>{xs.f().slot(j), s.X.parity(1).d()}, 1);
+        else axpby_views(c, xs.f().slot(j), xs.f().slot(j), C2(0.0), C2(0.0));
+        const bool restarted = hs.restart[j] != 0;
+        hs.restart[j] = 0;
         double rrS, rrN;
         true_res(j, rrS, rrN);
         ++s.updates;
-        if (rrS < s.epsS) {
+        if (!std::isfinite(rrS) || !std::isfinite(rrN)) {
+            s.nonfinite = true;
+            finish(j);
+        } else if (rrS < s.epsS) {
             s.converged = 1;
             finish(j);
+        } else if (restarted) {  // CG again from the true residual
+            axpby_views(c, (*rN).d(), rs.f().slot(j), C2(1.0), C2(0.0));
+            set_direction(j, 0.0);
+            hs.rr[j] = hs.rr_max[j] = rrN;
+            hs.active[j] = 1;
         } else {
             if (hs.converged[j]) hs.eps[j] = std::max(hs.eps[j] * 0.5 * s.epsS / rrS, 1e-300);
             const double b = rrN / hs.rr_prev[j];
@@ -2234,7 +2267,7 @@ private:
     {
         Slot &s = slot[j];
         s.finished = true;
-        if (s.gave_up) {  // nothing to reconstruct: the source is solved again elsewhere
+        if (s.gave_up || s.nonfinite) {  // nothing to reconstruct (solved again elsewhere, or not finite)
             s.iters = hs.its[j];
             hs.active[j] = 0;
             hs.need_update[j] = 0;
@@ -2703,8 +2736,17 @@ static int do_solve(lym_context *c, int op_id, int solver, double precision, int
         const Spinor *gp = gs ? &**gs : nullptr;
         CK(cudaEventRecord(c->ev0, c->st));
         int rc = LYM_OK;
+        // a source or guess with a non-finite entry: not converged at once (the reference
+        // iterates on its non-finite residuals until max_steps and returns false)
+        const double bb = norm2_now(c, *b), gg = gp ? norm2_now(c, *gp) : 0.0;
+        const bool finite_inputs = std::isfinite(bb) && std::isfinite(gg);
         try {
-            if (shifted) {
+            if (!finite_inputs) {
+                zero(c, *x);
+                local.last_error = local.true_residual = std::numeric_limits<double>::quiet_NaN();
+                c->err = "the source or the initial guess has non-finite entries";
+                rc = LYM_NOT_CONVERGED;
+            } else if (shifted) {
                 auto mv = [&](const Spinor &out, const Spinor &in, const int *skip) {
                     op_apply(c, op, PREC_D, out, in, &in, shift, skip);
                 };
@@ -3721,6 +3763,15 @@ int lym_get_batch_tile(lym_context *c, int prec, int batch, int has_clover, int 
         *by = t.by;
         *bz = t.bz;
         *minb = t.minb;
+        return LYM_OK;
+    });
+}
+
+int lym_context_inject_alloc_failures(lym_context *c, int n)
+{
+    if (n < 0) return LYM_ERR_ARGUMENT;
+    return guarded(c, [&]() {
+        c->inject_alloc_failures = n;
         return LYM_OK;
     });
 }

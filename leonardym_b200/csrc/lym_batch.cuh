@@ -1171,7 +1171,7 @@ struct BatchCGState {
     int its[kMaxBatch];        // iterations each slot took part in
     int failed;
     double2 rho[kMaxBatch], omega[kMaxBatch], bbeta[kMaxBatch];  // BiCGStab only
-    int restart[kMaxBatch];                    // BiCGStab broke down: restart at the update
+    int restart[kMaxBatch];                    // broke down: restart at the update
                                                // (2: non-finite, drop the FP32 accumulator)
     int last_update_its[kMaxBatch];            // its at the last reliable update
 };
@@ -1296,9 +1296,10 @@ template <class SX, class SP, class SR, class SAp> struct OpBUpdate {
         s->beta[r] = rr_new / s->rr[r];
         s->rr[r] = rr_new;
         if (rr_new > s->rr_max[r]) s->rr_max[r] = rr_new;
-        if (!(rr_new == rr_new)) {
-            s->failed = 1;
-            s->pause = 1;
+        if (!(rr_new <= 1e300)) {  // non-finite: this RHS leaves the iteration; the host restarts
+            s->restart[r] = 2;     // it from its FP64 solution or stops it (the others go on)
+            s->need_update[r] = 1;
+            s->active[r] = 0;
         } else if (rr_new < s->eps[r]) {
             s->converged[r] = 1;
             s->need_update[r] = 1;

@@ -35,6 +35,7 @@ def _bind():
     L.lym_server_submit.argtypes = [vp, i, dp, dp, i, C.POINTER(vp), C.POINTER(vp), dp, i, C.POINTER(C.c_longlong)]
     L.lym_server_wait.argtypes = [vp, C.c_longlong, dp, C.POINTER(RequestStats)]
     L.lym_server_poll.argtypes = [vp, C.c_longlong, C.POINTER(C.c_int)]
+    L.lym_server_inject_alloc_failures.argtypes = [vp, i, i]
     return L
 
 
@@ -109,6 +110,13 @@ class SolveServer:
         d = C.c_int(0)
         self._L.lym_server_poll(self._ptr, C.c_longlong(ticket), C.byref(d))
         return bool(d.value)
+
+    def inject_alloc_failures(self, key, n):
+        """Host-side fault injection for tests: the next n device allocations of the lane
+        holding gauge field `key` fail as an out-of-memory cudaMalloc would."""
+        rc = self._L.lym_server_inject_alloc_failures(self._ptr, int(key), int(n))
+        if rc != 0:
+            self._err(rc)
 
     def device_bytes(self):
         return int(self._L.lym_server_device_bytes(self._ptr))

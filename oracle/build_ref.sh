@@ -59,8 +59,15 @@ build su3 "${COMMON[@]}" -DNUMCOLORS=3
 build su2adj "${COMMON[@]}" -DNUMCOLORS=2 -DADJOINT
 build su3_native "${COMMON[@]}" -march=native -DNUMCOLORS=3
 gcc -march=native -Q --help=target 2>/dev/null | grep -E '^\s+-march=' | head -1 | awk '{print $2}' > "$OUT/native_arch.txt"
-# the C++ adapter of include/ must compile against the reference's own headers
-for flags in "-DNUMCOLORS=3" "-DNUMCOLORS=2 -DADJOINT"; do
-  # shellcheck disable=SC2086
-  g++ "${COMMON[@]}" $flags -fsyntax-only -I"$HERE/../include" -x c++ "$HERE/../include/lym_leonard_adapter.hpp"
+# the C++ adapter of include/ compiled against the reference's own headers, in a driver
+# (oracle/adapter_driver.cpp) linked with the reference's objects and the GPU library
+LIBDIR="$HERE/../leonardym_b200"
+for name in su3 su2adj; do
+  if [ "$name" = su3 ]; then flags=(-DNUMCOLORS=3); else flags=(-DNUMCOLORS=2 -DADJOINT); fi
+  objdir="$OUT/obj_$name"
+  g++ "${COMMON[@]}" "${flags[@]}" -I"$HERE/../include" -c "$HERE/adapter_driver.cpp" -o "$objdir/adapter_driver.o"
+  if [ -f "$LIBDIR/liblym_b200.so" ]; then
+    g++ -fopenmp -o "$OUT/adapter_driver_$name" "$objdir"/*.o -L"$LIBDIR" -llym_b200 \
+        -Wl,-rpath,'$ORIGIN/../../leonardym_b200'
+  fi
 done
