@@ -103,14 +103,59 @@ SERVE_EPS = {"su3": 0.25, "su2adj": 0.3}
 SERVE_POOL = 4  # distinct sources per field (reused across requests; every request gets its own solutions)
 
 
-def run_serving(window_s, batch=16, precision="single", solver="bicgstab"):
-    """Open-loop serving measurement: requests arrive for window_s seconds at Poisson times
-    (seeded) and are submitted to the solve server as they arrive; the result is the
-    completed sources per second over the whole run, per-request latency p50 / p99 (submit
-    to completion, the server's own clock) and the largest FP64 true residual."""
-    from leonardym_b200 import synth
+def _percentiles(lat):
+    lat = sorted(lat)
+    return {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]}
+
+
+def serving_stream(srv, fields, pools, rate, window_s, seed):
+    """Open loop: requests arrive for window_s seconds at Poisson times of mean rate `rate`
+    (seeded) and are submitted as they arrive; returns the completed sources per second
+    over the whole run, per-request latency p50 / p99 (submit to completion, the server's
+    own clock) and the largest FP64 true residual."""
+    rng = np.random.default_rng(seed)
+    t, arrivals = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > window_s:
+            break
+        key = int(rng.integers(len(fields)))
+        rep = fields[key][1]
+        arrivals.append((t, key, float(rng.uniform(*SERVE_KAPPA[rep])), int(rng.integers(1, 17))))
+    tickets = []
+    t0 = time.perf_counter()
+    for (ta, key, kappa, nsrc) in arrivals:
+        delay = t0 + ta - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        srcs = [pools[key][j % SERVE_POOL] for j in range(nsrc)]
+        tickets.append(srv.submit(key, kappa, SERVE_CSW[fields[key][1]], srcs)[0])
+    lat, worst, nsolved, failed = [], 0.0, 0, 0
+    for tk in tickets:
+        ok, st = srv.wait(tk, timeout=1800.0)
+        lat.append(st.latency_s * 1e3)
+        worst = max(worst, st.max_true_residual)
+        nsolved += st.nsrc
+        failed += 0 if ok else 1
+    elapsed = time.perf_counter() - t0
+    return {"requests": len(tickets), "sources": nsolved, "arrival_window_s": window_s,
+            "offered_requests_per_s": rate, "elapsed_s": elapsed,
+            "throughput_solves_per_s": nsolved / elapsed, "throughput_requests_per_s": len(tickets) / elapsed,
+            "latency_ms": _percentiles(lat) if lat else None, "max_true_residual": worst, "failed_requests": failed}
+
+
+SERVE_MEAN_SOURCES = 8.5  # mean of the uniform 1..16 sources per request
+SERVE_LOADS = (0.25, 0.5, 0.9)
+
+
+def run_serving(window_s, sweep_window_s, batch=16, precision="single", solver="bicgstab"):
+    """The configs' serving loop on one server: 8 resident seeded fields (4 volumes x 2
+    representations), each lane warmed by one request; then the configs' Poisson stream
+    (200 requests/s) for window_s seconds, whose completion rate is the server's capacity
+    on this mix; then the same mix offered at 25 %, 50 % and 90 % of that capacity for
+    sweep_window_s seconds each, where the latency is that of batching, not of a queue."""
     from leonardym_b200.server import SolveServer
-    rng = np.random.default_rng(SEED + 7)
+    synth = synth_module()
     fields = [(dims, rep) for dims in SERVE_VOLUMES for rep in ("su3", "su2adj")]
     srv = SolveServer(batch=batch, precision=precision, solver=solver)
     pools = {}
@@ -118,42 +163,52 @@ def run_serving(window_s, batch=16, precision="single", solver="bicgstab"):
         for key, (dims, rep) in enumerate(fields):
             srv.add_gauge(key, dims, rep, synth.fermion_links(dims, rep, SERVE_EPS[rep], SEED + 4 * key))
             pools[key] = [synth.gaussian_spinor(dims, 3, SEED + 100 * key + j) for j in range(SERVE_POOL)]
-        t, arrivals = 0.0, []
-        while True:
-            t += rng.exponential(1.0 / SERVE_RATE)
-            if t > window_s:
-                break
-            key = int(rng.integers(len(fields)))
-            rep = fields[key][1]
-            kappa = float(rng.uniform(*SERVE_KAPPA[rep]))
-            nsrc = int(rng.integers(1, 17))
-            arrivals.append((t, key, kappa, nsrc))
-        tickets = []
+        warm = [srv.submit(key, SERVE_KAPPA[rep][0], SERVE_CSW[rep], pools[key][:2])[0]
+                for key, (dims, rep) in enumerate(fields)]
+        for tk in warm:
+            srv.wait(tk, timeout=1800.0)
+        out = serving_stream(srv, fields, pools, SERVE_RATE, window_s, SEED + 7)
+        capacity = out["throughput_solves_per_s"]
+        sweep = []
+        if sweep_window_s > 0:
+            for k, f in enumerate(SERVE_LOADS):
+                r = serving_stream(srv, fields, pools, f * capacity / SERVE_MEAN_SOURCES, sweep_window_s,
+                                   SEED + 8 + k)
+                r["load_fraction_of_capacity"] = f
+                sweep.append(r)
+    finally:
+        srv.close()
+    out.update({"fields": [f"{'x'.join(map(str, d))} {r}" for d, r in fields],
+                "solver": f"{SOLVER_NAMES[solver]}, {batch} slots per field, {precision} storage, continuous batching",
+                "capacity_solves_per_s": capacity, "load_sweep": sweep})
+    return out
+
+
+def run_serving_headline(links, srcs, batch=16, precision="single", solver="bicgstab", per_request=4):
+    """The headline's 44 sources served through SolveServer on one resident 24^3x48 SU(3)
+    field (kappa 0.137, c_sw 1.7): 11 requests of 4 sources submitted together after one
+    warm-up request; served solves/s over the whole run and per-request latency."""
+    from leonardym_b200.server import SolveServer
+    srv = SolveServer(batch=batch, precision=precision, solver=solver)
+    try:
+        srv.add_gauge(0, DIMS, "su3", links)
+        srv.wait(srv.submit(0, KAPPA, CSW, srcs[:per_request])[0], timeout=1800.0)
         t0 = time.perf_counter()
-        for (ta, key, kappa, nsrc) in arrivals:
-            delay = t0 + ta - time.perf_counter()
-            if delay > 0:
-                time.sleep(delay)
-            srcs = [pools[key][j % SERVE_POOL] for j in range(nsrc)]
-            tickets.append(srv.submit(key, kappa, SERVE_CSW[fields[key][1]], srcs)[0])
-        lat, worst, nsolved, failed = [], 0.0, 0, 0
+        tickets = [srv.submit(0, KAPPA, CSW, srcs[k:k + per_request])[0] for k in range(0, len(srcs), per_request)]
+        lat, worst, n = [], 0.0, 0
         for tk in tickets:
             ok, st = srv.wait(tk, timeout=1800.0)
+            if not ok:
+                raise RuntimeError(f"headline serving request failed: status {st.status}")
             lat.append(st.latency_s * 1e3)
             worst = max(worst, st.max_true_residual)
-            nsolved += st.nsrc
-            failed += 0 if ok else 1
+            n += st.nsrc
         elapsed = time.perf_counter() - t0
     finally:
         srv.close()
-    lat.sort()
-    return {"requests": len(tickets), "sources": nsolved, "arrival_window_s": window_s,
-            "offered_requests_per_s": SERVE_RATE, "elapsed_s": elapsed,
-            "throughput_solves_per_s": nsolved / elapsed, "throughput_requests_per_s": len(tickets) / elapsed,
-            "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
-            "max_true_residual": worst, "failed_requests": failed,
-            "fields": [f"{'x'.join(map(str, d))} {r}" for d, r in fields],
-            "solver": f"{SOLVER_NAMES[solver]}, {batch} slots per field, {precision} storage, continuous batching"}
+    return {"requests": len(tickets), "sources": n, "elapsed_s": elapsed, "served_solves_per_s": n / elapsed,
+            "latency_ms": _percentiles(lat), "max_true_residual": worst,
+            "solver": f"{SOLVER_NAMES[solver]}, {batch} slots, {precision} storage, continuous batching"}
 
 
 class ClockSampler:
@@ -542,9 +597,12 @@ def run_ours(args, world, rank, local):
             consumers[f"{name}_converged"] = bool(res["converged"])
         consumers["sources"] = {"meson_correlator": 12, "chiral_condensate": N_NOISE}
     lat.close()
-    serving = None
+    serving = serving24 = None
     if rank == 0 and args.serve_window > 0:  # after the timed region: its own clock
-        serving = run_serving(args.serve_window, batch=args.batch, precision=args.precision, solver=args.solver)
+        serving = run_serving(args.serve_window, args.serve_sweep_window, batch=args.batch, precision=args.precision,
+                              solver=args.solver)
+        serving24 = run_serving_headline(links, srcs, batch=args.batch, precision=args.precision, solver=args.solver)
+        serving24["served_over_fp64_eo_cg"] = serving24["served_solves_per_s"] / (fp64_value / world)
     if rank != 0:
         return
     line = {
@@ -577,6 +635,7 @@ def run_ours(args, world, rank, local):
                 "d2h_bytes_per_step": nrhs * nbytes},
         "cpu_baseline": cpu,
         "serving": serving,
+        "serving_24c48": serving24,
         "consumers": consumers,
     }
     print(json.dumps(line), flush=True)
@@ -909,7 +968,9 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--profile", action="store_true", help="small fixed case for ncu captures")
     ap.add_argument("--serve-window", type=float, default=0.25,
-                    help="seconds of Poisson arrivals for the serving measurement (0: skip it)")
+                    help="seconds of the configs' 200 requests/s Poisson stream (0: skip the serving measurements)")
+    ap.add_argument("--serve-sweep-window", type=float, default=15.0,
+                    help="seconds of arrivals at each load of the sweep below the measured capacity (0: no sweep)")
     ap.add_argument("--tile", default="", help="with --profile: batched stencil column and variant 'by,bz,minb'")
     args = ap.parse_args()
     if args.workload == "propagators" and args.precision is None:

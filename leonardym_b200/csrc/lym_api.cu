@@ -67,6 +67,7 @@ struct lym_context {
     // reductions
     double *partials = nullptr;
     double *bpartials = nullptr;  // per-RHS partial sums of the batched reductions
+    double *spartials = nullptr;  // one partial sum per block of a single-RHS stencil launch
     int *nbr = nullptr;           // neighbour half-site table [2][8][stride] (batched stencil)
     std::map<int, int *> orders;  // traversal tables [stride] by column by * 4096 + bz
     std::map<int, BatchTile> tiles;  // tuned configuration by (precision, batch, clover)
@@ -466,6 +467,46 @@ void apply_schur(lym_context *c, OpEntry &op, int prec, const Spinor &out_o, con
     count(c, 2);
 }
 
+// Q in_o = gamma5 S in_o inside the even-odd CG on (gamma5 S)^2, with the CG's vector work in
+// the second launch (launch_dslash_cg): mode CG_NORM stores q = Q p in out_o and sets the
+// state's alpha from |q|^2; mode CG_UPDATE (in_o = q) forms A p = Q q in registers and
+// updates x and r with the state's alpha, then the CG step's scalars.  p, x, r: one parity.
+void apply_schur_cg(lym_context *c, OpEntry &op, int prec, int mode, const Spinor &out_o, const Spinor &in_o,
+                    const Spinor &tmp_e, const Spinor &p, const Spinor &x, const Spinor &r, void *state,
+                    const int *skip)
+{
+    GaugeEntry &ge = gauge_of(c, op.gauge_id);
+    const bool clov = kind_has_clover(op.kind);
+    if (clov) ensure_clover(c, op);
+    require_recon(c, ge, prec);
+    DslashParams P;
+    P.g = c->g;
+    P.prec = prec;
+    P.rep = c->rep;
+    P.U = &ge.dev;
+    P.skip_if = skip;
+    P.epi = clov ? EPI_CLOVINV_ : EPI_SCALE_;
+    P.parity = 0;
+    P.in = in_o;
+    P.out = tmp_e;
+    P.y = tmp_e;
+    P.v2 = tmp_e;
+    P.clover = clov ? op.clover.Tinv[prec] : nullptr;
+    P.a = 1.0;
+    launch_dslash(P, c->st);
+    P.epi = EPI_XPAY_;
+    P.parity = 1;
+    P.in = tmp_e;
+    P.out = out_o;
+    P.y = in_o;
+    P.v2 = p;
+    P.clover = clov ? op.clover.T[prec] : nullptr;
+    P.b = -op.kappa * op.kappa;
+    P.gamma5 = 1;
+    launch_dslash_cg(P, mode, p, x, r, state, c->spartials, c->counter, c->st);
+    count(c, 2);
+}
+
 bool is_even_odd(int kind) { return kind == LYM_OP_EVEN_ODD_IMPROVED || kind == LYM_OP_SQUARE_EVEN_ODD_IMPROVED; }
 
 // DiracOperator::multiply / multiplyAdd on full device spinors (reference semantics).
@@ -822,7 +863,7 @@ int eo_cg(lym_context *c, OpEntry &op, int sprec, const Spinor &b, const Spinor 
     if (kind_has_clover(op.kind)) ensure_clover(c, op);
     Vec bp(c, PREC_D, 1), rS(c, PREC_D, 1), rN(c, PREC_D, 1), te(c, PREC_D, 1), t1(c, PREC_D, 1);
     Vec xs(c, sprec == PREC_H ? PREC_F : sprec, 1), rs(c, sprec == PREC_H ? PREC_F : sprec, 1);
-    Vec ps(c, sprec, 1), aps(c, sprec, 1), tes(c, sprec, 1), tos(c, sprec, 1);
+    Vec ps(c, sprec, 1), tes(c, sprec, 1), tos(c, sprec, 1);
     const Spinor xo = x.parity(1);
     schur_source(c, op, b, *bp);
     const double bb = norm2_now(c, b);
@@ -863,20 +904,14 @@ int eo_cg(lym_context *c, OpEntry &op, int sprec, const Spinor &b, const Spinor 
         H.delta2 = delta * delta;
         H.max_iter = max_steps;
         push_state(c, sizeof(CGState));
-        auto matvec = [&](const Spinor &out, const Spinor &in, const int *skip) {
-            apply_schur(c, eo, sprec, *tos, in, *tes, 1, nullptr, C2(0.0), skip);
-            apply_schur(c, eo, sprec, out, *tos, *tes, 1, nullptr, C2(0.0), skip);
-        };
+        // one iteration, 5 launches: q = Q p with alpha from |q|^2 = <p, A p>; A p = Q q with
+        // x += alpha p, r -= alpha A p and |r|^2 in the same launch; then p = r + beta p
         auto step = [&]() {
-            matvec(*aps, *ps, &S->pause);
-            auto go = [&](auto P, auto AP, auto X, auto R) {
-                run_site(c, OpCGAlpha<decltype(P), decltype(AP)>{P, AP, S}, 1, gate);
-                run_site(c, OpCGUpdate<decltype(X), decltype(P), decltype(R), decltype(AP)>{X, P, R, AP, S}, 1, gate);
-                run_site(c, OpCGDirection<decltype(P), decltype(R)>{P, R, S}, 1, gate);
-            };
-            if (sprec == PREC_D) go((*ps).d(), (*aps).d(), (*xs).d(), (*rs).d());
-            else if (sprec == PREC_F) go((*ps).f(), (*aps).f(), (*xs).f(), (*rs).f());
-            else go((*ps).h(), (*aps).h(), (*xs).f(), (*rs).f());
+            apply_schur_cg(c, eo, sprec, CG_NORM, *tos, *ps, *tes, *ps, *xs, *rs, S, &S->pause);
+            apply_schur_cg(c, eo, sprec, CG_UPDATE, *tos, *tos, *tes, *ps, *xs, *rs, S, &S->pause);
+            if (sprec == PREC_D) run_site(c, OpCGDirection<SpinorD, SpinorD>{(*ps).d(), (*rs).d(), S}, 1, gate);
+            else if (sprec == PREC_F) run_site(c, OpCGDirection<SpinorF, SpinorF>{(*ps).f(), (*rs).f(), S}, 1, gate);
+            else run_site(c, OpCGDirection<SpinorH, SpinorF>{(*ps).h(), (*rs).f(), S}, 1, gate);
         };
         for (int outer = 0; outer < 10000; ++outer) {
             run_gated_state(c, S, step, 8, (long)max_steps - cg_host(c).iter + 8);
@@ -2388,6 +2423,7 @@ int lym_context_create(const int dims[4], int rep, int device, lym_context **out
         CK(cudaStreamCreateWithFlags(&c->st_copy, cudaStreamNonBlocking));
         c->partials = (double *)dev_alloc(c, (size_t)kBlasGridMax * kMaxRed * sizeof(double));
         c->bpartials = (double *)dev_alloc(c, (size_t)kBlasGridMax * kMaxBatch * kBatchMaxRed * sizeof(double));
+        c->spartials = (double *)dev_alloc(c, ((size_t)c->g.Vh + 127) / 128 * sizeof(double));
         c->nbr = (int *)dev_alloc(c, (size_t)16 * c->g.stride * sizeof(int));
         launch_nbr_table(c->g, c->nbr, c->st);
         c->counter = (unsigned int *)dev_alloc(c, 64);
@@ -2430,6 +2466,7 @@ void lym_context_destroy(lym_context *c)
     for (auto &b : c->blocks) cudaFree(b.second);
     for (int k = 0; k < 3; ++k) cudaFree(c->aos[k]);
     cudaFree(c->partials);
+    cudaFree(c->spartials);
     cudaFree(c->bpartials);
     cudaFree(c->nbr);
     for (auto &kv : c->orders) cudaFree(kv.second);

@@ -226,6 +226,100 @@ __global__ void __launch_bounds__(128) dslash_kernel(const DslashArg<SpinorT, Ga
     arg.out.template store<R>(h, res);
 }
 
+// The second launch of a Schur product inside the even-odd CG on (gamma5 S)^2 (the CG of
+// ConjugateGradient.cpp:10-74 run on the normal equations of the Schur system), with the
+// CG's vector work in the epilogue.  Q = gamma5 S is Hermitian, so with A = Q Q,
+// <p, A p> = |Q p|^2:
+//   CG_NORM:   q = G5 (T y + b H x) (y = p) is stored and |q|^2 is reduced; fin(|q|^2) sets
+//              alpha = |r|^2 / <p, A p> (so no pass over p and A p is needed for alpha);
+//   CG_UPDATE: A p = G5 (T y + b H x) (y = q) stays in registers: x += alpha p (p read from
+//              v2), r -= alpha A p, and |r|^2 is reduced; fin(|r|^2) runs the CG step's
+//              scalar recursion (beta, stop and reliable-update tests).  A p is never written.
+// The per-block sums go to fixed slots; the last block (atomic ticket) adds them in a fixed
+// order, so the result is the same on every run.
+enum CGFuseMode : int { CG_NORM = 0, CG_UPDATE = 1 };
+
+template <class SX, class SR, class Fin> struct CGEpilogue {
+    SX x;
+    SR r;
+    const double2 *alpha;    // CG_UPDATE: the state's alpha
+    Fin fin;
+    double *partials;        // [gridDim.x]
+    unsigned int *counter;   // zero between launches
+};
+
+template <typename R, int MODE, class SpinorT, class GaugeT, class CloverT, class SX, class SR, class Fin>
+__global__ void __launch_bounds__(128)
+    dslash_cg_kernel(const DslashArg<SpinorT, GaugeT, CloverT> arg, const CGEpilogue<SX, SR, Fin> f)
+{
+    if (arg.skip_if && *arg.skip_if) return;  // the whole grid: the CG state is paused
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    double part = 0.0;
+    if (h < arg.g.Vh) {
+        cx<R> acc[12], yv[12], res[12];
+        hopping<R>(arg.g, arg.in, arg.U, arg.parity, h, acc);
+        arg.y.template load<R>(h, yv);
+        if (arg.has_clover) {
+            clover_apply<R>(arg.T, arg.parity, h, yv, res);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 12; ++k) res[k] = yv[k];
+        }
+        const R b = (R)arg.b;
+#pragma unroll
+        for (int k = 0; k < 12; ++k) fma_r(res[k], b, acc[k]);
+#pragma unroll
+        for (int k = 6; k < 12; ++k) res[k] = -res[k];  // gamma5
+        if (MODE == CG_NORM) {
+            arg.out.template store<R>(h, res);
+#pragma unroll
+            for (int k = 0; k < 12; ++k) part += (double)res[k].re * res[k].re + (double)res[k].im * res[k].im;
+        } else {
+            const double2 a = *f.alpha;
+            const cx<double> al = {a.x, a.y};
+            cx<double> xv[12], pv[12], rv[12];
+            f.x.template load<double>(h, xv);
+            arg.v2.template load<double>(h, pv);
+            f.r.template load<double>(h, rv);
+#pragma unroll
+            for (int k = 0; k < 12; ++k) {
+                fma_c(xv[k], al, pv[k]);
+                const cx<double> ap = {(double)res[k].re, (double)res[k].im};
+                rv[k] = rv[k] - al * ap;
+                part += rv[k].re * rv[k].re + rv[k].im * rv[k].im;
+            }
+            f.x.template store<double>(h, xv);
+            f.r.template store<double>(h, rv);
+        }
+    }
+    // fixed-order reduction: warps, then the block's 4 warps, then the blocks in order
+    __shared__ double wsum[4];
+    __shared__ bool last;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = part;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        f.partials[blockIdx.x] = (wsum[0] + wsum[1]) + (wsum[2] + wsum[3]);
+        __threadfence();
+        last = atomicAdd(f.counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double t = 0.0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) t += ((volatile double *)f.partials)[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        f.fin((wsum[0] + wsum[1]) + (wsum[2] + wsum[3]));
+        *f.counter = 0u;
+    }
+}
+
 // Stand-alone clover application: out = G5^g (T x) on one parity (no hopping).
 template <typename R, class SpinorT, class CloverT>
 __global__ void clover_kernel(Geom g, SpinorT out, SpinorT in, CloverT T, int parity, int gamma5)

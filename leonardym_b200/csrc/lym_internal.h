@@ -64,6 +64,11 @@ struct DslashParams {
 
 // kernels (lym_kernels.cu)
 void launch_dslash(const DslashParams &P, cudaStream_t st);
+// the second Schur launch of the even-odd CG on (gamma5 S)^2 with its vector work fused
+// (mode CG_NORM / CG_UPDATE of lym_dslash.cuh); p, x, r: one parity; state: the CGState;
+// partials: one double per block of the launch
+void launch_dslash_cg(const DslashParams &P, int mode, const Spinor &p, const Spinor &x, const Spinor &r, void *state,
+                      double *partials, unsigned int *counter, cudaStream_t st);
 void launch_clover(const Geom &g, int prec, const Spinor &out, const Spinor &in, const void *clover, int parity,
                    int gamma5, cudaStream_t st);
 void launch_pack(const Geom &g, const double *aos, const Spinor &full, cudaStream_t st);

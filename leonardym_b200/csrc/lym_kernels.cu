@@ -3,6 +3,7 @@
 #include "lym_blas.cuh"
 #include "lym_dslash.cuh"
 #include "lym_internal.h"
+#include "lym_solver_ops.cuh"
 
 namespace lym {
 
@@ -630,6 +631,86 @@ void launch_dslash(const DslashParams &P, cudaStream_t st)
         else
             run_dslash<float>(P, P.in.h(), P.out.h(), P.y.h(), P.v2.h(), GaugeH6{(const __half2 *)U.h16, U.sign, s}, T,
                               st);
+    }
+}
+
+// ---------------------------------------------------- stencil + CG epilogue --
+struct CGAlphaFromNorm {  // alpha = |r|^2 / <p, A p> with <p, A p> = |Q p|^2
+    CGState *s;
+    LYM_D void operator()(double qq) const { s->alpha = make_double2(s->rr / qq, 0.0); }
+};
+template <class Upd> struct CGUpdateFin {  // the scalar step of OpCGUpdate
+    Upd u;
+    LYM_D void operator()(double rr) const
+    {
+        const double t[1] = {rr};
+        u.finalize(t);
+    }
+};
+
+template <typename R, class S, class SX, class SR, class G, class C>
+static void run_dslash_cg(const DslashParams &P, int mode, const S &in, const S &out, const S &y, const S &p,
+                          const SX &x, const SR &r, const G &U, const C &T, void *state, double *partials,
+                          unsigned int *counter, cudaStream_t st)
+{
+    DslashArg<S, G, C> a;
+    a.g = P.g;
+    a.in = in;
+    a.out = out;
+    a.y = y;
+    a.v2 = p;
+    a.U = U;
+    a.T = T;
+    a.parity = P.parity;
+    a.gamma5 = 1;
+    a.has_v2 = 0;
+    a.has_clover = P.clover != nullptr;
+    a.a = P.a;
+    a.b = P.b;
+    a.alpha_re = a.alpha_im = 0.0;
+    a.skip_if = P.skip_if;
+    CGState *cs = (CGState *)state;
+    const int nb = nblocks(P.g.Vh, 128);
+    if (mode == CG_NORM) {
+        CGEpilogue<SX, SR, CGAlphaFromNorm> f{x, r, &cs->alpha, CGAlphaFromNorm{cs}, partials, counter};
+        dslash_cg_kernel<R, CG_NORM><<<nb, 128, 0, st>>>(a, f);
+    } else {
+        typedef OpCGUpdate<SX, S, SR, S> Upd;
+        CGEpilogue<SX, SR, CGUpdateFin<Upd>> f{x, r, &cs->alpha, CGUpdateFin<Upd>{Upd{x, p, r, p, cs}}, partials,
+                                                counter};
+        dslash_cg_kernel<R, CG_UPDATE><<<nb, 128, 0, st>>>(a, f);
+    }
+}
+
+void launch_dslash_cg(const DslashParams &P, int mode, const Spinor &p, const Spinor &x, const Spinor &r, void *state,
+                      double *partials, unsigned int *counter, cudaStream_t st)
+{
+    const GaugeDev &U = *P.U;
+    const int s = P.g.stride;
+    if (P.prec == PREC_D) {
+        CloverD T{(const double2 *)P.clover, s};
+        if (P.rep == REP_SU3)
+            run_dslash_cg<double>(P, mode, P.in.d(), P.out.d(), P.y.d(), p.d(), x.d(), r.d(),
+                                  GaugeD18{(const double2 *)U.d64, s}, T, state, partials, counter, st);
+        else
+            run_dslash_cg<double>(P, mode, P.in.d(), P.out.d(), P.y.d(), p.d(), x.d(), r.d(),
+                                  GaugeD9{(const double *)U.d64, s}, T, state, partials, counter, st);
+    } else if (P.prec == PREC_F) {
+        CloverF T{(const float4 *)P.clover, s};
+        if (P.rep == REP_SU3)
+            run_dslash_cg<float>(P, mode, P.in.f(), P.out.f(), P.y.f(), p.f(), x.f(), r.f(),
+                                 GaugeF12{(const float4 *)U.f32, U.sign, s}, T, state, partials, counter, st);
+        else
+            run_dslash_cg<float>(P, mode, P.in.f(), P.out.f(), P.y.f(), p.f(), x.f(), r.f(),
+                                 GaugeF6{(const float2 *)U.f32, U.sign, s}, T, state, partials, counter, st);
+    } else {
+        CloverH T{(const uint2 *)P.clover, s};
+        if (P.rep == REP_SU3)
+            run_dslash_cg<float>(P, mode, P.in.h(), P.out.h(), P.y.h(), p.h(), x.f(), r.f(),
+                                 GaugeH12{(const uint2 *)U.h16, U.sign, s}, T, state, partials, counter, st);
+        else
+            run_dslash_cg<float>(P, mode, P.in.h(), P.out.h(), P.y.h(), p.h(), x.f(), r.f(),
+                                 GaugeH6{(const __half2 *)U.h16, U.sign, s}, T, state, partials, counter, st);
     }
 }
 

@@ -692,7 +692,7 @@ struct MsFlushArg {
 
 constexpr int kMsFlushThreads = 256;
 
-__global__ void __launch_bounds__(kMsFlushThreads) ms_flush_kernel(MsFlushArg a)
+static __global__ void __launch_bounds__(kMsFlushThreads) ms_flush_kernel(MsFlushArg a)
 {
     __shared__ float cxs[kMaxShifts][kMsWin + 1], cps[kMaxShifts][kMsWin + 1];
     __shared__ int fl[kMaxShifts];
@@ -745,7 +745,7 @@ __global__ void __launch_bounds__(kMsFlushThreads) ms_flush_kernel(MsFlushArg a)
 }
 
 // start a new window (after the flush)
-__global__ void ms_window_reset_kernel(MultishiftState *s, int nshift)
+static __global__ void ms_window_reset_kernel(MultishiftState *s, int nshift)
 {
     const int i = threadIdx.x;
     if (i < nshift) {

@@ -88,3 +88,46 @@ def test_server_budget_too_small_fails_request(links):
             srv.wait(t)
     finally:
         srv.close()
+
+
+def test_server_mix_with_a_16c32_field(links, oracle):
+    """A 16^3 x 32 field among the small ones: its requests and the small fields' requests
+    are batched in the same server (one lane per field, overlapping on the device); every
+    result meets the oracle's 1e-10 true residual and equals the same source solved alone."""
+    big_key, big = 4, ((16, 16, 16, 32), "su3", 0.25, 14)
+    big_links = synth.fermion_links(big[0], big[1], big[2], big[3])
+    rng = np.random.default_rng(8)
+    reqs = [(1, 0.125, 1.0, [synth.gaussian_spinor(FIELDS[1][0], 3, 2000 + j) for j in range(3)]),
+            (big_key, 0.13, 1.7, [synth.gaussian_spinor(big[0], 3, 2100 + j) for j in range(3)]),
+            (2, 0.175, 1.5, [synth.gaussian_spinor(FIELDS[2][0], 3, 2200 + j) for j in range(2)]),
+            (big_key, float(rng.uniform(0.12, 0.135)), 1.7, [synth.gaussian_spinor(big[0], 3, 2300)]),
+            (3, 0.13, 1.2, [synth.gaussian_spinor(FIELDS[3][0], 3, 2400 + j) for j in range(4)])]
+    srv = SolveServer(batch=8, precision="single", solver="bicgstab")
+    try:
+        for key, (dims, rep, _, _) in FIELDS.items():
+            srv.add_gauge(key, dims, rep, links[key])
+        srv.add_gauge(big_key, big[0], big[1], big_links)
+        tickets = [srv.submit(key, kappa, csw, srcs) for key, kappa, csw, srcs in reqs]
+        results = [srv.wait(t, timeout=600) for t, _ in tickets]
+    finally:
+        srv.close()
+    all_links = dict(links)
+    all_links[big_key] = big_links
+    dims_of = {k: v[0] for k, v in FIELDS.items()}
+    dims_of[big_key] = big[0]
+    rep_of = {k: v[1] for k, v in FIELDS.items()}
+    rep_of[big_key] = big[1]
+    for (key, kappa, csw, srcs), (t, sols), (ok, st) in zip(reqs, tickets, results):
+        assert ok and st.status == 0 and st.max_true_residual <= 1e-10
+        D = oracle.Operator(oracle.Geometry(dims_of[key]), all_links[key], "Improved", kappa, csw, False)
+        lat = L.Lattice(dims_of[key], rep_of[key])
+        try:
+            op = L.ImprovedDiracWilsonOperator(lat, kappa, csw, gamma5=False)
+            op.setLattice(all_links[key])
+            for b, x in zip(srcs, sols):
+                assert np.linalg.norm(b - D.multiply(x)) / np.linalg.norm(b) <= 1e-10
+                alone = lat.new_vector()
+                assert L.EvenOddBiCGStab("single", 1e-10).solve(op, b, alone)
+                assert rel(x, alone) < 1e-8
+        finally:
+            lat.close()
