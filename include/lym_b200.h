@@ -355,8 +355,11 @@ int lym_gauge_read(lym_context *ctx, int gauge_id, int format, const char *direc
  * field are continuously batched: they enter free slots of the running batch as earlier
  * ones finish, whatever their kappa.  A request's clover term is built when its first
  * source is admitted and freed with its last; a new clover term is admitted only while
- * the server's device memory stays within hbm_budget_bytes (0 = no limit).  Host source /
- * solution buffers must stay valid until lym_server_wait returns for the ticket. */
+ * the server's device memory stays within hbm_budget_bytes (0 = no limit).  Each field's
+ * lane copies sources in and solutions out on a second thread through 4 + 4 device staging
+ * buffers (one full FP64 spinor each, counted in the server's device bytes), so the copies
+ * overlap the solves.  Host source / solution buffers must stay valid until
+ * lym_server_wait returns for the ticket. */
 typedef struct lym_server lym_server;
 typedef struct {
     double latency_s;          /* submit -> last solution written                   */

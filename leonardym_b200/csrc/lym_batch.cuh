@@ -228,15 +228,15 @@ struct SlotH {
         float m = 0.f;
 #pragma unroll
         for (int k = 0; k < 12; ++k) m = fmaxf(m, fmaxf(fabsf((float)s[k].re), fabsf((float)s[k].im)));
-        const float inv = m > 0.f ? 1.0f / m : 0.f;
+        const HalfScale sc(m);
         norm[((size_t)h << (lognp + 1)) + r] = m;
 #pragma unroll
         for (int w = 0; w < 6; ++w) {
             const size_t b = base(w, h);
-            hv[b] = __float2half_rn((float)s[2 * w].re * inv);
-            hv[b + 2] = __float2half_rn((float)s[2 * w].im * inv);
-            hv[b + 4] = __float2half_rn((float)s[2 * w + 1].re * inv);
-            hv[b + 6] = __float2half_rn((float)s[2 * w + 1].im * inv);
+            hv[b] = __float2half_rn(sc((float)s[2 * w].re));
+            hv[b + 2] = __float2half_rn(sc((float)s[2 * w].im));
+            hv[b + 4] = __float2half_rn(sc((float)s[2 * w + 1].re));
+            hv[b + 6] = __float2half_rn(sc((float)s[2 * w + 1].im));
         }
     }
 };
@@ -267,17 +267,18 @@ struct BatchH {
             ma = fmaxf(ma, fmaxf(fabsf(x[c].re.x), fabsf(x[c].im.x)));
             mb = fmaxf(mb, fmaxf(fabsf(x[c].re.y), fabsf(x[c].im.y)));
         }
-        const float2 inv = make_float2(ma > 0.f ? 1.0f / ma : 0.f, mb > 0.f ? 1.0f / mb : 0.f);
+        const HalfScale sa(ma), sb(mb);
+        const float2 pre = make_float2(sa.pre, sb.pre), inv = make_float2(sa.inv, sb.inv);
         norm[((unsigned)h << lognp) + q] = make_float2(ma, mb);
         const unsigned b = at(0, h, q), s = (unsigned)stride << lognp;
 #pragma unroll
         for (int w = 0; w < 6; ++w) {
             int4 u;
             __half2 *hp = reinterpret_cast<__half2 *>(&u);
-            hp[0] = __float22half2_rn(mul2(x[2 * w].re, inv));
-            hp[1] = __float22half2_rn(mul2(x[2 * w].im, inv));
-            hp[2] = __float22half2_rn(mul2(x[2 * w + 1].re, inv));
-            hp[3] = __float22half2_rn(mul2(x[2 * w + 1].im, inv));
+            hp[0] = __float22half2_rn(mul2(mul2(x[2 * w].re, pre), inv));
+            hp[1] = __float22half2_rn(mul2(mul2(x[2 * w].im, pre), inv));
+            hp[2] = __float22half2_rn(mul2(mul2(x[2 * w + 1].re, pre), inv));
+            hp[3] = __float22half2_rn(mul2(mul2(x[2 * w + 1].im, pre), inv));
             v[b + w * s] = u;
         }
     }

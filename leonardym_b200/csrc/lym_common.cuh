@@ -152,6 +152,19 @@ struct SpinorF {  // FP32: 6 x float4 words (two complex per word)
 };
 
 // FP16 spinor with one FP32 norm per site: value = half * norm
+// v / m for the FP16 storage of a site whose largest magnitude is m (|v| <= m): 1 / m
+// overflows FP32 when m is subnormal (the far tail of a point-source solve on a large
+// lattice), so such a site is first scaled by 2^64, exactly.
+struct HalfScale {
+    float pre, inv;
+    LYM_D explicit HalfScale(float m)
+    {
+        pre = (m > 0.f && m < 1.17549435e-38f) ? 18446744073709551616.f : 1.f;
+        inv = m > 0.f ? 1.0f / (m * pre) : 0.f;
+    }
+    LYM_D float operator()(float v) const { return (v * pre) * inv; }
+};
+
 struct SpinorH {
     int4 *v;       // 3 words of 8 halves
     float *norm;
@@ -177,15 +190,14 @@ struct SpinorH {
         float m = 0.f;
 #pragma unroll
         for (int k = 0; k < 12; ++k) m = fmaxf(m, fmaxf(fabsf((float)s[k].re), fabsf((float)s[k].im)));
-        const float inv = m > 0.f ? 1.0f / m : 0.f;
+        const HalfScale sc(m);
         norm[h] = m;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             int4 w;
             __half2 *hp = reinterpret_cast<__half2 *>(&w);
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-                hp[j] = __floats2half2_rn((float)s[4 * k + j].re * inv, (float)s[4 * k + j].im * inv);
+            for (int j = 0; j < 4; ++j) hp[j] = __floats2half2_rn(sc((float)s[4 * k + j].re), sc((float)s[4 * k + j].im));
             v[(size_t)k * stride + h] = w;
         }
     }
