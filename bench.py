@@ -38,6 +38,7 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "which": "fallback"}
 # clover term (out_o = T_oo y_o - kappa^2 H_oe a_e): 8 links (+ 2 sign-table bytes for the
 # reconstructed formats), 1 neighbour spinor (each read once), the y spinor, T_oo, the output
 STENCIL_BYTES = {0: 8 * 144 + 3 * 192 + 576, 1: 8 * 48 + 2 + 3 * 96 + 288, 2: 8 * 24 + 2 + 3 * 52 + 144}
+STENCIL_BYTES_8REAL = 8 * 32 + 2 + 3 * 96 + 288  # FP32 with SU(3) links in 8 reals
 # the batched kernel reads links, sign bytes and T once per site for the whole batch and
 # three spinors (neighbour, y, out) per right-hand side
 STENCIL_SITE_BYTES = {1: 8 * 48 + 2 + 288, 2: 8 * 24 + 2 + 144}
@@ -567,9 +568,12 @@ def run_ours(args, world, rank, local):
     achieved = bytes_launch / (ms.value * 1e-3) / 1e9
     pk = peaks()
     traffic = traffic_from_profiles(sprec, args.batch)
-    ms1, ms64 = C.c_double(0), C.c_double(0)
+    ms1, ms64, ms8 = C.c_double(0), C.c_double(0), C.c_double(0)
     lib.lym_time_stencil(ctx, opid, sprec, 0, 30, C.byref(ms1))
     lib.lym_time_stencil(ctx, opid, 0, 0, 20, C.byref(ms64))
+    lib.lym_set_link_format(ctx, 8)
+    lib.lym_time_stencil(ctx, opid, 1, 0, 30, C.byref(ms8))
+    lib.lym_set_link_format(ctx, 12)
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
@@ -628,7 +632,10 @@ def run_ours(args, world, rank, local):
                      "peak_source": f"{pk['which']} hbm_gbs",
                      "gflops": STENCIL_FLOPS * Vh * args.batch / (ms.value * 1e-3) / 1e9,
                      "single_rhs_kernel_gbs": STENCIL_BYTES[sprec] * Vh / (ms1.value * 1e-3) / 1e9,
-                     "fp64_single_rhs_kernel_gbs": STENCIL_BYTES[0] * Vh / (ms64.value * 1e-3) / 1e9},
+                     "fp64_single_rhs_kernel_gbs": STENCIL_BYTES[0] * Vh / (ms64.value * 1e-3) / 1e9,
+                     "single_rhs_kernel_8real_links_gbs": STENCIL_BYTES_8REAL * Vh / (ms8.value * 1e-3) / 1e9,
+                     "single_rhs_kernel_us": {"fp32_12real": ms1.value * 1e3, "fp32_8real": ms8.value * 1e3,
+                                              "fp64": ms64.value * 1e3}},
         "clocks": clocks,
         "gpu_launches": launches,
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": nrhs * nbytes,

@@ -426,6 +426,17 @@ int lym_multiply_batch(lym_context *ctx, int prec, int nrhs, const int *op_ids, 
 int lym_set_batch_tile(lym_context *ctx, int by, int bz, int minb);
 int lym_get_batch_tile(lym_context *ctx, int prec, int batch, int has_clover, int *by, int *bz, int *minb);
 
+/* ---- FP32 link format (the north star's optional 12- or 8-real gauge reconstruction) ----
+ * The FP32 single-RHS stencils (the inner iterations of the mixed-precision solvers) read
+ * SU(3) links as 12 reals (rows 0 and 1, row 2 from their cross product; the default) or
+ * 8 reals (a2, a3, b1 and the phases of a1, c1; the rest from unitarity), both with the
+ * sign table that keeps antiperiodic links exact.  8 reals move 256 instead of 384 link bytes
+ * per half-site at the price of two sincos, two square roots and a division per link;
+ * their rounding grows as |U_00| nears 1.  Applies to every gauge field of the context;
+ * SU(2) adjoint links keep their 6-real format (LYM_ERR_UNSUPPORTED for 8).  The batched
+ * stencil reads 12 reals. */
+int lym_set_link_format(lym_context *ctx, int reals);
+
 /* ---- fault injection on the host (no reference counterpart: a test hook) -----------
  * The next n device allocations of the context (of the server lane holding gauge field
  * `key`) report failure as a cudaMalloc that returned cudaErrorMemoryAllocation would:

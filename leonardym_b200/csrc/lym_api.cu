@@ -90,6 +90,7 @@ struct lym_context {
     double engine_stats[7] = {};      // block solves: lym_context_engine_stats
     bool capturing = false;
     int inject_alloc_failures = 0;  // the next n device allocations report failure (tests)
+    int link_reals = 12;            // FP32 SU(3) link format of the single-RHS stencils: 12 or 8
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -2461,6 +2462,7 @@ void lym_context_destroy(lym_context *c)
         cudaFree(kv.second.dev.f32);
         cudaFree(kv.second.dev.h16);
         cudaFree(kv.second.dev.sign);
+        cudaFree(kv.second.dev.f32r8);
     }
     for (auto &s : c->pool) cudaFree(s.v);
     for (auto &b : c->blocks) cudaFree(b.second);
@@ -2521,6 +2523,8 @@ static int gauge_store(lym_context *c, int id, const double *links, bool device_
         e.dev.f32 = dev_alloc(c, f32);
         e.dev.h16 = dev_alloc(c, h16);
         e.dev.sign = (uint8_t *)dev_alloc(c, 2 * s);
+        e.dev.f32r8 = dev_alloc(c, 2 * 4 * 2 * s * sizeof(float4));  // written for SU(3) only
+        e.dev.link_reals = c->link_reals;
         ge = &(c->gauges[id] = e);
     } else {
         ge = &it->second;
@@ -2593,6 +2597,7 @@ int lym_gauge_evict(lym_context *c, int id)
         dev_free(c, it->second.dev.f32, su3 ? 2 * 4 * 3 * s * sizeof(float4) : 2 * 4 * 3 * s * sizeof(float2));
         dev_free(c, it->second.dev.h16, su3 ? 2 * 4 * 3 * s * sizeof(uint2) : 2 * 4 * 3 * s * sizeof(__half2));
         dev_free(c, it->second.dev.sign, 2 * s);
+        dev_free(c, it->second.dev.f32r8, 2 * 4 * 2 * s * sizeof(float4));
         c->gauges.erase(it);
         return LYM_OK;
     });
@@ -3800,6 +3805,18 @@ int lym_get_batch_tile(lym_context *c, int prec, int batch, int has_clover, int 
         *by = t.by;
         *bz = t.bz;
         *minb = t.minb;
+        return LYM_OK;
+    });
+}
+
+int lym_set_link_format(lym_context *c, int reals)
+{
+    return guarded(c, [&]() {
+        if (reals != 12 && reals != 8) fail(c, LYM_ERR_ARGUMENT, "link format: 12 or 8 reals");
+        if (reals == 8 && c->rep != REP_SU3)
+            fail(c, LYM_ERR_UNSUPPORTED, "the 8-real link format is for SU(3) fundamental links");
+        c->link_reals = reals;
+        for (auto &kv : c->gauges) kv.second.dev.link_reals = reals;
         return LYM_OK;
     });
 }

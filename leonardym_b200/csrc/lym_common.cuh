@@ -353,6 +353,46 @@ struct GaugeF12 {
     }
 };
 
+// FP32 complex, 8 reals (SU(3) only): for V = s U in SU(3) (s from the sign table), the
+// words (a2, a3) and (b1, arg a1, arg c1), with a, b, c the rows of V.  Rebuilt from the
+// unitarity of V: |a1|^2 = 1 - |a2|^2 - |a3|^2 = 1 - N (row a), |c1|^2 = N - |b1|^2
+// (column 1), and with a = conj(b x c) and the orthogonality of columns 1, 2 and 1, 3 the
+// 2 x 2 systems for (b2, c2) and (b3, c3), whose determinants are -N and N:
+//   b2 = -(conj(c1 a3) + conj(a1) a2 b1) / N,   c2 = (conj(b1 a3) - conj(a1) a2 c1) / N,
+//   b3 =  (conj(c1 a2) - conj(a1) a3 b1) / N,   c3 = -(conj(b1 a2) + conj(a1) a3 c1) / N.
+// N is 1 - |a1|^2, so the rounding of the rebuilt entries grows as |a1| nears 1.
+struct GaugeF8 {
+    typedef LinkC<float> Link;
+    const float4 *u;      // [parity][mu][2][stride]
+    const uint8_t *sign;  // [parity][stride]
+    int stride;
+    LYM_D void load(int p, int mu, int h, Link &U) const
+    {
+        const float4 *b = u + ((size_t)(p * 4 + mu) * 2) * stride + h;
+        const float4 w0 = __ldg(b), w1 = __ldg(b + stride);
+        const cx<float> a2 = {w0.x, w0.y}, a3 = {w0.z, w0.w}, b1 = {w1.x, w1.y};
+        const float N = w0.x * w0.x + w0.y * w0.y + w0.z * w0.z + w0.w * w0.w;
+        float sa, ca, sc, cc;
+        sincosf(w1.z, &sa, &ca);
+        sincosf(w1.w, &sc, &cc);
+        const float ra = sqrtf(fmaxf(1.f - N, 0.f)), rc = sqrtf(fmaxf(N - (b1.re * b1.re + b1.im * b1.im), 0.f));
+        const cx<float> a1 = {ra * ca, ra * sa}, c1 = {rc * cc, rc * sc};
+        const float inv = 1.f / N;
+        const cx<float> t2 = conj(a1) * a2, t3 = conj(a1) * a3;
+        const float s = ((__ldg(sign + (size_t)p * stride + h) >> mu) & 1) ? -1.f : 1.f;
+        const float si = s * inv;
+        U.u[0][0] = s * a1;
+        U.u[0][1] = s * a2;
+        U.u[0][2] = s * a3;
+        U.u[1][0] = s * b1;
+        U.u[2][0] = s * c1;
+        U.u[1][1] = -si * (conj(c1 * a3) + t2 * b1);
+        U.u[1][2] = si * (conj(c1 * a2) - t3 * b1);
+        U.u[2][1] = si * (conj(b1 * a3) - t2 * c1);
+        U.u[2][2] = -si * (conj(b1 * a2) + t3 * c1);
+    }
+};
+
 // FP32 real, 6 reals (adjoint): rows 0 and 1; row 2 = sign * (row0 x row1)
 struct GaugeF6 {
     typedef LinkR<float> Link;

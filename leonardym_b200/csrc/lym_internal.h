@@ -34,6 +34,10 @@ struct GaugeDev {
     void *f32 = nullptr;       // FP32 reconstructed: float4[2][4][3][stride] or float2[2][4][3][stride]
     void *h16 = nullptr;       // FP16 reconstructed: uint2[2][4][3][stride] or half2[2][4][3][stride]
     uint8_t *sign = nullptr;   // [2][stride]
+    // FP32 SU(3) links in 8 reals (GaugeF8): float4[2][4][2][stride]; link_reals 12 or 8 picks
+    // the format of the FP32 single-RHS stencils (lym_set_link_format)
+    void *f32r8 = nullptr;
+    int link_reals = 12;
     bool recon_ok = false;
 };
 

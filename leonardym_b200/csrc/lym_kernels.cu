@@ -162,7 +162,8 @@ LYM_D void load_link_d(const Geom &g, int rep, const void *d64, int p, int mu, i
 // Compress the FP64 links to the reconstructed FP32 / FP16 formats.  A link is
 // accepted when it is +-V with V special unitary (SU(3)) or special orthogonal
 // (adjoint); the sign goes to the sign table.
-__global__ void compress_gauge_kernel(Geom g, int rep, const void *d64, void *f32, void *h16, uint8_t *sign, int *err)
+__global__ void compress_gauge_kernel(Geom g, int rep, const void *d64, void *f32, void *h16, uint8_t *sign, int *err,
+                                      float4 *f32r8)
 {
     const int h = blockIdx.x * blockDim.x + threadIdx.x;
     const int p = blockIdx.y;
@@ -194,6 +195,12 @@ __global__ void compress_gauge_kernel(Geom g, int rep, const void *d64, void *f3
             F[w0] = make_float4(u[0][0].re, u[0][0].im, u[0][1].re, u[0][1].im);
             F[w0 + g.stride] = make_float4(u[0][2].re, u[0][2].im, u[1][0].re, u[1][0].im);
             F[w0 + 2 * (size_t)g.stride] = make_float4(u[1][1].re, u[1][1].im, u[1][2].re, u[1][2].im);
+            // 8 reals of V = s U (GaugeF8): (a2, a3), (b1, arg a1, arg c1)
+            const double sg = neg ? -1.0 : 1.0;
+            const size_t w8 = (size_t)(p * 4 + mu) * 2 * g.stride + h;
+            f32r8[w8] = make_float4(sg * u[0][1].re, sg * u[0][1].im, sg * u[0][2].re, sg * u[0][2].im);
+            f32r8[w8 + g.stride] = make_float4(sg * u[1][0].re, sg * u[1][0].im, atan2(sg * u[0][0].im, sg * u[0][0].re),
+                                               atan2(sg * u[2][0].im, sg * u[2][0].re));
             uint2 *H = (uint2 *)h16;
             double v[12] = {u[0][0].re, u[0][0].im, u[0][1].re, u[0][1].im, u[0][2].re, u[0][2].im,
                             u[1][0].re, u[1][0].im, u[1][1].re, u[1][1].im, u[1][2].re, u[1][2].im};
@@ -221,7 +228,7 @@ __global__ void compress_gauge_kernel(Geom g, int rep, const void *d64, void *f3
 void launch_compress_gauge(const Geom &g, GaugeDev &U, int *err, cudaStream_t st)
 {
     dim3 grid(nblocks(g.Vh, 128), 2);
-    compress_gauge_kernel<<<grid, 128, 0, st>>>(g, U.rep, U.d64, U.f32, U.h16, U.sign, err);
+    compress_gauge_kernel<<<grid, 128, 0, st>>>(g, U.rep, U.d64, U.f32, U.h16, U.sign, err, (float4 *)U.f32r8);
 }
 
 // Fundamental gauge links -> fermion links: the adjoint map for SU(2)
@@ -617,7 +624,10 @@ void launch_dslash(const DslashParams &P, cudaStream_t st)
             run_dslash<double>(P, P.in.d(), P.out.d(), P.y.d(), P.v2.d(), GaugeD9{(const double *)U.d64, s}, T, st);
     } else if (P.prec == PREC_F) {
         CloverF T{(const float4 *)P.clover, s};
-        if (P.rep == REP_SU3)
+        if (P.rep == REP_SU3 && U.link_reals == 8)
+            run_dslash<float>(P, P.in.f(), P.out.f(), P.y.f(), P.v2.f(), GaugeF8{(const float4 *)U.f32r8, U.sign, s}, T,
+                              st);
+        else if (P.rep == REP_SU3)
             run_dslash<float>(P, P.in.f(), P.out.f(), P.y.f(), P.v2.f(), GaugeF12{(const float4 *)U.f32, U.sign, s}, T,
                               st);
         else
@@ -697,7 +707,10 @@ void launch_dslash_cg(const DslashParams &P, int mode, const Spinor &p, const Sp
                                   GaugeD9{(const double *)U.d64, s}, T, state, partials, counter, st);
     } else if (P.prec == PREC_F) {
         CloverF T{(const float4 *)P.clover, s};
-        if (P.rep == REP_SU3)
+        if (P.rep == REP_SU3 && U.link_reals == 8)
+            run_dslash_cg<float>(P, mode, P.in.f(), P.out.f(), P.y.f(), p.f(), x.f(), r.f(),
+                                 GaugeF8{(const float4 *)U.f32r8, U.sign, s}, T, state, partials, counter, st);
+        else if (P.rep == REP_SU3)
             run_dslash_cg<float>(P, mode, P.in.f(), P.out.f(), P.y.f(), p.f(), x.f(), r.f(),
                                  GaugeF12{(const float4 *)U.f32, U.sign, s}, T, state, partials, counter, st);
         else

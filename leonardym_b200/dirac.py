@@ -78,6 +78,11 @@ class Lattice:
     def link_dtype(self):
         return np.complex128 if self.rep == "su3" else np.float64
 
+    def set_link_format(self, reals):
+        """FP32 SU(3) link format of the single-RHS stencils (the mixed solvers' inner
+        iterations): 12 reals (default) or 8 reals, for every gauge field of this lattice."""
+        _check(self._ptr, lib().lym_set_link_format(self._ptr, int(reals)))
+
     def upload(self, fermion_links, gauge_id=None):
         """Make a fermion link field resident; returns its id."""
         links = np.ascontiguousarray(fermion_links, dtype=self.link_dtype())

@@ -116,6 +116,46 @@ def test_sloppy_precision_stencil(setup, precision, tol, kind, oracle):
     assert rel(gpu.multiply_precision(x, precision), orc.multiply(x)) < tol
 
 
+@pytest.mark.parametrize("kind", ["DiracWilson", "Improved", "EvenOddImproved", "SquareImproved"])
+@pytest.mark.parametrize("gamma5", [True, False])
+def test_eight_real_links_stencil(setup, kind, gamma5, oracle):
+    """The FP32 stencil on SU(3) links stored in 8 reals (lym_set_link_format) against the FP64
+    oracle, 1e-6 as the 12-real format; SU(2) adjoint links refuse the format."""
+    lat = setup["lat"]
+    if setup["rep"] != "su3":
+        with pytest.raises(L.LymError):
+            lat.set_link_format(8)
+        return
+    gpu, orc = make(setup, kind, gamma5, oracle)
+    x = synth.gaussian_spinor(setup["dims"], 3, 15)
+    want = orc.multiply(x)
+    try:
+        lat.set_link_format(8)
+        e8 = rel(gpu.multiply_precision(x, "single"), want)
+    finally:
+        lat.set_link_format(12)
+    e12 = rel(gpu.multiply_precision(x, "single"), want)
+    print(f"{kind} gamma5={gamma5}: FP32 stencil error 8 reals {e8:.2e}, 12 reals {e12:.2e}")
+    assert e8 < 1e-6 and e12 < 1e-6
+
+
+def test_eight_real_links_mixed_solve(setup, oracle):
+    """The mixed-precision even-odd CG with its FP32 inner iterations on 8-real links still
+    reaches the FP64 true residual 1e-10 (re-measured with the oracle)."""
+    if setup["rep"] != "su3":
+        return
+    lat = setup["lat"]
+    gpu, orc = make(setup, "Improved", False, oracle)
+    b = synth.gaussian_spinor(setup["dims"], 3, 16)
+    x = lat.new_vector()
+    try:
+        lat.set_link_format(8)
+        assert L.EvenOddConjugateGradient("single", 1e-10).solve(gpu, b, x)
+    finally:
+        lat.set_link_format(12)
+    assert np.linalg.norm(b - orc.multiply(x)) / np.linalg.norm(b) <= 1e-10
+
+
 def test_neighbour_tables_bit_exact(setup, oracle):
     sup, sdn = setup["lat"].neighbour_tables()
     osup, osdn, _ = oracle.geom_tables(setup["dims"])
