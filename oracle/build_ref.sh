@@ -39,6 +39,11 @@ TUS=(
   program_options/StorageParameters.cpp
   hmc_forces/Force.cpp hmc_forces/FermionForce.cpp hmc_forces/DiracWilsonFermionForce.cpp
   hmc_forces/ImprovedFermionForce.cpp hmc_forces/OverlapFermionForce.cpp
+  correlators/MesonCorrelator.cpp fermion_measurements/ChiralCondensate.cpp
+  fermion_measurements/StochasticEstimator.cpp dirac_operators/Propagator.cpp io/GlobalOutput.cpp
+  utils/StoutSmearing.cpp actions/WilsonGaugeAction.cpp actions/GaugeAction.cpp actions/ImprovedGaugeAction.cpp
+  wilson_loops/Plaquette.cpp actions/Energy.cpp hmc_forces/GaugeForce.cpp
+  starters/ReadStartGaugeConfiguration.cpp io/OutputSweep.cpp Environment.cpp
 )
 build() {
   local name=$1; shift
@@ -55,9 +60,11 @@ build() {
   done
   wait
   g++ "${flags[@]}" -c "$HERE/ref_harness.cpp" -o "$objdir/ref_harness.o"
-  g++ -shared -fopenmp -o "$OUT/libleonard_ref_$name.so" "${objs[@]}" "$objdir/ref_harness.o"
+  g++ "${flags[@]}" -c "$HERE/ref_stubs.cpp" -o "$objdir/ref_stubs.o"
+  g++ -shared -fopenmp -Wl,--no-undefined -o "$OUT/libleonard_ref_$name.so" "${objs[@]}" "$objdir/ref_harness.o" \
+      "$objdir/ref_stubs.o"
 }
-COMMON=(-O2 -fPIC -fopenmp -std=c++17 -w -include ctime -include cstring -I"$HERE/eigen_shim" -I"$REF"
+COMMON=(-O2 -fPIC -fopenmp -std=c++17 -w -include ctime -include cstring -I"$HERE/eigen_shim" -I"$HERE/xdr_shim" -I"$REF"
         -DMBE="\"$REF/utils/MatrixBaseExtension.h\"" -DEIGEN -DMULTITHREADING)
 build su3 "${COMMON[@]}" -DNUMCOLORS=3
 build su2adj "${COMMON[@]}" -DNUMCOLORS=2 -DADJOINT

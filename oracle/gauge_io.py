@@ -4,8 +4,8 @@ starters/ReadStartGaugeConfiguration.cpp:51-480, writers io/OutputSweep.cpp:32-4
 process; XDR values as numpy big-endian types.  Links: complex128[V, 4, N, N] with
 [site, mu, j, i] = U_mu(site)(i, j), site t + Lt (z + Lz (y + Ly x)).
 
-Parity unpinned against the compiled reference: its readers and writers need an XDR
-library (rpc/xdr.h), which this image does not have."""
+Pinned to the reference's own reader and writer, compiled with the XDR shim of
+oracle/xdr_shim (tests/test_gauge_io.py)."""
 from __future__ import annotations
 
 import os

@@ -77,6 +77,10 @@ def lib(rep):
         L.ref_antiperiodic.argtypes = [ip, vp]
         if hasattr(L, "ref_to_adjoint"):
             L.ref_to_adjoint.argtypes = [i, vp, vp]
+        L.ref_meson_correlator.argtypes = [ip, dp, dp, vp, dp, i, vp]
+        L.ref_chiral_condensate.argtypes = [ip, dp, dp, vp, dp, i, i, i, C.c_uint, vp, vp]
+        L.ref_gauge_write.argtypes = [ip, i, C.c_char_p, C.c_char_p, i, vp, dp, dp]
+        L.ref_gauge_read.argtypes = [ip, i, C.c_char_p, C.c_char_p, i, vp, dp, dp]
         L.ref_bench_prepare.argtypes = [ip, dp, dp, vp]
         L.ref_bench_solve.argtypes = [dp, i, vp, vp, ip]
         L.ref_bench_release.argtypes = []
@@ -90,6 +94,32 @@ def _d(dims):
 
 def _p(a):
     return a.ctypes.data_as(C.c_void_p)
+
+
+FORMATS = {"leonard_format": 0, "muenster_format": 1}
+
+
+def _dirname(directory):
+    d = str(directory)
+    return (d if d.endswith(os.sep) else d + os.sep).encode()
+
+
+def gauge_write(rep, dims, format_name, directory, name, number, links, beta=0.0, kappa=0.0):
+    """io/OutputSweep.cpp's writer (one process) on fundamental links complex128[V, 4, N, N]
+    (N = 3 for the "su3" build, 2 for "su2adj"); the file number is `number`."""
+    links = np.ascontiguousarray(links, np.complex128)
+    rc = lib(rep).ref_gauge_write(_d(dims), FORMATS[format_name], _dirname(directory), str(name).encode(),
+                                  int(number), _p(links), float(beta), float(kappa))
+    assert rc == 0
+
+
+def gauge_read(rep, dims, format_name, directory, name, number, beta=0.0, kappa=0.0):
+    """ReadStartGaugeConfiguration::readConfiguration: (success, fundamental links)."""
+    n = 3 if rep.startswith("su3") else 2
+    links = np.zeros((int(np.prod(dims)), 4, n, n), np.complex128)
+    rc = lib(rep).ref_gauge_read(_d(dims), FORMATS[format_name], _dirname(directory), str(name).encode(),
+                                 int(number), _p(links), float(beta), float(kappa))
+    return rc == 1, links
 
 
 class Reference:
@@ -136,6 +166,29 @@ class Reference:
         rc = self.L.ref_solve(_d(self.dims), KIND[kind], kappa, csw, int(gamma5), _p(self.links), SOLVER[solver],
                               float(precision), int(max_steps), s.real, s.imag, _p(b), _p(x), C.byref(steps))
         return rc, x, steps.value
+
+    # the reference's propagator consumers on these links (Improved operator, default options)
+    def meson_correlator(self, kappa, csw, precision, max_steps):
+        """MesonCorrelator::execute: pion_exact, scalar_exact, ps_exact, pcac_mass per t."""
+        Lt = self.dims[3]
+        out = np.zeros(4 * Lt)
+        rc = self.L.ref_meson_correlator(_d(self.dims), float(kappa), float(csw), _p(self.links), float(precision),
+                                         int(max_steps), _p(out))
+        assert rc == 0
+        o = out.reshape(4, Lt)
+        return {"pion_exact": o[0], "scalar_exact": o[1], "ps_exact": o[2], "pcac_mass": o[3]}
+
+    def chiral_condensate(self, kappa, csw, precision, max_steps, n, connected, seed):
+        """ChiralCondensate::execute with n estimators from a seeded generator (one thread):
+        (mean, standard deviation) of condensate, pseudo-condensate, connected part and pion
+        norm (re, im each), and the real Z2 noise vectors the reference drew."""
+        out = np.zeros(16)
+        noise = np.zeros((n, self.V, 4, 3))
+        rc = self.L.ref_chiral_condensate(_d(self.dims), float(kappa), float(csw), _p(self.links), float(precision),
+                                          int(max_steps), int(n), int(bool(connected)), int(seed), _p(out),
+                                          _p(noise))
+        assert rc == 0
+        return out.reshape(8, 2), noise.astype(np.complex128)
 
     # the benchmark's CPU baseline: PreconditionedBiCGStab::solve on one held Improved operator
     def bench_prepare(self, kappa, csw):

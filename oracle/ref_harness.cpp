@@ -27,6 +27,13 @@
 #include "inverters/ChronologicalMultishiftSolver.h"
 #include "inverters/PreconditionedBiCGStab.h"
 #include "utils/ConvertLattice.h"
+#include "correlators/MesonCorrelator.h"
+#include "io/OutputSweep.h"
+#include "starters/ReadStartGaugeConfiguration.h"
+#include "fermion_measurements/ChiralCondensate.h"
+#include <omp.h>
+#include <sstream>
+#include <string>
 
 using namespace Update;
 
@@ -366,6 +373,195 @@ int ref_bench_solve(double precision, int max_steps, const double *src, double *
     const bool ok = pb.solve(g_bench_op, b, x);
     *steps = pb.getLastSteps();
     if (sol) store(x, sol);
+    return ok ? 1 : 0;
+}
+
+// ---- the reference's propagator consumers ----------------------------------------------
+// MesonCorrelator::execute and ChiralCondensate::execute on an Environment holding the given
+// fermion links, with their registered default options and the Improved operator of kappa,
+// c_sw.  Their results reach only std::cout (and GlobalOutput, off without a format), so the
+// stream is captured with 17 significant digits and parsed.
+namespace {
+
+std::map<std::string, Option> consumer_options(double kappa, double csw)
+{
+    std::map<std::string, Option> m;
+    MesonCorrelator::registerParameters(m);
+    ChiralCondensate::registerParameters(m);
+    m["dirac_operator"] = Option("dirac_operator", std::string("Improved"), "");
+    m["kappa"] = Option("kappa", kappa, "");
+    m["csw"] = Option("csw", csw, "");
+    return m;
+}
+
+struct CoutCapture {
+    std::ostringstream ss;
+    std::streambuf *old;
+    std::streamsize prec;
+    CoutCapture() : old(std::cout.rdbuf(ss.rdbuf())), prec(std::cout.precision(17)) {}
+    ~CoutCapture()
+    {
+        std::cout.rdbuf(old);
+        std::cout.precision(prec);
+    }
+};
+
+struct SeededChiralCondensate : public ChiralCondensate {
+    // one generator per OpenMP thread, as the reference's constructor makes them, seeded
+    void seed(unsigned int s)
+    {
+        // the integer generators hold a reference to their engine: reseeding it is enough
+        for (int i = 0; i < omp_get_max_threads(); ++i) randomGenerator[i]->seed(s + 7919u * (unsigned int)i);
+    }
+};
+
+}  // namespace
+
+// out[4][Lt]: pion, scalar, PS correlators (with the 4 kappa^2 factor) and PCAC mass per t
+int ref_meson_correlator(const int dims[4], double kappa, double csw, const double *links, double precision,
+                         int max_steps, double *out)
+{
+    init_layout(dims);
+    std::map<std::string, Option> opts = consumer_options(kappa, csw);
+    opts["MesonCorrelator::inverter_precision"] = Option("MesonCorrelator::inverter_precision", precision, "");
+    opts["MesonCorrelator::inverter_max_steps"] = Option("MesonCorrelator::inverter_max_steps", max_steps, "");
+    environment_t env(opts);
+    load(env.fermionicLinkConfiguration, links);
+    env.measurement = true;
+    std::string text;
+    {
+        CoutCapture cap;
+        MesonCorrelator mc;
+        mc.execute(env);
+        text = cap.ss.str();
+    }
+    const char *keys[4] = {"Pion Exact Correlator at t", "Scalar Exact Correlator at t", "PS Exact Correlator at t",
+                           "PCAC mass at t"};
+    const int Lt = dims[3];
+    for (int k = 0; k < 4; ++k) {
+        std::vector<double> v;
+        std::istringstream in(text);
+        std::string line;
+        while (std::getline(in, line))
+            if (line.find(keys[k]) != std::string::npos) v.push_back(std::strtod(line.c_str() + line.rfind(" is ") + 4, nullptr));
+        if ((int)v.size() != Lt) return -1;
+        for (int t = 0; t < Lt; ++t) out[k * Lt + t] = v[t];
+    }
+    return 0;
+}
+
+// ChiralCondensate::execute with n estimators on one OpenMP thread, its generator seeded;
+// out[16]: mean and standard deviation of the condensate (re, im), pseudo-condensate (re, im),
+// connected part (re, im), pion norm (re, im); noise[n][V][4][3] (if not null): the real Z2
+// noise the same seed gives, in the reference's order of drawing
+int ref_chiral_condensate(const int dims[4], double kappa, double csw, const double *links, double precision,
+                          int max_steps, int n, int connected, unsigned int seed, double *out, double *noise)
+{
+    init_layout(dims);
+    std::map<std::string, Option> opts = consumer_options(kappa, csw);
+    opts["ChiralCondensate::inverter_precision"] = Option("ChiralCondensate::inverter_precision", precision, "");
+    opts["ChiralCondensate::inverter_max_steps"] = Option("ChiralCondensate::inverter_max_steps", max_steps, "");
+    opts["ChiralCondensate::number_stochastic_estimators"] =
+        Option("ChiralCondensate::number_stochastic_estimators", n, "");
+    opts["ChiralCondensate::measure_condensate_connected"] =
+        Option("ChiralCondensate::measure_condensate_connected", std::string(connected ? "true" : "false"), "");
+    environment_t env(opts);
+    load(env.fermionicLinkConfiguration, links);
+    env.measurement = true;
+    const int threads = omp_get_max_threads();
+    omp_set_num_threads(1);  // one generator, drawn site after site
+    std::string text;
+    {
+        CoutCapture cap;
+        SeededChiralCondensate cc;
+        cc.seed(seed);
+        cc.execute(env);
+        text = cap.ss.str();
+    }
+    if (noise) {
+        random_generator_t g(seed);
+        random_integer_generator_t ri = RandomSeed::getRandomIntegerGenerator(g);
+        const size_t count = (size_t)n * Lattice::LocalLayout::localsize * 4 * diracVectorLength;
+        for (size_t k = 0; k < count; ++k) noise[k] = ri() == 0 ? -1.0 : 1.0;
+    }
+    omp_set_num_threads(threads);
+    const char *keys[8] = {"Chiral condensate is (re)", "Chiral condensate is (im)", "Pseudo condensate is (re)",
+                           "Pseudo condensate is (im)", "Connected chiral condensate susceptibility is (re)",
+                           "Connected chiral condensate susceptibility is (im)", "Pion norm is (re)",
+                           "Pion norm is (im)"};
+    for (int k = 0; k < 8; ++k) {
+        std::istringstream in(text);
+        std::string line;
+        bool found = false;
+        while (std::getline(in, line)) {
+            const size_t p = line.find(keys[k]);
+            if (p == std::string::npos) continue;
+            const char *c = line.c_str() + p + std::strlen(keys[k]);
+            char *end = nullptr;
+            out[2 * k] = std::strtod(c, &end);
+            const char *pm = std::strstr(end, "+/-");
+            out[2 * k + 1] = pm ? std::strtod(pm + 3, nullptr) : 0.0;
+            found = true;
+        }
+        if (!found) return -1;
+    }
+    return 0;
+}
+
+// ---- the reference's gauge-configuration files ------------------------------------------
+// OutputSweep::execute writes, ReadStartGaugeConfiguration::readConfiguration reads the
+// fundamental links (extended_gauge_lattice_t raw storage) of one process; format 0
+// leonard_format, 1 muenster_format; `directory` ends with a separator; the file number is
+// OutputSweep's sweep + output_offset (sweep 0 here).
+namespace {
+std::map<std::string, Option> file_options(int format, const char *directory, const char *name, int number,
+                                           double beta, double kappa)
+{
+    std::map<std::string, Option> m;
+    const std::string fmt = format ? "muenster_format" : "leonard_format";
+    m["output_format_name"] = Option("output_format_name", fmt, "");
+    m["input_format_name"] = Option("input_format_name", fmt, "");
+    m["output_configuration_name"] = Option("output_configuration_name", std::string(name), "");
+    m["input_name"] = Option("input_name", std::string(name), "");
+    m["output_directory_configurations"] = Option("output_directory_configurations", std::string(directory), "");
+    m["input_directory_configurations"] = Option("input_directory_configurations", std::string(directory), "");
+    m["output_offset"] = Option("output_offset", number, "");
+    m["input_number"] = Option("input_number", number, "");
+    m["beta"] = Option("beta", beta, "");
+    m["kappa"] = Option("kappa", kappa, "");
+    // Environment::synchronize after reading: no smearing, the fermion links' boundary
+    m["stout_smearing_levels"] = Option("stout_smearing_levels", 0, "");
+    m["boundary_conditions"] = Option("boundary_conditions", std::string("fermion_antiperiodic"), "");
+    return m;
+}
+}  // namespace
+
+int ref_gauge_write(const int dims[4], int format, const char *directory, const char *name, int number,
+                    const double *links, double beta, double kappa)
+{
+    init_layout(dims);
+    environment_t env(file_options(format, directory, name, number, beta, kappa));
+    load(env.gaugeLinkConfiguration, links);
+    env.sweep = 0;
+    std::ostringstream sink;
+    std::streambuf *old = std::cout.rdbuf(sink.rdbuf());
+    OutputSweep out;
+    out.execute(env);
+    std::cout.rdbuf(old);
+    return 0;
+}
+
+// returns 1 when the reference's reader reports success
+int ref_gauge_read(const int dims[4], int format, const char *directory, const char *name, int number, double *links,
+                   double beta, double kappa)
+{
+    init_layout(dims);
+    environment_t env(file_options(format, directory, name, number, beta, kappa));
+    std::ostringstream sink;
+    std::streambuf *old = std::cout.rdbuf(sink.rdbuf());
+    const bool ok = ReadStartGaugeConfiguration::readConfiguration(env, number);
+    std::cout.rdbuf(old);
+    store(env.gaugeLinkConfiguration, links);
     return ok ? 1 : 0;
 }
 

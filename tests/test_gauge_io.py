@@ -79,3 +79,43 @@ def test_load_configuration_on_gpu(tmp_path, rep, nc):
         assert np.array_equal(a.multiply(x), b.multiply(x))
     finally:
         lat.close()
+
+
+# ---- pinned to the reference's own reader and writer (compiled with an XDR shim) ----------
+def _needs_reference():
+    from oracle import ref as R
+    if not (R.available("su3") and R.available("su2adj")):
+        pytest.skip("compiled reference not built")
+    return R
+
+
+@pytest.mark.parametrize("nc,fmt", [(3, "leonard_format"), (2, "leonard_format"), (2, "muenster_format"),
+                                    (3, "muenster_format")])
+def test_files_of_the_reference_load_here_and_back(tmp_path, nc, fmt):
+    """A configuration written by the reference's OutputSweep reads back here (the library's
+    host reader and the oracle restatement) as the reference's own reader reads it, and one
+    written here reads in the reference's ReadStartGaugeConfiguration."""
+    R = _needs_reference()
+    rep = "su3" if nc == 3 else "su2adj"
+    U = fund(nc)
+    beta, kappa = (5.6, 0.13) if nc == 3 else (2.25, 0.18)
+    R.gauge_write(rep, DIMS, fmt, tmp_path, "refcfg", 5, U, beta, kappa)
+    ok, Ur = R.gauge_read(rep, DIMS, fmt, tmp_path, "refcfg", 5, beta, kappa)
+    assert ok
+    A, _ = gauge_io.read_configuration(fmt, DIMS, nc, tmp_path, "refcfg", 5)
+    if fmt == "leonard_format":
+        assert np.array_equal(Ur, U) and np.array_equal(A, U)
+        B, _ = OG.read_leonard(DIMS, nc, str(tmp_path), "refcfg", 5)
+    elif nc == 2:
+        assert np.array_equal(A, Ur) and np.max(np.abs(A - U)) < 1e-6
+        B, _ = OG.read_muenster_su2(DIMS, str(tmp_path), "refcfg", 5)
+    else:  # SU(3): two columns as floats, the third rebuilt and re-orthonormalised on reading
+        assert np.max(np.abs(A - Ur)) < 1e-14 and np.max(np.abs(A - U)) < 2e-6
+        B, _ = OG.read_muenster_su3(DIMS, str(tmp_path), "refcfg", 5)
+    assert np.max(np.abs(B - A)) < 1e-14
+    # and the other way: written by the library, read by the reference
+    gauge_io.write_configuration(fmt, U, DIMS, tmp_path, "ourcfg", 6, plaquette=0.5, beta=beta, kappa=kappa)
+    ok, Ur2 = R.gauge_read(rep, DIMS, fmt, tmp_path, "ourcfg", 6, beta, kappa)
+    assert ok
+    A2, _ = gauge_io.read_configuration(fmt, DIMS, nc, tmp_path, "ourcfg", 6)
+    assert np.max(np.abs(Ur2 - A2)) < (0 if fmt == "leonard_format" or nc == 2 else 1e-14) + 1e-300
