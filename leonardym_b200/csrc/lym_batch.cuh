@@ -537,53 +537,36 @@ LYM_HD constexpr int tri_row(int t) { return t < 1 ? 1 : t < 3 ? 2 : t < 6 ? 3 :
 // subtracted once per row, so no negated operand is formed.
 template <int SIGN, bool HAS_ADD, class CW> LYM_D void clover_block_apply(const CW &cw, int blk, const c2 x[6], c2 out[6])
 {
-    float2 nre[6], nim[6];
+    // the products that enter with a minus sign take a negated word (one negation per word,
+    // shared by its uses), so no separate accumulators are held
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
         float2 w[4];
         cw.get(blk, k, w);
+        if (SIGN < 0)
+#pragma unroll
+            for (int l = 0; l < 4; ++l) w[l] = make_float2(-w[l].x, -w[l].y);
 #pragma unroll
         for (int l = 0; l < 4; ++l) {
             const int e = 4 * k + l;
             if (e < 6) {  // diagonal entry d_e (the first words: every row starts here)
-                if (SIGN > 0) {
-                    out[e].re = HAS_ADD ? fma2(w[l], x[e].re, out[e].re) : mul2(w[l], x[e].re);
-                    out[e].im = HAS_ADD ? fma2(w[l], x[e].im, out[e].im) : mul2(w[l], x[e].im);
-                } else {
-                    nre[e] = mul2(w[l], x[e].re);
-                    nim[e] = mul2(w[l], x[e].im);
-                }
+                out[e].re = HAS_ADD ? fma2(w[l], x[e].re, out[e].re) : mul2(w[l], x[e].re);
+                out[e].im = HAS_ADD ? fma2(w[l], x[e].im, out[e].im) : mul2(w[l], x[e].im);
             } else if (((e - 6) & 1) == 0) {  // entry t = (i, j), i > j: (re, im) = w[l], w[l + 1]
                 const int t = (e - 6) / 2, i = tri_row(t), j = t - i * (i - 1) / 2;
-                const float2 are = w[l], aim = w[l + 1];
-                if (SIGN > 0) {
-                    // y_i += a x_j
-                    out[i].re = fma2(are, x[j].re, out[i].re);
-                    nre[i] = j == 0 ? mul2(aim, x[j].im) : fma2(aim, x[j].im, nre[i]);
-                    out[i].im = fma2(are, x[j].im, out[i].im);
-                    out[i].im = fma2(aim, x[j].re, out[i].im);
-                    // y_j += conj(a) x_i
-                    out[j].re = fma2(are, x[i].re, out[j].re);
-                    out[j].re = fma2(aim, x[i].im, out[j].re);
-                    out[j].im = fma2(are, x[i].im, out[j].im);
-                    nim[j] = i == j + 1 ? mul2(aim, x[i].re) : fma2(aim, x[i].re, nim[j]);
-                } else {
-                    nre[i] = fma2(are, x[j].re, nre[i]);
-                    out[i].re = fma2(aim, x[j].im, out[i].re);
-                    nim[i] = fma2(are, x[j].im, nim[i]);
-                    nim[i] = fma2(aim, x[j].re, nim[i]);
-                    nre[j] = fma2(are, x[i].re, nre[j]);
-                    nre[j] = fma2(aim, x[i].im, nre[j]);
-                    nim[j] = fma2(are, x[i].im, nim[j]);
-                    out[j].im = fma2(aim, x[i].re, out[j].im);
-                }
+                const float2 are = w[l], aim = w[l + 1], naim = make_float2(-aim.x, -aim.y);
+                // y_i += a x_j
+                out[i].re = fma2(are, x[j].re, out[i].re);
+                out[i].re = fma2(naim, x[j].im, out[i].re);
+                out[i].im = fma2(are, x[j].im, out[i].im);
+                out[i].im = fma2(aim, x[j].re, out[i].im);
+                // y_j += conj(a) x_i
+                out[j].re = fma2(are, x[i].re, out[j].re);
+                out[j].re = fma2(aim, x[i].im, out[j].re);
+                out[j].im = fma2(are, x[i].im, out[j].im);
+                out[j].im = fma2(naim, x[i].re, out[j].im);
             }
         }
-    }
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-        if (SIGN < 0 || i > 0) out[i].re = sub2(out[i].re, nre[i]);
-        if (SIGN < 0 || i < 5) out[i].im = sub2(out[i].im, nim[i]);
     }
 }
 

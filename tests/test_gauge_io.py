@@ -119,3 +119,30 @@ def test_files_of_the_reference_load_here_and_back(tmp_path, nc, fmt):
     assert ok
     A2, _ = gauge_io.read_configuration(fmt, DIMS, nc, tmp_path, "ourcfg", 6)
     assert np.max(np.abs(Ur2 - A2)) < (0 if fmt == "leonard_format" or nc == 2 else 1e-14) + 1e-300
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rep,nc,fmt", [("su3", 3, "leonard_format"), ("su3", 3, "muenster_format"),
+                                        ("su2adj", 2, "muenster_format")])
+def test_reference_file_on_gpu(tmp_path, rep, nc, fmt):
+    """A file the reference's OutputSweep wrote, loaded into a resident gauge id on the GPU,
+    gives the same operator as the links the reference's reader returns for it."""
+    R = _needs_reference()
+    U = fund(nc)
+    beta, kappa = (5.6, 0.13) if nc == 3 else (2.25, 0.18)
+    R.gauge_write(rep, DIMS, fmt, tmp_path, "refcfg", 2, U, beta, kappa)
+    ok, Ur = R.gauge_read(rep, DIMS, fmt, tmp_path, "refcfg", 2, beta, kappa)
+    assert ok
+    lat = L.Lattice(DIMS, rep)
+    try:
+        gid, _ = gauge_io.load_configuration(lat, fmt, tmp_path, "refcfg", 2)
+        gid2 = lat.upload_fundamental(Ur)
+        x = synth.gaussian_spinor(DIMS, 3, 3)
+        a = L.ImprovedDiracWilsonOperator(lat, 0.13, 1.0, gamma5=False)
+        a.setLattice(gid)
+        b = L.ImprovedDiracWilsonOperator(lat, 0.13, 1.0, gamma5=False)
+        b.setLattice(gid2)
+        ya, yb = a.multiply(x), b.multiply(x)
+        assert np.linalg.norm(ya - yb) <= 1e-14 * np.linalg.norm(yb)
+    finally:
+        lat.close()
