@@ -627,7 +627,8 @@ def run_ours(args, world, rank, local):
                                 f"{args.precision} storage, {ms.value * 1e3:.1f} us/launch"),
                      "algorithmic_bytes_per_launch": bytes_launch,
                      "variant": (f"column {tby.value}x{tbz.value}, "
-                                 + ("staged" if tminb.value >= 16 else "direct")
+                                 + ("staged (bulk copies)" if tminb.value >= 32 else
+                                    "staged (cp.async)" if tminb.value >= 16 else "direct")
                                  + f" kernel, {tminb.value % 16} blocks/SM"),
                      "peak_source": f"{pk['which']} hbm_gbs",
                      "gflops": STENCIL_FLOPS * Vh * args.batch / (ms.value * 1e-3) / 1e9,

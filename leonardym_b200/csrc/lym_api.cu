@@ -1498,6 +1498,7 @@ void apply_schur_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, c
     P.active = active;
     P.nbr = c->nbr;
     P.order = order_table(c, tile.by, tile.bz);
+    P.err = c->d_err + 1;  // the copy-wait word of the bulk-copy variant
     P.walk_by = tile.by;
     P.walk_bz = tile.bz;
     P.minb = tile.minb;
@@ -1549,6 +1550,22 @@ void apply_schur_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, c
 #define LYM_BLOCK_PARK_FRACTION 8
 #endif
 
+// The bulk-copy variant of the batched stencil (minb & 32) gives up a copy wait after a
+// bounded number of polls and sets a word of its own (d_err[1]); the calls that ran it read
+// that word once they have synchronised and fail with LYM_ERR_TIMEOUT when it is set.
+void check_copy_waits(lym_context *c, const BatchTile &t)
+{
+    if (!(t.minb & 32)) return;
+    CK(cudaMemcpyAsync(c->h_scal, c->d_err + 1, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    int e = 0;
+    memcpy(&e, c->h_scal, sizeof(int));
+    if (e) {
+        CK(cudaMemsetAsync(c->d_err + 1, 0, sizeof(int), c->st));
+        fail(c, LYM_ERR_TIMEOUT, "a bulk copy of the batched stencil did not complete in its bounded wait");
+    }
+}
+
 // Autotuner of the batched stencil: times one batched Schur application for every
 // traversal column and kernel variant on the caller's fields (in is read, tmp and out
 // are overwritten) and keeps the fastest per (precision, batch width, clover).
@@ -1567,7 +1584,7 @@ BatchTile tune_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, con
     BatchTile best;
     float best_ms = 1e30f;
     for (BatchTile t : tile_candidates(c->g)) {
-        for (int k = 0; k < kBatchMinBlocksCount; ++k) {
+        for (int k = 0; k < kBatchTunedCount; ++k) {
             t.minb = kBatchMinBlocks[k];
             apply_schur_batch(c, U, clov, prec, out, in, tmp, 1, nullptr, nullptr, b_slot, T_slot, Ti_slot, t, uniform);
             CK(cudaEventRecord(c->ev0, c->st));
@@ -2218,6 +2235,7 @@ private:
     void service()
     {
         const double t0 = wall();
+        check_copy_waits(c, tile);
         for (int j = 0; j < nb; ++j) {
             Slot &s = slot[j];
             if (!s.busy || s.finished || !hs.need_update[j]) continue;
@@ -2429,6 +2447,7 @@ int lym_context_create(const int dims[4], int rep, int device, lym_context **out
         launch_nbr_table(c->g, c->nbr, c->st);
         c->counter = (unsigned int *)dev_alloc(c, 64);
         c->d_err = (int *)dev_alloc(c, 64);
+        CK(cudaMemsetAsync(c->d_err, 0, 64, c->st));
         c->d_state = dev_alloc(c, kStateBytes);
         c->d_scal = (double *)dev_alloc(c, 64 * sizeof(double));
         CK(cudaHostAlloc(&c->h_state, kStateBytes, cudaHostAllocDefault));
@@ -3692,6 +3711,7 @@ int lym_time_stencil_batch(lym_context *c, int op_id, int prec, int which, int b
         P.U = &ge.dev;
         P.nbr = c->nbr;
         P.order = order_table(c, tile.by, tile.bz);
+        P.err = c->d_err + 1;  // the copy-wait word of the bulk-copy variant
         P.walk_by = tile.by;
         P.walk_bz = tile.bz;
         P.minb = tile.minb;
@@ -3716,6 +3736,7 @@ int lym_time_stencil_batch(lym_context *c, int op_id, int prec, int which, int b
         CK(cudaEventRecord(c->ev1, c->st));
         CK(cudaStreamSynchronize(c->st));
         CK(cudaGetLastError());
+        check_copy_waits(c, tile);
         count(c, iters + 3);
         float ms = 0.f;
         CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
@@ -3767,6 +3788,7 @@ int lym_multiply_batch(lym_context *c, int prec, int nrhs, const int *op_ids, co
             CK(cudaStreamSynchronize(c->st));
         }
         CK(cudaGetLastError());
+        check_copy_waits(c, tile);
         return LYM_OK;
     });
 }

@@ -5,24 +5,31 @@
 
 namespace lym {
 
-// Variants of the batched stencil the autotuner times: the register budget the compiler
-// is held to (__launch_bounds__(128, minb)) for the direct-load kernel (codes 1, 3, 4),
-// and the same for the kernel that stages neighbour spinors in shared memory (codes
-// 16 + minb: 19, 20).
-const int kBatchMinBlocks[] = {1, 3, 4, 19, 20};
-const int kBatchMinBlocksCount = 5;
+// Compiled variants of the batched stencil: the register budget the compiler is held to
+// (__launch_bounds__(128, minb)) for the direct-load kernel (codes 1, 3, 4), the same for
+// the kernel that stages neighbour spinors in shared memory with per-thread cp.async
+// (codes 16 + minb: 19, 20) and for the one that stages them with bulk copies completing on
+// mbarriers (codes 32 + minb: 35, 36; FP32 batches, else as 19, 20).  The autotuner times
+// the first kBatchTunedCount; the bulk-copy kernel is selected only by lym_set_batch_tile
+// (on 24^3 x 48 with 16 right-hand sides it takes 829 us per launch against 434 us for the
+// cp.async kernel: one 16 np-byte copy per spinor component costs more to issue than the
+// per-thread 16-byte copies it replaces).
+const int kBatchMinBlocks[] = {1, 3, 4, 19, 20, 35, 36};
+const int kBatchMinBlocksCount = 7;
+const int kBatchTunedCount = 5;
 
-template <int EPI, int MINB, class SB, class G>
+template <int EPI, int MINB, bool BULK = false, class SB, class G>
 static void launch_staged(const DslashBatchArg<SB, G> &a, int nblk, cudaStream_t st)
 {
+    constexpr bool BK = BULK && std::is_same<SB, BatchF>::value;  // FP16 batches: the cp.async kernel
     static bool attr = false;  // the shared-memory limit above 48 KB, once per instantiation
     const int bytes = staged_smem_bytes(a.lognp);
     if (!attr) {
-        cudaFuncSetAttribute(dslash_batch_staged_kernel<EPI, MINB, SB, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             staged_smem_bytes(0));
+        cudaFuncSetAttribute(dslash_batch_staged_kernel<EPI, MINB, BK, SB, G>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, staged_smem_bytes(0));
         attr = true;
     }
-    dslash_batch_staged_kernel<EPI, MINB><<<nblk, kStagedThreads, bytes, st>>>(a);
+    dslash_batch_staged_kernel<EPI, MINB, BK><<<nblk, kStagedThreads, bytes, st>>>(a);
 }
 
 static BatchF fview(const SpinorBatch &s) { return BatchF{(float4 *)s.v, s.stride, s.lognb - 1}; }
@@ -40,6 +47,8 @@ static void launch_minb(const DslashBatchParams &P, const DslashBatchArg<SB, G> 
     case 4: dslash_batch_kernel<EPI, 4><<<nb, 128, 0, st>>>(a); break;
     case 19: launch_staged<EPI, 3>(a, nb, st); break;
     case 20: launch_staged<EPI, 4>(a, nb, st); break;
+    case 35: launch_staged<EPI, 3, true>(a, nb, st); break;
+    case 36: launch_staged<EPI, 4, true>(a, nb, st); break;
     default: dslash_batch_kernel<EPI, 1><<<nb, 128, 0, st>>>(a); break;
     }
 }
@@ -82,15 +91,19 @@ static void run(const DslashBatchParams &P, const SB &in, const SB &out, const S
                             (float)P.b, NbrTable{P.nbr, P.g.stride}, P.order, P.skip_if, P.active,
                             P.b_slot,  P.clover_slot, P.uniform, P.res_r.v ? fview(P.res_r) : BatchF{},
                             res_s,     P.res_alpha, P.om_rhat.v ? fview(P.om_rhat) : BatchF{}, P.om_partials,
-                            column_walk(P.g, P.walk_by, P.walk_bz)};
+                            column_walk(P.g, P.walk_by, P.walk_bz), P.err};
     switch (P.epi) {
     case EPI_SCALE_: launch_minb<EPI_SCALE>(P, a, st); break;
     case EPI_CLOVINV_: launch_minb<EPI_CLOVINV>(P, a, st); break;
     case EPI_XPAY_RES_: launch_minb<EPI_XPAY_RES>(P, a, st); break;
     case EPI_XPAY_OMEGA_: {  // staged variants only (batch_omega_fusable)
         const int nblk = (int)batch_stencil_blocks(P.g, in.lognp + 1);
-        if (P.minb == 19) launch_staged<EPI_XPAY_OMEGA, 3>(a, nblk, st);
-        else launch_staged<EPI_XPAY_OMEGA, 4>(a, nblk, st);
+        switch (P.minb) {
+        case 19: launch_staged<EPI_XPAY_OMEGA, 3>(a, nblk, st); break;
+        case 35: launch_staged<EPI_XPAY_OMEGA, 3, true>(a, nblk, st); break;
+        case 36: launch_staged<EPI_XPAY_OMEGA, 4, true>(a, nblk, st); break;
+        default: launch_staged<EPI_XPAY_OMEGA, 4>(a, nblk, st); break;
+        }
         break;
     }
     default: launch_minb<EPI_XPAY>(P, a, st); break;
@@ -143,7 +156,10 @@ __global__ void __launch_bounds__(kOmegaThreads) omega_finalize_kernel(const dou
     if (threadIdx.x == 0) omega_finalize(S, r, sm[0]);
 }
 
-bool batch_omega_fusable(int minb, int prec) { return prec == PREC_F && (minb == 19 || minb == 20); }
+bool batch_omega_fusable(int minb, int prec)
+{
+    return prec == PREC_F && (minb == 19 || minb == 20 || minb == 35 || minb == 36);
+}
 
 long omega_scratch_doubles(const Geom &g, int lognb)
 {

@@ -19,6 +19,8 @@
 // links are read in the 12-real format and expanded in registers.
 #pragma once
 
+#include <type_traits>
+
 #include "lym_blas.cuh"
 #include "lym_dslash.cuh"
 
@@ -74,6 +76,40 @@ LYM_D void cp_async8(unsigned saddr, const void *g)
 }
 LYM_D void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N> LYM_D void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Bulk copies (cp.async.bulk, this GPU's global memory -> this CTA's shared memory, no
+// multicast) completing on an mbarrier in shared memory.
+LYM_D void mbar_init(unsigned mb)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mb) : "memory");
+}
+LYM_D void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+LYM_D void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+LYM_D void mbar_expect(unsigned mb, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(mb), "r"(bytes) : "memory");
+}
+LYM_D void bulk_copy(unsigned dst, const void *src, unsigned bytes, unsigned mb)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(mb)
+                 : "memory");
+}
+// waits for the phase of the given parity; gives up after a bounded number of polls (a
+// copy that never lands must not hang the GPU) and returns whether the phase completed
+LYM_D bool mbar_wait(unsigned mb, unsigned parity)
+{
+    for (int it = 0; it < (1 << 16); ++it) {
+        unsigned done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done)
+                     : "r"(mb), "r"(parity)
+                     : "memory");
+        if (done) return true;
+    }
+    return false;
+}
 
 // ------------------------------------------------------------- batch views --
 // One RHS r of a FP32 pair-layout batch, as a single half-spinor view (slot set-up and
@@ -703,6 +739,7 @@ template <class SB, class GaugeT> struct DslashBatchArg {
     BatchF om_rhat;
     double *om_partials;
     ColumnWalk walk;  // the staged kernel's indices without tables (walk.on)
+    int *err;         // bulk-copy variant: set to 1 when a copy wait gave up
 };
 
 // The epilogue on H x (acc) for the pair q at half-site h, written to out.  ysrc(blk, y6)
@@ -840,10 +877,17 @@ __global__ void __launch_bounds__(128, MINB) dslash_batch_kernel(const DslashBat
 // link words between them and meet at __syncwarp before reading.
 LYM_HD int staged_smem_bytes(int lognp)
 {
-    return (2 * 12 * kStagedThreads + 2 * (kStagedThreads >> lognp) * 9) * 16;
+    // spinor buffers, link / clover slots, then one mbarrier per (buffer, half-site) of the
+    // bulk-copy variant
+    return (2 * 12 * kStagedThreads + 2 * (kStagedThreads >> lognp) * 9) * 16 + 2 * (kStagedThreads >> lognp) * 8;
 }
 
-template <bool STAGE_Y, class SB, class GaugeT> struct StagedHop {
+// BULK: the neighbour spinor words of a direction arrive by bulk copies, one per component
+// of the half-site (16 np contiguous bytes in global and in shared memory), completing on the
+// half-site's mbarrier of that buffer (FP32 batches).  When a wait of any lane of the warp
+// gives up, the warp issues no further bulk copies, raises the error word and, before it
+// leaves, waits once more (bounded) for the copies it has in flight.
+template <bool STAGE_Y, bool BULK, class SB, class GaugeT> struct StagedHop {
     const DslashBatchArg<SB, GaugeT> &arg;
     float4 *smem;
     int h, q, np, site, lane_in;
@@ -852,6 +896,7 @@ template <bool STAGE_Y, class SB, class GaugeT> struct StagedHop {
     unsigned vmask;
     bool clov_smem;       // the batch shares one operator: its clover words go through shared memory
     const float4 *clov;   // that operator's clover term
+    int stalled = -1;     // BULK: the direction whose wait gave up (-1: none)
 
     // the 9 words of clover block blk of this half-site into link buffer blk
     LYM_D void stage_clover(int blk) const
@@ -862,6 +907,20 @@ template <bool STAGE_Y, class SB, class GaugeT> struct StagedHop {
     }
 
     LYM_D float4 *sx(int buf) const { return smem + buf * 12 * kStagedThreads + threadIdx.x; }
+    LYM_D unsigned mbar(int buf) const
+    {
+        const float4 *after = smem + 2 * 12 * kStagedThreads + 2 * (kStagedThreads / np) * 9;
+        return smem_u32(after) + (unsigned)(buf * (kStagedThreads / np) + site) * 8u;
+    }
+    LYM_D void init_bulk() const
+    {
+        if (lane_in == 0) {
+            mbar_init(mbar(0));
+            mbar_init(mbar(1));
+            mbar_init_fence();
+        }
+        __syncwarp(vmask);
+    }
     LYM_D float4 *sl(int buf) const
     {
         return smem + 2 * 12 * kStagedThreads + (buf * (kStagedThreads / np) + site) * 9;
@@ -870,12 +929,22 @@ template <bool STAGE_Y, class SB, class GaugeT> struct StagedHop {
     {
         constexpr int MU = D / 2, DIR = D % 2;
         const int n = DIR == 0 ? nf[MU] : nbk[MU];
-        if (live) arg.in.stage(smem_u32(sx(D & 1)), kStagedThreads * 16, n, q);
+        if constexpr (BULK) {
+            if (stalled >= 0) return;  // nothing new after a wait gave up (the error word is set)
+            const unsigned bytes = 16u * np, mb = mbar(D & 1);
+            const unsigned dst0 = smem_u32(smem + (D & 1) * 12 * kStagedThreads + site * np);
+            if (lane_in == 0) mbar_expect(mb, 12u * bytes);
+            fence_proxy_async();
+            for (int c = lane_in; c < 12; c += np)
+                bulk_copy(dst0 + (unsigned)c * kStagedThreads * 16u, arg.in.v + arg.in.at(c, n, 0), bytes, mb);
+        } else {
+            if (live) arg.in.stage(smem_u32(sx(D & 1)), kStagedThreads * 16, n, q);
+        }
         const int lp = DIR == 0 ? arg.parity : 1 - arg.parity, lh = DIR == 0 ? h : n;
         float4 *L = sl(D & 1);
         for (int k = lane_in; k < GaugeT::kStageWords; k += np) arg.U.stage(lp, MU, k, lh, smem_u32(L + k));
     }
-    template <int D> LYM_D void step(c2 acc[12]) const
+    template <int D> LYM_D void step(c2 acc[12])
     {
         if constexpr (D < 7) {
             issue<D + 1>();
@@ -885,6 +954,12 @@ template <bool STAGE_Y, class SB, class GaugeT> struct StagedHop {
         }
         cp_async_commit();
         cp_async_wait<1>();  // the copies of direction D (this thread's)
+        if constexpr (BULK) {  // its spinor words
+            if (stalled < 0 && __any_sync(vmask, !mbar_wait(mbar(D & 1), (D >> 1) & 1))) {
+                stalled = D;
+                if (lane_in == 0) atomicOr(arg.err, 1);
+            }
+        }
         __syncwarp(vmask);   // ... and those of the other lanes of the half-site
         if (live) {
             c2 x[12];
@@ -894,6 +969,14 @@ template <bool STAGE_Y, class SB, class GaugeT> struct StagedHop {
             accumulate_dir<GaugeT::kReal, D / 2, D % 2>(x, L, acc);
         }
         __syncwarp(vmask);  // every lane is done with buffer D & 1 before it is refilled
+    }
+    // BULK, after a wait gave up at direction d: the copies of d and of d + 1 (issued before
+    // that wait) may still be in flight; wait for them, bounded, before the block leaves
+    LYM_D void drain() const
+    {
+        if (stalled < 0) return;
+        mbar_wait(mbar(stalled & 1), (stalled >> 1) & 1);
+        if (stalled < 7) mbar_wait(mbar((stalled + 1) & 1), ((stalled + 1) >> 1) & 1);
     }
 };
 
@@ -927,10 +1010,12 @@ LYM_D void omega_block_reduce(const DslashBatchArg<SB, GaugeT> &arg, float4 *sme
     }
 }
 
-template <int EPI, int MINB, class SB, class GaugeT>
+template <int EPI, int MINB, bool BULK, class SB, class GaugeT>
 __global__ void __launch_bounds__(kStagedThreads, MINB)
     dslash_batch_staged_kernel(const DslashBatchArg<SB, GaugeT> arg)
 {
+    static_assert(!BULK || std::is_same<SB, BatchF>::value, "bulk copies stage FP32 batches");
+    constexpr bool B = BULK;
     extern __shared__ float4 stage_smem[];
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int wi = tid >> arg.lognp, q = tid & ((1 << arg.lognp) - 1);
@@ -957,7 +1042,7 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
         }
         const bool act_a = flag_a != 0, act_b = flag_b != 0;
         const int np = 1 << arg.lognp;
-        StagedHop<EPI == EPI_XPAY || EPI == EPI_XPAY_RES || EPI == EPI_XPAY_OMEGA, SB, GaugeT> s{
+        StagedHop<EPI == EPI_XPAY || EPI == EPI_XPAY_RES || EPI == EPI_XPAY_OMEGA, B, SB, GaugeT> s{
             arg, stage_smem, 0, q, np, (int)threadIdx.x >> arg.lognp, (int)threadIdx.x & (np - 1)};
         if (arg.walk.on) {
             s.h = walk_site(arg.walk, arg.parity, (unsigned)wi, s.nf, s.nbk);
@@ -976,6 +1061,7 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
         c2 acc[12];
 #pragma unroll
         for (int k = 0; k < 12; ++k) acc[k] = c2{make_float2(0.f, 0.f), make_float2(0.f, 0.f)};
+        if constexpr (B) s.init_bulk();
         s.template issue<0>();
         cp_async_commit();
         s.template step<0>(acc);
@@ -995,6 +1081,7 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
             if (s.live) arg.om_rhat.stage(smem_u32(s.sx(1)), kStagedThreads * 16, s.h, q);
         cp_async_commit();
         cp_async_wait<0>();
+        if constexpr (B) s.drain();
         __syncwarp(vmask);
         if (!s.live) return false;
         auto ysrc = [&](int blk, c2 y6[6]) { arg.y.unstage_block(s.sx(0), kStagedThreads, blk, y6); };

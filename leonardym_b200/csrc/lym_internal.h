@@ -122,6 +122,7 @@ struct DslashBatchParams {
     // [block][nb][7] of <out, y>, |out|^2, <rhat, y>, <rhat, out>
     SpinorBatch om_rhat;
     double *om_partials = nullptr;
+    int *err = nullptr;  // bulk-copy variants: set to 1 when a copy wait gave up
 };
 // blocks of the batched stencil launch (the size of the EPI_XPAY_OMEGA partials)
 inline long batch_stencil_blocks(const Geom &g, int lognb) { return (((long)g.Vh << (lognb - 1)) + 127) / 128; }
@@ -146,6 +147,7 @@ void launch_nbr_table(const Geom &g, int *nbr, cudaStream_t st);
 void launch_order_table(const Geom &g, int by, int bz, int *order, cudaStream_t st);
 extern const int kBatchMinBlocks[];  // the compiled variants of the batched stencil
 extern const int kBatchMinBlocksCount;
+extern const int kBatchTunedCount;  // the leading entries the autotuner times
 
 // measurements on AoS spinors in device memory (lym_measure.cu)
 struct MesonProps {

@@ -27,6 +27,7 @@ pytestmark = pytest.mark.gpu
 
 TOL = {"single": 1e-6, "half": 1e-2}
 HEADLINE_TILE = (8, 24, 20)  # (y, z) column 8 x 24, staged kernel variant with 4 blocks per SM
+BULK_TILE = (8, 24, 36)  # the same column, spinors staged by bulk copies
 
 
 @pytest.fixture(scope="module")
@@ -47,7 +48,7 @@ def slot_params(bench):
 
 
 @pytest.mark.parametrize("precision", ["single", "half"])
-@pytest.mark.parametrize("tile", ["headline", "autotuned"])
+@pytest.mark.parametrize("tile", ["headline", "bulk", "autotuned"])
 def test_batched_stencil_24c48_16rhs(headline, precision, tile, oracle):
     bench, lat = headline["bench"], headline["lat"]
     params = slot_params(bench)
@@ -64,14 +65,16 @@ def test_batched_stencil_24c48_16rhs(headline, precision, tile, oracle):
     try:
         if tile == "headline":
             set_batch_tile(lat, *HEADLINE_TILE)
+        elif tile == "bulk":
+            set_batch_tile(lat, *BULK_TILE)
         else:
             set_batch_tile(lat, -1, 0)
         got = multiply_batch(slot_ops, xs, precision)
         used = batch_tile(lat, precision, 16)
     finally:
         set_batch_tile(lat, -1, 0)
-    if tile == "headline":
-        assert used == HEADLINE_TILE
+    if tile != "autotuned":
+        assert used == (HEADLINE_TILE if tile == "headline" else BULK_TILE)
     worst = 0.0
     for k, (kappa, csw) in enumerate(params):
         D = oracle.Operator(headline["geom"], headline["links"], "EvenOddImproved", kappa, csw, False)
