@@ -1092,9 +1092,14 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
                                 s.sx(1));
         }
         if constexpr (RED) {
-            // the omega sums of the two lanes: <t, s>, |t|^2, <rhat, s>, <rhat, t> (t = out, s = y)
+            // the omega sums of the two lanes: <t, s>, |t|^2, <rhat, s>, <rhat, t> (t = out,
+            // s = y), over the 12 components of this half-site in packed FP32 (one lane per
+            // RHS, a fixed order), then FP64 from the per-thread totals on: the block and
+            // grid reductions add 2^22 and more such totals, each of 12 products
+            const float2 zero = make_float2(0.f, 0.f);
+            float2 P[7];
 #pragma unroll
-            for (int k = 0; k < 14; ++k) red[k] = 0.0;
+            for (int k = 0; k < 7; ++k) P[k] = zero;
 #pragma unroll
             for (int blk = 0; blk < 2; ++blk) {
                 c2 y6[6], r6[6];
@@ -1103,22 +1108,21 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
 #pragma unroll
                 for (int k = 0; k < 6; ++k) {
                     const c2 t = acc[6 * blk + k], sv = y6[k], rh = r6[k];
-                    const double tr[2] = {t.re.x, t.re.y}, ti[2] = {t.im.x, t.im.y};
-                    const double sr[2] = {sv.re.x, sv.re.y}, si[2] = {sv.im.x, sv.im.y};
-                    const double rr[2] = {rh.re.x, rh.re.y}, ri[2] = {rh.im.x, rh.im.y};
-#pragma unroll
-                    for (int l = 0; l < 2; ++l) {
-                        if (l == 0 ? !act_a : !act_b) continue;
-                        double *a = red + 7 * l;
-                        a[0] += tr[l] * sr[l] + ti[l] * si[l];
-                        a[1] += tr[l] * si[l] - ti[l] * sr[l];
-                        a[2] += tr[l] * tr[l] + ti[l] * ti[l];
-                        a[3] += rr[l] * sr[l] + ri[l] * si[l];
-                        a[4] += rr[l] * si[l] - ri[l] * sr[l];
-                        a[5] += rr[l] * tr[l] + ri[l] * ti[l];
-                        a[6] += rr[l] * ti[l] - ri[l] * tr[l];
-                    }
+                    const float2 nti = sub2(zero, t.im), nri = sub2(zero, rh.im);
+                    P[0] = fma2(t.im, sv.im, fma2(t.re, sv.re, P[0]));   // Re <t, s>
+                    P[1] = fma2(nti, sv.re, fma2(t.re, sv.im, P[1]));    // Im <t, s>
+                    P[2] = fma2(t.im, t.im, fma2(t.re, t.re, P[2]));     // |t|^2
+                    P[3] = fma2(rh.im, sv.im, fma2(rh.re, sv.re, P[3])); // Re <rhat, s>
+                    P[4] = fma2(nri, sv.re, fma2(rh.re, sv.im, P[4]));   // Im <rhat, s>
+                    P[5] = fma2(rh.im, t.im, fma2(rh.re, t.re, P[5]));   // Re <rhat, t>
+                    P[6] = fma2(nri, t.re, fma2(rh.re, t.im, P[6]));     // Im <rhat, t>
                 }
+            }
+            // an idle lane's sums are dropped (its words may hold anything)
+#pragma unroll
+            for (int k = 0; k < 7; ++k) {
+                red[k] = act_a ? (double)P[k].x : 0.0;
+                red[7 + k] = act_b ? (double)P[k].y : 0.0;
             }
         }
         return true;
