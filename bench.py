@@ -39,9 +39,11 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "which": "fallback"}
 # reconstructed formats), 1 neighbour spinor (each read once), the y spinor, T_oo, the output
 STENCIL_BYTES = {0: 8 * 144 + 3 * 192 + 576, 1: 8 * 48 + 2 + 3 * 96 + 288, 2: 8 * 24 + 2 + 3 * 52 + 144}
 STENCIL_BYTES_8REAL = 8 * 32 + 2 + 3 * 96 + 288  # FP32 with SU(3) links in 8 reals
-# the batched kernel reads links, sign bytes and T once per site for the whole batch and
-# three spinors (neighbour, y, out) per right-hand side
-STENCIL_SITE_BYTES = {1: 8 * 48 + 2 + 288, 2: 8 * 24 + 2 + 144}
+# the batched kernel reads links and T once per site for the whole batch, in FP32 for either
+# spinor storage (links in 12 reals + 2 sign-table bytes, or in all 18 reals: the 8 padding
+# bytes of the fifth word are not counted), and three spinors (neighbour, y, out) per
+# right-hand side
+STENCIL_SITE_BYTES = {12: 8 * 48 + 2 + 288, 18: 8 * 72 + 288}
 STENCIL_RHS_BYTES = {1: 3 * 96, 2: 3 * 52}
 STENCIL_FLOPS = 1320 + 504 + 48  # hopping + clover apply + xpay, per site
 
@@ -260,10 +262,11 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def traffic_from_profiles(prec, batch):
+def traffic_from_profiles(prec, batch, link_reals):
     """DRAM bytes per launch of the batched stencil kernel from the committed ncu summary."""
     for name in sorted(os.listdir(os.path.join(ROOT, "profiles"))):
-        m = re.search(rf"traffic_bytes_per_launch\[prec={prec},kernel=xpay,batch={batch}\]:\s*([0-9.eE+]+)",
+        m = re.search(rf"traffic_bytes_per_launch\[prec={prec},kernel=xpay,batch={batch},links={link_reals}\]:"
+                      rf"\s*([0-9.eE+]+)",
                       open(os.path.join(ROOT, "profiles", name)).read())
         if m:
             return float(m.group(1))
@@ -564,10 +567,11 @@ def run_ours(args, world, rank, local):
     if lib.lym_get_batch_tile(ctx, sprec, args.batch, 1, C.byref(tby), C.byref(tbz), C.byref(tminb)) != 0:
         raise RuntimeError(f"lym_get_batch_tile failed: {lib.lym_last_error(ctx)}")
     Vh = V // 2
-    bytes_launch = (STENCIL_SITE_BYTES[sprec] + args.batch * STENCIL_RHS_BYTES[sprec]) * Vh
+    link_reals = 18 if tminb.value & 64 else 12
+    bytes_launch = (STENCIL_SITE_BYTES[link_reals] + args.batch * STENCIL_RHS_BYTES[sprec]) * Vh
     achieved = bytes_launch / (ms.value * 1e-3) / 1e9
     pk = peaks()
-    traffic = traffic_from_profiles(sprec, args.batch)
+    traffic = traffic_from_profiles(sprec, args.batch, link_reals)
     ms1, ms64, ms8 = C.c_double(0), C.c_double(0), C.c_double(0)
     lib.lym_time_stencil(ctx, opid, sprec, 0, 30, C.byref(ms1))
     lib.lym_time_stencil(ctx, opid, 0, 0, 20, C.byref(ms64))
@@ -627,9 +631,10 @@ def run_ours(args, world, rank, local):
                                 f"{args.precision} storage, {ms.value * 1e3:.1f} us/launch"),
                      "algorithmic_bytes_per_launch": bytes_launch,
                      "variant": (f"column {tby.value}x{tbz.value}, "
-                                 + ("staged (bulk copies)" if tminb.value >= 32 else
-                                    "staged (cp.async)" if tminb.value >= 16 else "direct")
-                                 + f" kernel, {tminb.value % 16} blocks/SM"),
+                                 + ("staged (bulk copies)" if tminb.value & 32 else
+                                    "staged (cp.async)" if tminb.value & 16 else "direct")
+                                 + f" kernel, {tminb.value % 16} blocks/SM, "
+                                 + ("18-real" if tminb.value & 64 else "12-real") + " links"),
                      "peak_source": f"{pk['which']} hbm_gbs",
                      "gflops": STENCIL_FLOPS * Vh * args.batch / (ms.value * 1e-3) / 1e9,
                      "single_rhs_kernel_gbs": STENCIL_BYTES[sprec] * Vh / (ms1.value * 1e-3) / 1e9,
@@ -874,14 +879,15 @@ def run_profile(args):
     ms = C.c_double(0)
     sp = 1 if args.precision == "single" else 2
     lib.lym_time_stencil(lat.handle, op.op_id, sp, 0, 10, C.byref(ms))
-    msb = C.c_double(0)
+    msb, msc = C.c_double(0), C.c_double(0)
     lib.lym_time_stencil_batch(lat.handle, op.op_id, sp, 0, args.batch, 10, C.byref(msb))
+    lib.lym_time_stencil_batch(lat.handle, op.op_id, sp, 1, args.batch, 10, C.byref(msc))
     tby, tbz, tminb = C.c_int(), C.c_int(), C.c_int()
     lib.lym_get_batch_tile(lat.handle, sp, args.batch, 1, C.byref(tby), C.byref(tbz), C.byref(tminb))
     print(f"profile case: rc {rc}, block solve {t_solve:.3f} s, updates {st.reliable_updates}, "
           f"iterations {st.iterations}, true residual {st.true_residual:.2e}, "
-          f"stencil {ms.value * 1e3:.1f} us, batched stencil ({args.batch}) {msb.value * 1e3:.1f} us, "
-          f"tile {tby.value},{tbz.value},{tminb.value}")
+          f"stencil {ms.value * 1e3:.1f} us, batched stencil ({args.batch}) {msb.value * 1e3:.1f} us "
+          f"(T^-1 half {msc.value * 1e3:.1f} us), tile {tby.value},{tbz.value},{tminb.value}")
     lat.close()
     if rc != 0:
         sys.exit(1)

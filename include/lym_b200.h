@@ -419,8 +419,10 @@ int lym_multiply_batch(lym_context *ctx, int prec, int nrhs, const int *op_ids, 
  * column is by * bz sites of the (y, z) plane, walked x first and t fastest inside
  * (by = 0: plain half-site order, x slowest); minb selects the kernel variant: 1, 3
  * or 4 = direct loads with that register budget (minimum resident blocks per SM), 19
- * or 20 = neighbour spinors staged through shared memory with 3 or 4 blocks per SM.
- * lym_set_batch_tile forces a
+ * or 20 = neighbour spinors staged through shared memory by per-thread cp.async with 3
+ * or 4 blocks per SM, 35 or 36 = the same staged by bulk copies completing on mbarriers
+ * (FP32 batches; not timed by the autotuner), 83 or 84 = 19 or 20 reading SU(3) links in
+ * all 18 reals instead of 12 reals and a sign bit.  lym_set_batch_tile forces a
  * configuration for the context (by < 0 returns to tuning); lym_get_batch_tile reports
  * the one in use (LYM_ERR_NOT_FOUND before the first tuning of that key). */
 int lym_set_batch_tile(lym_context *ctx, int by, int bz, int minb);

@@ -2499,6 +2499,7 @@ void lym_context_destroy(lym_context *c)
         cudaFree(kv.second.dev.h16);
         cudaFree(kv.second.dev.sign);
         cudaFree(kv.second.dev.f32r8);
+        cudaFree(kv.second.dev.f32r18);
     }
     for (auto &s : c->pool) cudaFree(s.v);
     for (auto &b : c->blocks) cudaFree(b.second);
@@ -2560,6 +2561,7 @@ static int gauge_store(lym_context *c, int id, const double *links, bool device_
         e.dev.h16 = dev_alloc(c, h16);
         e.dev.sign = (uint8_t *)dev_alloc(c, 2 * s);
         e.dev.f32r8 = dev_alloc(c, 2 * 4 * 2 * s * sizeof(float4));  // written for SU(3) only
+        if (c->rep == REP_SU3) e.dev.f32r18 = dev_alloc(c, 2 * 4 * 5 * s * sizeof(float4));
         e.dev.link_reals = c->link_reals;
         ge = &(c->gauges[id] = e);
     } else {
@@ -2634,6 +2636,7 @@ int lym_gauge_evict(lym_context *c, int id)
         dev_free(c, it->second.dev.h16, su3 ? 2 * 4 * 3 * s * sizeof(uint2) : 2 * 4 * 3 * s * sizeof(__half2));
         dev_free(c, it->second.dev.sign, 2 * s);
         dev_free(c, it->second.dev.f32r8, 2 * 4 * 2 * s * sizeof(float4));
+        if (su3) dev_free(c, it->second.dev.f32r18, 2 * 4 * 5 * s * sizeof(float4));
         c->gauges.erase(it);
         return LYM_OK;
     });

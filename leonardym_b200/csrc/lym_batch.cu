@@ -8,15 +8,16 @@ namespace lym {
 // Compiled variants of the batched stencil: the register budget the compiler is held to
 // (__launch_bounds__(128, minb)) for the direct-load kernel (codes 1, 3, 4), the same for
 // the kernel that stages neighbour spinors in shared memory with per-thread cp.async
-// (codes 16 + minb: 19, 20) and for the one that stages them with bulk copies completing on
-// mbarriers (codes 32 + minb: 35, 36; FP32 batches, else as 19, 20).  The autotuner times
-// the first kBatchTunedCount; the bulk-copy kernel is selected only by lym_set_batch_tile
-// (on 24^3 x 48 with 16 right-hand sides it takes 829 us per launch against 434 us for the
-// cp.async kernel: one 16 np-byte copy per spinor component costs more to issue than the
-// per-thread 16-byte copies it replaces).
-const int kBatchMinBlocks[] = {1, 3, 4, 19, 20, 35, 36};
-const int kBatchMinBlocksCount = 7;
-const int kBatchTunedCount = 5;
+// (codes 16 + minb: 19, 20), the same reading SU(3) links in all 18 reals (codes 64 + 19,
+// 20: 83, 84; as 19, 20 for the adjoint representation) and the one that stages the
+// spinors with bulk copies completing on mbarriers (codes 32 + minb: 35, 36; FP32 batches,
+// else as 19, 20).  The autotuner times the first kBatchTunedCount; the bulk-copy kernel is
+// selected only by lym_set_batch_tile (on 24^3 x 48 with 16 right-hand sides it takes 829
+// us per launch against 434 us for the cp.async kernel: one 16 np-byte copy per spinor
+// component costs more to issue than the per-thread 16-byte copies it replaces).
+const int kBatchMinBlocks[] = {1, 3, 4, 19, 20, 83, 84, 35, 36};
+const int kBatchMinBlocksCount = 9;
+const int kBatchTunedCount = 7;
 
 template <int EPI, int MINB, bool BULK = false, class SB, class G>
 static void launch_staged(const DslashBatchArg<SB, G> &a, int nblk, cudaStream_t st)
@@ -158,7 +159,8 @@ __global__ void __launch_bounds__(kOmegaThreads) omega_finalize_kernel(const dou
 
 bool batch_omega_fusable(int minb, int prec)
 {
-    return prec == PREC_F && (minb == 19 || minb == 20 || minb == 35 || minb == 36);
+    const int m = minb & ~64;
+    return prec == PREC_F && (m == 19 || m == 20 || m == 35 || m == 36);
 }
 
 long omega_scratch_doubles(const Geom &g, int lognb)
@@ -175,18 +177,25 @@ void launch_omega_finalize(double *scratch, const Geom &g, int lognb, void *stat
     omega_finalize_kernel<<<nb, kOmegaThreads, 0, st>>>(chunks, nb, (BatchCGState *)state);
 }
 
-void launch_dslash_batch(const DslashBatchParams &P, cudaStream_t st)
+void launch_dslash_batch(const DslashBatchParams &P0, cudaStream_t st)
 {
+    // variant bit 64: SU(3) links read in all 18 reals; the kernel variant is the code without it
+    DslashBatchParams P = P0;
+    const bool f18 = (P.minb & 64) && P.rep == REP_SU3 && P.U->f32r18;
+    P.minb &= ~64;
     const GaugeDev &U = *P.U;
     const int s = P.g.stride;
     const GaugeC12P c12{(const float4 *)U.f32, U.sign, s};
+    const GaugeF18P l18{(const float4 *)U.f32r18, s};
     const GaugeR6P r6{(const float2 *)U.f32, U.sign, s};
     if (P.prec == PREC_F) {
-        if (P.rep == REP_SU3) run(P, fview(P.in), fview(P.out), fview(P.y), c12, st);
-        else run(P, fview(P.in), fview(P.out), fview(P.y), r6, st);
+        if (P.rep != REP_SU3) run(P, fview(P.in), fview(P.out), fview(P.y), r6, st);
+        else if (f18) run(P, fview(P.in), fview(P.out), fview(P.y), l18, st);
+        else run(P, fview(P.in), fview(P.out), fview(P.y), c12, st);
     } else {
-        if (P.rep == REP_SU3) run(P, hview(P.in), hview(P.out), hview(P.y), c12, st);
-        else run(P, hview(P.in), hview(P.out), hview(P.y), r6, st);
+        if (P.rep != REP_SU3) run(P, hview(P.in), hview(P.out), hview(P.y), r6, st);
+        else if (f18) run(P, hview(P.in), hview(P.out), hview(P.y), l18, st);
+        else run(P, hview(P.in), hview(P.out), hview(P.y), c12, st);
     }
 }
 

@@ -445,6 +445,40 @@ struct GaugeC12P {  // SU(3)
     }
 };
 
+// SU(3) links in all 18 reals, entries row-major two per word (the boundary sign is part
+// of the stored link): 5 words staged per link and no row to rebuild, against 3 words and a
+// sign byte for GaugeC12P, whose rebuilt row costs every thread of the half-site about 50
+// scalar instructions per link
+struct GaugeF18P {
+    static constexpr bool kReal = false;
+    static constexpr int kStageWords = 5;
+    const float4 *u;  // [parity][mu][5][stride]
+    int stride;
+    LYM_D static void expand(const float4 w0, const float4 w1, const float4 w2, const float4 w3, const float4 w4,
+                             LinkP &L)
+    {
+        const float r[9] = {w0.x, w0.z, w1.x, w1.z, w2.x, w2.z, w3.x, w3.z, w4.x};
+        const float i[9] = {w0.y, w0.w, w1.y, w1.w, w2.y, w2.w, w3.y, w3.w, w4.y};
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                L.ur[a][b] = make_float2(r[3 * a + b], r[3 * a + b]);
+                L.ui[a][b] = make_float2(i[3 * a + b], i[3 * a + b]);
+            }
+    }
+    LYM_D void load(int p, int mu, int h, LinkP &L) const
+    {
+        const float4 *b = u + ((unsigned)(p * 4 + mu) * 5 * stride + h);
+        expand(__ldcs(b), __ldcs(b + stride), __ldcs(b + 2 * stride), __ldcs(b + 3 * stride), __ldcs(b + 4 * stride), L);
+    }
+    LYM_D void stage(int p, int mu, int k, int h, unsigned saddr) const
+    {
+        cp_async16(saddr, u + ((unsigned)((p * 4 + mu) * 5 + k) * stride + h));
+    }
+    LYM_D void unstage(const float4 *w4, int, int, LinkP &L) const { expand(w4[0], w4[1], w4[2], w4[3], w4[4], L); }
+};
+
 struct GaugeR6P {  // real adjoint links: 3 float2 words (rows 0 and 1), row 2 = s (row0 x row1)
     static constexpr bool kReal = true;
     static constexpr int kStageWords = 4;

@@ -37,6 +37,9 @@ struct GaugeDev {
     // FP32 SU(3) links in 8 reals (GaugeF8): float4[2][4][2][stride]; link_reals 12 or 8 picks
     // the format of the FP32 single-RHS stencils (lym_set_link_format)
     void *f32r8 = nullptr;
+    // FP32 SU(3) links in all 18 reals for the batched stencil (GaugeF18P):
+    // float4[2][4][5][stride], the boundary sign included
+    void *f32r18 = nullptr;
     int link_reals = 12;
     bool recon_ok = false;
 };

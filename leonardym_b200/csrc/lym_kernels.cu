@@ -163,7 +163,7 @@ LYM_D void load_link_d(const Geom &g, int rep, const void *d64, int p, int mu, i
 // accepted when it is +-V with V special unitary (SU(3)) or special orthogonal
 // (adjoint); the sign goes to the sign table.
 __global__ void compress_gauge_kernel(Geom g, int rep, const void *d64, void *f32, void *h16, uint8_t *sign, int *err,
-                                      float4 *f32r8)
+                                      float4 *f32r8, float4 *f32r18)
 {
     const int h = blockIdx.x * blockDim.x + threadIdx.x;
     const int p = blockIdx.y;
@@ -201,6 +201,13 @@ __global__ void compress_gauge_kernel(Geom g, int rep, const void *d64, void *f3
             f32r8[w8] = make_float4(sg * u[0][1].re, sg * u[0][1].im, sg * u[0][2].re, sg * u[0][2].im);
             f32r8[w8 + g.stride] = make_float4(sg * u[1][0].re, sg * u[1][0].im, atan2(sg * u[0][0].im, sg * u[0][0].re),
                                                atan2(sg * u[2][0].im, sg * u[2][0].re));
+            // all 18 reals (GaugeF18P): entries row-major, two per word, the last word half used
+            const size_t w18 = (size_t)(p * 4 + mu) * 5 * g.stride + h;
+            for (int k = 0; k < 5; ++k) {
+                const cx<double> a = u[(2 * k) / 3][(2 * k) % 3];
+                const cx<double> b = k < 4 ? u[(2 * k + 1) / 3][(2 * k + 1) % 3] : cx<double>{0.0, 0.0};
+                f32r18[w18 + (size_t)k * g.stride] = make_float4(a.re, a.im, b.re, b.im);
+            }
             uint2 *H = (uint2 *)h16;
             double v[12] = {u[0][0].re, u[0][0].im, u[0][1].re, u[0][1].im, u[0][2].re, u[0][2].im,
                             u[1][0].re, u[1][0].im, u[1][1].re, u[1][1].im, u[1][2].re, u[1][2].im};
@@ -228,7 +235,8 @@ __global__ void compress_gauge_kernel(Geom g, int rep, const void *d64, void *f3
 void launch_compress_gauge(const Geom &g, GaugeDev &U, int *err, cudaStream_t st)
 {
     dim3 grid(nblocks(g.Vh, 128), 2);
-    compress_gauge_kernel<<<grid, 128, 0, st>>>(g, U.rep, U.d64, U.f32, U.h16, U.sign, err, (float4 *)U.f32r8);
+    compress_gauge_kernel<<<grid, 128, 0, st>>>(g, U.rep, U.d64, U.f32, U.h16, U.sign, err, (float4 *)U.f32r8,
+                                                (float4 *)U.f32r18);
 }
 
 // Fundamental gauge links -> fermion links: the adjoint map for SU(2)

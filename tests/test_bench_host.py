@@ -18,14 +18,15 @@ def test_config_names_the_workload_and_no_model():
 
 def test_traffic_comes_from_the_profile_summary():
     text = (ROOT / "profiles" / "batched_stencil_schur_clover_24c48_nb16.md").read_text()
-    m = re.search(r"traffic_bytes_per_launch\[prec=1,kernel=xpay,batch=16\]:\s*(\d+)", text)
-    assert m, "the profile summary lost its traffic line"
-    assert bench.traffic_from_profiles(1, 16) == float(m.group(1))
-    # algorithmic bytes of one 16-RHS FP32 launch against the measured traffic: the format's
-    # duplicated links and re-reads keep the traffic within 30 % above them
     Vh = 24 * 24 * 24 * 48 // 2
-    alg = (bench.STENCIL_SITE_BYTES[1] + 16 * bench.STENCIL_RHS_BYTES[1]) * Vh
-    assert 1.0 <= float(m.group(1)) / alg <= 1.3
+    for reals in (12, 18):
+        m = re.search(rf"traffic_bytes_per_launch\[prec=1,kernel=xpay,batch=16,links={reals}\]:\s*(\d+)", text)
+        assert m, f"the profile summary lost its traffic line ({reals}-real links)"
+        assert bench.traffic_from_profiles(1, 16, reals) == float(m.group(1))
+        # algorithmic bytes of one 16-RHS FP32 launch against the measured traffic: re-read
+        # neighbour spinors and the links' padding keep it within 20 % above them
+        alg = (bench.STENCIL_SITE_BYTES[reals] + 16 * bench.STENCIL_RHS_BYTES[1]) * Vh
+        assert 1.0 <= float(m.group(1)) / alg <= 1.2, reals
 
 
 def test_peaks_are_measured_or_the_stated_fallback():

@@ -47,9 +47,10 @@ def operators(setup, gamma5):
 
 def tiles(dims):
     Ly, Lz = dims[1], dims[2]
-    # direct-load variants (minb 1, 3, 4), shared-memory staged ones (19, 20) and staged with
-    # bulk copies (35, 36)
-    return [(0, 0, 1), (Ly, Lz, 3), (2, Lz, 4), (2, 2, 19), (1, 1, 20), (0, 0, 19), (2, 2, 35), (Ly, Lz, 36)]
+    # direct-load variants (minb 1, 3, 4), shared-memory staged ones (19, 20), staged with
+    # bulk copies (35, 36) and staged with 18-real SU(3) links (83, 84; 19, 20 for the adjoint)
+    return [(0, 0, 1), (Ly, Lz, 3), (2, Lz, 4), (2, 2, 19), (1, 1, 20), (0, 0, 19), (2, 2, 35), (Ly, Lz, 36),
+            (2, 2, 83), (Ly, Lz, 84)]
 
 
 @pytest.mark.parametrize("gamma5", [False, True])
@@ -77,7 +78,7 @@ def test_batched_stencil_autotuned(setup, oracle):
     xs = [synth.gaussian_spinor(setup["dims"], 3, 400 + j) for j in range(3)]
     got = multiply_batch(gpu, xs, "single")
     by, bz, minb = batch_tile(setup["lat"], "single", 4)
-    assert minb in (1, 3, 4, 19, 20, 35, 36)
+    assert minb in (1, 3, 4, 19, 20, 35, 36, 83, 84)
     assert by == 0 or (setup["dims"][1] % by == 0 and setup["dims"][2] % bz == 0)
     for j, x in enumerate(xs):
         D = oracle.Operator(setup["geom"], setup["links"], "EvenOddImproved", params[j][0], params[j][1], False)

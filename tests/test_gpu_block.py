@@ -52,7 +52,7 @@ def test_block_rejects_bad_batch(setup):
         s.solve_block(setup["op"], setup["srcs"], batch=3)
 
 
-@pytest.mark.parametrize("minb", [19, 20, 36])
+@pytest.mark.parametrize("minb", [19, 20, 36, 84])
 def test_block_bicgstab_fused_omega_matches_separate_pass(setup, minb):
     """The staged stencil variants fold the BiCGStab omega sums into the epilogue of the
     t = S s launch; a direct variant keeps them in a separate pass.  Both meet the 1e-10

@@ -5,10 +5,10 @@ exp(0.25 i H) seeded exactly as the benchmark seeds them, antiperiodic in time.
 
 * The batched stencil (lym_multiply_batch: EvenOddImprovedDiracWilsonOperator::multiply,
   EvenOddImprovedDiracWilsonOperator.cpp:26-47, of each slot's own operator) with 16
-  right-hand sides, both with the traversal column and kernel variant the benchmark's
-  autotuner settles on at this size (column 8 x 24, staged kernel, 4 blocks per SM, the
-  arithmetic index walk) forced, and with whatever the autotuner picks here.  Bars: FP32
-  storage 1e-6, FP16 storage 1e-2 relative.
+  right-hand sides: with the kind of configuration the benchmark's autotuner settles on at
+  this size forced (column 8 x 24, staged kernel, 4 blocks per SM, the arithmetic index
+  walk, 18-real links), with the same on 12-real links and with bulk-copy staging, and with
+  whatever the autotuner picks here.  Bars: FP32 storage 1e-6, FP16 storage 1e-2 relative.
 * The block BiCGStab (mixed single) through lym_solve_block with HOST buffers, on four of
   the benchmark's 44 sources (two point sources, two Z2 x Z2 noise sources) in a batch of
   16 slots: each downloaded solution's true residual |b - D x| / |b| is re-measured on the
@@ -26,8 +26,9 @@ from tests.helpers import rel
 pytestmark = pytest.mark.gpu
 
 TOL = {"single": 1e-6, "half": 1e-2}
-HEADLINE_TILE = (8, 24, 20)  # (y, z) column 8 x 24, staged kernel variant with 4 blocks per SM
-BULK_TILE = (8, 24, 36)  # the same column, spinors staged by bulk copies
+# (y, z) column 8 x 24, staged kernel with 4 blocks per SM: 18-real links, 12-real links,
+# bulk-copy staging
+TILES = {"headline": (8, 24, 84), "link12": (8, 24, 20), "bulk": (8, 24, 36)}
 
 
 @pytest.fixture(scope="module")
@@ -48,7 +49,7 @@ def slot_params(bench):
 
 
 @pytest.mark.parametrize("precision", ["single", "half"])
-@pytest.mark.parametrize("tile", ["headline", "bulk", "autotuned"])
+@pytest.mark.parametrize("tile", ["headline", "link12", "bulk", "autotuned"])
 def test_batched_stencil_24c48_16rhs(headline, precision, tile, oracle):
     bench, lat = headline["bench"], headline["lat"]
     params = slot_params(bench)
@@ -63,18 +64,16 @@ def test_batched_stencil_24c48_16rhs(headline, precision, tile, oracle):
     xs = srcs[0:12:3] + srcs[12:16] + [synth.gaussian_spinor(bench.DIMS, 3, 500 + j) for j in range(8)]
     slot_ops = [ops[j % 4] for j in range(16)]
     try:
-        if tile == "headline":
-            set_batch_tile(lat, *HEADLINE_TILE)
-        elif tile == "bulk":
-            set_batch_tile(lat, *BULK_TILE)
+        if tile in TILES:
+            set_batch_tile(lat, *TILES[tile])
         else:
             set_batch_tile(lat, -1, 0)
         got = multiply_batch(slot_ops, xs, precision)
         used = batch_tile(lat, precision, 16)
     finally:
         set_batch_tile(lat, -1, 0)
-    if tile != "autotuned":
-        assert used == (HEADLINE_TILE if tile == "headline" else BULK_TILE)
+    if tile in TILES:
+        assert used == TILES[tile]
     worst = 0.0
     for k, (kappa, csw) in enumerate(params):
         D = oracle.Operator(headline["geom"], headline["links"], "EvenOddImproved", kappa, csw, False)
