@@ -166,10 +166,10 @@ def run_serving(window_s, sweep_window_s, batch=16, precision="single", solver="
         for key, (dims, rep) in enumerate(fields):
             srv.add_gauge(key, dims, rep, synth.fermion_links(dims, rep, SERVE_EPS[rep], SEED + 4 * key))
             pools[key] = [synth.gaussian_spinor(dims, 3, SEED + 100 * key + j) for j in range(SERVE_POOL)]
-        warm = [srv.submit(key, SERVE_KAPPA[rep][0], SERVE_CSW[rep], pools[key][:2])[0]
-                for key, (dims, rep) in enumerate(fields)]
-        for tk in warm:
-            srv.wait(tk, timeout=1800.0)
+        # one lane at a time, so that each lane's first batch (which tunes its batched
+        # stencil) runs on an otherwise idle GPU
+        for key, (dims, rep) in enumerate(fields):
+            srv.wait(srv.submit(key, SERVE_KAPPA[rep][0], SERVE_CSW[rep], pools[key][:2])[0], timeout=1800.0)
         out = serving_stream(srv, fields, pools, SERVE_RATE, window_s, SEED + 7)
         capacity = out["throughput_solves_per_s"]
         sweep = []

@@ -1581,6 +1581,10 @@ BatchTile tune_batch(lym_context *c, const GaugeDev &U, bool clov, int prec, con
     auto it = c->tiles.find(key);
     if (it != c->tiles.end()) return it->second;
     if (c->capturing) fail(c, LYM_ERR_ARGUMENT, "the batched stencil must be tuned before graph capture");
+    // one tuning at a time in the process: contexts that tune together (a server's lanes
+    // taking their first requests) would time each other's launches
+    static std::mutex tune_mu;
+    std::lock_guard<std::mutex> tune_lock(tune_mu);
     auto time_of = [&](const BatchTile &t, int reps) {
         CK(cudaEventRecord(c->ev0, c->st));
         for (int r = 0; r < reps; ++r)
