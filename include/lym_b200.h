@@ -446,6 +446,11 @@ int lym_set_link_format(lym_context *ctx, int reals);
  * involved.  A server lane fails only the request whose admission met the failure. */
 int lym_context_inject_alloc_failures(lym_context *ctx, int n);
 int lym_server_inject_alloc_failures(lym_server *server, int key, int n);
+/* The next host check of the word in which the bulk-copy variant of the batched stencil
+ * (lym_set_batch_tile codes 35, 36) records a copy wait that gave up reads it as set: the
+ * call that ran the variant returns LYM_ERR_TIMEOUT and the word is cleared.  The kernels
+ * run as usual; only the host's reading of their status is faked. */
+int lym_context_inject_copy_wait_timeout(lym_context *ctx);
 
 /* ---- pinned host memory for callers that want fast transfers ---------------------- */
 void *lym_host_alloc(size_t bytes);

@@ -122,6 +122,7 @@ def lib():
         "lym_set_batch_tile": (i, [vp, i, i, i]),
         "lym_get_batch_tile": (i, [vp, i, i, i, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "lym_context_inject_alloc_failures": (i, [vp, i]),
+        "lym_context_inject_copy_wait_timeout": (i, [vp]),
         "lym_set_link_format": (i, [vp, i]),
         "lym_host_alloc": (vp, [C.c_size_t]),
         "lym_host_free": (None, [vp]),

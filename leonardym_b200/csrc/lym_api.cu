@@ -90,6 +90,7 @@ struct lym_context {
     double engine_stats[7] = {};      // block solves: lym_context_engine_stats
     bool capturing = false;
     int inject_alloc_failures = 0;  // the next n device allocations report failure (tests)
+    bool inject_copy_wait = false;  // the next check of the bulk-copy wait word reports a give-up (tests)
     int link_reals = 12;            // FP32 SU(3) link format of the single-RHS stencils: 12 or 8
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
@@ -1560,6 +1561,10 @@ void check_copy_waits(lym_context *c, const BatchTile &t)
     CK(cudaStreamSynchronize(c->st));
     int e = 0;
     memcpy(&e, c->h_scal, sizeof(int));
+    if (c->inject_copy_wait) {  // host-side fault injection (lym_context_inject_copy_wait_timeout)
+        c->inject_copy_wait = false;
+        e = 1;
+    }
     if (e) {
         CK(cudaMemsetAsync(c->d_err + 1, 0, sizeof(int), c->st));
         fail(c, LYM_ERR_TIMEOUT, "a bulk copy of the batched stencil did not complete in its bounded wait");
@@ -2013,8 +2018,9 @@ public:
         set_tables(j, b, T, Ti);
         axpby_views(c, xs.f().slot(j), xs.f().slot(j), C2(0.0), C2(0.0));
         double rrS, rrN = 0.0;
-        if (algo == ALGO_BICGSTAB) true_res_S(j, rrS);  // synchronises: the host values above were consumed
-        else true_res(j, rrS, rrN);
+        // x = 0: the residual is the Schur source itself (S 0 = 0), so no operator is applied
+        if (algo == ALGO_BICGSTAB) true_res_S(j, rrS, true);  // synchronises: the host values above were consumed
+        else true_res(j, rrS, rrN, true);
         if (rrS < s.epsS || s.bb == 0.0) {
             s.converged = 1;
             finish(j);
@@ -2133,12 +2139,18 @@ private:
             if (hs.active[j]) return true;
         return false;
     }
-    void true_res(int j, double &rrS, double &rrN)
+    // |b' - S x|^2 and |S^+ (b' - S x)|^2 of slot j (zero_x: x = 0, the residual is b')
+    void true_res(int j, double &rrS, double &rrN, bool zero_x = false)
     {
         Slot &s = slot[j];
         const Spinor xo = s.X.parity(1);
-        apply_schur(c, *s.op, PREC_D, *t1, xo, *te, 0);
-        run_site(c, OpSubNorm<SpinorD, SpinorD, SpinorD>{(**s.bp).d(), (*t1).d(), (*rS).d(), c->d_scal}, 1);
+        if (zero_x) {
+            copy(c, *rS, **s.bp);
+            run_site(c, OpNorm<SpinorD>{(*rS).d(), c->d_scal}, 1);
+        } else {
+            apply_schur(c, *s.op, PREC_D, *t1, xo, *te, 0);
+            run_site(c, OpSubNorm<SpinorD, SpinorD, SpinorD>{(**s.bp).d(), (*t1).d(), (*rS).d(), c->d_scal}, 1);
+        }
         copy(c, *t1, *rS);
         gamma5_inplace(c, *t1);
         apply_schur(c, *s.op, PREC_D, *rN, *t1, *te, 1);
@@ -2148,12 +2160,17 @@ private:
         rrS = c->h_scal[0];
         rrN = c->h_scal[1];
     }
-    // |b' - S x|^2 of slot j, the residual left in rS
-    void true_res_S(int j, double &rrS)
+    // |b' - S x|^2 of slot j, the residual left in rS (zero_x: x = 0, the residual is b')
+    void true_res_S(int j, double &rrS, bool zero_x = false)
     {
         Slot &s = slot[j];
-        apply_schur(c, *s.op, PREC_D, *t1, s.X.parity(1), *te, 0);
-        run_site(c, OpSubNorm<SpinorD, SpinorD, SpinorD>{(**s.bp).d(), (*t1).d(), (*rS).d(), c->d_scal}, 1);
+        if (zero_x) {
+            copy(c, *rS, **s.bp);
+            run_site(c, OpNorm<SpinorD>{(*rS).d(), c->d_scal}, 1);
+        } else {
+            apply_schur(c, *s.op, PREC_D, *t1, s.X.parity(1), *te, 0);
+            run_site(c, OpSubNorm<SpinorD, SpinorD, SpinorD>{(**s.bp).d(), (*t1).d(), (*rS).d(), c->d_scal}, 1);
+        }
         CK(cudaMemcpyAsync(c->h_scal, c->d_scal, sizeof(double), cudaMemcpyDeviceToHost, c->st));
         CK(cudaStreamSynchronize(c->st));
         rrS = c->h_scal[0];
@@ -2943,9 +2960,13 @@ static int run_block(lym_context *c, OpEntry &op, int sp, int algo, double tol, 
     auto now = []() { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
     std::vector<double> t_start(tags.size(), 0.0);
     // host buffers: the sources' H2D copies run ahead on the copy stream through a ring of
-    // device staging buffers, and every solution's D2H copy runs there while the solves go on
+    // K device staging buffers, and every solution's D2H copy runs there while the solves go
+    // on, through a ring of KD: as many as the engine has slots, so that collecting a whole
+    // wave of finished slots never waits on an earlier download (the host thread would hold
+    // back the engine's next launches meanwhile)
     const size_t vb = (size_t)c->g.V * 24 * sizeof(double);
     const int K = device_ptr ? 0 : (int)std::min<size_t>(4, tags.size());
+    const int KD = device_ptr ? 0 : (int)std::min<size_t>((size_t)width, tags.size());
     std::vector<std::unique_ptr<DevBuf>> up, down;
     struct Events {
         std::vector<cudaEvent_t> e;
@@ -2961,12 +2982,14 @@ static int run_block(lym_context *c, OpEntry &op, int sp, int algo, double tol, 
             return x;
         }
     } events;
-    std::vector<cudaEvent_t> ev_up(K), ev_used(K), ev_unpacked(K), ev_down(K);
+    std::vector<cudaEvent_t> ev_up(K), ev_used(K), ev_unpacked(KD), ev_down(KD);
     for (int r = 0; r < K; ++r) {
         up.emplace_back(new DevBuf(c, vb));
-        down.emplace_back(new DevBuf(c, vb));
         ev_up[r] = events.make();
         ev_used[r] = events.make();
+    }
+    for (int r = 0; r < KD; ++r) {
+        down.emplace_back(new DevBuf(c, vb));
         ev_unpacked[r] = events.make();
         ev_down[r] = events.make();
     }
@@ -3000,8 +3023,8 @@ static int run_block(lym_context *c, OpEntry &op, int sp, int algo, double tol, 
             if (device_ptr) {
                 download_vec(c, solutions[tag], s.X, true, 2);
             } else {
-                const int r = (int)(ndown % K);
-                if (ndown >= (size_t)K) CK(cudaEventSynchronize(ev_down[r]));  // the buffer's last copy is done
+                const int r = (int)(ndown % KD);
+                if (ndown >= (size_t)KD) CK(cudaEventSynchronize(ev_down[r]));  // the buffer's last copy is done
                 launch_unpack(c->g, s.X, (double *)down[r]->p, c->st);
                 CK(cudaEventRecord(ev_unpacked[r], c->st));
                 CK(cudaStreamWaitEvent(c->st_copy, ev_unpacked[r], 0));
@@ -3872,6 +3895,14 @@ int lym_context_inject_alloc_failures(lym_context *c, int n)
     if (n < 0) return LYM_ERR_ARGUMENT;
     return guarded(c, [&]() {
         c->inject_alloc_failures = n;
+        return LYM_OK;
+    });
+}
+
+int lym_context_inject_copy_wait_timeout(lym_context *c)
+{
+    return guarded(c, [&]() {
+        c->inject_copy_wait = true;
         return LYM_OK;
     });
 }

@@ -1,7 +1,8 @@
 """Failures made on the host, never on the GPU: a source with NaN or Inf entries, a step
-limit of one, an unreachable tolerance, a BiCGStab breakdown (rho = 0), and a device
+limit of one, an unreachable tolerance, a BiCGStab breakdown (rho = 0), a device
 allocation that fails inside a server lane (an injected error code in place of a failing
-cudaMalloc).  Each must end its own solve or request with a status while everything else
+cudaMalloc), and a bulk-copy wait of the batched stencil reported as given up (the host's
+reading of the kernel's status word faked).  Each must end its own solve or request with a status while everything else
 completes within tolerance; the reference returns false on the same inputs
 (ConjugateGradient.cpp:70-73, BiConjugateGradient.cpp:381-384, 503-506), pinned here
 through its compiled code where it runs."""
@@ -21,7 +22,7 @@ from tests.helpers import CONFIGS, links_for
 
 pytestmark = pytest.mark.gpu
 
-OK, NOT_CONVERGED, ERR_MEMORY, ERR_BREAKDOWN = 0, 1, -3, -5
+OK, NOT_CONVERGED, ERR_MEMORY, ERR_BREAKDOWN, ERR_TIMEOUT = 0, 1, -3, -5, -7
 
 
 @pytest.fixture(scope="module")
@@ -220,3 +221,28 @@ def test_server_allocation_failure_fails_one_request(oracle):
         assert _residual(D3, srcs[0], solD[0]) <= 1e-10
     finally:
         srv.close()
+
+
+def test_bulk_copy_wait_timeout_fails_the_call(su3, oracle):
+    """The bulk-copy variant of the batched stencil records a copy wait that gave up in a
+    word the host reads after the call; the reading is faked on the host (the kernels run
+    as usual): the call returns LYM_ERR_TIMEOUT, and the next call on the same context, with
+    the same variant, gives the oracle's result."""
+    from leonardym_b200.dirac import multiply_batch, set_batch_tile
+    lat = su3["lat"]
+    op = L.EvenOddImprovedDiracWilsonOperator(lat, su3["kappa"], su3["csw"], gamma5=False)
+    op.setLattice(su3["gid"])
+    xs = [synth.gaussian_spinor(su3["dims"], 3, 700 + j) for j in range(4)]
+    D = oracle.Operator(oracle.Geometry(su3["dims"]), su3["links"], "EvenOddImproved", su3["kappa"], su3["csw"],
+                        False)
+    try:
+        set_batch_tile(lat, 0, 0, 36)
+        assert L.lib().lym_context_inject_copy_wait_timeout(lat.handle) == OK
+        with pytest.raises(L.LymError) as err:
+            multiply_batch([op] * 4, xs, "single")
+        assert err.value.code == ERR_TIMEOUT
+        got = multiply_batch([op] * 4, xs, "single")
+    finally:
+        set_batch_tile(lat, -1, 0)
+    for x, y in zip(xs, got):
+        assert np.linalg.norm(y - D.multiply(x)) / np.linalg.norm(D.multiply(x)) < 1e-6
