@@ -16,7 +16,8 @@
 //         norm n[h * np + q] = (max |.| of RHS 2q, of RHS 2q+1).
 // Link, clover and neighbour-index words of a half-site are read by all np threads
 // of that half-site (broadcast), so their bytes are shared by the whole batch; the
-// links are read in the 12-real format and expanded in registers.
+// links are read in the 12-real format or, for SU(3), in all 18 reals (GaugeF18P), and
+// expanded in registers.
 #pragma once
 
 #include <type_traits>
@@ -389,11 +390,12 @@ struct LinkP {  // a link with every component duplicated into both lanes
 // lanes of the half-site at once), so they are loaded with the evict-first hint and
 // leave L2 to the neighbour spinors, which are read eight times.
 //
-// The links are the 12-real FP32 words of the single-RHS stencils (GaugeF12 / GaugeF6:
-// rows 0 and 1, row 2 = s conj(row0 x row1), s = -1 where bit mu of the site's sign byte
-// is set) and are expanded in registers into lane-duplicated components for the packed
-// arithmetic.  Staged through shared memory, a link takes kStageWords slots: its 3 words
-// and the aligned 32-bit word of the sign table that holds its sign byte.
+// GaugeC12P / GaugeR6P read the 12-real FP32 words of the single-RHS stencils (GaugeF12 /
+// GaugeF6: rows 0 and 1, row 2 = s conj(row0 x row1), s = -1 where bit mu of the site's
+// sign byte is set); GaugeF18P reads all 18 reals.  Either is expanded in registers into
+// lane-duplicated components for the packed arithmetic.  Staged through shared memory, a
+// 12-real link takes kStageWords slots: its 3 words and the aligned 32-bit word of the
+// sign table that holds its sign byte.
 LYM_D void cp_async4(unsigned saddr, const void *g)
 {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(saddr), "l"(g) : "memory");
