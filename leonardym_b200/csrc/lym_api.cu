@@ -1935,6 +1935,10 @@ public:
             rhat.reset(new BVec(c, PREC_F, nb));
             what.reset(new BVec(c, PREC_F, nb));
             for (BVec *v : {svec.get(), rhat.get(), what.get()}) CK(cudaMemsetAsync(v->s.v, 0, v->bytes, c->st));
+            for (int j = 0; j < nb; ++j) {
+                rhat_c[j].reset(new Vec(c, PREC_F, 1));
+                what_c[j].reset(new Vec(c, PREC_F, 1));
+            }
         }
         tables = (char *)dev_alloc(c, kTableBytes);
         d_b = (double *)tables;
@@ -2097,6 +2101,10 @@ private:
     Vec te, t1, rS, rN;
     BVec xs, rs, ps, aps, tes, tos;       // CG: p, S^+S p (aps), tmp, S p (tos); BiCGStab: p, v, tmp, t
     std::unique_ptr<BVec> svec, rhat, what;  // BiCGStab only: s, the shadow residual rhat, S^+ rhat
+    // BiCGStab: each slot's rhat and S^+ rhat again as contiguous FP32 spinors (the same
+    // rounded values), which a reliable update reads coalesced: in the pair layout one
+    // right-hand side is 8 bytes of every 32-byte sector it touches
+    std::unique_ptr<Vec> rhat_c[kMaxBatch], what_c[kMaxBatch];
     std::unique_ptr<DevBuf> om_scratch;      // BiCGStab: partial omega sums of the fused stencil epilogue
     static constexpr size_t kTableBytes = 3 * kMaxBatch * sizeof(double) + 16;
     char *tables = nullptr;
@@ -2184,6 +2192,7 @@ private:
         gamma5_inplace(c, *t1);
         apply_schur(c, *slot[j].op, PREC_D, *rN, *t1, *te, 1);
         axpby_views(c, (*rN).d(), what->f().slot(j), C2(1.0), C2(0.0));
+        copy(c, **what_c[j], *rN);
         run_site(c, OpDot<SpinorD, SpinorD>{(*rN).d(), (*rS).d(), c->d_scal}, 1);
         CK(cudaMemcpyAsync(c->h_scal, c->d_scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
         CK(cudaStreamSynchronize(c->st));
@@ -2203,6 +2212,7 @@ private:
     {
         axpby_views(c, (*rS).d(), rs.f().slot(j), C2(1.0), C2(0.0));
         axpby_views(c, (*rS).d(), rhat->f().slot(j), C2(1.0), C2(0.0));
+        copy(c, **rhat_c[j], *rS);
         set_direction(j, 0.0);
         hs.rho[j] = make_double2(rrS, 0.0);
         hs.alpha[j] = cdiv(hs.rho[j], shadow_image(j));
@@ -2244,12 +2254,12 @@ private:
                 // one: p += r_true - r_rec (p was formed from r_rec), r = r_true,
                 // rho = <rhat, r>, alpha = rho / <what, p>
                 if (sprec == PREC_F)
-                    run_site(c, OpBiContinue<SlotF, SlotF, SpinorD, SlotF, SlotF>{
-                                    rs.f().slot(j), ps.f().slot(j), (*rS).d(), rhat->f().slot(j), what->f().slot(j),
+                    run_site(c, OpBiContinue<SlotF, SlotF, SpinorD, SpinorF, SpinorF>{
+                                    rs.f().slot(j), ps.f().slot(j), (*rS).d(), (**rhat_c[j]).f(), (**what_c[j]).f(),
                                     c->d_scal}, 1);
                 else
-                    run_site(c, OpBiContinue<SlotF, SlotH, SpinorD, SlotF, SlotF>{
-                                    rs.f().slot(j), ps.h().slot(j), (*rS).d(), rhat->f().slot(j), what->f().slot(j),
+                    run_site(c, OpBiContinue<SlotF, SlotH, SpinorD, SpinorF, SpinorF>{
+                                    rs.f().slot(j), ps.h().slot(j), (*rS).d(), (**rhat_c[j]).f(), (**what_c[j]).f(),
                                     c->d_scal}, 1);
                 CK(cudaMemcpyAsync(c->h_scal, c->d_scal, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
                 CK(cudaStreamSynchronize(c->st));

@@ -133,6 +133,12 @@ struct SpinorF {  // FP32: 6 x float4 words (two complex per word)
     int stride;
     static constexpr int kWords = 6;
     LYM_HD SpinorF par(int p) const { return SpinorF{v + (size_t)p * 6 * stride, stride}; }
+    // component k of half-site h (vector steps that stream one component at a time)
+    LYM_D cx<double> get(int k, int h) const
+    {
+        const float2 w = __ldg(reinterpret_cast<const float2 *>(v + (size_t)(k >> 1) * stride + h) + (k & 1));
+        return cx<double>{w.x, w.y};
+    }
     template <typename R> LYM_D void load(int h, cx<R> s[12]) const
     {
 #pragma unroll
