@@ -2020,7 +2020,7 @@ public:
         s.epsS = tol * tol * s.bb;
         zero(c, X.parity(1));
         set_tables(j, b, T, Ti);
-        axpby_views(c, xs.f().slot(j), xs.f().slot(j), C2(0.0), C2(0.0));
+        hs.x_reset[j] = 1;  // the slot's FP32 accumulator starts from zero in its first update pass
         double rrS, rrN = 0.0;
         // x = 0: the residual is the Schur source itself (S 0 = 0), so no operator is applied
         if (algo == ALGO_BICGSTAB) true_res_S(j, rrS, true);  // synchronises: the host values above were consumed
@@ -2076,7 +2076,7 @@ public:
             for (int j = 0; j < nb; ++j) {
                 Slot &s = slot[j];
                 if (s.busy && !s.finished && hs.active[j] && hs.its[j] >= s.max_iter) {
-                    axpby_views(c, xs.f().slot(j), s.X.parity(1).d(), C2(1.0), C2(1.0));
+                    if (!hs.x_reset[j]) axpby_views(c, xs.f().slot(j), s.X.parity(1).d(), C2(1.0), C2(1.0));
                     finish(j);
                 }
             }
@@ -2223,8 +2223,11 @@ private:
     void reliable_update_bicg(int j)
     {
         Slot &s = slot[j];
-        if (hs.restart[j] != 2) run_site(c, OpFoldClear<SlotF, SpinorD>{xs.f().slot(j), s.X.parity(1).d()}, 1);
-        else axpby_views(c, xs.f().slot(j), xs.f().slot(j), C2(0.0), C2(0.0));
+        // x += the FP32 accumulator (unless a non-finite recursion (restart 2) drops it); the
+        // accumulator counts as zero from the next update pass on
+        if (hs.restart[j] != 2 && !hs.x_reset[j])
+            axpby_views(c, xs.f().slot(j), s.X.parity(1).d(), C2(1.0), C2(1.0));
+        hs.x_reset[j] = 1;
         double rrS;
         true_res_S(j, rrS);
         ++s.updates;
@@ -2333,9 +2336,11 @@ private:
             return;
         }
         Slot &s = slot[j];
-        // a non-finite recursion (restart 2) drops its FP32 accumulator
-        if (hs.restart[j] != 2) run_site(c, OpFoldClear<SlotF, SpinorD>{xs.f().slot(j), s.X.parity(1).d()}, 1);
-        else axpby_views(c, xs.f().slot(j), xs.f().slot(j), C2(0.0), C2(0.0));
+        // x += the FP32 accumulator (unless a non-finite recursion (restart 2) drops it); the
+        // accumulator counts as zero from the next update pass on
+        if (hs.restart[j] != 2 && !hs.x_reset[j])
+            axpby_views(c, xs.f().slot(j), s.X.parity(1).d(), C2(1.0), C2(1.0));
+        hs.x_reset[j] = 1;
         const bool restarted = hs.restart[j] != 0;
         hs.restart[j] = 0;
         double rrS, rrN;

@@ -1285,6 +1285,10 @@ struct BatchCGState {
     int restart[kMaxBatch];                    // broke down: restart at the update
                                                // (2: non-finite, drop the FP32 accumulator)
     int last_update_its[kMaxBatch];            // its at the last reliable update
+    // the slot's FP32 solution accumulator counts as zero in the next update pass (it was
+    // folded into the FP64 solution or dropped, or the slot took a new source), which
+    // spares a pass that would clear one lane of the pair layout
+    int x_reset[kMaxBatch];
 };
 
 LYM_D cx<double> as_cx2(double2 z) { return cx<double>{z.x, z.y}; }
@@ -1376,6 +1380,7 @@ template <class SX, class SP, class SR, class SAp> struct OpBUpdate {
         const bool act[2] = {s->active[2 * q] != 0, s->active[2 * q + 1] != 0};
         if (!act[0] && !act[1]) return;
         const cx<double> al[2] = {as_cx2(s->alpha[2 * q]), as_cx2(s->alpha[2 * q + 1])};
+        const bool xr[2] = {s->x_reset[2 * q] != 0, s->x_reset[2 * q + 1] != 0};
         auto xo = pair_out(x, h, q);
         auto ro = pair_out(rv, h, q);
 #pragma unroll 2
@@ -1388,6 +1393,7 @@ template <class SX, class SP, class SR, class SAp> struct OpBUpdate {
 #pragma unroll
             for (int l = 0; l < 2; ++l) {
                 if (!act[l]) continue;
+                if (xr[l]) xv[l] = cx<double>{0.0, 0.0};
                 fma_c(xv[l], al[l], pv[l]);
                 res[l] = res[l] - al[l] * av[l];
                 acc[l] += nrm1(res[l]);
@@ -1401,6 +1407,7 @@ template <class SX, class SP, class SR, class SAp> struct OpBUpdate {
     LYM_D void finalize(int r, const double *t) const
     {
         if (!s->active[r]) return;
+        s->x_reset[r] = 0;
         s->its[r] += 1;
         const double rr_new = t[0];
         s->rr_prev[r] = s->rr[r];
@@ -1536,6 +1543,7 @@ template <class SX, class SP, class SS, class ST, class SV, class SR, class SW> 
             om[l] = as_cx(s->omega[2 * q + l]);
             be[l] = as_cx(s->bbeta[2 * q + l]);
         }
+        const bool xr[2] = {s->x_reset[2 * q] != 0, s->x_reset[2 * q + 1] != 0};
         auto xo = pair_out(x, h, q);
         auto ro = pair_out(rv, h, q);
         auto po = pair_out(p, h, q);
@@ -1552,6 +1560,7 @@ template <class SX, class SP, class SS, class ST, class SV, class SR, class SW> 
 #pragma unroll
             for (int l = 0; l < 2; ++l) {
                 if (!act[l]) continue;
+                if (xr[l]) xv[l] = cx<double>{0.0, 0.0};
                 fma_c(xv[l], al[l], pv[l]);
                 fma_c(xv[l], om[l], sw[l]);
                 rr[l] = sw[l] - om[l] * tw[l];
@@ -1570,6 +1579,7 @@ template <class SX, class SP, class SS, class ST, class SV, class SR, class SW> 
     LYM_D void finalize(int r, const double *t) const
     {
         if (!s->active[r]) return;
+        s->x_reset[r] = 0;
         s->its[r] += 1;
         const double rr_new = t[0];
         s->rr_prev[r] = s->rr[r];
