@@ -443,7 +443,7 @@ SOLVER_NAMES = {"cg": "block even-odd CG on (gamma5 S)^2", "bicgstab": "block ev
 
 
 ENGINE_KEYS = ("iterating_s", "reliable_updates_s", "adding_s", "collecting_s", "graph_replays", "pauses",
-               "reliable_updates")
+               "reliable_updates", "batch_iterations", "slot_iterations")
 
 
 def engine_stats(lib, ctx):
@@ -624,7 +624,8 @@ def run_ours(args, world, rank, local):
         "mixed_over_fp64": value / world / (fp64_value / world),
         "latency_ms": {"p50": lat_ms[len(lat_ms) // 2], "p99": lat_ms[min(len(lat_ms) - 1, int(0.99 * len(lat_ms)))]},
         "iterations": {"median": statistics.median(iters), "max": max(iters)},
-        "engine_per_step": {k: round(v, 4) for k, v in zip(ENGINE_KEYS, eng)},
+        "engine_per_step": dict({k: round(v, 4) for k, v in zip(ENGINE_KEYS, eng)},
+                                batch_occupancy=round(eng[8] / (eng[7] * args.batch), 4) if eng[7] else None),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
                      "kernel": (f"batched Schur stencil with clover, {args.batch} right-hand sides, "

@@ -396,7 +396,9 @@ unsigned long long lym_context_kernel_launches(lym_context *ctx);
  * counts as doubles): out[0] iterating (graph replays of the batched loop, host waiting),
  * out[1] reliable updates and restarts of parked slots, out[2] adding sources (Schur source,
  * first true residual), out[3] collecting solutions (reconstruction, true residual,
- * download), out[4] graph replays, out[5] loop pauses, out[6] reliable updates; n = 7 */
+ * download), out[4] graph replays, out[5] loop pauses, out[6] reliable updates, out[7]
+ * iterations of the batched loop, out[8] the slots' iterations summed over the slots (out[8]
+ * / (out[7] * batch width) is how full the batch was); n = 9 */
 int lym_context_engine_stats(lym_context *ctx, double *out, int n);
 int lym_time_stencil(lym_context *ctx, int op_id, int prec, int which, int iters, double *ms_per_launch);
 /* the same for the batched stencil of the block solves (prec 1 or 2, batch a power of 2,

@@ -87,7 +87,7 @@ struct lym_context {
     std::vector<std::pair<size_t, void *>> blocks;
     size_t bytes = 0;
     unsigned long long launches = 0;  // kernels enqueued (graph replays count their nodes)
-    double engine_stats[7] = {};      // block solves: lym_context_engine_stats
+    double engine_stats[9] = {};      // block solves: lym_context_engine_stats
     bool capturing = false;
     int inject_alloc_failures = 0;  // the next n device allocations report failure (tests)
     bool inject_copy_wait = false;  // the next check of the bulk-copy wait word reports a give-up (tests)
@@ -2066,11 +2066,18 @@ public:
             *(BatchCGState *)c->h_state = hs;
             CK(cudaMemcpyAsync(c->d_state, c->h_state, sizeof(BatchCGState), cudaMemcpyHostToDevice, c->st));
             BatchCGState *S = (BatchCGState *)c->d_state;
+            const int iter0 = hs.iter;
+            long its0 = 0;
+            for (int j = 0; j < nb; ++j) its0 += hs.its[j];
             const double t0 = wall();
             run_loop(S, (long)left + kGraphIters);
             c->engine_stats[0] += wall() - t0;
             c->engine_stats[5] += 1;
             hs = *(BatchCGState *)c->h_state;
+            long its1 = 0;
+            for (int j = 0; j < nb; ++j) its1 += hs.its[j];
+            c->engine_stats[7] += hs.iter - iter0;  // batch iterations
+            c->engine_stats[8] += its1 - its0;      // iterations of the slots taking part
             if (hs.failed) fail(c, LYM_ERR_NUMERIC, "block CG produced a non-finite residual");
             direction_rest(S);
             for (int j = 0; j < nb; ++j) {
@@ -3703,7 +3710,7 @@ int lym_context_engine_stats(lym_context *c, double *out, int n)
 {
     if (!c || !out || n < 0) return LYM_ERR_ARGUMENT;
     std::lock_guard<std::recursive_mutex> g(c->mu);
-    for (int k = 0; k < n && k < 7; ++k) out[k] = c->engine_stats[k];
+    for (int k = 0; k < n && k < 9; ++k) out[k] = c->engine_stats[k];
     return LYM_OK;
 }
 

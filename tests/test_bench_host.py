@@ -37,5 +37,5 @@ def test_peaks_are_measured_or_the_stated_fallback():
 
 def test_engine_keys_match_the_library_hook():
     header = (ROOT / "include" / "lym_b200.h").read_text()
-    m = re.search(r"out\[6\][^;]*; n = (\d+)", header, re.S)
-    assert m and int(m.group(1)) == len(bench.ENGINE_KEYS) == 7
+    m = re.search(r"out\[8\][^;]*; n = (\d+)", header, re.S)
+    assert m and int(m.group(1)) == len(bench.ENGINE_KEYS) == 9
