@@ -778,11 +778,19 @@ template <class SB, class GaugeT> struct DslashBatchArg {
     int *err;         // bulk-copy variant: set to 1 when a copy wait gave up
 };
 
+struct NoWait {
+    LYM_D void operator()() const {}
+};
+
 // The epilogue on H x (acc) for the pair q at half-site h, written to out.  ysrc(blk, y6)
 // gives the 6 same-parity input components of block blk (EPI_XPAY); cw the clover words.
-template <int EPI, class SB, class GaugeT, class YSrc, class CW>
+// before_blk1() runs before anything of spin block 1, the clover words of that block or the
+// fused epilogue's own-site operand (r_smem) is read (the staged kernel waits there for the
+// copies it issued after the last direction).
+template <int EPI, class SB, class GaugeT, class YSrc, class CW, class Wait = NoWait>
 LYM_D void batch_epilogue(const DslashBatchArg<SB, GaugeT> &arg, int h, int q, bool act_a, bool act_b, c2 acc[12],
-                          const YSrc &ysrc, const CW &cw, const float4 *r_smem = nullptr)
+                          const YSrc &ysrc, const CW &cw, const float4 *r_smem = nullptr,
+                          const Wait &before_blk1 = Wait{})
 {
     const int ra = 2 * q, rb = 2 * q + 1;
     if (EPI == EPI_SCALE || EPI == EPI_CLOVINV) {
@@ -792,6 +800,7 @@ LYM_D void batch_epilogue(const DslashBatchArg<SB, GaugeT> &arg, int h, int q, b
         if (EPI == EPI_CLOVINV && arg.has_clover) {
 #pragma unroll
             for (int blk = 0; blk < 2; ++blk) {
+                if (blk == 1) before_blk1();
                 c2 res[6];
                 clover_block_apply<+1, false>(cw, blk, acc + 6 * blk, res);
 #pragma unroll
@@ -807,6 +816,7 @@ LYM_D void batch_epilogue(const DslashBatchArg<SB, GaugeT> &arg, int h, int q, b
         const float2 b = make_float2(ba, bb), nb = make_float2(-ba, -bb);
 #pragma unroll
         for (int blk = 0; blk < 2; ++blk) {
+            if (blk == 1) before_blk1();
             c2 y6[6];
             ysrc(blk, y6);
             c2 *o = acc + 6 * blk;
@@ -833,6 +843,7 @@ LYM_D void batch_epilogue(const DslashBatchArg<SB, GaugeT> &arg, int h, int q, b
     }
     arg.out.store(h, q, acc);
     if constexpr (EPI == EPI_XPAY_RES) {
+        before_blk1();
         c2 r[12];  // r from this thread's shared-memory slots (staged kernel) or from memory
         if (r_smem) arg.res_r.unstage(r_smem, kStagedThreads, r);
         else arg.res_r.load(h, q, r);
@@ -1116,17 +1127,36 @@ __global__ void __launch_bounds__(kStagedThreads, MINB)
         if constexpr (RED)
             if (s.live) arg.om_rhat.stage(smem_u32(s.sx(1)), kStagedThreads * 16, s.h, q);
         cp_async_commit();
-        cp_async_wait<0>();
+        // the copies of step 7 (y, clover block 0) now; those just issued (clover block 1,
+        // r or rhat) before the epilogue first reads them, so that their latency overlaps
+        // block 0 of the epilogue.  Every lane of the half-site meets both warp barriers
+        // (each waits for its own copies, which its neighbours read), a thread without an
+        // active right-hand side before it leaves.
+        cp_async_wait<1>();
         if constexpr (B) s.drain();
         __syncwarp(vmask);
-        if (!s.live) return false;
+        if (!s.live) {
+            cp_async_wait<0>();
+            __syncwarp(vmask);
+            return false;
+        }
+        bool waited = false;
+        auto wait_rest = [&]() {
+            if (!waited) {
+                cp_async_wait<0>();
+                __syncwarp(vmask);
+                waited = true;
+            }
+        };
         auto ysrc = [&](int blk, c2 y6[6]) { arg.y.unstage_block(s.sx(0), kStagedThreads, blk, y6); };
         if (s.clov_smem) {
-            batch_epilogue<EPI>(arg, s.h, q, act_a, act_b, acc, ysrc, CloverWordsSmem{s.sl(0), s.sl(1)}, s.sx(1));
+            batch_epilogue<EPI>(arg, s.h, q, act_a, act_b, acc, ysrc, CloverWordsSmem{s.sl(0), s.sl(1)}, s.sx(1),
+                                wait_rest);
         } else {
             batch_epilogue<EPI>(arg, s.h, q, act_a, act_b, acc, ysrc, clover_global<EPI>(arg, s.h, q, act_a, act_b),
-                                s.sx(1));
+                                s.sx(1), wait_rest);
         }
+        wait_rest();
         if constexpr (RED) {
             // the omega sums of the two lanes: <t, s>, |t|^2, <rhat, s>, <rhat, t> (t = out,
             // s = y), over the 12 components of this half-site in packed FP32 (one lane per
