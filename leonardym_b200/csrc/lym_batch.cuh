@@ -113,8 +113,11 @@ LYM_D bool mbar_wait(unsigned mb, unsigned parity)
 }
 
 // ------------------------------------------------------------- batch views --
-// One RHS r of a FP32 pair-layout batch, as a single half-spinor view (slot set-up and
-// extraction; not on the iteration path).
+// One RHS r of a FP32 pair-layout batch, as a single half-spinor view (slot set-up,
+// extraction and reliable updates; not on the iteration path).  A 16-byte word holds
+// component c of both RHS of the pair (re_a, re_b, im_a, im_b), so the words of one RHS
+// lie 16 << lognp bytes apart: reads take the whole word (one request per word instead
+// of one per float).
 struct SlotF {
     float *f;
     int stride, lognp, r;
@@ -124,11 +127,28 @@ struct SlotF {
     {
         return (((((size_t)c * stride + h) << lognp) + (r >> 1)) << 2) + (r & 1);
     }
-    LYM_D cx<double> get(int c, int h) const
+    LYM_D size_t word_at(int c, int h) const { return (((size_t)c * stride + h) << lognp) + (r >> 1); }
+    // the word of component c at half-site h (this RHS and its pair mate)
+    LYM_D float4 word(int c, int h) const { return reinterpret_cast<const float4 *>(f)[word_at(c, h)]; }
+    LYM_D cx<double> lane(float4 w) const
     {
-        const size_t b = base(c, h);
-        return cx<double>{(double)f[b], (double)f[b + 2]};
+        return (r & 1) ? cx<double>{(double)w.y, (double)w.w} : cx<double>{(double)w.x, (double)w.z};
     }
+    // w with this RHS's value replaced by s rounded to FP32; the mate's floats unchanged
+    LYM_D float4 with(float4 w, cx<double> s) const
+    {
+        if (r & 1) {
+            w.y = (float)s.re;
+            w.w = (float)s.im;
+        } else {
+            w.x = (float)s.re;
+            w.z = (float)s.im;
+        }
+        return w;
+    }
+    // writes a whole word back: only where nothing else writes the mate's lane meanwhile
+    LYM_D void put_word(int c, int h, float4 w) const { reinterpret_cast<float4 *>(f)[word_at(c, h)] = w; }
+    LYM_D cx<double> get(int c, int h) const { return lane(word(c, h)); }
     LYM_D void put(int c, int h, cx<double> s) const
     {
         const size_t b = base(c, h);
@@ -139,8 +159,8 @@ struct SlotF {
     {
 #pragma unroll
         for (int c = 0; c < 12; ++c) {
-            const size_t b = base(c, h);
-            s[c] = cx<R>{(R)f[b], (R)f[b + 2]};
+            const cx<double> v = get(c, h);
+            s[c] = cx<R>{(R)v.re, (R)v.im};
         }
     }
     template <typename R> LYM_D void store(int h, const cx<R> s[12]) const

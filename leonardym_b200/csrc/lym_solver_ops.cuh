@@ -92,20 +92,35 @@ template <class SR, class SP, class ST, class SH, class SW> struct OpBiContinue 
     LYM_D void site(int q, int h, double *acc) const
     {
         if constexpr (SP::kPerComponent) {
-            // FP32 direction: one component at a time; the stored direction is pn rounded
-            // to FP32, formed in registers
-#pragma unroll 2
-            for (int k = 0; k < 12; ++k) {
-                const cx<double> rv = r.par(q).get(k, h), tv = rt.par(q).get(k, h);
-                const cx<double> pn = p.par(q).get(k, h) + tv - rv;
-                p.par(q).put(k, h, pn);
-                r.par(q).put(k, h, tv);
-                const cx<double> ps{(double)(float)pn.re, (double)(float)pn.im};
-                const cx<double> hv = rh.par(q).get(k, h), wv = w.par(q).get(k, h);
-                acc[0] += hv.re * tv.re + hv.im * tv.im;
-                acc[1] += hv.re * tv.im - hv.im * tv.re;
-                acc[2] += wv.re * ps.re + wv.im * ps.im;
-                acc[3] += wv.re * ps.im - wv.im * ps.re;
+            // FP32 direction (pair-layout r and p): two components at a time, every load of
+            // both issued before their stores; r and p are read and written as whole 16-byte
+            // words, the pair mate's lane written back as read (the batched loop is paused
+            // during a reliable update, so nothing else writes those words).  The stored
+            // direction is pn rounded to FP32, formed in registers.
+#pragma unroll
+            for (int k0 = 0; k0 < 12; k0 += 2) {
+                float4 rw[2], pw[2];
+                cx<double> tv[2], hv[2], wv[2];
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    rw[i] = r.par(q).word(k0 + i, h);
+                    pw[i] = p.par(q).word(k0 + i, h);
+                    tv[i] = rt.par(q).get(k0 + i, h);
+                    hv[i] = rh.par(q).get(k0 + i, h);
+                    wv[i] = w.par(q).get(k0 + i, h);
+                }
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    const cx<double> rv = r.lane(rw[i]);
+                    const cx<double> pn = p.lane(pw[i]) + tv[i] - rv;
+                    p.par(q).put_word(k0 + i, h, p.with(pw[i], pn));
+                    r.par(q).put_word(k0 + i, h, r.with(rw[i], tv[i]));
+                    const cx<double> ps{(double)(float)pn.re, (double)(float)pn.im};
+                    acc[0] += hv[i].re * tv[i].re + hv[i].im * tv[i].im;
+                    acc[1] += hv[i].re * tv[i].im - hv[i].im * tv[i].re;
+                    acc[2] += wv[i].re * ps.re + wv[i].im * ps.im;
+                    acc[3] += wv[i].re * ps.im - wv[i].im * ps.re;
+                }
             }
             return;
         }
